@@ -1,0 +1,144 @@
+"""Host-side mirror of the reference driver's use of the GPU ABI.
+
+``ReferenceSession`` makes exactly the calls comcot.f90 makes
+(GCOMCOT_INIT_GPU, GCOMCOT_INIT_LAYER per layer, then per step MASS_LAUNCH,
+OPENBD_LAUNCH, ALL_GRID_LAUNCH, MOMT_LAUNCH, MAXAMP_LAUNCH, GCOMCOT_GET_Z per
+gauge, CUDA_UPDATE_LAYER), with the same argument meaning, so tests read like
+the reference's own DEBUG_CORE comparisons.  ``drive`` runs the same sequence
+inside the library (one call) for timing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .synth import Case, LayerSpec
+
+F32 = np.float32
+
+
+def _f(v):
+    return C.byref(C.c_float(float(v)))
+
+
+def _i(v):
+    return C.byref(C.c_int(int(v)))
+
+
+class ReferenceSession:
+    def __init__(self, case: Case, fusion: bool = True, arrival: bool = False):
+        self.lib = _lib.load()
+        self.case = case
+        self.lib.gcomcot_init_gpu_()
+        self.lib.gcomcot_set_fusion(1 if fusion else 0)
+        self._keep = []
+        for L in case.layers:
+            self._init_layer(L)
+        if arrival:
+            self.lib.gcomcot_set_arrival_(_i(case.root.id), _f(case.arrival_thr))
+
+    def _init_layer(self, L: LayerSpec):
+        lib = self.lib
+        ny, nx = L.ny, L.nx
+        if L.laycord == 1 or L.laygov != 0:
+            hp = np.ascontiguousarray(L.hp, dtype=F32)
+            hq = np.ascontiguousarray(L.hq, dtype=F32)
+            self._keep += [hp, hq]
+            lib.gcomcot_set_layer_params_(_i(L.id), _i(L.laycord), _i(L.laygov), _f(L.dt), _f(L.rx), _f(L.ry),
+                                          _f(L.grx), _f(L.gry), _i(L.fric_switch), _f(L.fric_coef),
+                                          _i(L.linchk), _i(L.modscm), _i(nx), _i(ny), _lib.fptr(hp),
+                                          _lib.fptr(hq))
+        if L.coefs is not None:
+            c = L.coefs
+            full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)
+            R1, R11, R3, R5 = full(c.r1), full(c.r11), full(c.r3), full(c.r5)
+            R2 = np.ascontiguousarray(c.r2, dtype=F32)
+            R4 = np.ascontiguousarray(c.r4, dtype=F32)
+            R6 = np.ascontiguousarray(c.r6, dtype=F32)
+        else:
+            z = np.zeros((ny, nx), F32)
+            R1 = R11 = R3 = R5 = R2 = R4 = z
+            R6 = np.zeros(ny, F32)
+        H = np.ascontiguousarray(L.H, dtype=F32)
+        Z = np.ascontiguousarray(L.Z0, dtype=F32)
+        corners = np.array(L.corners, dtype=np.int32)
+        lib.gcomcot_init_layer_(_i(L.id), _i(L.parent), _i(L.level), _i(L.rel_size), _i(L.rel_time),
+                                _lib.iptr(corners), _f(L.grx), _f(L.gry), _lib.fptr(R1), _lib.fptr(R2),
+                                _lib.fptr(R3), _lib.fptr(R4), _lib.fptr(R5), _lib.fptr(R6), _lib.fptr(R11),
+                                _lib.fptr(H), _lib.fptr(Z), _i(nx), _i(ny))
+
+    # ---- one outer step exactly as comcot.f90:359-439 ----
+    def step(self, maxamp: bool = True):
+        lib, rid = self.lib, self.case.root.id
+        lib.mass_launch_(None, None, None, _i(rid))
+        lib.openbd_launch_(None)
+        if len(self.case.layers) > 1:
+            lib.all_grid_launch_()
+        lib.momt_launch_(None, None, None, _i(rid))
+        if maxamp:
+            lib.maxamp_launch_(_i(rid))
+        ts = [self.get_ts(g) for g in self.case.gauges]
+        lib.cuda_update_layer_(_i(rid))
+        return ts
+
+    def get_ts(self, gauge):
+        """GET_TS: bilinear interpolation of the 2x2 stencil (output.f90:1078-1090)."""
+        lid, ki, kj, cx, cy = gauge
+        l = [C.c_float() for _ in range(4)]
+        self.lib.gcomcot_get_z_(_i(lid), *[C.byref(v) for v in l], _i(ki), _i(kj))
+        l1, l2, l3, l4 = (F32(v.value) for v in l)
+        cx, cy = F32(cx), F32(cy)
+        one = F32(1.0)
+        return float(l1 * (one - cx) * (one - cy) + l2 * cx * (one - cy) + l3 * (one - cx) * cy + l4 * cx * cy)
+
+    def drive(self, nsteps: int, maxamp: bool = True):
+        """The same sequence issued from inside the library; returns the raw
+        2x2 gauge stencils [nsteps, ngauges, 4]."""
+        g = self.case.gauges
+        ng = len(g)
+        gl = np.array([x[0] for x in g] or [0], dtype=np.int32)
+        gi = np.array([x[1] for x in g] or [0], dtype=np.int32)
+        gj = np.array([x[2] for x in g] or [0], dtype=np.int32)
+        out = np.zeros((max(nsteps, 1), max(ng, 1), 4), dtype=F32)
+        rc = self.lib.gcomcot_drive(nsteps, 1 if maxamp else 0, ng, _lib.iptr(gl), _lib.iptr(gi), _lib.iptr(gj),
+                                    _lib.fptr(out))
+        if rc != 0:
+            raise RuntimeError(f"gcomcot_drive failed: {rc}")
+        return out[:nsteps, :ng]
+
+    # ---- whole-field reads (Fortran Z(:,:,2), M(:,:,2), N(:,:,2)) ----
+    def _layer(self, lid):
+        return next(L for L in self.case.layers if L.id == lid)
+
+    def getz(self, lid=1):
+        L = self._layer(lid)
+        z = np.zeros((L.ny, L.nx), F32)
+        self.lib.cuda_getz_(_lib.fptr(z), _i(lid))
+        return z
+
+    def getmn(self, lid=1):
+        L = self._layer(lid)
+        m = np.zeros((L.ny, L.nx), F32)
+        n = np.zeros((L.ny, L.nx), F32)
+        self.lib.cuda_getmn_(_lib.fptr(m), _lib.fptr(n), _i(lid))
+        return m, n
+
+    def getzmax(self, lid=1):
+        L = self._layer(lid)
+        z = np.zeros((L.ny, L.nx), F32)
+        self.lib.cuda_getzmax_(_lib.fptr(z), _i(lid))
+        return z
+
+    def getarrival(self, lid=1):
+        L = self._layer(lid)
+        a = np.zeros((L.ny, L.nx), np.int32)
+        self.lib.gcomcot_get_arrival_(_lib.iptr(a), _i(lid))
+        return a
+
+    def launches(self):
+        return int(self.lib.gcomcot_launch_count())
+
+    def close(self):
+        self.lib.cuda_shutdown_()

@@ -1,0 +1,185 @@
+"""Once-per-run set-up of a COMCOT layer: grid axes, still-water depth at the
+flux points, spherical coefficients, sub-level time ratio, nesting corners
+and gauge interpolation weights.
+
+These restate the reference's initialisation routines:
+
+* ``axes``          DX_CALC, normal spherical grid (initialization.f90:853-870)
+* ``pq_depth``      PQ_DEPTH (initialization.f90:2501-2526)
+* ``para``          PARA, LAYGOV 0/1 (comcot.f90:694-752)
+* ``rel_time``      CR_CHECK sub-level rule (initialization.f90:1210-1237)
+* ``corners``       SUBGRID_MATCHING corner search (initialization.f90:913-936)
+* ``locate_gauge``  GET_TS index search and weights (output.f90:1054-1080)
+
+PARA's trigonometry is evaluated in float64 and rounded once to float32 (the
+reference evaluates it in REAL); R2 and R4 are then formed in float32 as
+``CX(J) * max(HP,0)`` exactly like ``RS/COS_M/(DX*RAD_MIN)*AMAX1(HP,0)``, so
+the per-row factor CX(J) reproduces every cell of R2 bit for bit.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+GRAV = np.float32(9.807)
+GX = np.float32(1.0e-5)
+R_EARTH = 6378000.0
+RAD_DEG = 0.01745329252
+RAD_MIN = 0.000290888208665721
+CORI_W = 7.2722e-5
+
+F32 = np.float32
+
+
+def axes(x_start: float, y_start: float, nx: int, ny: int, dx_min: float, dy_min: float | None = None):
+    """Longitude/latitude axes in degrees of a normal spherical grid."""
+    dy_min = dx_min if dy_min is None else dy_min
+    dx = F32(dx_min) / F32(60.0)
+    dy = F32(dy_min) / F32(60.0)
+    x = (F32(x_start) + np.arange(nx, dtype=np.float32) * dx).astype(np.float32)
+    y = (F32(y_start) + np.arange(ny, dtype=np.float32) * dy).astype(np.float32)
+    return x, y
+
+
+def pq_depth(h: np.ndarray):
+    """HP, HQ [ny, nx] (row-major view of the column-major field)."""
+    h = h.astype(np.float32)
+    hp = np.zeros_like(h)
+    hq = np.zeros_like(h)
+    hip1 = np.concatenate([h[:, 1:], h[:, -1:]], axis=1)
+    hjp1 = np.concatenate([h[1:, :], h[-1:, :]], axis=0)
+    wet = h > GX
+    hp[wet] = (F32(0.5) * (h + hip1))[wet]
+    hq[wet] = (F32(0.5) * (h + hjp1))[wet]
+    return hp, hq
+
+
+@dataclass
+class Coefs:
+    r1: np.ndarray   # [ny] R1(1,J)
+    r11: np.ndarray  # [ny]
+    r6: np.ndarray   # [ny]
+    r3: np.ndarray   # [ny]
+    r5: np.ndarray   # [ny]
+    cx: np.ndarray   # [ny]  R2 = CX * max(HP,0)
+    cy: np.ndarray   # [ny]  R4 = CY * max(HQ,0)
+    r2: np.ndarray = field(default=None)  # [ny, nx]
+    r4: np.ndarray = field(default=None)
+
+    def rows(self) -> np.ndarray:
+        return np.stack([self.r1, self.r11, self.r6, self.r3, self.r5, self.cx, self.cy]).astype(np.float32)
+
+
+def para(h: np.ndarray, lat: np.ndarray, dx_min: float, dt: float, del_y_min=None, laygov: int = 0) -> Coefs:
+    ny, nx = h.shape
+    lat = np.asarray(lat, dtype=np.float64)
+    dely = np.full(ny, dx_min, dtype=np.float64) if del_y_min is None else np.asarray(del_y_min, np.float64)
+    rr = dt / R_EARTH
+    rs = 9.807 * rr
+    rt = 0.5 * dt * CORI_W
+    ang_m = lat * RAD_DEG
+    ang_n = (lat + 0.5 * dely / 60.0) * RAD_DEG
+    cos_m, cos_n = np.cos(ang_m), np.cos(ang_n)
+    sin_m, sin_n = np.sin(ang_m), np.sin(ang_n)
+    r1 = (rr / cos_m / (dx_min * RAD_MIN)).astype(np.float32)
+    r11 = (rr / cos_m / (dely * RAD_MIN)).astype(np.float32)
+    cx = (rs / cos_m / (dx_min * RAD_MIN)).astype(np.float32)
+    cy = (rs / (dely * RAD_MIN)).astype(np.float32)
+    r3 = (rt * sin_m).astype(np.float32)
+    r5 = (rt * sin_n).astype(np.float32)
+    r6 = cos_n.astype(np.float32)
+    hp, hq = pq_depth(h)
+    if laygov == 0:
+        r2 = (cx[:, None] * np.maximum(hp, F32(0))).astype(np.float32)
+        r4 = (cy[:, None] * np.maximum(hq, F32(0))).astype(np.float32)
+    else:
+        r2 = np.repeat(cx[:, None], nx, axis=1).astype(np.float32)
+        r4 = np.repeat(cy[:, None], nx, axis=1).astype(np.float32)
+    return Coefs(r1, r11, r6, r3, r5, cx, cy, r2, r4)
+
+
+def rel_time(dt_parent: float, dx_m: float, dy_m: float, hmax: float, nonlinear: bool):
+    """(rel_time, dt_child) from the Courant rule with CR 0.5 (0.35 nonlinear)."""
+    h_max = max(np.float32(hmax), GX)
+    cr = F32(0.35) if nonlinear else F32(0.5)
+    dt = cr * F32(min(dx_m, dy_m)) / np.sqrt(GRAV * F32(h_max))
+    dtp = F32(dt_parent)
+    if dt >= dtp:
+        return 1, float(dtp)
+    ir = int(math.floor(float(dtp / dt))) + 1
+    return ir, float(dtp / F32(ir))
+
+
+def corners(xp: np.ndarray, yp: np.ndarray, xs: float, xe: float, ys: float, ye: float):
+    """[IS, IE, JS, JE] (1-based) of a child window inside the parent axes."""
+    c = [1, 1, 1, 1]
+    xp = xp.astype(np.float32)
+    yp = yp.astype(np.float32)
+    for k in range(2, len(xp)):
+        lo = (xp[k - 2] + xp[k - 1]) / F32(2)
+        hi = (xp[k - 1] + xp[k]) / F32(2)
+        if lo <= F32(xs) < hi:
+            c[0] = k + 1
+        if lo <= F32(xe) < hi:
+            c[1] = k - 1
+    for k in range(2, len(yp)):
+        lo = (yp[k - 2] + yp[k - 1]) / F32(2)
+        hi = (yp[k - 1] + yp[k]) / F32(2)
+        if lo <= F32(ys) < hi:
+            c[2] = k + 1
+        if lo <= F32(ye) < hi:
+            c[3] = k - 1
+    return c
+
+
+def locate_gauge(x: np.ndarray, y: np.ndarray, x0: float, y0: float, first: int = 1):
+    """(KI, KJ, CX, CY) with GET_TS's search (1-based; first=1 layer 1, 2 inner)."""
+    nx, ny = len(x), len(y)
+    x0, y0 = F32(x0), F32(y0)
+    ki = kj = 0
+    for i in range(first, nx):
+        if x[i - 1] <= x0 < x[i]:
+            ki = i
+        if x0 < x[first - 1]:
+            ki = first
+        if x0 >= x[nx - 1]:
+            ki = nx - 1
+    for j in range(first, ny):
+        if y[j - 1] <= y0 < y[j]:
+            kj = j
+        if y0 < y[first - 1]:
+            kj = first
+        if y0 >= y[ny - 1]:
+            kj = ny - 1
+    cx = (x0 - x[ki - 1]) / (x[ki] - x[ki - 1])
+    cy = (y0 - y[kj - 1]) / (y[kj] - y[kj - 1])
+    return ki, kj, F32(cx), F32(cy)
+
+
+def child_axes_spherical(xp, yp, corners_, rel_size, dx_min_parent):
+    """Child axes for a spherical child of a spherical parent (SUBGRID_MATCHING
+    initialization.f90:970-1000), uniform DEL_Y."""
+    is_, ie, js, je = corners_
+    nx = (ie - is_ + 1) * rel_size + 1
+    ny = (je - js + 1) * rel_size + 1
+    dx = F32(dx_min_parent) / F32(rel_size) / F32(60.0)
+    xs = F32(0.5) * (xp[is_ - 1] + xp[is_ - 2]) - dx / F32(2.0)
+    ys = F32(0.5) * (yp[js - 1] + yp[js - 2]) - dx / F32(2.0)
+    x = (np.arange(nx, dtype=np.float32) * dx + xs).astype(np.float32)
+    y = (np.arange(ny, dtype=np.float32) * dx + ys).astype(np.float32)
+    return x, y
+
+
+def child_cartesian_spacing(yp, corners_, rel_size, dx_min_parent):
+    """Metres per child cell of a Cartesian child in a spherical parent: the
+    parent cell at the window's south edge divided by the ratio (the reference
+    converts the window corners with its UTM routine, initialization.f90:1004-1050;
+    this uses the local arc lengths, which agree to <0.1% inside a 1-degree window)."""
+    is_, ie, js, je = corners_
+    lat = float(0.5 * (yp[js - 1] + yp[js - 2]))
+    dlon = dx_min_parent / 60.0 * RAD_DEG
+    dx = R_EARTH * math.cos(lat * RAD_DEG) * dlon / rel_size
+    dy = R_EARTH * dlon / rel_size
+    return dx, dy

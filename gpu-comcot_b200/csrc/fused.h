@@ -1,0 +1,50 @@
+/*
+ * Descriptor of one grid in the fused linear-spherical step and in the
+ * batched work-list launch (ensemble members, serving slots).
+ */
+#ifndef GC_FUSED_H
+#define GC_FUSED_H
+
+#include "gc_internal.h"
+
+#define GC_F_MAXAMP 1
+#define GC_F_ARRIVAL 2
+
+struct GcFusedGrid {
+    int nx, ny, pitch, root, explicit_r24;
+    int tiles_x;      /* tiles along I */
+    int step0, cur0;  /* at step `step0`, buffer `cur0` holds time level 1 */
+    int nsteps;       /* steps this grid runs; the step after the last only samples gauges */
+    int flags;        /* GC_F_MAXAMP | GC_F_ARRIVAL */
+    float thr;        /* arrival threshold */
+    float *z[2], *m[2], *n[2];
+    const float *h, *rows, *r2, *r4;
+    float *zmax;
+    int *arrival;
+    /* gauges: the step-s kernel samples the surface left by step s-1 into
+     * ts[(s-1-step0)*ng + g] (bilinear, GET_TS weights) when s-1 >= step0 */
+    int ng;
+    const int *gij;     /* [2*ng] 1-based (KI, KJ) */
+    const float *gw;    /* [2*ng] (CX, CY) */
+    float *ts;
+    int ts_len;         /* steps the ts buffer can hold */
+};
+
+/* tile shape of one launch variant */
+struct GcTileCfg {
+    int tx, ty;
+};
+
+int gc_fused_num_variants();
+GcTileCfg gc_fused_variant(int v);
+/* launches the fused step over a work list: tiles[t] = {grid, tile within
+ * that grid}; step = *step_base + step_off (step_base may be NULL) */
+cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles,
+                                  int ntiles, const int *d_step_base, int step_off, int nctas,
+                                  cudaStream_t s);
+int gc_fused_max_ctas(int variant);
+/* single grid, descriptor by value */
+cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s);
+int gc_fused_tiles(int variant, int nx, int ny, int *tiles_x);
+
+#endif

@@ -1,0 +1,103 @@
+/*
+ * Internal definitions of the B200 COMCOT library: device layer view, row
+ * coefficient layout, launch helpers and error plumbing.
+ *
+ * Device layout of one layer (Fortran (I,J) -> 0-based (i,j) = (I-1,J-1)):
+ *   every NX x NY field is stored row-pitched, I fastest, with the row
+ *   pitch rounded up to 32 floats (128 B) so every row starts on a 128-byte
+ *   boundary; element (i,j) is at p[j*pitch + i].
+ *   Z, M, N are ping-pong pairs; `cur` names the buffer holding time level 1
+ *   (the reference's Zdat/MNdat), the other holds level 2 (Zout/MNout).
+ *   Per-row coefficients live in one [GC_NROW][ny] array (see GcRow).
+ */
+#ifndef GC_INTERNAL_H
+#define GC_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include "comcot_consts.h"
+#include "comcot_math.h"
+
+#define GC_MAX_LAYERS 20
+
+/* rows of the per-row coefficient block: R1(1,J), R11(1,J), R6(J),
+ * R3(1,J), R5(1,J) from PARA (comcot.f90:713-752), and the factored
+ * R2 = CX(J)*max(HP,0), R4 = CY(J)*max(HQ,0) multipliers. */
+enum GcRow { GC_R1 = 0, GC_R11, GC_R6, GC_R3, GC_R5, GC_CX, GC_CY, GC_NROW };
+
+/* What a kernel needs to know about one layer.  Passed by value. */
+struct GcLayerDev {
+    int nx, ny, pitch;
+    int root;          /* 1 for the outermost layer (reference layer id 1) */
+    int laycord, laygov, linchk, modscm, fric_switch;
+    int explicit_r24;  /* 1: R2/R4 stored as fields; 0: factored per row */
+    float rx, ry, grx, gry, dt, fric_coef;
+    const float *z1, *m1, *n1;   /* time level 1 */
+    float *z2, *m2, *n2;         /* time level 2 */
+    float *m1w, *n1w;            /* writable alias of level 1 (nesting edges) */
+    float *z1w;
+    const float *h, *hp, *hq;
+    const float *r2, *r4;        /* only when explicit_r24 */
+    const float *rows;           /* [GC_NROW][ny] */
+    float *dz2;                  /* nonlinear layers */
+    float *xflux, *yflux;        /* [2*nx], [2*ny] forecast caches */
+    float *zmax;
+    int *arrival;
+};
+
+#define GC_AT(p, L, i, j) ((p)[(size_t)(j) * (size_t)(L).pitch + (size_t)(i)])
+#define GC_ROW(L, k, j) ((L).rows[(size_t)(k) * (size_t)(L).ny + (size_t)(j)])
+
+/* status codes of the extended API */
+#define GC_OK 0
+#define GC_EINVAL -1
+#define GC_ENOMEM -2
+#define GC_ECUDA -3
+#define GC_ESTATE -4
+#define GC_ETIMEOUT -5
+#define GC_ENOTSUP -6
+
+const char *gc_status_str(int code);
+
+#define GC_CUDA_OR_RET(call)                                                       \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            fprintf(stderr, "gcomcot: %s at %s:%d\n", cudaGetErrorString(e_),      \
+                    __FILE__, __LINE__);                                           \
+            return GC_ECUDA;                                                       \
+        }                                                                          \
+    } while (0)
+
+/* legacy entry points mirror the reference: print and exit on a CUDA error */
+#define GC_CUDA_OR_DIE(call)                                                       \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            fprintf(stderr, "gcomcot: %s in %s at line %d\n",                      \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);                   \
+            exit(EXIT_FAILURE);                                                    \
+        }                                                                          \
+    } while (0)
+
+/* ---- per-phase kernels (kernels_phase.cu) ---- */
+void gc_launch_mass(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_open(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_moment(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_update_edges(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                     const int *corners, int t, cudaStream_t s);
+void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                   const int *corners, cudaStream_t s);
+void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);
+void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s);
+
+/* ---- fused step (kernels_fused.cu) ---- */
+struct GcFusedGrid;
+struct GcTile;
+
+#endif

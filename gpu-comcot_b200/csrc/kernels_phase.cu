@@ -1,0 +1,752 @@
+/*
+ * Per-phase sm_100a kernels of the COMCOT time stepper: one launch per phase
+ * and layer.  These are the building blocks of the nested sub-cycle and the
+ * "plain" path the fused and batched kernels are measured against.
+ *
+ * Every kernel evaluates the Fortran expression in the Fortran order with
+ * separately rounded float operations (the library is built with
+ * -fmad=false; IEEE division and square root), so results are bit-identical
+ * to the REAL arithmetic of the reference solvers cited per kernel.
+ * Indices are 0-based: Fortran (I,J) = (i+1, j+1).
+ */
+#include "gc_internal.h"
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+__device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
+
+/* ---------------------------------------------------------------- */
+/* continuity                                                        */
+/* ---------------------------------------------------------------- */
+/* MASS_S (mass.f90:61-100).  Child edge rows i==0 / j==0 are not computed by
+ * the reference; they keep the value of time level 1 (the UPDATE edge copy of
+ * all_grids.f90:323-324 made them equal), so they are carried over here. */
+__global__ void k_mass_s(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    if (L.root) {
+        if (i < 1 || i > L.nx - 2 || j < 1 || j > L.ny - 2) return;
+    } else if (i == 0 || j == 0) {
+        L.z2[c] = L.z1[c];
+        return;
+    }
+    float h = L.h[c];
+    float out;
+    if (h > CC_GX) {
+        float r1 = GC_ROW(L, GC_R1, j), r11 = GC_ROW(L, GC_R11, j);
+        float r6 = GC_ROW(L, GC_R6, j), r6m = GC_ROW(L, GC_R6, j - 1);
+        float zz = L.z1[c] - r1 * (L.m1[c] - L.m1[c - 1])
+                   - r11 * (L.n1[c] * r6 - L.n1[c - L.pitch] * r6m);
+        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if ((zz + h) <= CC_EPS) zz = -h;
+        out = zz;
+    } else {
+        out = 0.0f;
+    }
+    L.z2[c] = out;
+}
+
+/* MASS_C (mass.f90:103-157) and CONMASS (mass.f90:162-224) */
+template <bool NONLIN>
+__global__ void k_mass_c(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    if (L.root) {
+        if (i < 1 || i > L.nx - 2 || j < 1 || j > L.ny - 2) return;
+    } else if (i == 0 || j == 0) {
+        L.z2[c] = L.z1[c];
+        return;
+    }
+    float h = L.h[c];
+    float zz = L.z1[c] - L.rx * (L.m1[c] - L.m1[c - 1]) - L.ry * (L.n1[c] - L.n1[c - L.pitch]);
+    if (fabs_(zz) < CC_EPS) zz = 0.0f;
+    if (!NONLIN) {
+        float out;
+        if (h > CC_GX) {
+            if ((zz + h) <= CC_EPS) zz = -h;
+            out = zz;
+        } else {
+            out = 0.0f;
+        }
+        L.z2[c] = out;
+    } else {
+        float dz, z;
+        if (h > CC_ELMAX) {
+            float dd = zz + h;
+            if (dd >= CC_GX) { dz = dd; z = zz; }
+            else { dz = 0.0f; z = -h; }
+        } else {
+            dz = 0.0f; z = -h;
+        }
+        L.dz2[c] = dz;
+        L.z2[c] = z;
+    }
+}
+
+/* ---------------------------------------------------------------- */
+/* linear spherical momentum (moment.f90:65-149)                     */
+/* ---------------------------------------------------------------- */
+__device__ __forceinline__ float r2_at(const GcLayerDev &L, int i, int j, size_t c, float h,
+                                       float hp1) {
+    if (L.explicit_r24) return L.r2[c];
+    /* R2 = RS/COS_M/(DX*RAD_MIN) * AMAX1(HP,0) with HP from PQ_DEPTH; the
+     * caller only needs it where H(i)>GX and H(i+1)>GX, so HP>0 there. */
+    return GC_ROW(L, GC_CX, j) * (0.5f * (h + hp1));
+}
+__device__ __forceinline__ float r4_at(const GcLayerDev &L, int i, int j, size_t c, float h,
+                                       float hq1) {
+    if (L.explicit_r24) return L.r4[c];
+    return GC_ROW(L, GC_CY, j) * (0.5f * (h + hq1));
+}
+
+__global__ void k_momt_s(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const int P = L.pitch;
+    size_t c = (size_t)j * P + i;
+    int lo = L.root ? 0 : 1;
+    /* x-momentum: i in [lo, nx-2], j in [lo, ny-1]; 0 elsewhere */
+    float xm = 0.0f;
+    if (i >= lo && i <= L.nx - 2 && j >= lo) {
+        float h = L.h[c], hp1 = L.h[c + 1];
+        if (h > CC_GX && hp1 > CC_GX) {
+            size_t cm = (j > 0) ? c - P : c;  /* JM1 = max(J-1,1) */
+            float tot_n = L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1];
+            xm = L.m1[c] - r2_at(L, i, j, c, h, hp1) * (L.z2[c + 1] - L.z2[c])
+                 + GC_ROW(L, GC_R3, j) * tot_n;
+            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+        }
+    }
+    L.m2[c] = xm;
+    /* y-momentum: j in [lo, ny-2], i in [lo, nx-1]; 0 elsewhere */
+    float xn = 0.0f;
+    if (j >= lo && j <= L.ny - 2 && i >= lo) {
+        float h = L.h[c], hq1 = L.h[c + P];
+        if (h > CC_GX && hq1 > CC_GX) {
+            size_t cw = (i > 0) ? c - 1 : c;  /* IM1 = max(I-1,1) */
+            float tot_m = L.m1[cw] + L.m1[cw + P] + L.m1[c] + L.m1[c + P];
+            xn = L.n1[c] - r4_at(L, i, j, c, h, hq1) * (L.z2[c + P] - L.z2[c])
+                 - GC_ROW(L, GC_R5, j) * tot_m;
+            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+        }
+    }
+    L.n2[c] = xn;
+}
+
+/* ---------------------------------------------------------------- */
+/* linear Cartesian momentum (moment.f90:152-277)                    */
+/* ---------------------------------------------------------------- */
+__global__ void k_momt_c(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const int P = L.pitch, nx = L.nx, ny = L.ny;
+    size_t c = (size_t)j * P + i;
+    int lo = L.root ? 0 : 1;
+    const float konst = 0.5f * L.dt * CC_GRAV;
+    const float fm = L.fric_coef;
+    const float *z = L.z2;
+    float xm = 0.0f;
+    if (i >= lo && i <= nx - 2 && j >= lo) {
+        float h = L.h[c], hp1 = L.h[c + 1];
+        if (h > CC_GX && hp1 > CC_GX) {
+            int jm1 = j > 0 ? j - 1 : 0, jp1 = j < ny - 1 ? j + 1 : ny - 1;
+            size_t cm = (size_t)jm1 * P + i, cpj = (size_t)jp1 * P + i;
+            float ff = 0.0f;
+            float hm = L.hp[c] + 0.5f * (z[c] + z[c + 1]);
+            xm = L.m1[c] - L.grx * hm * (z[c + 1] - z[c]);
+            if (L.fric_switch != 1) {
+                float xqq = 0.25f * (L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1]);
+                if (hm >= 1.0e-3f)
+                    ff = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq)
+                         / cc_powf(hm, CC_MANNEXP);
+                else
+                    ff = 0.0f;
+                xm = xm - ff * L.m1[c];
+            }
+            if (L.modscm == 0) {
+                float scm = L.grx * CC_TWLVTH * hm
+                            * ((z[cpj + 1] - 2.0f * z[c + 1] + z[cm + 1])
+                               - (z[cpj] - 2.0f * z[c] + z[cm]));
+                xm = xm - scm;
+            }
+            if (L.fric_switch != 1) xm = xm / (1.0f + ff);
+            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+        }
+    }
+    L.m2[c] = xm;
+    float xn = 0.0f;
+    if (j >= lo && j <= ny - 2 && i >= lo) {
+        float h = L.h[c], hq1 = L.h[c + P];
+        if (h > CC_GX && hq1 > CC_GX) {
+            int im1 = i > 0 ? i - 1 : 0, ip1 = i < nx - 1 ? i + 1 : nx - 1;
+            size_t cq = c + P;
+            float ff = 0.0f;
+            float hn = L.hq[c] + 0.5f * (z[c] + z[cq]);
+            xn = L.n1[c] - L.gry * hn * (z[cq] - z[c]);
+            if (L.fric_switch != 1) {
+                float xpp = 0.25f * (L.m1[c] + L.m1[cq] + L.m1[(size_t)j * P + im1]
+                                     + L.m1[(size_t)(j + 1) * P + im1]);
+                if (hn >= 1.0e-5f)
+                    ff = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp)
+                         / cc_powf(hn, CC_MANNEXP);
+                else
+                    ff = 0.0f;
+                xn = xn - ff * L.n1[c];
+            }
+            if (L.modscm == 0) {
+                size_t r0 = (size_t)j * P, r1 = (size_t)(j + 1) * P;
+                float scm = L.gry * CC_TWLVTH * hn
+                            * ((z[r1 + ip1] - 2.0f * z[r1 + i] + z[r1 + im1])
+                               - (z[r0 + ip1] - 2.0f * z[r0 + i] + z[r0 + im1]));
+                xn = xn - scm;
+            }
+            if (L.fric_switch != 1) xn = xn / (1.0f + ff);
+            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+        }
+    }
+    L.n2[c] = xn;
+}
+
+/* ---------------------------------------------------------------- */
+/* nonlinear Cartesian momentum: CONMOME (moment.f90:280-780) with    */
+/* WAVE_BREAKING (moment.f90:1272-1384).  DZ(:,:,1) is identically    */
+/* zero in the reference, so DP1 = 0.25*(DZ2(I)+DZ2(I+1)) etc.         */
+/* ---------------------------------------------------------------- */
+struct NlView {
+    const float *dz;
+    int nx, ny, P;
+    __device__ __forceinline__ float d(int i, int j) const { return dz[(size_t)j * P + i]; }
+    __device__ __forceinline__ float dp1(int i, int j) const {
+        int ip1 = i + 1 < nx ? i + 1 : nx - 1;
+        float v = 0.25f * (d(i, j) + 0.0f + d(ip1, j) + 0.0f);
+        return v < CC_GX ? 0.0f : v;
+    }
+    __device__ __forceinline__ float dp2(int i, int j) const {
+        int ip1 = i + 1 < nx ? i + 1 : nx - 1;
+        float v = 0.50f * (d(i, j) + d(ip1, j));
+        return v < CC_GX ? 0.0f : v;
+    }
+    __device__ __forceinline__ float dq1(int i, int j) const {
+        int jp1 = j + 1 < ny ? j + 1 : ny - 1;
+        float v = 0.25f * (d(i, j) + 0.0f + d(i, jp1) + 0.0f);
+        return v < CC_GX ? 0.0f : v;
+    }
+    __device__ __forceinline__ float dq2(int i, int j) const {
+        int jp1 = j + 1 < ny ? j + 1 : ny - 1;
+        float v = 0.50f * (d(i, j) + d(i, jp1));
+        return v < CC_GX ? 0.0f : v;
+    }
+};
+
+__device__ __forceinline__ void wave_breaking(const GcLayerDev &L, size_t c, float &advx,
+                                              float &advy) {
+    float cc = sqrtf(CC_GRAV * L.dz2[c]);
+    float dzdt_f = CC_BRK_F * cc;
+    float dzdt_i = CC_BRK_I * cc;
+    float dzdt = fabs_(L.z2[c] - L.z1[c]) / L.dt;
+    if (dzdt > dzdt_f) {
+        float ref = (dzdt - dzdt_f) / (dzdt_i - dzdt_f);
+        float coef = cc_expf(-(1.0f * ref));
+        advx = coef * advx;
+        advy = coef * advy;
+    }
+}
+
+__global__ void k_conmome(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const int P = L.pitch, ix = L.nx, jy = L.ny;
+    const size_t c = (size_t)j * P + i;
+    const NlView D{L.dz2, ix, jy, P};
+    const float *z = L.z2, *hz = L.h, *p = L.m1, *q = L.n1;
+    const float konst = (L.fric_switch != 1) ? 0.5f * L.dt * CC_GRAV : 0.0f;
+    const float fm = L.fric_coef;
+    /* Fortran spans: I > 10 .AND. I < IX-10 with I = i+1 */
+    const bool span = (i + 1 > CC_SPAN) && (i + 1 < ix - CC_SPAN) && (j + 1 > CC_SPAN)
+                      && (j + 1 < jy - CC_SPAN);
+    const int im1 = i > 0 ? i - 1 : 0, ip1 = i + 1 < ix ? i + 1 : ix - 1;
+    const int jm1 = j > 0 ? j - 1 : 0, jp1 = j + 1 < jy ? j + 1 : jy - 1;
+#define AT(a, ii, jj) (a)[(size_t)(jj) * P + (ii)]
+
+    /* ---------------- x direction ---------------- */
+    {
+        bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
+        float out = 0.0f;
+        if (inx) {
+            size_t cp = (size_t)j * P + ip1;
+            float dd = 0.0f, df = 0.0f, ff;
+            bool noflux = false;
+            if (hz[c] <= CC_ELMAX || L.hp[c] <= CC_ELMAX) {
+                noflux = true;
+            } else {
+                float dzc = D.d(i, j), dzp = D.d(ip1, j);
+                if (dzc > CC_GX && dzp > CC_GX) {
+                    dd = D.dp2(i, j); df = D.dp1(i, j);
+                } else if (dzc > CC_GX && dzp <= CC_GX && hz[cp] + z[c] > CC_GX) {
+                    dd = 0.5f * dzc; df = dd;
+                } else if (dzc <= CC_GX && dzp > CC_GX && hz[c] + z[cp] > CC_GX) {
+                    dd = 0.5f * dzp; df = dd;
+                } else {
+                    noflux = true;
+                }
+                if (!noflux && dd < CC_GX) noflux = true;
+            }
+            if (!noflux) {
+                if (df < CC_DFMIN) df = CC_DFMIN;
+                float xqq = 0.25f * (q[c] + q[cp] + AT(q, i, jm1) + AT(q, ip1, jm1));
+                if (L.fric_switch != 1)
+                    ff = konst * fm * fm * sqrtf(p[c] * p[c] + xqq * xqq) / cc_powf(df, CC_MANNEXP);
+                else
+                    ff = 0.0f;
+                float xp = p[c] - L.grx * dd * (z[cp] - z[c]);
+                if (L.modscm == 0 && j + 1 < jy) {
+                    float scm = L.grx * dd / 12.0f
+                                * ((AT(z, ip1, jp1) - 2.0f * z[cp] + AT(z, ip1, jm1))
+                                   - (AT(z, i, jp1) - 2.0f * z[c] + AT(z, i, jm1)));
+                    xp = xp - scm;
+                }
+                if (L.fric_switch != 1) xp = xp - ff * p[c];
+                float dp1c = D.dp1(i, j);
+                if (L.linchk == 1 && dp1c >= CC_GX && span) {
+                    float advx, advy;
+                    if (p[c] < 0.0f) {
+                        float dp1p = D.dp1(ip1, j);
+                        if (dp1p < CC_GX || D.d(ip1, j) < CC_GX)
+                            advx = L.rx * (-(p[c] * p[c] / dp1c));
+                        else
+                            advx = L.rx * (p[cp] * p[cp] / dp1p - p[c] * p[c] / dp1c);
+                    } else {
+                        float dp1m = D.dp1(im1, j);
+                        float pm = AT(p, im1, j);
+                        if (dp1m < CC_GX || D.d(i, j) < CC_GX)
+                            advx = L.rx * (p[c] * p[c] / dp1c);
+                        else
+                            advx = L.rx * (p[c] * p[c] / dp1c - pm * pm / dp1m);
+                    }
+                    if (xqq < 0.0f) {
+                        if (D.d(i, jp1) < CC_GX || D.d(ip1, jp1) < CC_GX) {
+                            advy = L.ry * (-(p[c] * xqq / dp1c));
+                        } else if (D.dp1(i, jp1) < CC_GX) {
+                            advy = L.ry * (-(p[c] * xqq / dp1c));
+                        } else {
+                            float xqe = 0.25f * (AT(q, i, jp1) + AT(q, ip1, jp1) + q[c] + q[cp]);
+                            advy = L.ry * (AT(p, i, jp1) * xqe / D.dp1(i, jp1) - p[c] * xqq / dp1c);
+                        }
+                    } else {
+                        if (D.d(i, jm1) < CC_GX || D.d(ip1, jm1) < CC_GX) {
+                            advy = L.ry * (p[c] * xqq / dp1c);
+                        } else if (D.dp1(i, jm1) < CC_GX) {
+                            advy = L.ry * (p[c] * xqq / dp1c);
+                        } else {
+                            float xqe = 0.25f * (AT(q, i, jm1) + AT(q, ip1, jm1) + AT(q, i, j - 2)
+                                                 + AT(q, ip1, j - 2));
+                            advy = L.ry * (p[c] * xqq / dp1c - AT(p, i, jm1) * xqe / D.dp1(i, jm1));
+                        }
+                    }
+                    wave_breaking(L, c, advx, advy);
+                    xp = xp - advx - advy;
+                }
+                if (L.fric_switch != 1) xp = xp / (1.0f + ff);
+                if (fabs_(xp) < CC_EPS) xp = 0.0f;
+                float lim = CC_VLIMIT * dd;
+                if (xp > lim) xp = lim;
+                if (xp < -lim) xp = -lim;
+                out = xp;
+            }
+        }
+        L.m2[c] = out;
+    }
+    /* ---------------- y direction ---------------- */
+    {
+        bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
+        float out = 0.0f;
+        if (iny) {
+            size_t cq = (size_t)jp1 * P + i;
+            float dd = 0.0f, df = 0.0f, ff;
+            bool noflux = false;
+            if (hz[c] <= CC_ELMAX || L.hq[c] <= CC_ELMAX) {
+                noflux = true;
+            } else {
+                float dzc = D.d(i, j), dzq = D.d(i, jp1);
+                if (dzc > CC_GX && dzq > CC_GX) {
+                    dd = D.dq2(i, j); df = D.dq1(i, j);
+                } else if (dzc > CC_GX && dzq <= CC_GX && hz[cq] + z[c] > CC_GX) {
+                    dd = 0.5f * dzc; df = dd;
+                } else if (dzc <= CC_GX && dzq > CC_GX && hz[c] + z[cq] > CC_GX) {
+                    dd = 0.5f * dzq; df = dd;
+                } else {
+                    noflux = true;
+                }
+                if (!noflux && dd < CC_GX) noflux = true;
+            }
+            if (!noflux) {
+                if (df < CC_DFMIN) df = CC_DFMIN;
+                float xpp = 0.25f * (p[c] + p[cq] + AT(p, im1, j) + AT(p, im1, jp1));
+                if (L.fric_switch != 1)
+                    ff = konst * fm * fm * sqrtf(q[c] * q[c] + xpp * xpp) / cc_powf(df, CC_MANNEXP);
+                else
+                    ff = 0.0f;
+                float xq = q[c] - L.gry * dd * (z[cq] - z[c]);
+                if (L.modscm == 0 && i + 1 < ix) {
+                    float scm = L.gry * dd / 12.0f
+                                * ((AT(z, ip1, jp1) - 2.0f * z[cq] + AT(z, im1, jp1))
+                                   - (AT(z, ip1, j) - 2.0f * z[c] + AT(z, im1, j)));
+                    xq = xq - scm;
+                }
+                /* moment.f90:672 applies -FF*Q to XP, which is unused: no term on XQ */
+                float dq1c = D.dq1(i, j);
+                if (L.linchk == 1 && dq1c >= CC_GX && span) {
+                    float advx, advy;
+                    if (q[c] < 0.0f) {
+                        float dq1q = D.dq1(i, jp1);
+                        if (dq1q < CC_GX || D.d(i, jp1) < CC_GX)
+                            advy = L.ry * (-(q[c] * q[c] / dq1c));
+                        else
+                            advy = L.ry * (q[cq] * q[cq] / dq1q - q[c] * q[c] / dq1c);
+                    } else {
+                        float dq1m = D.dq1(i, jm1);
+                        float qm = AT(q, i, jm1);
+                        if (dq1m < CC_GX || D.d(i, j) < CC_GX)
+                            advy = L.ry * (q[c] * q[c] / dq1c);
+                        else
+                            advy = L.ry * (q[c] * q[c] / dq1c - qm * qm / dq1m);
+                    }
+                    if (xpp < 0.0f) {
+                        if (D.d(ip1, j) < CC_GX || D.d(ip1, jp1) < CC_GX) {
+                            advx = L.rx * (-(q[c] * xpp / dq1c));
+                        } else if (D.dq1(ip1, j) < CC_GX) {
+                            advx = L.rx * (-(q[c] * xpp / dq1c));
+                        } else {
+                            float xpe = 0.25f * (AT(p, ip1, j) + AT(p, ip1, jp1) + p[c] + p[cq]);
+                            advx = L.rx * (AT(q, ip1, j) * xpe / D.dq1(ip1, j) - q[c] * xpp / dq1c);
+                        }
+                    } else {
+                        if (D.d(im1, j) < CC_GX || D.d(im1, jp1) < CC_GX) {
+                            advx = L.rx * (q[c] * xpp / dq1c);
+                        } else if (D.dq1(i - 1, j) < CC_GX) {
+                            advx = L.rx * (q[c] * xpp / dq1c);
+                        } else {
+                            float xpe = 0.25f * (AT(p, im1, j) + AT(p, im1, jp1) + AT(p, i - 2, j)
+                                                 + AT(p, i - 2, jp1));
+                            advx = L.rx * (q[c] * xpp / dq1c - AT(q, im1, j) * xpe / D.dq1(im1, j));
+                        }
+                    }
+                    wave_breaking(L, c, advx, advy);
+                    xq = xq - advx - advy;
+                }
+                if (L.fric_switch != 1) xq = xq / (1.0f + ff);
+                if (fabs_(xq) < CC_EPS) xq = 0.0f;
+                float lim = CC_VLIMIT * dd;
+                if (xq > lim) xq = lim;
+                if (xq < -lim) xq = -lim;
+                out = xq;
+            }
+        }
+        L.n2[c] = out;
+    }
+#undef AT
+}
+
+/* ---------------------------------------------------------------- */
+/* OPEN radiation boundary (boundaries.f90:22-202), outermost layer  */
+/* ---------------------------------------------------------------- */
+__device__ float open_cell(const GcLayerDev &L, int i, int j) {
+    const int nx = L.nx, ny = L.ny, P = L.pitch;
+    const float *m = L.m1, *n = L.n1, *h = L.h;
+    size_t c = (size_t)j * P + i;
+    float hc = h[c];
+    if (!(hc > CC_GX)) return 0.0f;
+    float cc = sqrtf(CC_GRAV * hc);
+    float zz;
+    bool corner = (i == 0 || i == nx - 1) && (j == 0 || j == ny - 1);
+    if (!corner) {
+        if (j == 0) {
+            float uh = 0.5f * (m[c] + m[c - 1]);
+            float uu = sqrtf(uh * uh + n[c] * n[c]);
+            zz = uu / cc;
+            if (n[c] > 0.0f) zz = -zz;
+        } else if (j == ny - 1) {
+            float ns = n[c - P];
+            float uh = 0.5f * (m[c] + m[c - 1]);
+            float uu = sqrtf(uh * uh + ns * ns);
+            zz = uu / cc;
+            if (ns < 0.0f) zz = -zz;
+        } else if (i == 0) {
+            float uh = (h[c - P] > CC_GX) ? 0.5f * (n[c] + n[c - P]) : n[c];
+            float uu = sqrtf(uh * uh + m[c] * m[c]);
+            zz = uu / cc;
+            if (m[c] > 0.0f) zz = -zz;
+        } else { /* i == nx-1 */
+            float mw = m[c - 1];
+            float uh = 0.5f * (n[c] + n[c - P]);
+            float uu = sqrtf(uh * uh + mw * mw);
+            zz = uu / cc;
+            if (mw < 0.0f) zz = -zz;
+        }
+    } else {
+        float qx, qy;
+        bool neg;
+        if (i == 0 && j == 0) {
+            qx = m[c]; qy = n[c];
+        } else if (i == nx - 1 && j == 0) {
+            qx = m[c - 1]; qy = n[c];
+        } else if (i == 0) {
+            qx = m[c]; qy = n[c - P];
+        } else {
+            qx = m[c - 1]; qy = n[c - P];
+        }
+        float uh = sqrtf(qx * qx + qy * qy);
+        zz = uh / cc;
+        if (i == 0 && j == 0) neg = (qx > 0.0f || qy > 0.0f);
+        else if (j == 0) neg = (qx < 0.0f || qy > 0.0f);
+        else if (i == 0) neg = (qx > 0.0f || qy < 0.0f);
+        else neg = (qx < 0.0f || qy < 0.0f);
+        if (neg) zz = -zz;
+    }
+    if (fabs_(zz) > CC_UB) zz = 0.0f;
+    return zz;
+}
+
+/* one thread per perimeter cell: index k walks J=1 row, J=NY row, I=1, I=NX */
+__global__ void k_open(GcLayerDev L) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = L.nx, ny = L.ny;
+    int i, j;
+    if (k < nx) { i = k; j = 0; }
+    else if (k < 2 * nx) { i = k - nx; j = ny - 1; }
+    else if (k < 2 * nx + (ny - 2)) { i = 0; j = k - 2 * nx + 1; }
+    else if (k < 2 * nx + 2 * (ny - 2)) { i = nx - 1; j = k - 2 * nx - (ny - 2) + 1; }
+    else return;
+    L.z2[(size_t)j * L.pitch + i] = open_cell(L, i, j);
+}
+
+/* UPDATE edge copy (all_grids.f90:323-324): Z2(1,:) = Z2(2,:), then
+ * Z2(:,1) = Z2(:,2), so Z2(1,1) = Z2(2,2). */
+__global__ void k_update_edges(GcLayerDev L) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t P = L.pitch;
+    if (k < L.ny) {
+        int j = k;
+        if (j >= 1) L.z2[(size_t)j * P] = L.z2[(size_t)j * P + 1];
+        else L.z2[0] = L.z2[P + 1];
+    } else if (k < L.ny + L.nx - 1) {
+        int i = k - L.ny + 1;
+        L.z2[i] = L.z2[P + i];
+    }
+}
+
+/* ---------------------------------------------------------------- */
+/* nesting: JNQ / NEWQ edge fluxes (all_grids.f90:452-801)           */
+/* one CTA per child side; phase 1 forms the parent flux profile in   */
+/* shared memory (with the T==2 forecast), phase 2 interpolates.      */
+/* ---------------------------------------------------------------- */
+constexpr int EDGE_THREADS = 256;
+
+__global__ void k_edges(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is, int ie,
+                        int js, int je, int t, int smem_len) {
+    extern __shared__ float prof[];
+    const int side = blockIdx.x; /* 0 left(M), 1 right(M), 2 bottom(N), 3 top(N) */
+    const bool vert = side < 2;
+    const int sd = side & 1;
+    /* parent line and range in Fortran 1-based indices */
+    const int line = vert ? (sd == 0 ? is - 1 : ie) : (sd == 0 ? js - 1 : je);
+    const int lo = vert ? js - 2 : is - 2, hi = vert ? je + 2 : ie + 2;
+    const int n = hi - lo + 1;
+    const int Pp = Pl.pitch;
+    const float c1 = ((float)t - 1.0f) / (float)rel_time;
+    const float c2 = 1.0f - c1;
+    for (int k = threadIdx.x; k < n && k < smem_len; k += blockDim.x) {
+        int a = lo + k;                      /* running index along the line */
+        int I = vert ? line : a, J = vert ? a : line;
+        size_t c = (size_t)(J - 1) * Pp + (I - 1);
+        float v;
+        if (t == 1) {
+            v = vert ? Pl.m1[c] : Pl.n1[c];
+        } else {
+            v = 0.0f;
+            size_t cn = vert ? c + 1 : c + Pp;   /* IP1 or JP1 neighbour */
+            if ((Pl.h[c] + Pl.z2[c] > CC_GX) && (Pl.h[cn] + Pl.z2[cn] > CC_GX)) {
+                float *cache = vert ? Pl.yflux + (size_t)sd * Pl.ny + (J - 1)
+                                    : Pl.xflux + (size_t)sd * Pl.nx + (I - 1);
+                if (t == 2) {
+                    float x;
+                    if (Pl.laycord == 0) {
+                        if (vert) {
+                            size_t cm = c - Pp; /* JM1 = J-1 */
+                            float tot_n = Pl.n1[c] + Pl.n1[c + 1] + Pl.n1[cm] + Pl.n1[cm + 1];
+                            float r2 = Pl.explicit_r24 ? Pl.r2[c]
+                                       : GC_ROW(Pl, GC_CX, J - 1) * fmaxf(Pl.hp ? Pl.hp[c] :
+                                         ((Pl.h[c] > CC_GX) ? 0.5f * (Pl.h[c] + Pl.h[c + 1]) : 0.0f), 0.0f);
+                            x = Pl.m1[c] - r2 * (Pl.z2[c + 1] - Pl.z2[c]) + GC_ROW(Pl, GC_R3, J - 1) * tot_n;
+                        } else {
+                            size_t cw = c - 1; /* IM1 = I-1 */
+                            float tot_m = Pl.m1[cw] + Pl.m1[cw + Pp] + Pl.m1[c] + Pl.m1[c + Pp];
+                            float r4 = Pl.explicit_r24 ? Pl.r4[c]
+                                       : GC_ROW(Pl, GC_CY, J - 1) * fmaxf(Pl.hq ? Pl.hq[c] :
+                                         ((Pl.h[c] > CC_GX) ? 0.5f * (Pl.h[c] + Pl.h[c + Pp]) : 0.0f), 0.0f);
+                            x = Pl.n1[c] - r4 * (Pl.z2[c + Pp] - Pl.z2[c]) - GC_ROW(Pl, GC_R5, J - 1) * tot_m;
+                        }
+                    } else {
+                        if (vert) {
+                            float hm = Pl.hp[c] + 0.5f * (Pl.z2[c] + Pl.z2[c + 1]);
+                            x = Pl.m1[c] - Pl.grx * hm * (Pl.z2[c + 1] - Pl.z2[c]);
+                        } else {
+                            float hn = Pl.hq[c] + 0.5f * (Pl.z2[c] + Pl.z2[c + Pp]);
+                            x = Pl.n1[c] - Pl.gry * hn * (Pl.z2[c + Pp] - Pl.z2[c]);
+                        }
+                    }
+                    if (fabs_(x) < CC_EPS) x = 0.0f;
+                    *cache = x;
+                }
+                v = c1 * (*cache) + c2 * (vert ? Pl.m1[c] : Pl.n1[c]);
+            }
+        }
+        prof[k] = v;
+    }
+    __syncthreads();
+    /* EDGEINTERP_VERT / _HORI (all_grids.f90:502-604) */
+    const int a0 = vert ? js : is, a1 = vert ? je : ie;
+    const int nn = 2 * ir;
+    const int fixed = vert ? (sd == 0 ? 0 : C.nx - 1) : (sd == 0 ? 0 : C.ny - 1);
+    const int total = (a1 - a0 + 1) * ir;
+    const int Pc = C.pitch;
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        int a = a0 + w / ir;
+        int kk = w % ir + 1;
+        int o = a - lo; /* profile offset of F(a) */
+        float fs = 0.5f * (prof[o - 1] + prof[o]);
+        float fe = 0.5f * (prof[o + 1] + prof[o]);
+        float cc1 = (float)((double)(fe - fs) / (double)nn);
+        float cc2 = -cc1 + fs;
+        int run = (a - a0) * ir + kk; /* 0-based child index along the edge */
+        size_t cc = vert ? (size_t)run * Pc + fixed : (size_t)fixed * Pc + run;
+        float val = 2.0f * (float)kk * cc1 + cc2;
+        if (C.h[cc] + C.z1[cc] <= CC_GX) val = 0.0f;
+        if (vert) C.m1w[cc] = val;
+        else C.n1w[cc] = val;
+    }
+}
+
+/* JNZ (all_grids.f90:342-421): mean of wet child surface over each r x r
+ * block, summed in the Fortran order (KI outer, KJ inner). */
+__global__ void k_jnz(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is, int ie, int js,
+                      int je) {
+    int I = is + blockIdx.x * blockDim.x + threadIdx.x;
+    int J = js + blockIdx.y;
+    if (I > ie || J > je) return;
+    const float half = (float)(ir * ir) / 2.0f;
+    const bool even = (rel_time % 2) == 0;
+    int i0 = (I - is) * ir; /* 0-based child index of KI = 1 is i0 */
+    int j0 = (J - js) * ir;
+    float sum = 0.0f, count = 0.0f;
+    for (int ki = 1; ki <= ir; ki++) {
+        for (int kj = 1; kj <= ir; kj++) {
+            size_t c = (size_t)(j0 + kj) * C.pitch + (i0 + ki);
+            float z2 = C.z2[c];
+            if (C.h[c] + z2 > CC_GX) {
+                if (even) sum = sum + 0.5f * (C.z1[c] + z2);
+                else sum = sum + z2;
+                count = count + 1.0f;
+            }
+        }
+    }
+    Pl.z2[(size_t)(J - 1) * Pl.pitch + (I - 1)] = (count > half) ? sum / count : 0.0f;
+}
+
+/* ---------------------------------------------------------------- */
+/* outputs                                                           */
+/* ---------------------------------------------------------------- */
+__global__ void k_maxamp(GcLayerDev L) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    float z = L.z2[c], m = L.zmax[c];
+    if (!(m >= z)) L.zmax[c] = z;
+}
+
+__global__ void k_arrival(GcLayerDev L, int step, float thr) {
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    if (L.arrival[c] < 0 && L.h[c] > CC_GX && L.z2[c] > thr) L.arrival[c] = step;
+}
+
+/* gauge stencil: for each (ki,kj) 1-based, the four surface values the
+ * reference's gcomcot_get_z_ returns (GPUOutput.cu:29-44) */
+__global__ void k_gauges(GcLayerDev L, int ng, const int *ij, float *out) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng) return;
+    int i = ij[2 * g] - 1, j = ij[2 * g + 1] - 1;
+    size_t c = (size_t)j * L.pitch + i;
+    out[4 * g + 0] = L.z2[c];
+    out[4 * g + 1] = L.z2[c + 1];
+    out[4 * g + 2] = L.z2[c + L.pitch];
+    out[4 * g + 3] = L.z2[c + L.pitch + 1];
+}
+
+inline dim3 grid2(const GcLayerDev &L) {
+    return dim3((unsigned)((L.nx + BX - 1) / BX), (unsigned)((L.ny + BY - 1) / BY), 1);
+}
+
+} // namespace
+
+void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
+    if (L.laycord == 0) k_mass_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    else if (L.laygov == 1) k_mass_c<true><<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    else k_mass_c<false><<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+}
+
+void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
+    if (L.laycord == 0) k_momt_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    else if (L.laygov == 1) k_conmome<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    else k_momt_c<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+}
+
+void gc_launch_open(const GcLayerDev &L, cudaStream_t s) {
+    int n = 2 * L.nx + 2 * (L.ny - 2);
+    k_open<<<(n + 127) / 128, 128, 0, s>>>(L);
+}
+
+void gc_launch_update_edges(const GcLayerDev &L, cudaStream_t s) {
+    int n = L.ny + L.nx - 1;
+    k_update_edges<<<(n + 127) / 128, 128, 0, s>>>(L);
+}
+
+void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                     const int *corners, int t, cudaStream_t s) {
+    int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
+    int len = (ie - is + 5) > (je - js + 5) ? (ie - is + 5) : (je - js + 5);
+    size_t smem = (size_t)len * sizeof(float);
+    k_edges<<<4, EDGE_THREADS, smem, s>>>(P, C, rel_size, rel_time, is, ie, js, je, t, len);
+}
+
+void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                   const int *corners, cudaStream_t s) {
+    int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
+    dim3 grid((unsigned)((ie - is + 1 + 127) / 128), (unsigned)(je - js + 1), 1);
+    k_jnz<<<grid, 128, 0, s>>>(P, C, rel_size, rel_time, is, ie, js, je);
+}
+
+void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s) {
+    k_maxamp<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+}
+
+void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s) {
+    k_arrival<<<grid2(L), dim3(BX, BY), 0, s>>>(L, step, thr);
+}
+
+void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s) {
+    if (ng <= 0) return;
+    k_gauges<<<(ng + 127) / 128, 128, 0, s>>>(L, ng, d_ij, d_out);
+}

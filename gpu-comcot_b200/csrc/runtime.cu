@@ -1,0 +1,568 @@
+/*
+ * Layer registry and the reference's C ABI (GPUcomcot.cu, GPUMass_s.cu,
+ * GPUMoment_s.cu, GPUOpen_BD.cu, GPUall_grids.cu, GPUOutput.cu entry points).
+ *
+ * Every export keeps the reference's gfortran calling convention: lower-case
+ * name with a trailing underscore, every argument by reference, arrays as the
+ * address of a contiguous column-major NX x NY section.  Like the reference,
+ * these legacy entry points have no return code and stop the program on a
+ * CUDA error.  Unlike the reference they do not synchronise after every
+ * launch: all work is ordered on one library stream and every call that hands
+ * data back to the host synchronises, which the caller cannot tell apart.
+ *
+ * Time levels follow the Fortran copy semantics (CHANGE / UPDATE copy level 2
+ * into level 1) although the device swaps buffers: readers of Z(:,:,2) after a
+ * swap are served from the buffer that now holds level 1, which has the same
+ * contents the Fortran Z(:,:,2) would have.
+ */
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "runtime.h"
+
+void gc_gauge_invalidate();
+bool gc_gauge_lookup(int lid, int i, int j, float *out4);
+void gc_gauge_release();
+
+static GcRuntime g_rt;
+GcRuntime &gc_rt() { return g_rt; }
+
+const char *gc_status_str(int code) {
+    switch (code) {
+    case GC_OK: return "ok";
+    case GC_EINVAL: return "invalid argument";
+    case GC_ENOMEM: return "out of device memory";
+    case GC_ECUDA: return "CUDA error";
+    case GC_ESTATE: return "invalid state";
+    case GC_ETIMEOUT: return "timeout";
+    case GC_ENOTSUP: return "not supported";
+    default: return "unknown";
+    }
+}
+
+GcLayer *gc_layer(int id) {
+    if (id < 0 || id >= GC_MAX_LAYERS) {
+        fprintf(stderr, "invalid layer id %d\n", id);
+        return nullptr;
+    }
+    return &g_rt.layers[id];
+}
+
+static GcLayer &layer_or_die(int id) {
+    GcLayer *L = gc_layer(id);
+    if (!L || !L->used) {
+        fprintf(stderr, "gcomcot: layer %d is not initialised\n", id);
+        exit(EXIT_FAILURE);
+    }
+    return *L;
+}
+
+GcLayerDev GcLayer::view() const {
+    GcLayerDev d;
+    memset(&d, 0, sizeof d);
+    d.nx = nx; d.ny = ny; d.pitch = pitch;
+    d.root = (parent == -1) ? 1 : 0;
+    d.laycord = laycord; d.laygov = laygov; d.linchk = linchk; d.modscm = modscm;
+    d.fric_switch = fric_switch;
+    d.explicit_r24 = explicit_r24 ? 1 : 0;
+    d.rx = rx; d.ry = ry; d.grx = grx; d.gry = gry; d.dt = dt; d.fric_coef = fric_coef;
+    int o = cur ^ 1;
+    d.z1 = z[cur]; d.m1 = m[cur]; d.n1 = n[cur];
+    d.z1w = z[cur]; d.m1w = m[cur]; d.n1w = n[cur];
+    d.z2 = z[o]; d.m2 = m[o]; d.n2 = n[o];
+    d.h = h; d.hp = hp; d.hq = hq; d.r2 = r2; d.r4 = r4; d.rows = rows; d.dz2 = dz2;
+    d.xflux = xflux; d.yflux = yflux; d.zmax = zmax; d.arrival = arrival;
+    return d;
+}
+
+/* ------------------------------------------------------------------ */
+/* storage                                                             */
+/* ------------------------------------------------------------------ */
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int gc_layer_alloc(GcLayer &L) {
+    L.pitch = (L.nx + 31) & ~31;
+    size_t field = align256((size_t)L.pitch * L.ny * sizeof(float));
+    size_t rows = align256((size_t)GC_NROW * L.ny * sizeof(float));
+    size_t nfield = 6 /* z,m,n x2 */ + 1 /* h */ + 1 /* zmax */ + 1 /* arrival */;
+    bool cart = L.laycord == 1;
+    if (cart) nfield += 2;           /* hp, hq */
+    if (L.laygov == 1) nfield += 1;  /* dz2 */
+    if (L.explicit_r24) nfield += 2; /* r2, r4 */
+    size_t flux = align256((size_t)2 * L.nx * sizeof(float)) + align256((size_t)2 * L.ny * sizeof(float));
+    size_t total = nfield * field + rows + flux;
+    void *blk = nullptr;
+    cudaError_t e = cudaMalloc(&blk, total);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "gcomcot: cudaMalloc(%zu) for layer %d: %s\n", total, L.id, cudaGetErrorString(e));
+        return GC_ENOMEM;
+    }
+    GC_CUDA_OR_RET(cudaMemsetAsync(blk, 0, total, g_rt.stream));
+    char *p = (char *)blk;
+    auto take = [&](size_t b) { char *q = p; p += b; return q; };
+    for (int k = 0; k < 2; k++) {
+        L.z[k] = (float *)take(field);
+        L.m[k] = (float *)take(field);
+        L.n[k] = (float *)take(field);
+    }
+    L.h = (float *)take(field);
+    L.zmax = (float *)take(field);
+    L.arrival = (int *)take(field);
+    L.hp = cart ? (float *)take(field) : nullptr;
+    L.hq = cart ? (float *)take(field) : nullptr;
+    L.dz2 = (L.laygov == 1) ? (float *)take(field) : nullptr;
+    L.r2 = L.explicit_r24 ? (float *)take(field) : nullptr;
+    L.r4 = L.explicit_r24 ? (float *)take(field) : nullptr;
+    L.rows = (float *)take(rows);
+    L.xflux = (float *)take(align256((size_t)2 * L.nx * sizeof(float)));
+    L.yflux = (float *)take(align256((size_t)2 * L.ny * sizeof(float)));
+    L.block = blk;
+    L.block_bytes = total;
+    /* arrival starts at -1 (no arrival yet) */
+    GC_CUDA_OR_RET(cudaMemsetAsync(L.arrival, 0xff, (size_t)L.pitch * L.ny * sizeof(int), g_rt.stream));
+    L.cur = 0;
+    L.z2_valid = false;
+    L.mn2_valid = false;
+    return GC_OK;
+}
+
+int gc_layer_upload_field(GcLayer &L, float *dst, const float *src) {
+    GC_CUDA_OR_RET(cudaMemcpy2DAsync(dst, (size_t)L.pitch * sizeof(float), src,
+                                     (size_t)L.nx * sizeof(float), (size_t)L.nx * sizeof(float),
+                                     (size_t)L.ny, cudaMemcpyHostToDevice, g_rt.stream));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(g_rt.stream));
+    return GC_OK;
+}
+
+int gc_layer_download_field(GcLayer &L, const float *src, float *dst) {
+    GC_CUDA_OR_RET(cudaMemcpy2DAsync(dst, (size_t)L.nx * sizeof(float), src,
+                                     (size_t)L.pitch * sizeof(float), (size_t)L.nx * sizeof(float),
+                                     (size_t)L.ny, cudaMemcpyDeviceToHost, g_rt.stream));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(g_rt.stream));
+    return GC_OK;
+}
+
+/* R2 = C(J) * AMAX1(HP(I,J),0) (comcot.f90:733-736) with HP from PQ_DEPTH
+ * (initialization.f90:2512-2523).  Returns the per-row factors when the
+ * caller's field has exactly that form in every cell, so the kernels can
+ * rebuild R2 from H instead of streaming a second field. */
+static bool factor_rows(int nx, int ny, const float *H, const float *R, bool xdir, float *fac) {
+    std::vector<float> hp((size_t)nx);
+    for (int j = 0; j < ny; j++) {
+        float best = 0.0f;
+        int bi = -1;
+        for (int i = 0; i < nx; i++) {
+            size_t c = (size_t)j * nx + i;
+            float v = 0.0f;
+            if (H[c] > CC_GX) {
+                size_t c2;
+                if (xdir) c2 = (size_t)j * nx + std::min(i + 1, nx - 1);
+                else c2 = (size_t)std::min(j + 1, ny - 1) * nx + i;
+                v = 0.5f * (H[c] + H[c2]);
+            }
+            hp[i] = v > 0.0f ? v : 0.0f;
+            if (hp[i] > best) { best = hp[i]; bi = i; }
+        }
+        float cands[3];
+        int nc;
+        if (bi < 0) {
+            cands[0] = 0.0f; nc = 1;
+        } else {
+            float c0 = (float)((double)R[(size_t)j * nx + bi] / (double)best);
+            cands[0] = c0; cands[1] = nextafterf(c0, 3.0e38f); cands[2] = nextafterf(c0, -3.0e38f);
+            nc = 3;
+        }
+        bool ok = false;
+        for (int k = 0; k < nc && !ok; k++) {
+            ok = true;
+            for (int i = 0; i < nx && ok; i++) {
+                float want = R[(size_t)j * nx + i];
+                float got = cands[k] * hp[i];
+                if (memcmp(&want, &got, sizeof(float)) != 0 && !(want == 0.0f && got == 0.0f)) ok = false;
+            }
+            if (ok) fac[j] = cands[k];
+        }
+        if (!ok) return false;
+    }
+    return true;
+}
+
+static void init_runtime() {
+    if (g_rt.inited) return;
+    GC_CUDA_OR_DIE(cudaStreamCreateWithFlags(&g_rt.stream, cudaStreamNonBlocking));
+    g_rt.inited = true;
+    g_rt.root = -1;
+    const char *f = getenv("GCOMCOT_FUSE");
+    g_rt.fuse_enabled = (f && f[0] == '0') ? 0 : 1;
+}
+
+void gc_swap(GcLayer &L) {
+    L.cur ^= 1;
+    L.z2_valid = false;
+    L.mn2_valid = false;
+}
+
+/* ------------------------------------------------------------------ */
+/* reference ABI                                                       */
+/* ------------------------------------------------------------------ */
+extern "C" {
+
+/* GPUcomcot.cu:192-211 */
+void gcomcot_init_gpu_(void) {
+    int dev = 0;
+    GC_CUDA_OR_DIE(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    GC_CUDA_OR_DIE(cudaGetDeviceProperties(&prop, dev));
+    printf("GPU INFORMATIONS:                      %s\n", prop.name);
+    printf("-->Compute Capabilities [Major.Minor]: %d.%d\n", prop.major, prop.minor);
+    printf("-->Streaming Multi-Processor Count:    %d\n", prop.multiProcessorCount);
+    init_runtime();
+}
+
+/* extension: layer physics the reference ABI cannot express (coordinate
+ * system, governing equation, Cartesian ratios, friction, HP/HQ).  Call it
+ * before gcomcot_init_layer_ for every layer that is not linear spherical. */
+void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, float *rx, float *ry,
+                               float *grx, float *gry, int *fric_switch, float *fric_coef,
+                               int *linchk, int *modscm, int *nx, int *ny, float *HP, float *HQ) {
+    init_runtime();
+    if (*id < 0 || *id >= GC_MAX_LAYERS) {
+        fprintf(stderr, "ERROR: invalid layerid\n");
+        exit(EXIT_FAILURE);
+    }
+    if (*fric_switch != 0 && *fric_switch != 1) {
+        fprintf(stderr, "gcomcot: FRIC_SWITCH=%d is not supported (0 or 1)\n", *fric_switch);
+        exit(EXIT_FAILURE);
+    }
+    GcPendingParams &p = g_rt.pending[*id];
+    p.set = true;
+    p.laycord = *laycord; p.laygov = *laygov; p.dt = *dt; p.rx = *rx; p.ry = *ry;
+    p.grx = *grx; p.gry = *gry; p.fric_switch = *fric_switch; p.fric_coef = *fric_coef;
+    p.linchk = *linchk; p.modscm = *modscm;
+    size_t cells = (size_t)(*nx) * (*ny);
+    p.hp.assign(HP ? HP : (const float *)nullptr, HP ? HP + cells : (const float *)nullptr);
+    p.hq.assign(HQ ? HQ : (const float *)nullptr, HQ ? HQ + cells : (const float *)nullptr);
+}
+
+/* GPUcomcot.cu:214-251 */
+void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, int *rel_time,
+                         int *corners, float *grx, float *gry, float *R1_f, float *R2_f,
+                         float *R3_f, float *R4_f, float *R5_f, float *R6_f, float *R11_f,
+                         float *H_f, float *Z_f, int *row, int *col) {
+    init_runtime();
+    if (*layerid < 0) {
+        printf("ERROR: invalid layerid\n");
+        exit(-1);
+    }
+    if (*layerid >= GC_MAX_LAYERS) {
+        printf("ERROR: number of layer exceed MAX_LAYERS\n");
+        exit(-1);
+    }
+    GcLayer &L = g_rt.layers[*layerid];
+    if (L.used && L.block) cudaFree(L.block);
+    L = GcLayer();
+    L.used = true;
+    L.id = *layerid; L.parent = *parent; L.level = *level;
+    L.rel_size = *rel_size; L.rel_time = *rel_time;
+    memcpy(L.corners, corners, sizeof L.corners);
+    L.grx = *grx; L.gry = *gry;
+    L.nx = *row; L.ny = *col;
+    const GcPendingParams &pp = g_rt.pending[*layerid];
+    if (pp.set) {
+        L.laycord = pp.laycord; L.laygov = pp.laygov; L.linchk = pp.linchk; L.modscm = pp.modscm;
+        L.fric_switch = pp.fric_switch; L.dt = pp.dt; L.rx = pp.rx; L.ry = pp.ry;
+        L.fric_coef = pp.fric_coef;
+        if (pp.grx != 0.0f || pp.gry != 0.0f) { L.grx = pp.grx; L.gry = pp.gry; }
+    }
+    if (L.nx < 3 || L.ny < 3) {
+        fprintf(stderr, "gcomcot: layer %d is %dx%d, need at least 3x3\n", L.id, L.nx, L.ny);
+        exit(EXIT_FAILURE);
+    }
+    if (L.parent != -1) {
+        GcLayer *P = gc_layer(L.parent);
+        if (!P || !P->used) {
+            printf("Error, Root grid is not initialized\n");
+            exit(EXIT_FAILURE);
+        }
+        int is = L.corners[0], ie = L.corners[1], js = L.corners[2], je = L.corners[3];
+        /* the NEWQ forecast reads parent rows JS-3 and columns IS-3
+         * (all_grids.f90:692-700,765-772), so the window must start at 4 */
+        if (is < 4 || js < 4 || ie > P->nx - 2 || je > P->ny - 2 || ie < is || je < js
+            || L.nx != (ie - is + 1) * L.rel_size + 1 || L.ny != (je - js + 1) * L.rel_size + 1
+            || L.rel_size < 1 || L.rel_time < 1) {
+            fprintf(stderr,
+                    "gcomcot: layer %d corners (%d,%d,%d,%d) ratio %d do not match %dx%d inside "
+                    "parent %dx%d\n",
+                    L.id, is, ie, js, je, L.rel_size, L.nx, L.ny, P->nx, P->ny);
+            exit(EXIT_FAILURE);
+        }
+        P->children.push_back(L.id);
+    } else {
+        g_rt.root = L.id;
+    }
+    const size_t cells = (size_t)L.nx * L.ny;
+    /* spherical layers: try the factored R2/R4 form, else keep the fields */
+    std::vector<float> rowblk((size_t)GC_NROW * L.ny, 0.0f);
+    if (L.laycord == 0) {
+        bool f2 = factor_rows(L.nx, L.ny, H_f, R2_f, true, &rowblk[(size_t)GC_CX * L.ny]);
+        bool f4 = factor_rows(L.nx, L.ny, H_f, R4_f, false, &rowblk[(size_t)GC_CY * L.ny]);
+        L.explicit_r24 = !(f2 && f4);
+        for (int j = 0; j < L.ny; j++) {
+            rowblk[(size_t)GC_R1 * L.ny + j] = R1_f[(size_t)j * L.nx];
+            rowblk[(size_t)GC_R11 * L.ny + j] = R11_f[(size_t)j * L.nx];
+            rowblk[(size_t)GC_R6 * L.ny + j] = R6_f[j];
+            rowblk[(size_t)GC_R3 * L.ny + j] = R3_f[(size_t)j * L.nx];
+            rowblk[(size_t)GC_R5 * L.ny + j] = R5_f[(size_t)j * L.nx];
+        }
+    }
+    if (gc_layer_alloc(L) != GC_OK) exit(EXIT_FAILURE);
+    GC_CUDA_OR_DIE(cudaMemcpyAsync(L.rows, rowblk.data(), rowblk.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, g_rt.stream));
+    if (gc_layer_upload_field(L, L.h, H_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_upload_field(L, L.z[0], Z_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_upload_field(L, L.zmax, Z_f) != GC_OK) exit(EXIT_FAILURE);
+    if (L.explicit_r24) {
+        if (gc_layer_upload_field(L, L.r2, R2_f) != GC_OK) exit(EXIT_FAILURE);
+        if (gc_layer_upload_field(L, L.r4, R4_f) != GC_OK) exit(EXIT_FAILURE);
+    }
+    if (L.laycord == 1) {
+        /* HP/HQ from the caller, else PQ_DEPTH (initialization.f90:2501-2526) */
+        std::vector<float> hp(cells, 0.0f), hq(cells, 0.0f);
+        if (pp.set && pp.hp.size() == cells && pp.hq.size() == cells) {
+            hp = pp.hp; hq = pp.hq;
+        } else {
+            for (int j = 0; j < L.ny; j++)
+                for (int i = 0; i < L.nx; i++) {
+                    size_t c = (size_t)j * L.nx + i;
+                    if (H_f[c] > CC_GX) {
+                        hp[c] = 0.5f * (H_f[c] + H_f[(size_t)j * L.nx + std::min(i + 1, L.nx - 1)]);
+                        hq[c] = 0.5f * (H_f[c] + H_f[(size_t)std::min(j + 1, L.ny - 1) * L.nx + i]);
+                    }
+                }
+        }
+        if (gc_layer_upload_field(L, L.hp, hp.data()) != GC_OK) exit(EXIT_FAILURE);
+        if (gc_layer_upload_field(L, L.hq, hq.data()) != GC_OK) exit(EXIT_FAILURE);
+    }
+    GC_CUDA_OR_DIE(cudaStreamSynchronize(g_rt.stream));
+    printf("Initializing layer id %d\n", L.id);
+}
+
+/* GPUMass_s.cu:9-37: host arrays are only used by the reference's debug compare */
+void mass_launch_(const float *Z_f, float *Z_f_complete, const float *H_f, const int *lid) {
+    gc_gauge_invalidate();
+    (void)Z_f; (void)Z_f_complete; (void)H_f;
+    GcLayer &L = layer_or_die(*lid);
+    if (L.parent == -1 && g_rt.fuse_enabled) {
+        gc_flush();
+        g_rt.pend_mass = 1;
+        L.z2_valid = true;
+        return;
+    }
+    gc_flush();
+    gc_launch_mass(L.view(), g_rt.stream);
+    g_rt.launches++;
+    L.z2_valid = true;
+}
+
+/* GPUOpen_BD.cu:13-37: outermost layer only */
+void openbd_launch_(float *Z_f_complete) {
+    gc_gauge_invalidate();
+    (void)Z_f_complete;
+    GcLayer &L = layer_or_die(g_rt.root);
+    if (g_rt.pend_mass && !g_rt.pend_open && g_rt.fuse_enabled) {
+        g_rt.pend_open = 1;
+        return;
+    }
+    gc_flush();
+    gc_launch_open(L.view(), g_rt.stream);
+    g_rt.launches++;
+}
+
+/* GPUMoment_s.cu:10-56 */
+void momt_launch_(float *M_f, float *N_f, float *Z_f, const int *lid) {
+    gc_gauge_invalidate();
+    (void)M_f; (void)N_f; (void)Z_f;
+    GcLayer &L = layer_or_die(*lid);
+    if (L.parent == -1 && g_rt.pend_mass && g_rt.pend_open && !g_rt.pend_momt) {
+        g_rt.pend_momt = 1;
+        L.mn2_valid = true;
+        return;
+    }
+    gc_flush();
+    gc_launch_moment(L.view(), g_rt.stream);
+    g_rt.launches++;
+    L.mn2_valid = true;
+}
+
+/* GPUOutput.cu:11-27 */
+void maxamp_launch_(const int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid);
+    if (L.parent == -1 && g_rt.pend_momt && !g_rt.pend_maxamp) {
+        g_rt.pend_maxamp = 1;
+        return;
+    }
+    gc_flush();
+    GcLayerDev d = L.view();
+    if (!L.z2_valid) d.z2 = L.z[L.cur];
+    gc_launch_maxamp(d, g_rt.stream);
+    g_rt.launches++;
+}
+
+/* GPUall_grids.cu:701-705: the nested sub-cycle of every child of layer 1 */
+void all_grid_launch_(void) {
+    gc_gauge_invalidate();
+    gc_flush();
+    if (g_rt.root >= 0) gc_subcycle(g_rt.root);
+}
+
+/* GPUcomcot.cu:144-155 (CHANGE for the outer layer) */
+void cuda_update_layer_(int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid);
+    gc_flush();
+    if (L.parent != -1) {
+        gc_launch_update_edges(L.view(), g_rt.stream);
+        g_rt.launches++;
+    } else {
+        gc_root_change_hook(L);
+    }
+    gc_swap(L);
+}
+
+/* GPUOutput.cu:29-44: the 2x2 surface stencil at 1-based (i,j) */
+void gcomcot_get_z_(int *lid, float *l1, float *l2, float *l3, float *l4, int *i, int *j) {
+    GcLayer &L = layer_or_die(*lid);
+    if (*i < 1 || *j < 1 || *i >= L.nx || *j >= L.ny) {
+        fprintf(stderr, "gcomcot: gauge (%d,%d) outside layer %d\n", *i, *j, *lid);
+        exit(EXIT_FAILURE);
+    }
+    float tmp[4];
+    if (!gc_gauge_lookup(*lid, *i, *j, tmp)) {
+        fprintf(stderr, "gcomcot: gauge read failed\n");
+        exit(EXIT_FAILURE);
+    }
+    *l1 = tmp[0]; *l2 = tmp[1]; *l3 = tmp[2]; *l4 = tmp[3];
+}
+
+/* GPUOutput.cu:55-102: whole-field transfers */
+void cuda_getz1_(float *Z_f, int *lid) {
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_download_field(L, L.z[L.cur], Z_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_setz1_(float *Z_f, int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_upload_field(L, L.z[L.cur], Z_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_getz_(float *Z_f, int *lid) {
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    const float *z = L.z2_valid ? L.z[L.cur ^ 1] : L.z[L.cur];
+    if (gc_layer_download_field(L, z, Z_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_setz_(float *Z_f, int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (!L.z2_valid) {
+        /* Z(:,:,2) equals Z(:,:,1) at this point: materialise it before the write */
+        GC_CUDA_OR_DIE(cudaMemcpyAsync(L.z[L.cur ^ 1], L.z[L.cur], (size_t)L.pitch * L.ny * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, g_rt.stream));
+    }
+    if (gc_layer_upload_field(L, L.z[L.cur ^ 1], Z_f) != GC_OK) exit(EXIT_FAILURE);
+    L.z2_valid = true;
+}
+void cuda_getmn1_(float *M_f, float *N_f, int *lid) {
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_download_field(L, L.m[L.cur], M_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_download_field(L, L.n[L.cur], N_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_setmn1_(float *M_f, float *N_f, int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_upload_field(L, L.m[L.cur], M_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_upload_field(L, L.n[L.cur], N_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_getmn_(float *M_f, float *N_f, int *lid) {
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    int b = L.mn2_valid ? (L.cur ^ 1) : L.cur;
+    if (gc_layer_download_field(L, L.m[b], M_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_download_field(L, L.n[b], N_f) != GC_OK) exit(EXIT_FAILURE);
+}
+void cuda_setmn_(float *M_f, float *N_f, int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_upload_field(L, L.m[L.cur ^ 1], M_f) != GC_OK) exit(EXIT_FAILURE);
+    if (gc_layer_upload_field(L, L.n[L.cur ^ 1], N_f) != GC_OK) exit(EXIT_FAILURE);
+    L.mn2_valid = true;
+}
+void cuda_getzmax_(float *Zmax_f, int *lid) {
+    GcLayer &L = layer_or_die(*lid); gc_flush();
+    if (gc_layer_download_field(L, L.zmax, Zmax_f) != GC_OK) exit(EXIT_FAILURE);
+}
+
+/* GPUall_grids.cu:26-30 */
+static void show_rec(int id) {
+    GcLayer &L = g_rt.layers[id];
+    printf("lid = %d\n", L.id);
+    printf("parent = %d\n", L.parent);
+    printf("level = %d\n", L.level);
+    printf("size = %d x %d\n", L.nx, L.ny);
+    for (int c : L.children) show_rec(c);
+}
+void gcomcot_show_grids_(void) {
+    if (g_rt.root >= 0) show_rec(g_rt.root);
+}
+
+/* GPUcomcot.cu:253-256 (empty in the reference): releases everything */
+void cuda_shutdown_(void) {
+    if (!g_rt.inited) return;
+    cudaStreamSynchronize(g_rt.stream);
+    for (int k = 0; k < GC_MAX_LAYERS; k++) {
+        if (g_rt.layers[k].block) cudaFree(g_rt.layers[k].block);
+        g_rt.layers[k] = GcLayer();
+        g_rt.pending[k] = GcPendingParams();
+    }
+    gc_gauge_release();
+    if (g_rt.d_gauge_ij) cudaFree(g_rt.d_gauge_ij);
+    if (g_rt.d_gauge_out) cudaFree(g_rt.d_gauge_out);
+    if (g_rt.h_gauge_out) cudaFreeHost(g_rt.h_gauge_out);
+    g_rt.d_gauge_ij = nullptr; g_rt.d_gauge_out = nullptr; g_rt.h_gauge_out = nullptr;
+    g_rt.gauge_cap = 0;
+    cudaStreamDestroy(g_rt.stream);
+    g_rt.stream = nullptr;
+    g_rt.inited = false;
+    g_rt.root = -1;
+    g_rt.pend_mass = g_rt.pend_open = g_rt.pend_momt = g_rt.pend_maxamp = 0;
+}
+
+} /* extern "C" */
+
+/* ------------------------------------------------------------------ */
+/* nested sub-cycle (GPUall_grids.cu:655-699; Fortran ALL_GRID order,  */
+/* all_grids.f90:34-306), dispatching each child by its equations      */
+/* ------------------------------------------------------------------ */
+void gc_subcycle(int parent_id) {
+    GcLayer &P = g_rt.layers[parent_id];
+    for (int cid : P.children) {
+        GcLayer &C = g_rt.layers[cid];
+        int nhalf = C.rel_time / 2 + 1;
+        for (int k = 1; k <= C.rel_time; k++) {
+            gc_launch_edges(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, k, g_rt.stream);
+            gc_launch_mass(C.view(), g_rt.stream);
+            C.z2_valid = true;
+            gc_subcycle(cid);
+            gc_launch_moment(C.view(), g_rt.stream);
+            C.mn2_valid = true;
+            if (k == nhalf) {
+                gc_launch_jnz(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, g_rt.stream);
+                g_rt.launches++;
+            }
+            gc_launch_update_edges(C.view(), g_rt.stream);
+            gc_swap(C);
+            g_rt.launches += 4;
+        }
+    }
+}

@@ -1,0 +1,131 @@
+/*
+ * libgcomcot: B200 (sm_100a) implementation of COMCOT's time-stepping hot
+ * path behind the reference GPU-comcot C ABI.
+ *
+ * Part 1 are the reference's exports, unchanged in name, argument list and
+ * meaning (gfortran implicit interface: lower-case name + '_', every argument
+ * by reference, arrays as contiguous column-major NX x NY sections).  Like the
+ * reference they return nothing and stop the program on a CUDA error.
+ * Part 2 are additions a Fortran caller can bind the same way.
+ * Part 3 is a plain C API with status returns (0 = ok, < 0 = error).
+ */
+#ifndef GCOMCOT_H
+#define GCOMCOT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- Part 1: the reference ABI ---------------- */
+
+/* replaces GPUcomcot.cu:192 gcomcot_init_gpu_ */
+void gcomcot_init_gpu_(void);
+/* replaces GPUcomcot.cu:214 gcomcot_init_layer_ (R1,R11,R3,R5 read at I=1;
+ * R6 is [NY]; R2/R4 are kept as per-row factors when they have the PARA form) */
+void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, int *rel_time,
+                         int *corners, float *grx, float *gry, float *R1, float *R2, float *R3,
+                         float *R4, float *R5, float *R6, float *R11, float *H, float *Z, int *nx,
+                         int *ny);
+/* replaces GPUMass_s.cu:9 mass_launch_ (host arrays unused, as in the reference) */
+void mass_launch_(const float *Z1, float *Z2, const float *H, const int *lid);
+/* replaces GPUMoment_s.cu:10 momt_launch_ */
+void momt_launch_(float *M2, float *N2, float *Z2, const int *lid);
+/* replaces GPUOpen_BD.cu:13 openbd_launch_ (outermost layer) */
+void openbd_launch_(float *Z2);
+/* replaces GPUall_grids.cu:701 all_grid_launch_ (nested sub-cycle) */
+void all_grid_launch_(void);
+/* replaces GPUOutput.cu:11 maxamp_launch_ */
+void maxamp_launch_(const int *lid);
+/* replaces GPUcomcot.cu:144 cuda_update_layer_ (time-level rotation) */
+void cuda_update_layer_(int *lid);
+/* replaces GPUOutput.cu:29 gcomcot_get_z_ (2x2 surface stencil at 1-based i,j) */
+void gcomcot_get_z_(int *lid, float *l1, float *l2, float *l3, float *l4, int *i, int *j);
+/* replace GPUOutput.cu:55-102 whole-field transfers */
+void cuda_getz_(float *Z, int *lid);
+void cuda_setz_(float *Z, int *lid);
+void cuda_getz1_(float *Z, int *lid);
+void cuda_setz1_(float *Z, int *lid);
+void cuda_getmn_(float *M, float *N, int *lid);
+void cuda_setmn_(float *M, float *N, int *lid);
+void cuda_getmn1_(float *M, float *N, int *lid);
+void cuda_setmn1_(float *M, float *N, int *lid);
+void cuda_getzmax_(float *Zmax, int *lid);
+/* replaces GPUall_grids.cu:26 gcomcot_show_grids_ */
+void gcomcot_show_grids_(void);
+/* replaces GPUcomcot.cu:253 cuda_shutdown_ (the reference's is empty; this frees) */
+void cuda_shutdown_(void);
+/* replace the DEBUG_CORE comparators GPUall_grids.cu:299 and :626: run the
+ * device step and print cells that differ from the caller's arrays by more
+ * than the reference tolerance (1e-4) */
+void edgeinterp_dbglaunch_(float *mO, float *nO, int *idO, float *mA, float *nA, int *idA, int *t,
+                           float *yflux, float *xflux);
+void jnz_dbglaunch_(float *Z_f, int *outid, int *inid);
+
+/* ---------------- Part 2: Fortran-callable additions ---------------- */
+
+/* no counterpart in the reference, whose device path treats every layer as
+ * linear spherical: coordinate system / equations / Cartesian ratios /
+ * friction / HP,HQ of a layer.  Call before gcomcot_init_layer_. */
+void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, float *rx, float *ry,
+                               float *grx, float *gry, int *fric_switch, float *fric_coef,
+                               int *linchk, int *modscm, int *nx, int *ny, float *HP, float *HQ);
+/* no counterpart in the reference: arrival-step tracking on the outer layer */
+void gcomcot_set_arrival_(int *id, float *thr);
+void gcomcot_get_arrival_(int *arrival, int *id);
+
+/* ---------------- Part 3: C API ---------------- */
+
+/* kernels launched by the library since initialisation */
+long long gcomcot_launch_count(void);
+/* 1 (default): fuse mass/open/momentum/max of layer 1 into one kernel */
+void gcomcot_set_fusion(int on);
+/* waits for queued work; returns 0 or a negative status */
+int gcomcot_sync(void);
+/* the cudaStream_t the library issues work on */
+void *gcomcot_stream(void);
+
+/* Runs `nsteps` outer steps through the Part-1 entry points in the order of
+ * comcot.f90:359-439 (MASS, OPEN, ALL_GRID, MOMENT, MAX_AMP, GET_TS per
+ * gauge, CHANGE).  Gauge g reads layer g_layer[g] at 1-based (g_i, g_j);
+ * stencil values go to out4[(k*ngauges + g)*4 + 0..3].  Returns 0 or < 0. */
+int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const int *g_i,
+                  const int *g_j, float *out4);
+
+/* ---- batched ensemble / serving engine (engine.cu) ---- */
+typedef struct gc_engine gc_engine;
+
+/* A grid class: bathymetry and per-row coefficients shared by all members.
+ * rows is [7][ny]: R1(1,J), R11(1,J), R6(J), R3(1,J), R5(1,J), CX(J), CY(J)
+ * with R2 = CX(J)*max(HP,0), R4 = CY(J)*max(HQ,0) (comcot.f90:713-752). */
+int gc_engine_create(long long hbm_budget_bytes, gc_engine **out);
+int gc_engine_destroy(gc_engine *e);
+int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const float *rows);
+/* a member (scenario / request) on class `cls`: initial surface z0 [nx*ny],
+ * nsteps to run, gauges (1-based KI,KJ and weights CX,CY), arrival threshold
+ * (< 0 disables).  Returns the member id (>= 0) or a negative status; fails
+ * with -2 when the budget has no room. */
+int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int ngauges,
+                         const int *gij, const float *gw, float arrival_thr);
+/* advances every active member by up to `nsteps` steps (members stop at
+ * their own step count); returns the number of steps issued or < 0 */
+int gc_engine_step(gc_engine *e, int nsteps);
+/* 1 once the member has run all its steps (after gc_engine_sync) */
+int gc_engine_member_done(gc_engine *e, int member);
+int gc_engine_sync(gc_engine *e);
+/* results of a member: any pointer may be NULL */
+int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
+                   int *arrival, float *ts);
+int gc_engine_release(gc_engine *e, int member);
+long long gc_engine_bytes_in_use(gc_engine *e);
+long long gc_engine_member_bytes(gc_engine *e, int cls);
+/* tile variant (autotuned when < 0) and use of CUDA graphs for step chunks */
+int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk);
+int gc_engine_autotune(gc_engine *e, int reps);
+int gc_engine_variant(gc_engine *e);
+long long gc_engine_launches(gc_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

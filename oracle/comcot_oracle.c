@@ -1,0 +1,1037 @@
+/*
+ * CPU oracle for the COMCOT time-stepping hot path -- TEST INFRASTRUCTURE.
+ * Only tests/, __graft_entry__.smoke() and bench.py (cpu_baseline and the
+ * --impl reference arm) load this library.  It restates, formula by formula,
+ * the reference's Fortran solvers (file:line cited per routine).  Arithmetic is
+ * REAL (float by default, double in the FP64 twin), evaluated left to right as
+ * gfortran does, with no contraction (-ffp-contract=off).  Loop nests run with
+ * J outermost for memory locality; no routine reads a value it writes in the
+ * same sweep, so the nesting order does not change any result.
+ *
+ * Where the reference's live GPU path and its Fortran differ, this file follows
+ * the Fortran, except for the maximum-amplitude recorder, whose only live code
+ * is the GPU kernel (the Fortran recorder is commented out, output.f90:876-885).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "comcot_oracle.h"
+#include "comcot_consts.h"
+#include "comcot_math.h"
+
+#define R(x) ((REAL)(x))
+#define IDX(L, i, j) ((size_t)((j) - 1) * (size_t)(L)->nx + (size_t)((i) - 1))
+#define MAX(a, b) ((a) > (b) ? (a) : (b))
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+
+/* elementary functions: shared deterministic versions in float, libm in the twin */
+static inline REAL o_exp(REAL x) {
+    if (sizeof(REAL) == sizeof(float)) return (REAL)cc_expf((float)x);
+    return (REAL)exp((double)x);
+}
+static inline REAL o_pow(REAL x, REAL y) {
+    if (sizeof(REAL) == sizeof(float)) return (REAL)cc_powf((float)x, (float)y);
+    return (REAL)pow((double)x, (double)y);
+}
+static inline REAL o_sqrt(REAL x) {
+    if (sizeof(REAL) == sizeof(float)) return (REAL)sqrtf((float)x);
+    return (REAL)sqrt((double)x);
+}
+static inline REAL o_abs(REAL x) { return x < R(0) ? -x : x; }
+
+/* ------------------------------------------------------------------ */
+/* a small pthread parallel-for over J; every cell is independent.     */
+/* ------------------------------------------------------------------ */
+static int g_threads = 1;
+void ocl_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int ocl_get_threads(void) { return g_threads; }
+
+typedef void (*rowfn)(void *ctx, int j0, int j1);
+typedef struct { rowfn fn; void *ctx; int j0, j1; } par_job;
+static void *par_tramp(void *a) {
+    par_job *p = (par_job *)a;
+    p->fn(p->ctx, p->j0, p->j1);
+    return NULL;
+}
+/* runs fn over [lo, hi] inclusive */
+static void par_rows(rowfn fn, void *ctx, int lo, int hi) {
+    int n = hi - lo + 1;
+    if (n <= 0) return;
+    int t = g_threads;
+    if (t > n) t = n;
+    if (t <= 1 || n < 64) { fn(ctx, lo, hi); return; }
+    pthread_t th[256];
+    par_job jobs[256];
+    if (t > 256) t = 256;
+    int chunk = (n + t - 1) / t;
+    int used = 0;
+    for (int k = 0; k < t; k++) {
+        int a = lo + k * chunk, b = MIN(hi, a + chunk - 1);
+        if (a > b) break;
+        jobs[k].fn = fn; jobs[k].ctx = ctx; jobs[k].j0 = a; jobs[k].j1 = b;
+        if (pthread_create(&th[k], NULL, par_tramp, &jobs[k]) != 0) {
+            fn(ctx, a, b);
+            jobs[k].fn = NULL;
+        }
+        used++;
+    }
+    for (int k = 0; k < used; k++)
+        if (jobs[k].fn) pthread_join(th[k], NULL);
+}
+
+/* ------------------------------------------------------------------ */
+/* MASS_S  (mass.f90:61-100) linear continuity, spherical              */
+/* ------------------------------------------------------------------ */
+static void mass_s_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int is = 2, ie = (L->id == 1) ? L->nx - 1 : L->nx;
+    for (int j = js; j <= je; j++) {
+        int jm1 = j - 1;
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(L, i, j);
+            REAL h = L->h[c];
+            if (h > R(CC_GX)) {
+                REAL zz = L->z1[c] - L->r1[j - 1] * (L->m1[c] - L->m1[IDX(L, i - 1, j)])
+                          - L->r11[j - 1] * (L->n1[c] * L->r6[j - 1]
+                                             - L->n1[IDX(L, i, jm1)] * L->r6[jm1 - 1]);
+                if (o_abs(zz) < R(CC_EPS)) zz = R(0);
+                if ((zz + h) <= R(CC_EPS)) zz = -h;
+                L->z2[c] = zz;
+            } else {
+                L->z2[c] = R(0);
+            }
+        }
+    }
+}
+
+/* MASS_C (mass.f90:103-157) linear continuity, Cartesian */
+static void mass_c_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    REAL rx = R(L->rx), ry = R(L->ry);
+    int is = 2, ie = (L->id == 1) ? L->nx - 1 : L->nx;
+    for (int j = js; j <= je; j++) {
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(L, i, j);
+            REAL h = L->h[c];
+            if (h > R(CC_GX)) {
+                REAL zz = L->z1[c] - rx * (L->m1[c] - L->m1[IDX(L, i - 1, j)])
+                          - ry * (L->n1[c] - L->n1[IDX(L, i, j - 1)]);
+                if (o_abs(zz) < R(CC_EPS)) zz = R(0);
+                if ((zz + h) <= R(CC_EPS)) zz = -h;
+                L->z2[c] = zz;
+            } else {
+                L->z2[c] = R(0);
+            }
+        }
+    }
+}
+
+/* CONMASS (mass.f90:162-224) nonlinear continuity with moving shoreline */
+static void conmass_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    REAL rx = R(L->rx), ry = R(L->ry);
+    int is = 2, ie = (L->id == 1) ? L->nx - 1 : L->nx;
+    for (int j = js; j <= je; j++) {
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(L, i, j);
+            REAL h = L->h[c];
+            if (h > R(CC_ELMAX)) {
+                REAL zzz = L->z1[c] - rx * (L->m1[c] - L->m1[IDX(L, i - 1, j)])
+                           - ry * (L->n1[c] - L->n1[IDX(L, i, j - 1)]);
+                if (o_abs(zzz) < R(CC_EPS)) zzz = R(0);
+                REAL dd = zzz + h;
+                if (dd >= R(CC_GX)) {
+                    L->dz2[c] = dd;
+                    L->z2[c] = zzz;
+                } else {
+                    L->dz2[c] = R(0);
+                    L->z2[c] = -h;
+                }
+            } else {
+                L->dz2[c] = R(0);
+                L->z2[c] = -h;
+            }
+        }
+    }
+}
+
+void ocl_mass(ocl_layer *L) {
+    /* dispatcher: mass.f90:18-52.  Edge rows: I=2.., J=2.. (mass.f90:70-78) */
+    int je = (L->id == 1) ? L->ny - 1 : L->ny;
+    if (L->laycord == 0) {
+        par_rows(mass_s_rows, L, 2, je);
+    } else if (L->laygov == 1) {
+        par_rows(conmass_rows, L, 2, je);
+    } else {
+        par_rows(mass_c_rows, L, 2, je);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* MOMT_S (moment.f90:65-149) linear momentum with Coriolis, spherical */
+/* ------------------------------------------------------------------ */
+static void momt_s_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int nx = L->nx, ny = L->ny;
+    int is0 = (L->id == 1) ? 1 : 2, js0 = is0;
+    for (int j = js; j <= je; j++) {
+        /* x-momentum: I = IS..NX-1, J = JS..NY */
+        if (j >= js0) {
+            int jm1 = MAX(j - 1, 1);
+            for (int i = is0; i <= nx - 1; i++) {
+                size_t c = IDX(L, i, j), cp = IDX(L, i + 1, j);
+                if (L->h[c] > R(CC_GX) && L->h[cp] > R(CC_GX)) {
+                    REAL tot_n = L->n1[c] + L->n1[cp] + L->n1[IDX(L, i, jm1)]
+                                 + L->n1[IDX(L, i + 1, jm1)];
+                    REAL xm = L->m1[c] - L->r2[c] * (L->z2[cp] - L->z2[c])
+                              + L->r3[j - 1] * tot_n;
+                    if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                    L->m2[c] = xm;
+                } else {
+                    L->m2[c] = R(0);
+                }
+            }
+        }
+        /* y-momentum: J = JS..NY-1, I = IS..NX */
+        if (j >= js0 && j <= ny - 1) {
+            int jp1 = j + 1;
+            for (int i = is0; i <= nx; i++) {
+                size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+                if (L->h[c] > R(CC_GX) && L->h[cq] > R(CC_GX)) {
+                    int im1 = MAX(i - 1, 1);
+                    REAL tot_m = L->m1[IDX(L, im1, j)] + L->m1[IDX(L, im1, jp1)]
+                                 + L->m1[c] + L->m1[cq];
+                    REAL xn = L->n1[c] - L->r4[c] * (L->z2[cq] - L->z2[c])
+                              - L->r5[j - 1] * tot_m;
+                    if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                    L->n2[c] = xn;
+                } else {
+                    L->n2[c] = R(0);
+                }
+            }
+        }
+    }
+}
+
+/* MOMT_C (moment.f90:152-277) linear momentum, Cartesian, optional friction
+ * and modified scheme */
+static void momt_c_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int nx = L->nx, ny = L->ny;
+    int is0 = (L->id == 1) ? 1 : 2, js0 = is0;
+    REAL konst = R(0.5) * R(L->dt) * R(CC_GRAV);
+    REAL fm = R(L->fric_coef);
+    REAL grx = R(L->grx), gry = R(L->gry);
+    for (int j = js; j <= je; j++) {
+        if (j >= js0) { /* M: I = IS..NX-1, J = JS..NY */
+            int jm1 = MAX(j - 1, 1), jp1 = MIN(j + 1, ny);
+            for (int i = is0; i <= nx - 1; i++) {
+                int ip1 = i + 1;
+                size_t c = IDX(L, i, j), cp = IDX(L, ip1, j);
+                REAL xm;
+                if (L->h[c] > R(CC_GX) && L->h[cp] > R(CC_GX)) {
+                    REAL ff = R(0);
+                    REAL hm = L->hp[c] + R(0.5) * (L->z2[c] + L->z2[cp]);
+                    xm = L->m1[c] - grx * hm * (L->z2[cp] - L->z2[c]);
+                    if (L->fric_switch != 1) {
+                        REAL xqq = R(0.25) * (L->n1[c] + L->n1[cp] + L->n1[IDX(L, i, jm1)]
+                                              + L->n1[IDX(L, ip1, jm1)]);
+                        if (hm >= R(1.0e-3f))
+                            ff = konst * fm * fm * o_sqrt(L->m1[c] * L->m1[c] + xqq * xqq)
+                                 / o_pow(hm, R(CC_MANNEXP));
+                        else
+                            ff = R(0);
+                        xm = xm - ff * L->m1[c];
+                    }
+                    if (L->modscm == 0) {
+                        REAL scm = grx * R(CC_TWLVTH) * hm
+                                   * ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cp] + L->z2[IDX(L, ip1, jm1)])
+                                      - (L->z2[IDX(L, i, jp1)] - R(2) * L->z2[c] + L->z2[IDX(L, i, jm1)]));
+                        xm = xm - scm;
+                    }
+                    if (L->fric_switch != 1) xm = xm / (R(1) + ff);
+                    if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                } else {
+                    xm = R(0);
+                }
+                L->m2[c] = xm;
+            }
+        }
+        if (j >= js0 && j <= ny - 1) { /* N: J = JS..NY-1, I = IS..NX */
+            int jp1 = j + 1;
+            for (int i = is0; i <= nx; i++) {
+                size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+                if (L->h[c] > R(CC_GX) && L->h[cq] > R(CC_GX)) {
+                    int im1 = MAX(i - 1, 1), ip1 = MIN(i + 1, nx);
+                    REAL ff = R(0);
+                    REAL hn = L->hq[c] + R(0.5) * (L->z2[c] + L->z2[cq]);
+                    REAL xn = L->n1[c] - gry * hn * (L->z2[cq] - L->z2[c]);
+                    if (L->fric_switch != 1) {
+                        REAL xpp = R(0.25) * (L->m1[c] + L->m1[cq] + L->m1[IDX(L, im1, j)]
+                                              + L->m1[IDX(L, im1, jp1)]);
+                        if (hn >= R(1.0e-5f))
+                            ff = konst * fm * fm * o_sqrt(L->n1[c] * L->n1[c] + xpp * xpp)
+                                 / o_pow(hn, R(CC_MANNEXP));
+                        else
+                            ff = R(0);
+                        xn = xn - ff * L->n1[c];
+                    }
+                    if (L->modscm == 0) {
+                        REAL scm = gry * R(CC_TWLVTH) * hn
+                                   * ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cq] + L->z2[IDX(L, im1, jp1)])
+                                      - (L->z2[IDX(L, ip1, j)] - R(2) * L->z2[c] + L->z2[IDX(L, im1, j)]));
+                        xn = xn - scm;
+                    }
+                    if (L->fric_switch != 1) xn = xn / (R(1) + ff);
+                    if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                    L->n2[c] = xn;
+                } else {
+                    L->n2[c] = R(0);
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* CONMOME (moment.f90:280-780) + WAVE_BREAKING (moment.f90:1272-1384) */
+/* ------------------------------------------------------------------ */
+typedef struct { ocl_layer *L; REAL *dp1, *dp2, *dq1, *dq2; } conmome_ctx;
+
+/* face depths DP, DQ (moment.f90:345-366); DZ(:,:,1) is never written by the
+ * reference (only mass.f90:204-216 assign DZ(:,:,2)), so it is zero here. */
+static void conmome_pre_rows(void *vctx, int js, int je) {
+    conmome_ctx *x = (conmome_ctx *)vctx;
+    ocl_layer *L = x->L;
+    int ix = L->nx, jy = L->ny;
+    for (int j = js; j <= je; j++) {
+        int jp1 = MIN(j + 1, jy);
+        for (int i = 1; i <= ix; i++) {
+            int ip1 = MIN(i + 1, ix);
+            size_t c = IDX(L, i, j);
+            REAL d = L->dz2[c], dpx = L->dz2[IDX(L, ip1, j)], dqy = L->dz2[IDX(L, i, jp1)];
+            REAL dp1 = R(0.25) * (d + R(0) + dpx + R(0));
+            REAL dp2 = R(0.50) * (d + dpx);
+            REAL dq1 = R(0.25) * (d + R(0) + dqy + R(0));
+            REAL dq2 = R(0.50) * (d + dqy);
+            if (dp1 < R(CC_GX)) dp1 = R(0);
+            if (dp2 < R(CC_GX)) dp2 = R(0);
+            if (dq1 < R(CC_GX)) dq1 = R(0);
+            if (dq2 < R(CC_GX)) dq2 = R(0);
+            x->dp1[c] = dp1; x->dp2[c] = dp2; x->dq1[c] = dq1; x->dq2[c] = dq2;
+        }
+    }
+}
+
+/* WAVE_BREAKING: damps the convection terms where the surface rises faster
+ * than 0.08 sqrt(g d) (moment.f90:1300-1325) */
+static inline void wave_breaking(ocl_layer *L, size_t c, REAL *advx, REAL *advy) {
+    REAL cc = o_sqrt(R(CC_GRAV) * L->dz2[c]);
+    REAL dzdt_f = R(CC_BRK_F) * cc;
+    REAL dzdt_i = R(CC_BRK_I) * cc;
+    REAL dzdt = o_abs(L->z2[c] - L->z1[c]) / R(L->dt);
+    if (dzdt > dzdt_f) {
+        REAL ref = (dzdt - dzdt_f) / (dzdt_i - dzdt_f);
+        REAL coef = o_exp(-(R(1) * ref));
+        *advx = coef * *advx;
+        *advy = coef * *advy;
+    }
+}
+
+static void conmome_x_rows(void *vctx, int js, int je) {
+    conmome_ctx *x = (conmome_ctx *)vctx;
+    ocl_layer *L = x->L;
+    int ix = L->nx, jy = L->ny;
+    int is = 2, ie = ix - 1;
+    if (L->id == 1) is = 1;
+    REAL rx = R(L->rx), ry = R(L->ry), grx = R(L->grx);
+    REAL konst = (L->fric_switch != 1) ? R(0.5) * R(L->dt) * R(CC_GRAV) : R(0);
+    REAL fm = R(L->fric_coef);
+    int ispans = CC_SPAN, ispane = ix - CC_SPAN, jspans = CC_SPAN, jspane = jy - CC_SPAN;
+    const REAL *dp1 = x->dp1, *dp2 = x->dp2, *dz = L->dz2, *z = L->z2, *hz = L->h;
+    const REAL *p = L->m1, *q = L->n1;
+    for (int j = js; j <= je; j++) {
+        int jp1 = MIN(j + 1, jy), jm1 = MAX(j - 1, 1);
+        for (int i = is; i <= ie; i++) {
+            int ip1 = MIN(i + 1, ix), im1 = MAX(i - 1, 1);
+            size_t c = IDX(L, i, j), cp = IDX(L, ip1, j);
+            REAL dd = R(0), df = R(0), ff = R(0);
+            int noflux = 0;
+            if (hz[c] <= R(CC_ELMAX) || L->hp[c] <= R(CC_ELMAX)) {
+                noflux = 1;
+            } else {
+                if (dz[c] > R(CC_GX) && dz[cp] > R(CC_GX)) {
+                    dd = dp2[c]; df = dp1[c];
+                } else if (dz[c] > R(CC_GX) && dz[cp] <= R(CC_GX) && hz[cp] + z[c] > R(CC_GX)) {
+                    dd = R(0.5) * dz[c]; df = dd;
+                } else if (dz[c] <= R(CC_GX) && dz[cp] > R(CC_GX) && hz[c] + z[cp] > R(CC_GX)) {
+                    dd = R(0.5) * dz[cp]; df = dd;
+                } else {
+                    noflux = 1;
+                }
+                if (!noflux && dd < R(CC_GX)) noflux = 1;
+            }
+            if (noflux) { L->m2[c] = R(0); continue; }
+            if (df < R(CC_DFMIN)) df = R(CC_DFMIN);
+            REAL xqq = R(0.25) * (q[c] + q[cp] + q[IDX(L, i, jm1)] + q[IDX(L, ip1, jm1)]);
+            if (L->fric_switch != 1)
+                ff = konst * fm * fm * o_sqrt(p[c] * p[c] + xqq * xqq) / o_pow(df, R(CC_MANNEXP));
+            else
+                ff = R(0);
+            REAL xp = p[c] - grx * dd * (z[cp] - z[c]);
+            if (L->modscm == 0 && j < jy) {
+                REAL scm = grx * dd / R(12)
+                           * ((z[IDX(L, ip1, jp1)] - R(2) * z[cp] + z[IDX(L, ip1, jm1)])
+                              - (z[IDX(L, i, jp1)] - R(2) * z[c] + z[IDX(L, i, jm1)]));
+                xp = xp - scm;
+            }
+            if (L->fric_switch != 1) xp = xp - ff * p[c];
+            if (L->linchk == 1 && dp1[c] >= R(CC_GX) && i > ispans && i < ispane && j > jspans
+                && j < jspane) {
+                REAL advx = R(0), advy = R(0);
+                if (p[c] < R(0)) {
+                    if (dp1[cp] < R(CC_GX) || dz[cp] < R(CC_GX))
+                        advx = rx * (-(p[c] * p[c] / dp1[c]));
+                    else
+                        advx = rx * (p[cp] * p[cp] / dp1[cp] - p[c] * p[c] / dp1[c]);
+                } else {
+                    size_t cm = IDX(L, im1, j);
+                    if (dp1[cm] < R(CC_GX) || dz[c] < R(CC_GX))
+                        advx = rx * (p[c] * p[c] / dp1[c]);
+                    else
+                        advx = rx * (p[c] * p[c] / dp1[c] - p[cm] * p[cm] / dp1[cm]);
+                }
+                if (xqq < R(0)) {
+                    size_t cj = IDX(L, i, jp1);
+                    if (dz[cj] < R(CC_GX) || dz[IDX(L, ip1, jp1)] < R(CC_GX)) {
+                        advy = ry * (-(p[c] * xqq / dp1[c]));
+                    } else if (dp1[cj] < R(CC_GX)) {
+                        advy = ry * (-(p[c] * xqq / dp1[c]));
+                    } else {
+                        REAL xqe = R(0.25) * (q[cj] + q[IDX(L, ip1, jp1)] + q[c] + q[cp]);
+                        advy = ry * (p[cj] * xqe / dp1[cj] - p[c] * xqq / dp1[c]);
+                    }
+                } else {
+                    size_t cj = IDX(L, i, jm1);
+                    if (dz[cj] < R(CC_GX) || dz[IDX(L, ip1, jm1)] < R(CC_GX)) {
+                        advy = ry * (p[c] * xqq / dp1[c]);
+                    } else if (dp1[cj] < R(CC_GX)) {
+                        advy = ry * (p[c] * xqq / dp1[c]);
+                    } else {
+                        REAL xqe = R(0.25) * (q[cj] + q[IDX(L, ip1, jm1)] + q[IDX(L, i, j - 2)]
+                                              + q[IDX(L, ip1, j - 2)]);
+                        advy = ry * (p[c] * xqq / dp1[c] - p[cj] * xqe / dp1[cj]);
+                    }
+                }
+                wave_breaking(L, c, &advx, &advy);
+                xp = xp - advx - advy;
+            }
+            if (L->fric_switch != 1) xp = xp / (R(1) + ff);
+            if (o_abs(xp) < R(CC_EPS)) xp = R(0);
+            REAL lim = R(CC_VLIMIT) * dd;
+            if (xp > lim) xp = lim;
+            if (xp < -lim) xp = -lim;
+            L->m2[c] = xp;
+        }
+    }
+}
+
+static void conmome_y_rows(void *vctx, int js, int je) {
+    conmome_ctx *x = (conmome_ctx *)vctx;
+    ocl_layer *L = x->L;
+    int ix = L->nx, jy = L->ny;
+    int is = 2, ie = ix;
+    if (L->id == 1) { is = 1; ie = ix - 1; }
+    REAL rx = R(L->rx), ry = R(L->ry), gry = R(L->gry);
+    REAL konst = (L->fric_switch != 1) ? R(0.5) * R(L->dt) * R(CC_GRAV) : R(0);
+    REAL fm = R(L->fric_coef);
+    int ispans = CC_SPAN, ispane = ix - CC_SPAN, jspans = CC_SPAN, jspane = jy - CC_SPAN;
+    const REAL *dq1 = x->dq1, *dq2 = x->dq2, *dz = L->dz2, *z = L->z2, *hz = L->h;
+    const REAL *p = L->m1, *q = L->n1;
+    for (int j = js; j <= je; j++) {
+        int jp1 = MIN(j + 1, jy), jm1 = MAX(j - 1, 1);
+        for (int i = is; i <= ie; i++) {
+            int ip1 = MIN(i + 1, ix), im1 = MAX(i - 1, 1);
+            size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+            REAL dd = R(0), df = R(0), ff = R(0);
+            int noflux = 0;
+            if (hz[c] <= R(CC_ELMAX) || L->hq[c] <= R(CC_ELMAX)) {
+                noflux = 1;
+            } else {
+                if (dz[c] > R(CC_GX) && dz[cq] > R(CC_GX)) {
+                    dd = dq2[c]; df = dq1[c];
+                } else if (dz[c] > R(CC_GX) && dz[cq] <= R(CC_GX) && hz[cq] + z[c] > R(CC_GX)) {
+                    dd = R(0.5) * dz[c]; df = dd;
+                } else if (dz[c] <= R(CC_GX) && dz[cq] > R(CC_GX) && hz[c] + z[cq] > R(CC_GX)) {
+                    dd = R(0.5) * dz[cq]; df = dd;
+                } else {
+                    noflux = 1;
+                }
+                if (!noflux && dd < R(CC_GX)) noflux = 1;
+            }
+            if (noflux) { L->n2[c] = R(0); continue; }
+            if (df < R(CC_DFMIN)) df = R(CC_DFMIN);
+            REAL xpp = R(0.25) * (p[c] + p[cq] + p[IDX(L, im1, j)] + p[IDX(L, im1, jp1)]);
+            if (L->fric_switch != 1)
+                ff = konst * fm * fm * o_sqrt(q[c] * q[c] + xpp * xpp) / o_pow(df, R(CC_MANNEXP));
+            else
+                ff = R(0);
+            REAL xq = q[c] - gry * dd * (z[cq] - z[c]);
+            if (L->modscm == 0 && i < ix) {
+                REAL scm = gry * dd / R(12)
+                           * ((z[IDX(L, ip1, jp1)] - R(2) * z[cq] + z[IDX(L, im1, jp1)])
+                              - (z[IDX(L, ip1, j)] - R(2) * z[c] + z[IDX(L, im1, j)]));
+                xq = xq - scm;
+            }
+            /* moment.f90:672 subtracts the y friction from XP, not XQ; XP is
+             * not used afterwards, so XQ only sees the 1/(1+FF) division. */
+            if (L->linchk == 1 && dq1[c] >= R(CC_GX) && i > ispans && i < ispane && j > jspans
+                && j < jspane) {
+                REAL advx = R(0), advy = R(0);
+                if (q[c] < R(0)) {
+                    if (dq1[cq] < R(CC_GX) || dz[cq] < R(CC_GX))
+                        advy = ry * (-(q[c] * q[c] / dq1[c]));
+                    else
+                        advy = ry * (q[cq] * q[cq] / dq1[cq] - q[c] * q[c] / dq1[c]);
+                } else {
+                    size_t cm = IDX(L, i, jm1);
+                    if (dq1[cm] < R(CC_GX) || dz[c] < R(CC_GX))
+                        advy = ry * (q[c] * q[c] / dq1[c]);
+                    else
+                        advy = ry * (q[c] * q[c] / dq1[c] - q[cm] * q[cm] / dq1[cm]);
+                }
+                if (xpp < R(0)) {
+                    size_t ci = IDX(L, ip1, j);
+                    if (dz[ci] < R(CC_GX) || dz[IDX(L, ip1, jp1)] < R(CC_GX)) {
+                        advx = rx * (-(q[c] * xpp / dq1[c]));
+                    } else if (dq1[ci] < R(CC_GX)) {
+                        advx = rx * (-(q[c] * xpp / dq1[c]));
+                    } else {
+                        REAL xpe = R(0.25) * (p[ci] + p[IDX(L, ip1, jp1)] + p[c] + p[cq]);
+                        advx = rx * (q[ci] * xpe / dq1[ci] - q[c] * xpp / dq1[c]);
+                    }
+                } else {
+                    size_t ci = IDX(L, im1, j);
+                    if (dz[ci] < R(CC_GX) || dz[IDX(L, im1, jp1)] < R(CC_GX)) {
+                        advx = rx * (q[c] * xpp / dq1[c]);
+                    } else if (dq1[IDX(L, i - 1, j)] < R(CC_GX)) {
+                        advx = rx * (q[c] * xpp / dq1[c]);
+                    } else {
+                        REAL xpe = R(0.25) * (p[ci] + p[IDX(L, im1, jp1)] + p[IDX(L, i - 2, j)]
+                                              + p[IDX(L, i - 2, jp1)]);
+                        advx = rx * (q[c] * xpp / dq1[c] - q[ci] * xpe / dq1[ci]);
+                    }
+                }
+                wave_breaking(L, c, &advx, &advy);
+                xq = xq - advx - advy;
+            }
+            if (L->fric_switch != 1) xq = xq / (R(1) + ff);
+            if (o_abs(xq) < R(CC_EPS)) xq = R(0);
+            REAL lim = R(CC_VLIMIT) * dd;
+            if (xq > lim) xq = lim;
+            if (xq < -lim) xq = -lim;
+            L->n2[c] = xq;
+        }
+    }
+}
+
+static void conmome(ocl_layer *L) {
+    size_t n = (size_t)L->nx * L->ny;
+    conmome_ctx x;
+    x.L = L;
+    x.dp1 = (REAL *)malloc(4 * n * sizeof(REAL));
+    x.dp2 = x.dp1 + n; x.dq1 = x.dp2 + n; x.dq2 = x.dq1 + n;
+    par_rows(conmome_pre_rows, &x, 1, L->ny);
+    /* x: children I=2..NX-1, J=2..NY; root I=1..NX-1, J=1..NY-1 (moment.f90:376-389) */
+    if (L->id == 1) par_rows(conmome_x_rows, &x, 1, L->ny - 1);
+    else par_rows(conmome_x_rows, &x, 2, L->ny);
+    /* y: children I=2..NX, J=2..NY-1; root I=1..NX-1, J=1..NY-1 (moment.f90:586-599) */
+    if (L->id == 1) par_rows(conmome_y_rows, &x, 1, L->ny - 1);
+    else par_rows(conmome_y_rows, &x, 2, L->ny - 1);
+    free(x.dp1);
+}
+
+void ocl_moment(ocl_layer *L) {
+    /* dispatcher moment.f90:21-54 */
+    int js = (L->id == 1) ? 1 : 2;
+    if (L->laycord == 0) par_rows(momt_s_rows, L, js, L->ny);
+    else if (L->laygov == 1) conmome(L);
+    else par_rows(momt_c_rows, L, js, L->ny);
+}
+
+/* ------------------------------------------------------------------ */
+/* OPEN (boundaries.f90:22-202) radiation boundary on the outer layer  */
+/* ------------------------------------------------------------------ */
+void ocl_open(ocl_layer *L) {
+    int nx = L->nx, ny = L->ny;
+    const REAL *m = L->m1, *n = L->n1, *h = L->h;  /* M(:,:,2) == M(:,:,1) at call time */
+    REAL *z = L->z2;
+    const REAL grav = R(CC_GRAV), gx = R(CC_GX), ub = R(CC_UB);
+    for (int i = 2; i <= nx - 1; i++) { /* J = 1 */
+        size_t c = IDX(L, i, 1);
+        if (h[c] > gx) {
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = R(0.5) * (m[c] + m[IDX(L, i - 1, 1)]);
+            REAL uu = o_sqrt(uh * uh + n[c] * n[c]);
+            REAL zz = uu / cc;
+            if (n[c] > R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    for (int i = 2; i <= nx - 1; i++) { /* J = NY */
+        size_t c = IDX(L, i, ny), cs = IDX(L, i, ny - 1);
+        if (h[c] > gx) {
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = R(0.5) * (m[c] + m[IDX(L, i - 1, ny)]);
+            REAL uu = o_sqrt(uh * uh + n[cs] * n[cs]);
+            REAL zz = uu / cc;
+            if (n[cs] < R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    for (int j = 2; j <= ny - 1; j++) { /* I = 1 */
+        size_t c = IDX(L, 1, j), cs = IDX(L, 1, j - 1);
+        if (h[c] > gx) {
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh;
+            if (h[cs] > gx) uh = R(0.5) * (n[c] + n[cs]);
+            else uh = n[c];
+            REAL uu = o_sqrt(uh * uh + m[c] * m[c]);
+            REAL zz = uu / cc;
+            if (m[c] > R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    for (int j = 2; j <= ny - 1; j++) { /* I = NX */
+        size_t c = IDX(L, nx, j), cw = IDX(L, nx - 1, j);
+        if (h[c] > gx) {
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = R(0.5) * (n[c] + n[IDX(L, nx, j - 1)]);
+            REAL uu = o_sqrt(uh * uh + m[cw] * m[cw]);
+            REAL zz = uu / cc;
+            if (m[cw] < R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    { /* corner (1,1) */
+        size_t c = IDX(L, 1, 1);
+        if (h[c] > gx) {
+            REAL qx = m[c], qy = n[c];
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = o_sqrt(qx * qx + qy * qy);
+            REAL zz = uh / cc;
+            if (qx > R(0) || qy > R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    { /* corner (NX,1) */
+        size_t c = IDX(L, nx, 1);
+        if (h[c] > gx) {
+            REAL qx = m[IDX(L, nx - 1, 1)], qy = n[c];
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = o_sqrt(qx * qx + qy * qy);
+            REAL zz = uh / cc;
+            if (qx < R(0) || qy > R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    { /* corner (1,NY) */
+        size_t c = IDX(L, 1, ny);
+        if (h[c] > gx) {
+            REAL qx = m[c], qy = n[IDX(L, 1, ny - 1)];
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = o_sqrt(qx * qx + qy * qy);
+            REAL zz = uh / cc;
+            if (qx > R(0) || qy < R(0)) zz = -zz;
+            if (o_abs(zz) > ub) zz = R(0);
+            z[c] = zz;
+        } else z[c] = R(0);
+    }
+    { /* corner (NX,NY) */
+        size_t c = IDX(L, nx, ny);
+        if (h[c] > gx) {
+            REAL qx = m[IDX(L, nx - 1, ny)], qy = n[IDX(L, nx, ny - 1)];
+            REAL cc = o_sqrt(grav * h[c]);
+            REAL uh = o_sqrt(qx * qx + qy * qy);
+            REAL zz = uh / cc;
+            if (qx < R(0) || qy < R(0)) zz = -zz;
+            z[c] = zz;
+            if (o_abs(z[c]) > ub) z[c] = R(0);
+        } else z[c] = R(0);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* time-level rotation                                                 */
+/* ------------------------------------------------------------------ */
+void ocl_change(ocl_layer *L) {
+    /* CHANGE (comcot.f90:475-512): Z, M, N (:,:,2) -> (:,:,1) */
+    size_t n = (size_t)L->nx * L->ny;
+    memcpy(L->z1, L->z2, n * sizeof(REAL));
+    memcpy(L->m1, L->m2, n * sizeof(REAL));
+    memcpy(L->n1, L->n2, n * sizeof(REAL));
+}
+
+void ocl_update(ocl_layer *L) {
+    /* UPDATE (all_grids.f90:316-339): edge copy of Z(:,:,2), then rotation */
+    int nx = L->nx, ny = L->ny;
+    for (int j = 1; j <= ny; j++) L->z2[IDX(L, 1, j)] = L->z2[IDX(L, 2, j)];
+    for (int i = 1; i <= nx; i++) L->z2[IDX(L, i, 1)] = L->z2[IDX(L, i, 2)];
+    ocl_change(L);
+}
+
+/* ------------------------------------------------------------------ */
+/* JNQ / EDGEINTERP / NEWQ  (all_grids.f90:452-801)                    */
+/* ------------------------------------------------------------------ */
+/* EDGEINTERP_VERT (all_grids.f90:502-550): child M on column II from the
+ * parent flux profile flux[J], J = YS..YE */
+static void edgeinterp_vert(const REAL *flux, ocl_layer *C, int side) {
+    int nn = 2 * C->rel_size, ir = C->rel_size;
+    int ys = C->corners[2], ye = C->corners[3];
+    int j_shift = -ys * ir + 1;
+    int ii = (side == 0) ? 1 : C->nx;
+    for (int j = ys; j <= ye; j++) {
+        REAL flux_s = R(0.5) * (flux[j - 2] + flux[j - 1]);
+        REAL flux_e = R(0.5) * (flux[j] + flux[j - 1]);
+        REAL c1 = (REAL)((double)(flux_e - flux_s) / (double)nn);
+        REAL c2 = -c1 + flux_s;
+        int js = j * ir + j_shift;
+        for (int k = 1; k <= ir; k++) {
+            int jj = js + k;
+            size_t c = IDX(C, ii, jj);
+            C->m1[c] = R(2) * R(k) * c1 + c2;
+            if (C->h[c] + C->z1[c] <= R(CC_GX)) C->m1[c] = R(0);
+        }
+    }
+}
+
+/* EDGEINTERP_HORI (all_grids.f90:553-604): child N on row JJ */
+static void edgeinterp_hori(const REAL *flux, ocl_layer *C, int side) {
+    int nn = 2 * C->rel_size, ir = C->rel_size;
+    int xs = C->corners[0], xe = C->corners[1];
+    int i_shift = -xs * ir + 1;
+    int jj = (side == 0) ? 1 : C->ny;
+    for (int i = xs; i <= xe; i++) {
+        REAL flux_s = R(0.5) * (flux[i - 2] + flux[i - 1]);
+        REAL flux_e = R(0.5) * (flux[i] + flux[i - 1]);
+        REAL c1 = (REAL)((double)(flux_e - flux_s) / (double)nn);
+        REAL c2 = -c1 + flux_s;
+        int is = i * ir + i_shift;
+        for (int k = 1; k <= ir; k++) {
+            int ii = is + k;
+            size_t c = IDX(C, ii, jj);
+            C->n1[c] = R(2) * R(k) * c1 + c2;
+            if (C->h[c] + C->z1[c] <= R(CC_GX)) C->n1[c] = R(0);
+        }
+    }
+}
+
+void ocl_jnq(ocl_layer *P, ocl_layer *C) {
+    /* JNQ (all_grids.f90:452-498), SC_OPTION = 0 */
+    int is = C->corners[0], ie = C->corners[1], js = C->corners[2], je = C->corners[3];
+    REAL *col = (REAL *)malloc((size_t)(P->ny > P->nx ? P->ny : P->nx) * sizeof(REAL));
+    for (int j = 1; j <= P->ny; j++) col[j - 1] = P->m1[IDX(P, is - 1, j)];
+    edgeinterp_vert(col, C, 0);
+    for (int j = 1; j <= P->ny; j++) col[j - 1] = P->m1[IDX(P, ie, j)];
+    edgeinterp_vert(col, C, 1);
+    for (int i = 1; i <= P->nx; i++) col[i - 1] = P->n1[IDX(P, i, js - 1)];
+    edgeinterp_hori(col, C, 0);
+    for (int i = 1; i <= P->nx; i++) col[i - 1] = P->n1[IDX(P, i, je)];
+    edgeinterp_hori(col, C, 1);
+    free(col);
+}
+
+/* NEWQ_VERT (all_grids.f90:608-724) */
+static void newq_vert(ocl_layer *P, ocl_layer *C, int t, int side) {
+    int is = C->corners[0], ie = C->corners[1], js = C->corners[2], je = C->corners[3];
+    int i = (side == 0) ? is - 1 : ie;
+    REAL c1 = (R(t) - R(1)) / R(C->rel_time);
+    REAL c2 = R(1) - c1;
+    REAL *yflux = (REAL *)calloc((size_t)P->ny, sizeof(REAL));
+    int ip1 = i + 1;
+    REAL grx = R(P->grx);
+    for (int j = js - 2; j <= je + 2; j++) {
+        size_t c = IDX(P, i, j), cp = IDX(P, ip1, j);
+        if ((P->h[c] + P->z2[c] > R(CC_GX)) && (P->h[cp] + P->z2[cp] > R(CC_GX))) {
+            if (t == 2) {
+                REAL xm;
+                if (P->laycord == 0) {
+                    int jm1 = j - 1;
+                    REAL tot_n = P->n1[c] + P->n1[cp] + P->n1[IDX(P, i, jm1)] + P->n1[IDX(P, ip1, jm1)];
+                    xm = P->m1[c] - P->r2[c] * (P->z2[cp] - P->z2[c]) + P->r3[j - 1] * tot_n;
+                } else {
+                    REAL hm = P->hp[c] + R(0.5) * (P->z2[c] + P->z2[cp]);
+                    xm = P->m1[c] - grx * hm * (P->z2[cp] - P->z2[c]);
+                }
+                if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                P->yflux[(size_t)side * P->ny + (j - 1)] = xm;
+            }
+            yflux[j - 1] = c1 * P->yflux[(size_t)side * P->ny + (j - 1)] + c2 * P->m1[c];
+        }
+    }
+    edgeinterp_vert(yflux, C, side);
+    free(yflux);
+}
+
+/* NEWQ_HORI (all_grids.f90:728-801) */
+static void newq_hori(ocl_layer *P, ocl_layer *C, int t, int side) {
+    int is = C->corners[0], ie = C->corners[1], js = C->corners[2], je = C->corners[3];
+    int j = (side == 0) ? js - 1 : je;
+    REAL c1 = (R(t) - R(1)) / R(C->rel_time);
+    REAL c2 = R(1) - c1;
+    REAL *xflux = (REAL *)calloc((size_t)P->nx, sizeof(REAL));
+    int jp1 = j + 1;
+    REAL gry = R(P->gry);
+    for (int i = is - 2; i <= ie + 2; i++) {
+        size_t c = IDX(P, i, j), cq = IDX(P, i, jp1);
+        if ((P->h[c] + P->z2[c] > R(CC_GX)) && (P->h[cq] + P->z2[cq] > R(CC_GX))) {
+            if (t == 2) {
+                int im1 = i - 1;
+                REAL xn;
+                if (P->laycord == 0) {
+                    REAL tot_m = P->m1[IDX(P, im1, j)] + P->m1[IDX(P, im1, jp1)] + P->m1[c] + P->m1[cq];
+                    xn = P->n1[c] - P->r4[c] * (P->z2[cq] - P->z2[c]) - P->r5[j - 1] * tot_m;
+                } else {
+                    REAL hn = P->hq[c] + R(0.5) * (P->z2[c] + P->z2[cq]);
+                    xn = P->n1[c] - gry * hn * (P->z2[cq] - P->z2[c]);
+                }
+                if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                P->xflux[(size_t)side * P->nx + (i - 1)] = xn;
+            }
+            xflux[i - 1] = c1 * P->xflux[(size_t)side * P->nx + (i - 1)] + c2 * P->n1[c];
+        }
+    }
+    edgeinterp_hori(xflux, C, side);
+    free(xflux);
+}
+
+void ocl_newq(ocl_layer *P, ocl_layer *C, int t) {
+    /* NEWQ (all_grids.f90:608-660), SC_OPTION = 0 */
+    newq_vert(P, C, t, 0);
+    newq_vert(P, C, t, 1);
+    newq_hori(P, C, t, 0);
+    newq_hori(P, C, t, 1);
+}
+
+/* JNZ (all_grids.f90:342-421), SC_OPTION = 0: child -> parent surface */
+typedef struct { ocl_layer *P, *C; } jnz_ctx;
+static void jnz_rows(void *vctx, int js, int je) {
+    jnz_ctx *x = (jnz_ctx *)vctx;
+    ocl_layer *P = x->P, *C = x->C;
+    int ir = C->rel_size;
+    REAL half = R((C->rel_size * C->rel_size)) / R(2);
+    int is = C->corners[0], ie = C->corners[1], jsc = C->corners[2];
+    int i_shift = -is * ir + 1, j_shift = -jsc * ir + 1;
+    int even = (C->rel_time % 2) == 0;
+    for (int j = js; j <= je; j++) {
+        for (int i = is; i <= ie; i++) {
+            REAL sum = R(0), count = R(0);
+            int i0 = i * ir + i_shift, j0 = j * ir + j_shift;
+            for (int ki = 1; ki <= ir; ki++) {
+                for (int kj = 1; kj <= ir; kj++) {
+                    size_t c = IDX(C, i0 + ki, j0 + kj);
+                    if (C->h[c] + C->z2[c] > R(CC_GX)) {
+                        if (even) sum = sum + R(0.5) * (C->z1[c] + C->z2[c]);
+                        else sum = sum + C->z2[c];
+                        count = count + R(1);
+                    }
+                }
+            }
+            if (count > half) P->z2[IDX(P, i, j)] = sum / count;
+            else P->z2[IDX(P, i, j)] = R(0);
+        }
+    }
+}
+
+void ocl_jnz(ocl_layer *P, ocl_layer *C) {
+    jnz_ctx x = {P, C};
+    par_rows(jnz_rows, &x, C->corners[2], C->corners[3]);
+}
+
+/* ------------------------------------------------------------------ */
+/* outputs: running maximum, arrival step, gauges                      */
+/* ------------------------------------------------------------------ */
+void ocl_maxamp(ocl_layer *L) {
+    /* maximum_recorder_kernel (GPUOutput.cu:46-53): Zmax = max(Zmax, Z2),
+     * Zmax starts from the initial Z (GPUcomcot.cu:79) */
+    size_t n = (size_t)L->nx * L->ny;
+    for (size_t c = 0; c < n; c++)
+        if (!(L->zmax[c] >= L->z2[c])) L->zmax[c] = L->z2[c];
+}
+
+void ocl_arrival(ocl_layer *L, int step, double thr) {
+    /* arrival step: the first outer step after which a wet cell (H > GX)
+     * has Z2 > thr; -1 until then.  The reference has no arrival-time
+     * product; this definition is shared with the CUDA kernels. */
+    size_t n = (size_t)L->nx * L->ny;
+    REAL t = R(thr);
+    for (size_t c = 0; c < n; c++)
+        if (L->arrival[c] < 0 && L->h[c] > R(CC_GX) && L->z2[c] > t) L->arrival[c] = step;
+}
+
+double ocl_gauge(ocl_layer *L, int ki, int kj, double cx, double cy) {
+    /* GET_TS bilinear weights (output.f90:1078-1090) on Z(:,:,2) */
+    REAL l1 = L->z2[IDX(L, ki, kj)], l2 = L->z2[IDX(L, ki + 1, kj)];
+    REAL l3 = L->z2[IDX(L, ki, kj + 1)], l4 = L->z2[IDX(L, ki + 1, kj + 1)];
+    REAL x = R(cx), y = R(cy);
+    REAL z1 = l1 * (R(1) - x) * (R(1) - y);
+    REAL z2 = l2 * (x) * (R(1) - y);
+    REAL z3 = l3 * (R(1) - x) * (y);
+    REAL z4 = l4 * (x) * (y);
+    return (double)(z1 + z2 + z3 + z4);
+}
+
+/* ------------------------------------------------------------------ */
+/* ALL_GRID (all_grids.f90:4-312): recursive sub-cycling of the tree   */
+/* ------------------------------------------------------------------ */
+static void all_grid_rec(ocl_layer *layers, int n, int parent_idx) {
+    ocl_layer *P = &layers[parent_idx];
+    for (int c = 0; c < n; c++) {
+        ocl_layer *C = &layers[c];
+        if (c == parent_idx || C->parent != P->id) continue;
+        int nhalf = C->rel_time / 2 + 1;
+        for (int k = 1; k <= C->rel_time; k++) {
+            if (k == 1) ocl_jnq(P, C);
+            else ocl_newq(P, C, k);
+            ocl_mass(C);
+            all_grid_rec(layers, n, c);
+            ocl_moment(C);
+            if (k == nhalf) ocl_jnz(P, C);
+            ocl_update(C);
+        }
+    }
+}
+
+void ocl_all_grid(ocl_layer *layers, int n) { all_grid_rec(layers, n, 0); }
+
+void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr) {
+    /* one outer step in the GPU driver's order (comcot.f90:359-439) */
+    ocl_layer *L = &layers[0];
+    ocl_mass(L);
+    ocl_open(L);
+    ocl_all_grid(layers, n);
+    ocl_moment(L);
+    if (L->zmax) ocl_maxamp(L);
+    if (L->arrival) ocl_arrival(L, step, arrival_thr);
+}
+
+static ocl_layer *find_layer(ocl_layer *layers, int n, int id) {
+    for (int k = 0; k < n; k++)
+        if (layers[k].id == id) return &layers[k];
+    return NULL;
+}
+
+int ocl_run(ocl_layer *layers, int n, int nsteps, double arrival_thr, int ngauges,
+            const int *g_layer, const int *g_ki, const int *g_kj, const double *g_cx,
+            const double *g_cy, REAL *ts) {
+    for (int k = 1; k <= nsteps; k++) {
+        ocl_step(layers, n, k, arrival_thr);
+        for (int g = 0; g < ngauges; g++) {
+            ocl_layer *G = find_layer(layers, n, g_layer[g]);
+            if (!G) return -1;
+            ts[(size_t)(k - 1) * ngauges + g] = (REAL)ocl_gauge(G, g_ki[g], g_kj[g], g_cx[g], g_cy[g]);
+        }
+        ocl_change(&layers[0]);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* set-up restatements                                                 */
+/* ------------------------------------------------------------------ */
+void ocl_pq_depth(int nx, int ny, const REAL *h, REAL *hp, REAL *hq) {
+    /* PQ_DEPTH (initialization.f90:2501-2526); cells with H <= GX keep 0 */
+    for (int j = 1; j <= ny; j++) {
+        int jp1 = MIN(j + 1, ny);
+        for (int i = 1; i <= nx; i++) {
+            int ip1 = MIN(i + 1, nx);
+            size_t c = (size_t)(j - 1) * nx + (i - 1);
+            if (h[c] > R(CC_GX)) {
+                hp[c] = R(0.5) * (h[c] + h[(size_t)(j - 1) * nx + (ip1 - 1)]);
+                hq[c] = R(0.5) * (h[c] + h[(size_t)(jp1 - 1) * nx + (i - 1)]);
+            } else {
+                hp[c] = R(0);
+                hq[c] = R(0);
+            }
+        }
+    }
+}
+
+void ocl_para(int nx, int ny, int laygov, double dt, double dx_min, const double *lat,
+              const double *del_y_min, const REAL *hp, const REAL *hq, REAL *r1, REAL *r11,
+              REAL *r2, REAL *r3, REAL *r4, REAL *r5, REAL *r6) {
+    /* PARA (comcot.f90:694-752), LAYGOV 0/1, in REAL arithmetic */
+    REAL rr = R(dt) / R(CC_R_EARTH);
+    REAL rs = R(CC_GRAV) * rr;
+    REAL rt = R(0.5) * R(dt) * R(CC_CORI_W);
+    REAL osixty = R(0.016666666667);
+    REAL rad_deg = R(CC_RAD_DEG), rad_min = R(CC_RAD_MIN);
+    for (int j = 1; j <= ny; j++) {
+        REAL y = R(lat[j - 1]), dely = R(del_y_min[j - 1]);
+        REAL ang_m = y * rad_deg;
+        REAL ang_n = (y + R(0.5) * dely * osixty) * rad_deg;
+        REAL cos_m, cos_n, sin_m, sin_n;
+        if (sizeof(REAL) == sizeof(float)) {
+            cos_m = (REAL)cosf((float)ang_m); cos_n = (REAL)cosf((float)ang_n);
+            sin_m = (REAL)sinf((float)ang_m); sin_n = (REAL)sinf((float)ang_n);
+        } else {
+            cos_m = (REAL)cos((double)ang_m); cos_n = (REAL)cos((double)ang_n);
+            sin_m = (REAL)sin((double)ang_m); sin_n = (REAL)sin((double)ang_n);
+        }
+        r1[j - 1] = rr / cos_m / (R(dx_min) * rad_min);
+        r11[j - 1] = rr / cos_m / (dely * rad_min);
+        r3[j - 1] = rt * sin_m;
+        r5[j - 1] = rt * sin_n;
+        r6[j - 1] = cos_n;
+        for (int i = 1; i <= nx; i++) {
+            size_t c = (size_t)(j - 1) * nx + (i - 1);
+            if (laygov == 0) {
+                r2[c] = rs / cos_m / (R(dx_min) * rad_min) * MAX(hp[c], R(0));
+                r4[c] = rs / (dely * rad_min) * MAX(hq[c], R(0));
+            } else {
+                r2[c] = rs / cos_m / (R(dx_min) * rad_min);
+                r4[c] = rs / (dely * rad_min);
+            }
+        }
+    }
+}
+
+int ocl_rel_time(double dt_parent, double dx_m, double dy_m, double hmax, int nonlinear,
+                 double *dt_child) {
+    /* CR_CHECK sub-level rule (initialization.f90:1210-1237) */
+    REAL h_max = MAX(R(hmax), R(CC_GX));
+    REAL cr_limit = nonlinear ? R(0.35) : R(0.5);
+    REAL del_x = MIN(R(dx_m), R(dy_m));
+    REAL dt = cr_limit * del_x / o_sqrt(R(CC_GRAV) * h_max);
+    REAL dtp = R(dt_parent);
+    if (dt >= dtp) {
+        *dt_child = (double)dtp;
+        return 1;
+    }
+    int ir = (int)floor((double)(dtp / dt)) + 1;
+    *dt_child = (double)(dtp / R(ir));
+    return ir;
+}
+
+void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp, double xs, double xe,
+                 double ys, double ye, int *corners) {
+    /* SUBGRID_MATCHING corner search (initialization.f90:913-936) */
+    for (int k = 2; k <= nx_p - 1; k++) {
+        REAL lo = (R(xp[k - 2]) + R(xp[k - 1])) / R(2), hi = (R(xp[k - 1]) + R(xp[k])) / R(2);
+        if (R(xs) >= lo && R(xs) < hi) corners[0] = k + 1;
+        if (R(xe) >= lo && R(xe) < hi) corners[1] = k - 1;
+    }
+    for (int k = 2; k <= ny_p - 1; k++) {
+        REAL lo = (R(yp[k - 2]) + R(yp[k - 1])) / R(2), hi = (R(yp[k - 1]) + R(yp[k])) / R(2);
+        if (R(ys) >= lo && R(ys) < hi) corners[2] = k + 1;
+        if (R(ye) >= lo && R(ye) < hi) corners[3] = k - 1;
+    }
+}

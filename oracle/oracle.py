@@ -1,0 +1,154 @@
+"""ctypes driver of the CPU oracle -- TEST INFRASTRUCTURE.
+
+Loads oracle/_build/liboracle_f32.so (REAL = float, the reference's REAL
+arithmetic) or liboracle_f64.so (the FP64 twin) and runs a synthetic case
+through the restated Fortran solvers.  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU baseline legs use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+
+_libs = {}
+
+
+def build(quiet=True):
+    subprocess.run(["make", "-C", str(HERE)], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+def load(dtype=np.float32):
+    key = np.dtype(dtype).name
+    if key in _libs:
+        return _libs[key]
+    name = "liboracle_f32.so" if key == "float32" else "liboracle_f64.so"
+    path = BUILD / name
+    if not path.exists():
+        build()
+    lib = C.CDLL(str(path))
+    lib.ocl_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+    lib.ocl_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ocl_run.restype = C.c_int
+    lib.ocl_set_threads.argtypes = [C.c_int]
+    for fn in ("ocl_mass", "ocl_moment", "ocl_open", "ocl_change", "ocl_update", "ocl_maxamp"):
+        getattr(lib, fn).argtypes = [C.c_void_p]
+    lib.ocl_jnq.argtypes = [C.c_void_p, C.c_void_p]
+    lib.ocl_jnz.argtypes = [C.c_void_p, C.c_void_p]
+    lib.ocl_newq.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.ocl_all_grid.argtypes = [C.c_void_p, C.c_int]
+    lib.ocl_gauge.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double]
+    lib.ocl_gauge.restype = C.c_double
+    lib.ocl_pq_depth.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ocl_para.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_void_p] + [C.c_void_p] * 7
+    lib.ocl_rel_time.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                 C.POINTER(C.c_double)]
+    lib.ocl_rel_time.restype = C.c_int
+    lib.ocl_corners.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double,
+                                C.c_double, C.c_double, C.c_void_p]
+    _libs[key] = lib
+    return lib
+
+
+class OLayer(C.Structure):
+    _fields_ = ([(n, C.c_int) for n in ("id", "parent", "level", "nx", "ny", "laycord", "laygov", "linchk",
+                                        "modscm", "fric_switch", "rel_size", "rel_time")]
+                + [("corners", C.c_int * 4)]
+                + [(n, C.c_double) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
+                + [(n, C.c_void_p) for n in ("r1", "r11", "r6", "r3", "r5", "r2", "r4", "h", "hp", "hq",
+                                             "z1", "z2", "m1", "m2", "n1", "n2", "dz2", "xflux", "yflux",
+                                             "zmax", "arrival")])
+
+
+class OracleRun:
+    """Oracle state for every layer of a case."""
+
+    def __init__(self, case, dtype=np.float32, coefs64=None):
+        self.case = case
+        self.dtype = np.dtype(dtype)
+        self.lib = load(self.dtype)
+        n = len(case.layers)
+        self.arr = (OLayer * n)()
+        self.keep = []
+        self.fields = []
+        for k, L in enumerate(case.layers):
+            self.fields.append(self._fill(self.arr[k], L, k == 0, coefs64[k] if coefs64 else None))
+
+    def _a(self, x, dt=None):
+        a = np.ascontiguousarray(x, dtype=dt or self.dtype)
+        self.keep.append(a)
+        return a
+
+    def _fill(self, o, L, is_root, c64):
+        d = self.dtype
+        o.id, o.parent, o.level, o.nx, o.ny = L.id, L.parent, L.level, L.nx, L.ny
+        o.laycord, o.laygov, o.linchk, o.modscm, o.fric_switch = L.laycord, L.laygov, L.linchk, L.modscm, L.fric_switch
+        o.rel_size, o.rel_time = L.rel_size, L.rel_time
+        for q in range(4):
+            o.corners[q] = int(L.corners[q])
+        o.dt, o.rx, o.ry, o.grx, o.gry, o.fric_coef = L.dt, L.rx, L.ry, L.grx, L.gry, L.fric_coef
+        f = {}
+        ny, nx = L.ny, L.nx
+        c = c64 if c64 is not None else L.coefs
+        if c is not None:
+            for nm in ("r1", "r11", "r6", "r3", "r5", "r2", "r4"):
+                f[nm] = self._a(getattr(c, nm))
+        else:
+            for nm in ("r1", "r11", "r6", "r3", "r5"):
+                f[nm] = self._a(np.zeros(ny))
+            f["r2"] = self._a(np.zeros((ny, nx)))
+            f["r4"] = self._a(np.zeros((ny, nx)))
+        f["h"] = self._a(L.H)
+        f["hp"] = self._a(L.hp if L.hp is not None else np.zeros((ny, nx)))
+        f["hq"] = self._a(L.hq if L.hq is not None else np.zeros((ny, nx)))
+        f["z1"] = self._a(L.Z0.astype(np.float32).copy())
+        for nm in ("z2", "m1", "m2", "n1", "n2", "dz2"):
+            f[nm] = self._a(np.zeros((ny, nx)))
+        f["xflux"] = self._a(np.zeros(2 * nx))
+        f["yflux"] = self._a(np.zeros(2 * ny))
+        f["zmax"] = self._a(L.Z0.astype(np.float32).copy()) if is_root else None
+        f["arrival"] = self._a(np.full((ny, nx), -1), np.int32) if is_root else None
+        for nm, a in f.items():
+            setattr(o, nm, a.ctypes.data if a is not None else None)
+        return f
+
+    def run(self, nsteps, threads=1, arrival=True, maxamp=True):
+        """Runs nsteps outer steps; returns the gauge series [nsteps, ng]."""
+        self.lib.ocl_set_threads(int(threads))
+        root = self.arr[0]
+        saved_z, saved_a = root.zmax, root.arrival
+        if not maxamp:
+            root.zmax = None
+        if not arrival:
+            root.arrival = None
+        g = self.case.gauges
+        ng = len(g)
+        gl = np.array([x[0] for x in g] or [0], np.int32)
+        gi = np.array([x[1] for x in g] or [0], np.int32)
+        gj = np.array([x[2] for x in g] or [0], np.int32)
+        gx = np.array([x[3] for x in g] or [0], np.float64)
+        gy = np.array([x[4] for x in g] or [0], np.float64)
+        ts = np.zeros((max(nsteps, 1), max(ng, 1)), self.dtype)
+        rc = self.lib.ocl_run(C.addressof(self.arr), len(self.case.layers), int(nsteps),
+                              float(self.case.arrival_thr), ng, gl.ctypes.data, gi.ctypes.data,
+                              gj.ctypes.data, gx.ctypes.data, gy.ctypes.data, ts.ctypes.data)
+        root.zmax, root.arrival = saved_z, saved_a
+        if rc != 0:
+            raise RuntimeError("oracle run failed")
+        return ts[:nsteps, :ng]
+
+    def layer(self, k=0):
+        """Fortran (:,:,2) view of layer k after the last completed step."""
+        f = self.fields[k]
+        # after CHANGE / UPDATE the levels are equal; level 1 is the latest
+        return {"z": f["z1"], "m": f["m1"], "n": f["n1"], "zmax": f["zmax"], "arrival": f["arrival"],
+                "dz": f["dz2"]}
