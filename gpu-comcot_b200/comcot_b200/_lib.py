@@ -65,6 +65,7 @@ SIGNATURES = {
     "gc_engine_autotune": (C.c_int, [VP, C.c_int]),
     "gc_engine_variant": (C.c_int, [VP]),
     "gc_engine_launches": (C.c_longlong, [VP]),
+    "gc_engine_stream": (VP, [VP]),
 }
 
 

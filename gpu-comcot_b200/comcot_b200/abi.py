@@ -28,16 +28,24 @@ def _i(v):
 
 
 class ReferenceSession:
-    def __init__(self, case: Case, fusion: bool = True, arrival: bool = False):
+    def __init__(self, case: Case, fusion: bool = True, arrival: bool = False, init_layers: bool = True):
         self.lib = _lib.load()
         self.case = case
         self.lib.gcomcot_init_gpu_()
         self.lib.gcomcot_set_fusion(1 if fusion else 0)
         self._keep = []
-        for L in case.layers:
-            self._init_layer(L)
+        if init_layers:
+            self.init_layers()
         if arrival:
             self.lib.gcomcot_set_arrival_(_i(case.root.id), _f(case.arrival_thr))
+
+    def init_layers(self):
+        """GCOMCOT_INIT_LAYER for layer 1 then every sub-layer (comcot.f90:281-296)"""
+        for L in self.case.layers:
+            self._init_layer(L)
+
+    def stream(self) -> int:
+        return int(self.lib.gcomcot_stream() or 0)
 
     def _init_layer(self, L: LayerSpec):
         lib = self.lib

@@ -122,5 +122,6 @@ class Engine:
     def launches(self) -> int:
         return int(self.lib.gc_engine_launches(self.h))
 
-    def stream(self):
-        return None
+    def stream(self) -> int:
+        """cudaStream_t (as an int) the engine launches on"""
+        return int(self.lib.gc_engine_stream(self.h) or 0)

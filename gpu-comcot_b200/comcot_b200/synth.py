@@ -93,13 +93,22 @@ def bathymetry(x, y, rng, depth=4000.0, n_seamounts=20, shelf_cols=40, land_cols
                shelf_depth=50.0):
     nx, ny = len(x), len(y)
     h = np.full((ny, nx), depth, dtype=np.float64)
+    dlon = float(x[1] - x[0])
+    dlat = float(y[1] - y[0])
     for _ in range(n_seamounts):
         lon_c = rng.uniform(x[0], x[-1])
         lat_c = rng.uniform(y[0], y[-1])
         amp = rng.uniform(500.0, 2000.0)
         rad = rng.uniform(20.0, 80.0)
-        dxk, dyk = _dist_km(x, y, lon_c, lat_c)
-        h -= amp * np.exp(-(dxk ** 2 + dyk ** 2) / (2.0 * rad ** 2))
+        # evaluate inside +-5 radii only (the Gaussian is < 4e-6 of amp beyond)
+        wy = int(5.0 * rad / KM_PER_DEG_LAT / dlat) + 2
+        wx = int(5.0 * rad / (111.32 * max(math.cos(math.radians(lat_c)), 0.05)) / dlon) + 2
+        ic = int((lon_c - x[0]) / dlon)
+        jc = int((lat_c - y[0]) / dlat)
+        i0, i1 = max(0, ic - wx), min(nx, ic + wx + 1)
+        j0, j1 = max(0, jc - wy), min(ny, jc + wy + 1)
+        dxk, dyk = _dist_km(x[i0:i1], y[j0:j1], lon_c, lat_c)
+        h[j0:j1, i0:i1] -= amp * np.exp(-(dxk ** 2 + dyk ** 2) / (2.0 * rad ** 2))
     h = np.maximum(h, 200.0)
     if shelf_cols > 0:
         i0 = nx - land_cols - shelf_cols

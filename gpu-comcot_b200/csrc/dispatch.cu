@@ -14,6 +14,7 @@
 
 #include <vector>
 
+#include "fused.h"
 #include "runtime.h"
 
 bool gc_fused_step(GcLayer &L, bool maxamp, bool arrival, int step, float thr, int ngauges,
@@ -87,6 +88,7 @@ int gcomcot_sync(void) {
     gc_flush();
     GC_CUDA_OR_RET(cudaStreamSynchronize(gc_rt().stream));
     GC_CUDA_OR_RET(cudaGetLastError());
+    if (gc_fused_take_error()) return GC_ETIMEOUT;
     return GC_OK;
 }
 

@@ -30,7 +30,7 @@
 namespace {
 
 struct EngClass {
-    int nx, ny, pitch, tiles_x[16], ntiles[16];
+    int nx, ny, pitch;
     float *d_h = nullptr, *d_rows = nullptr;
     size_t bytes = 0;
 };
@@ -77,7 +77,11 @@ struct gc_engine {
 static int eng_rebuild(gc_engine *e) {
     std::vector<GcFusedGrid> grids;
     std::vector<int2> tiles;
-    GcTileCfg tc = gc_fused_variant(e->variant);
+    /* one tile height for the whole work list, chosen to fill whole waves */
+    std::vector<int> anx, any;
+    for (auto &M : e->members)
+        if (M.used && !M.done) { anx.push_back(e->classes[M.cls].nx); any.push_back(e->classes[M.cls].ny); }
+    const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data());
     /* active members grouped by class */
     for (size_t c = 0; c < e->classes.size(); c++) {
         EngClass &C = e->classes[c];
@@ -89,7 +93,8 @@ static int eng_rebuild(gc_engine *e) {
             GcFusedGrid g;
             memset(&g, 0, sizeof g);
             g.nx = C.nx; g.ny = C.ny; g.pitch = C.pitch; g.root = 1; g.explicit_r24 = 0;
-            g.tiles_x = (C.nx + tc.tx - 1) / tc.tx;
+            g.ty = ty;
+            gc_fused_tiles(C.nx, C.ny, ty, &g.tiles_x);
             g.step0 = M.step0; g.cur0 = 0; g.nsteps = M.nsteps;
             g.flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
             g.thr = M.thr;
@@ -99,7 +104,7 @@ static int eng_rebuild(gc_engine *e) {
             g.ng = M.ng; g.gij = M.gij; g.gw = M.gw; g.ts = M.ts; g.ts_len = M.nsteps;
             grids.push_back(g);
         }
-        int nt = ((C.nx + tc.tx - 1) / tc.tx) * ((C.ny + tc.ty - 1) / tc.ty);
+        int nt = gc_fused_tiles(C.nx, C.ny, ty, nullptr);
         for (int t = 0; t < nt; t++)
             for (int g : idx) tiles.push_back(make_int2(g, t));
     }
@@ -242,7 +247,7 @@ int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const floa
     EngClass C;
     C.nx = nx; C.ny = ny; C.pitch = (nx + 31) & ~31;
     size_t field = a256((size_t)C.pitch * ny * sizeof(float));
-    size_t rb = a256((size_t)GC_NROW * ny * sizeof(float));
+    size_t rb = a256((size_t)GC_ROWW * ny * sizeof(float));
     C.bytes = field + rb;
     if (e->in_use + (long long)C.bytes > e->budget) return GC_ENOMEM;
     void *blk = nullptr;
@@ -251,8 +256,12 @@ int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const floa
     C.d_rows = (float *)((char *)blk + field);
     GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_h, (size_t)C.pitch * sizeof(float), H, (size_t)nx * sizeof(float),
                                      (size_t)nx * sizeof(float), (size_t)ny, cudaMemcpyHostToDevice, e->stream));
-    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_rows, rows, (size_t)GC_NROW * ny * sizeof(float),
-                                   cudaMemcpyHostToDevice, e->stream));
+    /* caller's [7][ny] blocks -> the device's interleaved [ny][8] records */
+    std::vector<float> rec((size_t)GC_ROWW * ny, 0.0f);
+    for (int k = 0; k < GC_NROW; k++)
+        for (int j = 0; j < ny; j++) rec[(size_t)j * GC_ROWW + k] = rows[(size_t)k * ny + j];
+    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_rows, rec.data(), rec.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                   e->stream));
     e->in_use += (long long)C.bytes;
     e->classes.push_back(C);
     return (int)e->classes.size() - 1;
@@ -325,6 +334,7 @@ int gc_engine_sync(gc_engine *e) {
     if (!e) return GC_EINVAL;
     GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
     GC_CUDA_OR_RET(cudaGetLastError());
+    if (gc_fused_take_error()) return GC_ETIMEOUT;
     return GC_OK;
 }
 
@@ -417,6 +427,7 @@ int gc_engine_autotune(gc_engine *e, int reps) {
 }
 
 int gc_engine_variant(gc_engine *e) { return e ? e->variant : GC_EINVAL; }
+void *gc_engine_stream(gc_engine *e) { return e ? (void *)e->stream : nullptr; }
 long long gc_engine_launches(gc_engine *e) { return e ? e->launches : GC_EINVAL; }
 
 } /* extern "C" */

@@ -12,7 +12,8 @@
 
 struct GcFusedGrid {
     int nx, ny, pitch, root, explicit_r24;
-    int tiles_x;      /* tiles along I */
+    int tiles_x;      /* tiles along I (128 columns each) */
+    int ty;           /* rows per tile */
     int step0, cur0;  /* at step `step0`, buffer `cur0` holds time level 1 */
     int nsteps;       /* steps this grid runs; the step after the last only samples gauges */
     int flags;        /* GC_F_MAXAMP | GC_F_ARRIVAL */
@@ -30,21 +31,26 @@ struct GcFusedGrid {
     int ts_len;         /* steps the ts buffer can hold */
 };
 
-/* tile shape of one launch variant */
+/* one launch variant: warps per CTA and pipeline stages per warp */
 struct GcTileCfg {
-    int tx, ty;
+    int warps, stages;
 };
 
 int gc_fused_num_variants();
 GcTileCfg gc_fused_variant(int v);
+/* rows per tile for a work list of grids (nx[k], ny[k]) that fills whole
+ * waves of the variant's resident warps */
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny);
 /* launches the fused step over a work list: tiles[t] = {grid, tile within
  * that grid}; step = *step_base + step_off (step_base may be NULL) */
 cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles,
                                   int ntiles, const int *d_step_base, int step_off, int nctas,
                                   cudaStream_t s);
 int gc_fused_max_ctas(int variant);
+/* 1 if a pipeline wait in the fused kernel gave up since the last call (clears it) */
+int gc_fused_take_error();
 /* single grid, descriptor by value */
 cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s);
-int gc_fused_tiles(int variant, int nx, int ny, int *tiles_x);
+int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x);
 
 #endif

@@ -12,8 +12,8 @@ static int g_variant = -1;
 int gc_default_variant() {
     if (g_variant >= 0) return g_variant;
     const char *v = getenv("GCOMCOT_FUSED_VARIANT");
-    g_variant = v ? atoi(v) : 1;
-    if (g_variant < 0 || g_variant >= gc_fused_num_variants()) g_variant = 1;
+    g_variant = v ? atoi(v) : 0;
+    if (g_variant < 0 || g_variant >= gc_fused_num_variants()) g_variant = 0;
     return g_variant;
 }
 
@@ -35,7 +35,13 @@ bool gc_fused_step(GcLayer &L, bool maxamp, bool arrival, int step, float thr, i
     GcFusedGrid g;
     gc_fill_fused_grid(L, g);
     int v = gc_default_variant();
-    gc_fused_tiles(v, L.nx, L.ny, &g.tiles_x);
+    static int cached_nx = -1, cached_ny = -1, cached_v = -1, cached_ty = 16;
+    if (cached_nx != L.nx || cached_ny != L.ny || cached_v != v) {
+        cached_ty = gc_fused_pick_ty(v, 1, &L.nx, &L.ny);
+        cached_nx = L.nx; cached_ny = L.ny; cached_v = v;
+    }
+    g.ty = cached_ty;
+    gc_fused_tiles(L.nx, L.ny, g.ty, &g.tiles_x);
     g.step0 = step;
     g.cur0 = L.cur;
     g.nsteps = 0x3fffffff;

@@ -8,7 +8,9 @@
  *   boundary; element (i,j) is at p[j*pitch + i].
  *   Z, M, N are ping-pong pairs; `cur` names the buffer holding time level 1
  *   (the reference's Zdat/MNdat), the other holds level 2 (Zout/MNout).
- *   Per-row coefficients live in one [GC_NROW][ny] array (see GcRow).
+ *   Per-row coefficients live in one [ny][GC_ROWW] array (see GcRow): the
+ *   eight floats of a row are contiguous, 32 bytes, so one bulk copy
+ *   fetches them.
  */
 #ifndef GC_INTERNAL_H
 #define GC_INTERNAL_H
@@ -27,6 +29,7 @@
  * R3(1,J), R5(1,J) from PARA (comcot.f90:713-752), and the factored
  * R2 = CX(J)*max(HP,0), R4 = CY(J)*max(HQ,0) multipliers. */
 enum GcRow { GC_R1 = 0, GC_R11, GC_R6, GC_R3, GC_R5, GC_CX, GC_CY, GC_NROW };
+#define GC_ROWW 8 /* floats per row record (7 used, 1 pad) */
 
 /* What a kernel needs to know about one layer.  Passed by value. */
 struct GcLayerDev {
@@ -41,7 +44,7 @@ struct GcLayerDev {
     float *z1w;
     const float *h, *hp, *hq;
     const float *r2, *r4;        /* only when explicit_r24 */
-    const float *rows;           /* [GC_NROW][ny] */
+    const float *rows;           /* [ny][GC_ROWW] */
     float *dz2;                  /* nonlinear layers */
     float *xflux, *yflux;        /* [2*nx], [2*ny] forecast caches */
     float *zmax;
@@ -49,7 +52,7 @@ struct GcLayerDev {
 };
 
 #define GC_AT(p, L, i, j) ((p)[(size_t)(j) * (size_t)(L).pitch + (size_t)(i)])
-#define GC_ROW(L, k, j) ((L).rows[(size_t)(k) * (size_t)(L).ny + (size_t)(j)])
+#define GC_ROW(L, k, j) ((L).rows[(size_t)(j) * GC_ROWW + (size_t)(k)])
 
 /* status codes of the extended API */
 #define GC_OK 0

@@ -8,12 +8,17 @@
  * (GPUOutput.cu:46-53), the arrival-step record, and the gauge sampling of
  * the previous step (GET_TS, output.f90:1078-1090).
  *
- * Work decomposition: a CTA owns a TX x TY tile (I x J).  Its TX threads
- * march up the tile's rows; at row r they stage row r of M1, N1, H in a
- * four-row shared-memory ring, compute the new surface Z2 of row r (with a
- * one-column halo on the right), then the momentum of row r-1, which needs
- * Z2 of rows r-1 and r.  The halo row/column of Z2 is recomputed from the
- * same inputs by both neighbouring tiles, bit-identically.  Per cell the
+ * Work decomposition: a warp owns a 128 x TY tile (I x J); lane l owns the
+ * four consecutive cells I = i0+4l .. i0+4l+3 and moves them as float4.  The
+ * warp marches up the tile's rows keeping rows r-2..r of N, r-1..r of M, H
+ * and of the new surface in registers; the I+1 / I-1 neighbours come from
+ * the adjacent lane by warp shuffle, and lanes 31 / 0 load the one-column
+ * halos.  At row r the warp computes the new surface Z2 of row r (plus the
+ * halo column), then the momentum of row r-1, which needs Z2 of rows r-1 and
+ * r; the loads of row r+1 are issued before that arithmetic.  No shared
+ * memory and no block barrier: warps of a CTA work on independent tiles.
+ * The halo row/column of Z2 is recomputed by both neighbouring tiles from the
+ * same inputs, bit-identically.  Per cell the
  * kernel streams Z1, M1, N1, H in and Z2, M2, N2 out (28 bytes) plus the
  * 8-byte max-amplitude read/write; R2 and R4 are rebuilt from H and the
  * per-row factors instead of being streamed.
@@ -21,27 +26,20 @@
  * Arithmetic is evaluated in the Fortran order with separately rounded
  * float operations (the library is built with -fmad=false).
  */
+#include <type_traits>
+
 #include "fused.h"
 
 namespace {
 
-template <int TX>
-struct FusedSmem {
-    float m[4][TX + 2]; /* column c+1 <-> I = i0 + c; column 0 is i0-1 */
-    float n[4][TX + 1];
-    float h[4][TX + 1];
-    float z[4][TX + 1];
-};
+constexpr int TXW = 128; /* columns per warp tile: 32 lanes x 4 cells */
 
 __device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 
-__device__ __forceinline__ float ld_row(const float *__restrict__ a, int i, int nx, size_t roff) {
-    return (i < nx) ? __ldg(a + roff + i) : 0.0f;
-}
-
-/* OPEN on a perimeter cell, from the staged rows (boundaries.f90:42-200) */
-__device__ __forceinline__ float open_from_smem(int i, int j, int nx, int ny, float h, float hs,
-                                                float m, float mw, float n, float ns) {
+/* OPEN on a perimeter cell of the outermost layer (boundaries.f90:42-200).
+ * h, m, n at (i,j); hs, ns at (i,j-1); mw at (i-1,j). */
+__device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h, float hs, float m,
+                                           float mw, float n, float ns) {
     if (!(h > CC_GX)) return 0.0f;
     float cc = sqrtf(CC_GRAV * h);
     float zz;
@@ -84,230 +82,491 @@ __device__ __forceinline__ float open_from_smem(int i, int j, int nx, int ny, fl
     return zz;
 }
 
-template <int TX, int TY>
-__device__ __forceinline__ void fused_tile(const GcFusedGrid &G, int lt, int step,
-                                           FusedSmem<TX> &S) {
-    const int t = threadIdx.x;
-    const int nx = G.nx, ny = G.ny;
-    const size_t P = (size_t)G.pitch;
-    const int tx = lt % G.tiles_x, ty = lt / G.tiles_x;
-    const int i0 = tx * TX, j0 = ty * TY;
-    const int local = step - G.step0; /* 0-based index of the step being computed */
-    if (local < 0 || local > G.nsteps) return;
-    const int cur = G.cur0 ^ (local & 1);
-    const float *__restrict__ z1 = G.z[cur];
-    const float *__restrict__ m1 = G.m[cur];
-    const float *__restrict__ n1 = G.n[cur];
-    float *__restrict__ z2 = G.z[cur ^ 1];
-    float *__restrict__ m2 = G.m[cur ^ 1];
-    float *__restrict__ n2 = G.n[cur ^ 1];
-    const float *__restrict__ hh = G.h;
-    const float *__restrict__ rows = G.rows;
-    const bool root = G.root != 0;
-    const int i = i0 + t;
+/* new surface of one cell: OPEN on the outer layer's perimeter, carried
+ * level-1 value on a child's I=1 / J=1 edges, MASS_S elsewhere */
+__device__ __forceinline__ float z2_cell(bool root, int i, int r, int nx, int ny, float z1, float h,
+                                         float hs, float m, float mw, float n, float ns, float r1,
+                                         float r11, float r6, float r6m) {
+    if (root && (i == 0 || i == nx - 1 || r == 0 || r == ny - 1))
+        return open_cell(i, r, nx, ny, h, hs, m, mw, n, ns);
+    if (!root && (i == 0 || r == 0)) return z1;
+    if (h > CC_GX) {
+        float zz = z1 - r1 * (m - mw) - r11 * (n * r6 - ns * r6m);
+        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if ((zz + h) <= CC_EPS) zz = -h;
+        return zz;
+    }
+    return 0.0f;
+}
+
+/* ------------------------------------------------------------------ */
+/* bulk-copy pipeline primitives (PTX, sm_90+ / sm_100a)              */
+/* ------------------------------------------------------------------ */
+__device__ int g_pipe_error; /* set when a pipeline wait gave up */
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+/* 1-D bulk copy global -> this CTA's shared memory, completing on `bar`;
+ * dst, src and bytes must be multiples of 16 */
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+/* bounded wait: gives up after `limit` polls (each poll may suspend briefly) */
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
+    for (int it = 0; it < limit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+constexpr int WAIT_LIMIT = 1 << 22;
+
+/* one pipeline stage holds one grid row of a warp tile (byte offsets) */
+constexpr int ST_M = 0;                /* M: 136 floats, cols i0-4 .. i0+131 (index c+4) */
+constexpr int ST_N = ST_M + 136 * 4;   /* N: 132 floats, cols i0 .. i0+131 */
+constexpr int ST_H = ST_N + 132 * 4;
+constexpr int ST_Z = ST_H + 132 * 4;   /* Z1 */
+constexpr int ST_X = ST_Z + 132 * 4;   /* max-eta, 128 floats */
+constexpr int ST_C = ST_X + 128 * 4;   /* row coefficient record, 8 floats */
+constexpr int STAGE_BYTES = ((ST_C + 32) + 127) / 128 * 128;
+constexpr int ZR_FLOATS = 136;         /* new-surface ring row: cols i0 .. i0+128 */
+
+__host__ __device__ constexpr int warp_smem_bytes(int S) { return ((S * STAGE_BYTES + 2 * ZR_FLOATS * 4 + S * 8) + 127) / 128 * 128; }
+
+enum { F_M = 1, F_N = 2, F_H = 4, F_Z = 8, F_X = 16, F_C = 32 };
+
+
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+/* masked float4 store at p = &row[i] (cells at or beyond nx become 0) */
+__device__ __forceinline__ void st4p(float *p, int i, int nx, const float v[4]) {
+    if (i < nx) {
+        float4 t;
+        t.x = v[0];
+        t.y = (i + 1 < nx) ? v[1] : 0.0f;
+        t.z = (i + 2 < nx) ? v[2] : 0.0f;
+        t.w = (i + 3 < nx) ? v[3] : 0.0f;
+        *reinterpret_cast<float4 *>(p) = t;
+    }
+}
+
+template <int S, bool XR24>
+__device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int step, char *wsm, int &seq) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    /* descriptor fields in registers (stores could alias a descriptor in global memory) */
+    const int nx = Gref.nx, ny = Gref.ny, pitch = Gref.pitch;
+    const size_t P = (size_t)pitch;
+    const int tiles_x = Gref.tiles_x, step0 = Gref.step0, nsteps = Gref.nsteps, TY = Gref.ty;
+    const int flags = Gref.flags;
+    const float thr = Gref.thr;
+    const bool root = Gref.root != 0;
+    const int local = step - step0; /* 0-based index of the step being computed */
+    if (local < 0 || local > nsteps) return true;
+    const int cur = Gref.cur0 ^ (local & 1);
+    const float *__restrict__ z1 = Gref.z[cur];
+    const float *__restrict__ m1 = Gref.m[cur];
+    const float *__restrict__ n1 = Gref.n[cur];
+    float *__restrict__ z2 = Gref.z[cur ^ 1];
+    float *__restrict__ m2 = Gref.m[cur ^ 1];
+    float *__restrict__ n2 = Gref.n[cur ^ 1];
+    float *__restrict__ zmax = Gref.zmax;
+    int *__restrict__ arrival = Gref.arrival;
+    const bool do_max = (flags & GC_F_MAXAMP) != 0;
+    const bool do_arr = (flags & GC_F_ARRIVAL) != 0;
+    const int txi = lt % tiles_x, tyi = lt / tiles_x;
+    const int i0 = txi * TXW, j0 = tyi * TY;
 
     /* gauges: sample the surface the previous step left (its Z2 is our Z1) */
-    if (lt == 0 && G.ng > 0) {
+    if (lt == 0 && Gref.ng > 0) {
+        const int ng = Gref.ng;
         int prev = local - 1;
-        if (prev >= 0 && prev < G.ts_len) {
-            for (int g = t; g < G.ng; g += TX) {
-                int ki = G.gij[2 * g] - 1, kj = G.gij[2 * g + 1] - 1;
+        if (prev >= 0 && prev < Gref.ts_len) {
+            const int *gij = Gref.gij;
+            const float *gw = Gref.gw;
+            float *ts = Gref.ts;
+            for (int g = lane; g < ng; g += 32) {
+                int ki = gij[2 * g] - 1, kj = gij[2 * g + 1] - 1;
                 size_t c = (size_t)kj * P + ki;
                 float l1 = z1[c], l2 = z1[c + 1], l3 = z1[c + P], l4 = z1[c + P + 1];
-                float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
+                float cx = gw[2 * g], cy = gw[2 * g + 1];
                 float a = l1 * (1.0f - cx) * (1.0f - cy);
                 float b = l2 * (cx) * (1.0f - cy);
                 float d = l3 * (1.0f - cx) * (cy);
                 float e = l4 * (cx) * (cy);
-                G.ts[(size_t)prev * G.ng + g] = a + b + d + e;
+                ts[(size_t)prev * ng + g] = a + b + d + e;
             }
         }
     }
+    if (local >= nsteps) return true; /* finished: only the last gauge sample */
 
-    if (local >= G.nsteps) return; /* finished: only the last gauge sample */
+    /* rows of this tile: k = 0 is row max(j0-1,0) (N, H, coefficients only),
+     * k = 1..TY+1 are rows j0 .. j0+TY (the last one a halo row) */
+    const int K = 1 + min(TY + 1, ny - j0);
+    const int jr0 = j0 > 0 ? j0 - 1 : 0;
+    const uint32_t wbase = smem_u32(wsm);
+    const uint32_t bars = wbase + S * STAGE_BYTES + 2 * ZR_FLOATS * 4;
+    float *zr = reinterpret_cast<float *>(wsm + S * STAGE_BYTES);
+    const int seq0 = seq;
 
-    /* prologue: row max(j0-1,0) of N and H */
+    /* lanes 0..5 each own one field's copy: M, N, H, Z1, max-eta, coefficients;
+     * source column, byte count and stage offset are fixed for the tile */
+    const char *cp_src = nullptr;
+    size_t cp_stride = P * 4;
+    uint32_t cp_dst = 0, cp_bytes = 0;
+    int cp_bit = 0;
+    const int ms = i0 >= 4 ? i0 - 4 : 0;
+    const uint32_t bm = 4u * (i0 >= 4 ? min(136, pitch - ms) : min(132, pitch));
+    const uint32_t bn = 4u * min(132, pitch - i0), bx = 4u * min(128, pitch - i0);
+    if (lane == 0) { cp_src = (const char *)(m1 + ms); cp_dst = ST_M + (i0 >= 4 ? 0 : 16); cp_bytes = bm; cp_bit = F_M; }
+    if (lane == 1) { cp_src = (const char *)(n1 + i0); cp_dst = ST_N; cp_bytes = bn; cp_bit = F_N; }
+    if (lane == 2) { cp_src = (const char *)(Gref.h + i0); cp_dst = ST_H; cp_bytes = bn; cp_bit = F_H; }
+    if (lane == 3) { cp_src = (const char *)(z1 + i0); cp_dst = ST_Z; cp_bytes = bn; cp_bit = F_Z; }
+    if (lane == 4) { cp_src = (const char *)(zmax + i0); cp_dst = ST_X; cp_bytes = bx; cp_bit = F_X; }
+    if (lane == 5) { cp_src = (const char *)Gref.rows; cp_dst = ST_C; cp_bytes = 32u; cp_bit = F_C; cp_stride = GC_ROWW * 4; }
+    /* the three row kinds: the row above the tile, owned rows, the halo row below */
+    const int mk_pro = F_N | F_H | F_C;
+    const int mk_halo = F_M | F_N | F_H | F_Z | F_C;
+    const int mk_mid = mk_halo | (do_max ? F_X : 0);
+    const uint32_t by_pro = 2 * bn + 32u, by_halo = bm + 3 * bn + 32u;
+    const uint32_t by_mid = by_halo + (do_max ? bx : 0u);
+    auto issue = [&](int k, int st) {
+        const int mask = k == 0 ? mk_pro : (k <= TY ? mk_mid : mk_halo);
+        const uint32_t bytes = k == 0 ? by_pro : (k <= TY ? by_mid : by_halo);
+        const int jr = k == 0 ? jr0 : j0 + k - 1;
+        const uint32_t bar = bars + 8 * st;
+        if (lane == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(bar, bytes);
+        }
+        __syncwarp();
+        if (cp_bit & mask) {
+            fence_proxy_async(); /* this stage's earlier generic reads come first */
+            bulk_g2s(wbase + st * STAGE_BYTES + cp_dst, cp_src + (size_t)jr * cp_stride, cp_bytes, bar);
+        }
+    };
+    __syncwarp();
     {
-        const int jr = j0 > 0 ? j0 - 1 : 0;
-        const int s = (j0 - 1) & 3;
-        const size_t ro = (size_t)jr * P;
-        S.n[s][t] = ld_row(n1, i, nx, ro);
-        S.h[s][t] = ld_row(hh, i, nx, ro);
-        if (t == 0) {
-            S.n[s][TX] = ld_row(n1, i0 + TX, nx, ro);
-            S.h[s][TX] = ld_row(hh, i0 + TX, nx, ro);
+        int st = seq0 % S;
+        const int kk = min(S, K);
+        for (int k = 0; k < kk; k++) {
+            issue(k, st);
+            st = (st + 1 == S) ? 0 : st + 1;
         }
     }
+    auto wait = [&](int st, uint32_t par) {
+        const bool got = mbar_wait(bars + 8 * st, par, WAIT_LIMIT);
+        return __all_sync(FULL, got) != 0; /* warp-uniform outcome */
+    };
+    /* stages and phase parities tracked incrementally: row k+1 follows row k */
+    int stB = seq0 % S, stC = 0;
+    uint32_t parB = (uint32_t)((seq0 / S) & 1);
+    bool ok = wait(stB, parB);
+    const int c0 = 4 * lane;             /* this lane's first cell within the tile */
+    const int ib = i0 + c0;
+    const bool own = ib < nx;
+    const int ih = i0 + TXW;
+    const bool hasR = (lane == 31) && (ih < nx);
+    /* output row pointers at this lane's first cell: surface/max rows r, flux rows j = r-1 */
+    float *z2p = z2 + (size_t)j0 * P + ib;
+    float *zxp = zmax + (size_t)j0 * P + ib;
+    float *m2p = m2 + (size_t)j0 * P + ib;
+    float *n2p = n2 + (size_t)j0 * P + ib;
 
-    /* prefetch row j0 into registers */
-    float pm = 0.f, pn = 0.f, ph = 0.f, pz = 0.f, pmw = 0.f, pme = 0.f, pne = 0.f, phe = 0.f, pze = 0.f;
-#define GC_FETCH(R_)                                                   \
-    if ((R_) < ny) {                                                   \
-        const size_t ro_ = (size_t)(R_) * P;                           \
-        pm = ld_row(m1, i, nx, ro_);                                   \
-        pn = ld_row(n1, i, nx, ro_);                                   \
-        ph = ld_row(hh, i, nx, ro_);                                   \
-        pz = ld_row(z1, i, nx, ro_);                                   \
-        if (t == 0) {                                                  \
-            pmw = ld_row(m1, i0 > 0 ? i0 - 1 : 0, nx, ro_);            \
-            pme = ld_row(m1, i0 + TX, nx, ro_);                        \
-            pne = ld_row(n1, i0 + TX, nx, ro_);                        \
-            phe = ld_row(hh, i0 + TX, nx, ro_);                        \
-            pze = ld_row(z1, i0 + TX, nx, ro_);                        \
-        }                                                              \
-    }
-    GC_FETCH(j0)
-
-    for (int r = j0; r <= j0 + TY; r++) {
-        const bool rv = r < ny;
-        const int s = r & 3, sp = (r - 1) & 3;
-        float zc = pz, zce = pze;
+    /* a tile none of whose cells (halo row and column included) lies on a
+     * grid edge runs a body compiled without any boundary logic */
+    const bool edge = !(i0 >= 1 && i0 + TXW <= nx - 2 && j0 >= 1 && j0 + TY <= ny - 2);
+    for (int k = 1; k <= TY + 1 && ok; k++) {
+        const int r = j0 + k - 1;
+        const bool rv = k < K;
+        const int stA = (stB + 1 == S) ? 0 : stB + 1;
+        const uint32_t parA = (stA == 0) ? (parB ^ 1u) : parB;
+        float *SA = reinterpret_cast<float *>(wsm + stA * STAGE_BYTES);
+        float *SB = reinterpret_cast<float *>(wsm + stB * STAGE_BYTES);
+        float *SC = reinterpret_cast<float *>(wsm + stC * STAGE_BYTES);
         if (rv) {
-            S.m[s][t + 1] = pm;
-            S.n[s][t] = pn;
-            S.h[s][t] = ph;
-            if (t == 0) {
-                S.m[s][0] = pmw;
-                S.m[s][TX + 1] = pme;
-                S.n[s][TX] = pne;
-                S.h[s][TX] = phe;
+            ok = wait(stA, parA);
+            if (!ok) break;
+            if (i0 == 0 && lane == 0) SA[ST_M / 4 + 3] = SA[ST_M / 4 + 4]; /* IM1 = max(I-1,1) */
+        }
+        __syncwarp();
+        float *zA = zr + (k & 1) * ZR_FLOATS, *zB = zr + ((k - 1) & 1) * ZR_FLOATS;
+        auto body = [&](auto edge_tag) {
+            constexpr bool EDGE = decltype(edge_tag)::value;
+            if (rv) {
+                const float *mA = SA + ST_M / 4 + 4, *nA = SA + ST_N / 4, *hA = SA + ST_H / 4, *z1A = SA + ST_Z / 4;
+                const float *nB = SB + ST_N / 4, *hB = SB + ST_H / 4;
+                const float r1 = SA[ST_C / 4 + GC_R1], r11 = SA[ST_C / 4 + GC_R11], r6 = SA[ST_C / 4 + GC_R6];
+                const float r6m = (r > 0) ? SB[ST_C / 4 + GC_R6] : 0.0f;
+                const float4 m4 = lds4(mA + c0), n4 = lds4(nA + c0), nb4 = lds4(nB + c0);
+                const float4 h4 = lds4(hA + c0), hb4 = lds4(hB + c0), z4 = lds4(z1A + c0);
+                const float mv[4] = {m4.x, m4.y, m4.z, m4.w}, nv[4] = {n4.x, n4.y, n4.z, n4.w};
+                const float nbv[4] = {nb4.x, nb4.y, nb4.z, nb4.w}, hv[4] = {h4.x, h4.y, h4.z, h4.w};
+                const float hbv[4] = {hb4.x, hb4.y, hb4.z, hb4.w}, zv[4] = {z4.x, z4.y, z4.z, z4.w};
+                const float mwest = mA[c0 - 1];
+                float zn[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float mw = q == 0 ? mwest : mv[q - 1];
+                    if constexpr (EDGE) {
+                        zn[q] = z2_cell(root, ib + q, r, nx, ny, zv[q], hv[q], hbv[q], mv[q], mw, nv[q], nbv[q], r1,
+                                        r11, r6, r6m);
+                    } else {
+                        /* MASS_S (mass.f90:82-95) */
+                        const float h = hv[q];
+                        float zz = zv[q] - r1 * (mv[q] - mw) - r11 * (nv[q] * r6 - nbv[q] * r6m);
+                        zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+                        zz = ((zz + h) <= CC_EPS) ? -h : zz;
+                        zn[q] = (h > CC_GX) ? zz : 0.0f;
+                    }
+                }
+                *reinterpret_cast<float4 *>(zA + c0) = make_float4(zn[0], zn[1], zn[2], zn[3]);
+                if (lane == 31 && (!EDGE || hasR)) {
+                    if constexpr (EDGE) {
+                        zA[TXW] = z2_cell(root, ih, r, nx, ny, z1A[TXW], hA[TXW], hB[TXW], mA[TXW], mA[TXW - 1],
+                                          nA[TXW], nB[TXW], r1, r11, r6, r6m);
+                    } else {
+                        const float h = hA[TXW];
+                        float zz = z1A[TXW] - r1 * (mA[TXW] - mA[TXW - 1]) - r11 * (nA[TXW] * r6 - nB[TXW] * r6m);
+                        zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+                        zz = ((zz + h) <= CC_EPS) ? -h : zz;
+                        zA[TXW] = (h > CC_GX) ? zz : 0.0f;
+                    }
+                }
+                if (k <= TY && own) {
+                    if constexpr (EDGE) st4p(z2p, ib, nx, zn);
+                    else *reinterpret_cast<float4 *>(z2p) = make_float4(zn[0], zn[1], zn[2], zn[3]);
+                    if (do_max) {
+                        const float4 x4 = lds4(SA + ST_X / 4 + c0);
+                        float zx[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+                        for (int q = 0; q < 4; q++) zx[q] = (zx[q] >= zn[q]) ? zx[q] : zn[q];
+                        if constexpr (EDGE) st4p(zxp, ib, nx, zx);
+                        else *reinterpret_cast<float4 *>(zxp) = make_float4(zx[0], zx[1], zx[2], zx[3]);
+                    }
+                    if (do_arr) {
+                        const float zhi = fmaxf(fmaxf(zn[0], zn[1]), fmaxf(zn[2], zn[3]));
+                        if (zhi > thr) {
+#pragma unroll
+                            for (int q = 0; q < 4; q++) {
+                                if (ib + q < nx && zn[q] > thr && hv[q] > CC_GX) {
+                                    int *a = arrival + (size_t)r * P + ib + q;
+                                    if (*a < 0) *a = local + 1;
+                                }
+                            }
+                        }
+                    }
+                }
             }
-        }
-        GC_FETCH(r + 1) /* next row's loads overlap this row's compute */
-        __syncthreads();
-        if (rv) {
-            /* new surface of row r: TX owned columns + one halo column */
-            const float r1 = rows[GC_R1 * (size_t)ny + r];
-            const float r11 = rows[GC_R11 * (size_t)ny + r];
-            const float r6 = rows[GC_R6 * (size_t)ny + r];
-            const float r6m = r > 0 ? rows[GC_R6 * (size_t)ny + r - 1] : 0.0f;
-            for (int k = 0; k < (t == 0 ? 2 : 1); k++) {
-                const int c = (k == 0) ? t : TX;
-                const int ic = i0 + c;
-                if (ic >= nx) continue;
-                const float z1v = (k == 0) ? zc : zce;
-                const float h = S.h[s][c];
-                float zn;
-                if (root && (ic == 0 || ic == nx - 1 || r == 0 || r == ny - 1)) {
-                    zn = open_from_smem(ic, r, nx, ny, h, S.h[sp][c], S.m[s][c + 1], S.m[s][c],
-                                        S.n[s][c], S.n[sp][c]);
-                } else if (!root && (ic == 0 || r == 0)) {
-                    zn = z1v;
-                } else if (h > CC_GX) {
-                    float zz = z1v - r1 * (S.m[s][c + 1] - S.m[s][c])
-                               - r11 * (S.n[s][c] * r6 - S.n[sp][c] * r6m);
-                    if (fabs_(zz) < CC_EPS) zz = 0.0f;
-                    if ((zz + h) <= CC_EPS) zz = -h;
-                    zn = zz;
+            __syncwarp();
+            /* momentum of row j = r-1 (MOMT_S, moment.f90:86-145) */
+            const int j = r - 1;
+            if (k >= 2 && j < ny && own) {
+                const float *mB = SB + ST_M / 4 + 4, *mA = SA + ST_M / 4 + 4;
+                const float *nB = SB + ST_N / 4, *nC = SC + ST_N / 4;
+                const float *hB = SB + ST_H / 4, *hA = SA + ST_H / 4;
+                const float cx = SB[ST_C / 4 + GC_CX], r3 = SB[ST_C / 4 + GC_R3];
+                const float cy = SB[ST_C / 4 + GC_CY], r5 = SB[ST_C / 4 + GC_R5];
+                /* columns c0..c0+4 of H, N(j), N(j-1), Z2(j); c0-1..c0+3 of M(j), M(j+1) */
+                float hb[5], nb[5], nc[5], zb[5], mb[5], ma[5], ha[4], za[4];
+                {
+                    float4 t;
+                    t = lds4(hB + c0); hb[0] = t.x; hb[1] = t.y; hb[2] = t.z; hb[3] = t.w; hb[4] = hB[c0 + 4];
+                    t = lds4(nB + c0); nb[0] = t.x; nb[1] = t.y; nb[2] = t.z; nb[3] = t.w; nb[4] = nB[c0 + 4];
+                    t = lds4(nC + c0); nc[0] = t.x; nc[1] = t.y; nc[2] = t.z; nc[3] = t.w; nc[4] = nC[c0 + 4];
+                    t = lds4(zB + c0); zb[0] = t.x; zb[1] = t.y; zb[2] = t.z; zb[3] = t.w; zb[4] = zB[c0 + 4];
+                    t = lds4(mB + c0); mb[0] = mB[c0 - 1]; mb[1] = t.x; mb[2] = t.y; mb[3] = t.z; mb[4] = t.w;
+                    t = lds4(mA + c0); ma[0] = mA[c0 - 1]; ma[1] = t.x; ma[2] = t.y; ma[3] = t.z; ma[4] = t.w;
+                    t = lds4(hA + c0); ha[0] = t.x; ha[1] = t.y; ha[2] = t.z; ha[3] = t.w;
+                    t = lds4(zA + c0); za[0] = t.x; za[1] = t.y; za[2] = t.z; za[3] = t.w;
+                }
+                float xm[4], xn[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int i = ib + q;
+                    const float h0 = hb[q], hp1 = hb[q + 1];
+                    bool mdom = true, ndom = true;
+                    if constexpr (EDGE) {
+                        mdom = root ? (i <= nx - 2) : (i >= 1 && i <= nx - 2 && j >= 1);
+                        ndom = (root ? (j <= ny - 2) : (i >= 1 && j >= 1 && j <= ny - 2)) && i < nx;
+                    }
+                    /* evaluated unconditionally, then selected: four independent
+                     * straight-line chains per lane */
+                    const float tot_n = nb[q] + nb[q + 1] + nc[q] + nc[q + 1];
+                    float r2, r4;
+                    if constexpr (XR24) {
+                        r2 = __ldg(Gref.r2 + (size_t)j * P + i);
+                        r4 = __ldg(Gref.r4 + (size_t)j * P + i);
+                    } else {
+                        r2 = cx * (0.5f * (h0 + hp1));
+                        r4 = cy * (0.5f * (h0 + ha[q]));
+                    }
+                    float vm = mb[q + 1] - r2 * (zb[q + 1] - zb[q]) + r3 * tot_n;
+                    vm = (fabs_(vm) < CC_EPS) ? 0.0f : vm;
+                    xm[q] = (mdom && h0 > CC_GX && hp1 > CC_GX) ? vm : 0.0f;
+                    const float tot_m = mb[q] + ma[q] + mb[q + 1] + ma[q + 1];
+                    float vn = nb[q] - r4 * (za[q] - zb[q]) - r5 * tot_m;
+                    vn = (fabs_(vn) < CC_EPS) ? 0.0f : vn;
+                    xn[q] = (ndom && h0 > CC_GX && ha[q] > CC_GX) ? vn : 0.0f;
+                }
+                if constexpr (EDGE) {
+                    st4p(m2p, ib, nx, xm);
+                    st4p(n2p, ib, nx, xn);
                 } else {
-                    zn = 0.0f;
-                }
-                S.z[s][c] = zn;
-                if (k == 0 && r < j0 + TY) {
-                    const size_t cell = (size_t)r * P + ic;
-                    z2[cell] = zn;
-                    if (G.flags & GC_F_MAXAMP) {
-                        float zm = G.zmax[cell];
-                        if (!(zm >= zn)) G.zmax[cell] = zn;
-                    }
-                    if ((G.flags & GC_F_ARRIVAL) && zn > G.thr && h > CC_GX) {
-                        if (G.arrival[cell] < 0) G.arrival[cell] = local + 1;
-                    }
+                    *reinterpret_cast<float4 *>(m2p) = make_float4(xm[0], xm[1], xm[2], xm[3]);
+                    *reinterpret_cast<float4 *>(n2p) = make_float4(xn[0], xn[1], xn[2], xn[3]);
                 }
             }
-        }
-        __syncthreads();
-        /* momentum of row j = r-1 */
-        const int j = r - 1;
-        if (j >= j0 && j < ny && i < nx) {
-            const int a = j & 3, b = (j + 1) & 3, cm = j > 0 ? ((j - 1) & 3) : a;
-            const size_t cell = (size_t)j * P + i;
-            const int c = t;
-            float xm = 0.0f;
-            const bool mdom = root ? (i <= nx - 2) : (i >= 1 && i <= nx - 2 && j >= 1);
-            if (mdom) {
-                float h = S.h[a][c], hp1 = S.h[a][c + 1];
-                if (h > CC_GX && hp1 > CC_GX) {
-                    float tot_n = S.n[a][c] + S.n[a][c + 1] + S.n[cm][c] + S.n[cm][c + 1];
-                    float r2 = G.explicit_r24 ? G.r2[cell]
-                                              : rows[GC_CX * (size_t)ny + j] * (0.5f * (h + hp1));
-                    xm = S.m[a][c + 1] - r2 * (S.z[a][c + 1] - S.z[a][c])
-                         + rows[GC_R3 * (size_t)ny + j] * tot_n;
-                    if (fabs_(xm) < CC_EPS) xm = 0.0f;
-                }
-            }
-            m2[cell] = xm;
-            float xn = 0.0f;
-            const bool ndom = root ? (j <= ny - 2) : (i >= 1 && j >= 1 && j <= ny - 2);
-            if (ndom) {
-                float h = S.h[a][c], hq1 = S.h[b][c];
-                if (h > CC_GX && hq1 > CC_GX) {
-                    float tot_m = S.m[a][c] + S.m[b][c] + S.m[a][c + 1] + S.m[b][c + 1];
-                    float r4 = G.explicit_r24 ? G.r4[cell]
-                                              : rows[GC_CY * (size_t)ny + j] * (0.5f * (h + hq1));
-                    xn = S.n[a][c] - r4 * (S.z[b][c] - S.z[a][c])
-                         - rows[GC_R5 * (size_t)ny + j] * tot_m;
-                    if (fabs_(xn) < CC_EPS) xn = 0.0f;
-                }
-            }
-            n2[cell] = xn;
-        }
+        };
+        if (edge) body(std::true_type{});
+        else body(std::false_type{});
+        z2p += P;
+        zxp += P;
+        if (k >= 2) { m2p += P; n2p += P; }
+        __syncwarp();
+        /* row k-2 is no longer needed: refill its stage S rows ahead */
+        if (k >= 2 && k - 2 + S < K) issue(k - 2 + S, stC);
+        stC = stB; stB = stA; parB = parA;
     }
-    __syncthreads(); /* the next tile reuses the ring */
-#undef GC_FETCH
+    seq = seq0 + K;
+    if (!ok) {
+        /* record the failure, then give the copies still in flight a bounded
+         * chance to land before the warp leaves */
+        if (lane == 0) atomicExch(&g_pipe_error, 1);
+        for (int k = 0; k < K; k++) {
+            const int n = seq0 + k;
+            mbar_wait(bars + 8 * (n % S), (uint32_t)((n / S) & 1), 1 << 12);
+        }
+        return false;
+    }
+    __syncwarp();
+    return true;
 }
 
-template <int TX, int TY, bool MULTI>
-__global__ void __launch_bounds__(TX) k_fused(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
-                                              const int2 *__restrict__ tiles, int ntiles,
-                                              const int *__restrict__ step_base, int step_off) {
-    __shared__ FusedSmem<TX> S;
+template <int W, int S, bool MULTI>
+__global__ void __launch_bounds__(32 * W) k_fused(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                   const int2 *__restrict__ tiles, int ntiles,
+                                                   const int *__restrict__ step_base, int step_off) {
+    extern __shared__ __align__(128) char smem[];
     const int step = step_off + (step_base ? *step_base : 0);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char *wsm = smem + warp * warp_smem_bytes(S);
+    const uint32_t bars = smem_u32(wsm) + S * STAGE_BYTES + 2 * ZR_FLOATS * 4;
+    if (lane == 0) {
+        for (int s = 0; s < S; s++) mbar_init(bars + 8 * s, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    int seq = 0;
+    for (int tile = blockIdx.x * W + warp; tile < ntiles; tile += gridDim.x * W) {
+        bool ok;
         if (MULTI) {
             const int2 w = tiles[tile];
-            fused_tile<TX, TY>(grids[w.x], w.y, step, S);
+            const GcFusedGrid &G = grids[w.x];
+            ok = G.explicit_r24 ? warp_tile<S, true>(G, w.y, step, wsm, seq)
+                                : warp_tile<S, false>(G, w.y, step, wsm, seq);
         } else {
-            fused_tile<TX, TY>(one, tile, step, S);
+            ok = one.explicit_r24 ? warp_tile<S, true>(one, tile, step, wsm, seq)
+                                  : warp_tile<S, false>(one, tile, step, wsm, seq);
         }
+        if (!ok) return;
     }
 }
 
 struct Variant {
-    int tx, ty;
+    int w, s;
     void (*one)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int);
     void (*multi)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int);
 };
 
-#define GC_VARIANT(TX, TY) {TX, TY, k_fused<TX, TY, false>, k_fused<TX, TY, true>}
+#define GC_VARIANT(W, S) {W, S, k_fused<W, S, false>, k_fused<W, S, true>}
 const Variant kVariants[] = {
-    GC_VARIANT(128, 16), GC_VARIANT(128, 32), GC_VARIANT(128, 64),
-    GC_VARIANT(256, 16), GC_VARIANT(256, 32), GC_VARIANT(64, 32),
+    GC_VARIANT(4, 6), GC_VARIANT(2, 8), GC_VARIANT(4, 8), GC_VARIANT(8, 5),
+    GC_VARIANT(1, 8), GC_VARIANT(2, 6), GC_VARIANT(4, 5), GC_VARIANT(8, 4),
 };
 #undef GC_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+int variant_smem(const Variant &v) { return v.w * warp_smem_bytes(v.s); }
+
+void prepare(const Variant &v) {
+    static bool done[16] = {false};
+    int idx = (int)(&v - kVariants);
+    if (done[idx]) return;
+    cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
+    cudaFuncSetAttribute(v.multi, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
+    done[idx] = true;
+}
 
 } // namespace
 
 int gc_fused_num_variants() { return kNumVariants; }
 
-GcTileCfg gc_fused_variant(int v) {
-    if (v < 0 || v >= kNumVariants) v = 0;
-    return GcTileCfg{kVariants[v].tx, kVariants[v].ty};
+/* 1 if a pipeline wait in the fused kernel gave up since the last call */
+int gc_fused_take_error() {
+    int v = 0, z = 0;
+    cudaMemcpyFromSymbol(&v, g_pipe_error, sizeof v);
+    if (v) cudaMemcpyToSymbol(g_pipe_error, &z, sizeof z);
+    return v;
 }
 
-int gc_fused_tiles(int variant, int nx, int ny, int *tiles_x) {
-    GcTileCfg c = gc_fused_variant(variant);
-    int tx = (nx + c.tx - 1) / c.tx, ty = (ny + c.ty - 1) / c.ty;
+GcTileCfg gc_fused_variant(int v) {
+    if (v < 0 || v >= kNumVariants) v = 0;
+    return GcTileCfg{kVariants[v].w, kVariants[v].s};
+}
+
+int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x) {
+    int tx = (nx + TXW - 1) / TXW, tyn = (ny + ty - 1) / ty;
     if (tiles_x) *tiles_x = tx;
-    return tx * ty;
+    return tx * tyn;
+}
+
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny) {
+    const int slots = gc_fused_max_ctas(variant) * gc_fused_variant(variant).warps;
+    auto tiles = [&](int ty) {
+        long long t = 0;
+        for (int g = 0; g < ngrids; g++) t += gc_fused_tiles(nx[g], ny[g], ty, nullptr);
+        return t;
+    };
+    /* waves at 16 rows per tile; then the shortest tiles that keep that many waves */
+    long long waves = (tiles(16) + slots - 1) / slots;
+    if (waves < 1) waves = 1;
+    for (int ty = 8; ty <= 256; ty++)
+        if (tiles(ty) <= waves * slots) return ty;
+    return 256;
 }
 
 cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s) {
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant &v = kVariants[variant];
-    int ntiles = gc_fused_tiles(variant, g.nx, g.ny, nullptr);
-    v.one<<<ntiles, v.tx, 0, s>>>(g, nullptr, nullptr, ntiles, nullptr, step);
+    int ntiles = gc_fused_tiles(g.nx, g.ny, g.ty, nullptr);
+    prepare(v);
+    v.one<<<(ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s>>>(g, nullptr, nullptr, ntiles, nullptr, step);
     return cudaGetLastError();
 }
 
@@ -317,7 +576,8 @@ int gc_fused_max_ctas(int variant) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v.multi, v.tx, 0);
+    prepare(v);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v.multi, 32 * v.w, variant_smem(v));
     return sms * (per > 0 ? per : 1);
 }
 
@@ -327,9 +587,11 @@ cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant &v = kVariants[variant];
     if (ntiles <= 0) return cudaSuccess;
-    if (nctas <= 0 || nctas > ntiles) nctas = ntiles;
+    const int need = (ntiles + v.w - 1) / v.w;
+    if (nctas <= 0 || nctas > need) nctas = need;
     GcFusedGrid dummy;
     memset(&dummy, 0, sizeof dummy);
-    v.multi<<<nctas, v.tx, 0, s>>>(dummy, d_grids, d_tiles, ntiles, d_step_base, step_off);
+    prepare(v);
+    v.multi<<<nctas, 32 * v.w, variant_smem(v), s>>>(dummy, d_grids, d_tiles, ntiles, d_step_base, step_off);
     return cudaGetLastError();
 }

@@ -86,7 +86,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 int gc_layer_alloc(GcLayer &L) {
     L.pitch = (L.nx + 31) & ~31;
     size_t field = align256((size_t)L.pitch * L.ny * sizeof(float));
-    size_t rows = align256((size_t)GC_NROW * L.ny * sizeof(float));
+    size_t rows = align256((size_t)GC_ROWW * L.ny * sizeof(float));
     size_t nfield = 6 /* z,m,n x2 */ + 1 /* h */ + 1 /* zmax */ + 1 /* arrival */;
     bool cart = L.laycord == 1;
     if (cart) nfield += 2;           /* hp, hq */
@@ -305,17 +305,21 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
     }
     const size_t cells = (size_t)L.nx * L.ny;
     /* spherical layers: try the factored R2/R4 form, else keep the fields */
-    std::vector<float> rowblk((size_t)GC_NROW * L.ny, 0.0f);
+    std::vector<float> rowblk((size_t)GC_ROWW * L.ny, 0.0f);
     if (L.laycord == 0) {
-        bool f2 = factor_rows(L.nx, L.ny, H_f, R2_f, true, &rowblk[(size_t)GC_CX * L.ny]);
-        bool f4 = factor_rows(L.nx, L.ny, H_f, R4_f, false, &rowblk[(size_t)GC_CY * L.ny]);
+        std::vector<float> cx((size_t)L.ny, 0.0f), cy((size_t)L.ny, 0.0f);
+        bool f2 = factor_rows(L.nx, L.ny, H_f, R2_f, true, cx.data());
+        bool f4 = factor_rows(L.nx, L.ny, H_f, R4_f, false, cy.data());
         L.explicit_r24 = !(f2 && f4);
         for (int j = 0; j < L.ny; j++) {
-            rowblk[(size_t)GC_R1 * L.ny + j] = R1_f[(size_t)j * L.nx];
-            rowblk[(size_t)GC_R11 * L.ny + j] = R11_f[(size_t)j * L.nx];
-            rowblk[(size_t)GC_R6 * L.ny + j] = R6_f[j];
-            rowblk[(size_t)GC_R3 * L.ny + j] = R3_f[(size_t)j * L.nx];
-            rowblk[(size_t)GC_R5 * L.ny + j] = R5_f[(size_t)j * L.nx];
+            float *rw = &rowblk[(size_t)j * GC_ROWW];
+            rw[GC_R1] = R1_f[(size_t)j * L.nx];
+            rw[GC_R11] = R11_f[(size_t)j * L.nx];
+            rw[GC_R6] = R6_f[j];
+            rw[GC_R3] = R3_f[(size_t)j * L.nx];
+            rw[GC_R5] = R5_f[(size_t)j * L.nx];
+            rw[GC_CX] = cx[j];
+            rw[GC_CY] = cy[j];
         }
     }
     if (gc_layer_alloc(L) != GC_OK) exit(EXIT_FAILURE);

@@ -123,6 +123,8 @@ int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk)
 int gc_engine_autotune(gc_engine *e, int reps);
 int gc_engine_variant(gc_engine *e);
 long long gc_engine_launches(gc_engine *e);
+/* the cudaStream_t the engine issues its kernels on */
+void *gc_engine_stream(gc_engine *e);
 
 #ifdef __cplusplus
 }
