@@ -35,6 +35,7 @@ import time
 
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "gpu-comcot_b200"))
+os.environ.setdefault("GCOMCOT_QUIET", "1")  # the JSON line is the only stdout
 
 import numpy as np  # noqa: E402
 

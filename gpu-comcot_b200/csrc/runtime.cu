@@ -216,9 +216,11 @@ void gcomcot_init_gpu_(void) {
     GC_CUDA_OR_DIE(cudaGetDevice(&dev));
     cudaDeviceProp prop;
     GC_CUDA_OR_DIE(cudaGetDeviceProperties(&prop, dev));
-    printf("GPU INFORMATIONS:                      %s\n", prop.name);
-    printf("-->Compute Capabilities [Major.Minor]: %d.%d\n", prop.major, prop.minor);
-    printf("-->Streaming Multi-Processor Count:    %d\n", prop.multiProcessorCount);
+    if (!getenv("GCOMCOT_QUIET")) {
+        printf("GPU INFORMATIONS:                      %s\n", prop.name);
+        printf("-->Compute Capabilities [Major.Minor]: %d.%d\n", prop.major, prop.minor);
+        printf("-->Streaming Multi-Processor Count:    %d\n", prop.multiProcessorCount);
+    }
     init_runtime();
 }
 
@@ -351,7 +353,7 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
         if (gc_layer_upload_field(L, L.hq, hq.data()) != GC_OK) exit(EXIT_FAILURE);
     }
     GC_CUDA_OR_DIE(cudaStreamSynchronize(g_rt.stream));
-    printf("Initializing layer id %d\n", L.id);
+    if (!getenv("GCOMCOT_QUIET")) printf("Initializing layer id %d\n", L.id);
 }
 
 /* GPUMass_s.cu:9-37: host arrays are only used by the reference's debug compare */

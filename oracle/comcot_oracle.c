@@ -1035,3 +1035,7 @@ void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp, double 
         if (R(ye) >= lo && R(ye) < hi) corners[3] = k - 1;
     }
 }
+
+/* the shared deterministic elementary functions, exposed for their tests */
+float ocl_expf(float x) { return cc_expf(x); }
+float ocl_powf(float x, float y) { return cc_powf(x, y); }

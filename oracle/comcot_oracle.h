@@ -73,4 +73,7 @@ int  ocl_rel_time(double dt_parent, double dx_m, double dy_m, double hmax, int n
 void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp,
                  double xs, double xe, double ys, double ye, int *corners);
 
+float ocl_expf(float x);
+float ocl_powf(float x, float y);
+
 #endif

@@ -55,6 +55,10 @@ def load(dtype=np.float32):
     lib.ocl_rel_time.restype = C.c_int
     lib.ocl_corners.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double,
                                 C.c_double, C.c_double, C.c_void_p]
+    lib.ocl_expf.argtypes = [C.c_float]
+    lib.ocl_expf.restype = C.c_float
+    lib.ocl_powf.argtypes = [C.c_float, C.c_float]
+    lib.ocl_powf.restype = C.c_float
     _libs[key] = lib
     return lib
 
