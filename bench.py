@@ -215,7 +215,7 @@ def run_c4(args, torch, dist, rank, world, local):
     ev1.record(stream)
     ev1.synchronize()
     ck = clocks.stop()
-    launches = eng.launches() - l0 + (run_steps + 63) // 64
+    launches = eng.launches() - l0
     ms = ev0.elapsed_time(ev1)
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -274,6 +274,231 @@ def run_c4(args, torch, dist, rank, world, local):
     return 0
 
 
+def run_c3(args, torch, dist, rank, world, local):
+    """C3: two-level nested run -- 1201x1001 2' linear spherical outer grid and
+    a 601x501 nonlinear Cartesian child (wet/dry, Manning n = 0.025, ratio 5)
+    coupled by JNQ/NEWQ edge fluxes and JNZ feedback every outer step.  value:
+    the batched engine's nested path (per-phase kernels in a captured graph);
+    e2e: the reference C ABI call sequence with host buffers."""
+    from comcot_b200.abi import ReferenceSession
+    from comcot_b200.engine import Engine
+
+    total = args.warmup + args.steps
+    case = synth.config_c3(nsteps=total)
+    P, Cl = case.layers
+    cells = P.nx * P.ny + Cl.nx * Cl.ny * Cl.rel_time
+    eng = Engine(budget=8 << 30)
+    eng.config(variant=args.variant, use_graphs=1, chunk=64)
+    eng.add(case)
+    eng.step(args.warmup)
+    eng.sync()
+    stream = torch.cuda.ExternalStream(eng.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = eng.launches()
+    ev0.record(stream)
+    eng.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ck = clocks.stop()
+    launches = eng.launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    eng.close()
+    value = cells * args.steps * world / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        case_e = synth.config_c3(nsteps=args.steps)
+        s = ReferenceSession(case_e, fusion=True, arrival=True, init_layers=False)
+        st = torch.cuda.ExternalStream(s.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        s.init_layers()
+        s.drive(args.steps, maxamp=True)
+        z, zc, zm = s.getz(1), s.getz(2), s.getzmax(1)
+        b.record(st)
+        b.synchronize()
+        e2e_ms = a.elapsed_time(b)
+        s.close()
+        fp, fc = P.nx * P.ny * 4, Cl.nx * Cl.ny * 4
+        e2e = {"value": cells * args.steps * world / (e2e_ms * 1e-3), "unit": METRIC,
+               "h2d_bytes_per_step": int((9 * fp + 13 * fc) / args.steps),
+               "d2h_bytes_per_step": int((2 * fp + fc) / args.steps), "ms_per_step": e2e_ms / args.steps,
+               "path": "gcomcot_set_layer_params_/init_layer x2 + per step mass/openbd/all_grid/momt/maxamp/"
+                       "update + getz x2/getzmax"}
+        del z, zc, zm
+    peak, peak_kind = peaks()
+    # algorithmic bytes of one outer step: outer grid 28 B + max-eta 8 B + arrival 8 B per cell;
+    # child 28 B per cell per sub-step (Z, M, N, H in; Z, M, N out; DZ = Z + H) + JNZ 8 B per child cell
+    bstep = 44.0 * P.nx * P.ny + (28.0 * Cl.rel_time + 8.0) * Cl.nx * Cl.ny
+    achieved = bstep / (ms * 1e-3 / args.steps) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"C3: 1201x1001 2' linear spherical + {Cl.nx}x{Cl.ny} nonlinear Cartesian "
+                                   f"child (r=5, rel_time {Cl.rel_time}, Manning 0.025), dt 2 s",
+                       "cells_per_step": cells, "parallelism": f"replicas x{world}",
+                       "l2": "working set ~60 MB per step fits the 126 MB L2; no flush (L2 resident)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                         "algorithmic_bytes_per_step": bstep},
+            "clocks": ck, "gpu_launches": launches}
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+
+        o = oracle.OracleRun(synth.config_c3(nsteps=total))
+        t0 = time.perf_counter()
+        o.run(1, threads=1)
+        one = time.perf_counter() - t0
+        n = max(1, min(total, int(15.0 / max(one, 1e-6))))
+        t0 = time.perf_counter()
+        o.run(n, threads=1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cells * n / dt, "unit": METRIC, "cores": 1, "kind": "port",
+                                "sample": f"{n} outer steps of both layers, serial oracle, {dt:.1f} s"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def run_c5(args, torch, dist, rank, world, local):
+    """C5 serving: a seeded Poisson stream of forecast requests (mean 2 req/s;
+    outer grids 481x401, 961x801 or 1921x1601 at 2'; 30 % nested with a
+    301x251 ratio-5 nonlinear child; 30-120 simulated minutes at dt 2 s; a
+    dipole source and 16 gauges each) served by continuous batching with
+    admission by HBM footprint.  Reported: p50/p99 time-to-forecast under the
+    arrival load, scenarios/hour at saturation, and the same for the plain
+    one-request-at-a-time path (its per-class service times measured through
+    the reference C ABI with one kernel per phase, then queued FIFO on the
+    same arrival times)."""
+    from comcot_b200 import serving
+    from comcot_b200.abi import ReferenceSession
+    from comcot_b200.engine import Engine
+
+    tpl = synth.config_c5_templates()
+    trace = synth.poisson_trace(n=args.requests, rate=args.rate, seed=5 + rank)
+
+    def make_requests():
+        return [serving.Request(k, t, synth.c5_request_case(tpl, size, nsteps, nested, seed))
+                for k, (t, size, nsteps, nested, seed) in enumerate(trace)]
+
+    reqs = make_requests()
+    # tile variant: tuned once on a warm batch of the largest class (not timed)
+    variant = args.variant
+    if variant < 0:
+        big = [r for r in reqs if r.case.root.nx == 1921 and len(r.case.layers) == 1][:4]
+        with Engine(budget=16 << 30) as eng:
+            for r in big:
+                eng.add(r.case, nsteps=64)
+            variant = eng.autotune(2)
+    budget = int(args.budget_gb * (1 << 30))
+    # warm-up: a few requests through the server (module load, first graphs)
+    with serving.ForecastServer(budget, chunk=args.chunk, variant=variant) as srv:
+        warm = [serving.Request(k, 0.0, synth.c5_request_case(tpl, sz, 64, k % 2 == 1, 900 + k))
+                for k, sz in enumerate(synth.C5_SIZES)]
+        srv.serve(warm, speed=float("inf"))
+    torch.cuda.synchronize()
+    cell_updates = sum(r.case.nsteps * sum(L.nx * L.ny * L.rel_time for L in r.case.layers) for r in reqs)
+    # 1) the arrival load, in real time
+    clocks = ClockSampler(local)
+    clocks.start()
+    with serving.ForecastServer(budget, chunk=args.chunk, variant=variant) as srv:
+        l0 = srv.eng.launches()
+        srv.serve(reqs, speed=1.0)
+        launches = srv.eng.launches() - l0
+        max_active, refused = srv.max_active, srv.refused
+    ck = clocks.stop()
+    lat = np.array([r.latency for r in reqs])
+    span = max(r.t_done for r in reqs)
+    pl = serving.percentiles(lat)
+    # 2) saturation: every request at t = 0
+    reqs_sat = make_requests()
+    torch.cuda.synchronize()
+    with serving.ForecastServer(budget, chunk=args.chunk, variant=variant) as srv:
+        t0 = time.perf_counter()
+        srv.serve(reqs_sat, speed=float("inf"))
+        sat_s = time.perf_counter() - t0
+        sat_active = srv.max_active
+    capacity = len(reqs_sat) * 3600.0 / sat_s
+    # 3) plain path: per class service time through the reference C ABI, one kernel per phase
+    plain = None
+    if not args.no_plain:
+        svc_class = {}
+        for size in synth.C5_SIZES:
+            for nested in (False, True):
+                c = synth.c5_request_case(tpl, size, 200, nested, 7)
+                s = ReferenceSession(c, fusion=False, arrival=True, init_layers=False)
+                st = torch.cuda.ExternalStream(s.stream())
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                torch.cuda.synchronize()
+                ev[0].record(st)
+                s.init_layers()
+                ev[1].record(st)
+                s.drive(20, maxamp=True)
+                ev[2].record(st)
+                s.drive(180, maxamp=True)
+                ev[3].record(st)
+                ev[3].synchronize()
+                t_init = ev[0].elapsed_time(ev[1]) * 1e-3
+                t_step = ev[2].elapsed_time(ev[3]) * 1e-3 / 180
+                t0 = time.perf_counter()
+                s.getzmax(1)
+                s.getarrival(1)
+                t_read = time.perf_counter() - t0
+                s.close()
+                svc_class[(size, nested)] = (t_init + t_read, t_step)
+        service = [svc_class[(size, nested)][0] + nsteps * svc_class[(size, nested)][1]
+                   for (_t, size, nsteps, nested, _seed) in trace]
+        plat, _ = serving.fifo_latencies([t for (t, *_rest) in trace], service)
+        plain = {"p50_s": float(np.percentile(plat, 50)), "p99_s": float(np.percentile(plat, 99)),
+                 "scenarios_per_hour": 3600.0 / float(np.mean(service)),
+                 "method": "per class (size x nested) service time = init + reads + nsteps x measured step "
+                           "time through the reference C ABI (one kernel per phase); FIFO queue on the same "
+                           "arrival times"}
+    line = {"metric": "p99 time-to-forecast", "value": pl["p99"], "unit": "s", "n_gpus": world,
+            "steps": int(sum(r.case.nsteps for r in reqs)), "warmup": len(warm),
+            "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"C5: {len(reqs)} requests, Poisson {args.rate} req/s, outer "
+                                   "481x401/961x801/1921x1601 at 2', 30% nested 301x251 r=5 nonlinear child, "
+                                   "30-120 min at dt 2 s, 16 gauges", "hbm_budget_gb": args.budget_gb,
+                       "graph_chunk": args.chunk, "tile_variant": variant, "parallelism": f"replicas x{world}"},
+            "p50_s": pl["p50"], "p99_s": pl["p99"], "mean_s": float(lat.mean()), "max_s": float(lat.max()),
+            "scenarios_per_hour_under_load": len(reqs) * 3600.0 / span,
+            "scenarios_per_hour_saturated": capacity, "saturated_seconds": sat_s,
+            "cell_updates_per_s_saturated": cell_updates / sat_s,
+            "max_active": max_active, "max_active_saturated": sat_active, "admission_waits": refused,
+            "clocks": ck, "gpu_launches": launches,
+            "e2e": {"value": pl["p99"], "unit": "s",
+                    "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "time-to-forecast is end to end: the request's initial surface and gauges go "
+                            "host->device at admission, max-eta, arrival and gauge series device->host at "
+                            "completion"}}
+    if plain:
+        line["plain_path"] = plain
+        line["capacity_vs_plain"] = capacity / plain["scenarios_per_hour"]
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -283,13 +508,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed tile variant (skips the autotuner)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
-                    help="c2: the headline single grid; c4: the 64-scenario ensemble")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the headline single grid; c3: the nested run; c4: the 64-scenario ensemble; "
+                         "c5: the forecast-serving load")
+    ap.add_argument("--requests", type=int, default=400, help="C5: requests in the trace")
+    ap.add_argument("--rate", type=float, default=2.0, help="C5: mean arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="C5: HBM admission budget")
+    ap.add_argument("--chunk", type=int, default=32, help="C5: steps between harvests")
+    ap.add_argument("--no-plain", action="store_true", help="C5: skip the plain-path service times")
     ap.add_argument("--scenarios", type=int, default=64)
     ap.add_argument("--plain-sample", type=int, default=4, help="C4: scenarios run on the plain path")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 3600 if args.workload == "c4" else 7200
+        args.steps = 7200 if args.workload == "c2" else 3600
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -314,6 +545,10 @@ def main():
 
     if args.workload == "c4":
         return run_c4(args, torch, dist, rank, world, local)
+    if args.workload == "c3":
+        return run_c3(args, torch, dist, rank, world, local)
+    if args.workload == "c5":
+        return run_c5(args, torch, dist, rank, world, local)
 
     tune_reps = 3
     from comcot_b200 import _lib
@@ -348,7 +583,7 @@ def main():
     ck = clocks.stop()
     if dist:
         dist.barrier()
-    launches = eng.launches() - l0 + (args.steps + 63) // 64  # + the graph's step-counter node
+    launches = eng.launches() - l0  # fused steps + the graphs' step-counter kernels
     ms = ev0.elapsed_time(ev1)
     if dist:
         t = torch.tensor([ms], device="cuda")

@@ -16,6 +16,16 @@ P_I = C.POINTER(C.c_int)
 P_F = C.POINTER(C.c_float)
 VP = C.c_void_p
 
+
+class ChildDesc(C.Structure):
+    """gc_child_desc (include/gcomcot.h)"""
+    _fields_ = ([("nx", C.c_int), ("ny", C.c_int), ("corners", C.c_int * 4), ("rel_size", C.c_int),
+                 ("rel_time", C.c_int)]
+                + [(n, C.c_int) for n in ("laycord", "laygov", "linchk", "modscm", "fric_switch")]
+                + [(n, C.c_float) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
+                + [(n, P_F) for n in ("h", "hp", "hq", "rows")])
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "gcomcot_init_gpu_": (None, []),
@@ -66,6 +76,10 @@ SIGNATURES = {
     "gc_engine_variant": (C.c_int, [VP]),
     "gc_engine_launches": (C.c_longlong, [VP]),
     "gc_engine_stream": (VP, [VP]),
+    "gc_engine_add_nested_class": (C.c_int, [VP, C.c_int, C.POINTER(ChildDesc)]),
+    "gc_engine_add_nested_member": (C.c_int, [VP, C.c_int, P_F, P_F, C.c_int, C.c_int, P_I, P_I, P_F,
+                                              C.c_float]),
+    "gc_engine_read_child": (C.c_int, [VP, C.c_int, P_F, P_F, P_F]),
 }
 
 

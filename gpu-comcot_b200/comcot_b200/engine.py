@@ -1,6 +1,7 @@
 """Python front of the batched ensemble / serving engine (gc_engine_* in
-include/gcomcot.h).  Members are linear-spherical single-layer forecasts;
-members built on the same bathymetry share one grid class."""
+include/gcomcot.h).  A member is a linear-spherical forecast, optionally with
+one nested child layer; members built on the same bathymetry (and the same
+child) share one grid class."""
 from __future__ import annotations
 
 import ctypes as C
@@ -54,10 +55,45 @@ class Engine:
         self.classes[key] = (rc, L.nx, L.ny)
         return rc
 
-    def add(self, case: Case, z0=None, cls=None, nsteps=None, gauges=None, arrival_thr=None) -> int:
+    def add_nested_class(self, P, Cl) -> int:
+        """class for outer layer P with child layer Cl (a LayerSpec with parent P)"""
+        key = (id(P.H), id(Cl.H), tuple(Cl.corners), Cl.rel_size, Cl.rel_time)
+        if key in self.classes:
+            return self.classes[key][0]
+        pcls = self.add_class(P)
+        d = _lib.ChildDesc()
+        d.nx, d.ny = Cl.nx, Cl.ny
+        for q in range(4):
+            d.corners[q] = int(Cl.corners[q])
+        d.rel_size, d.rel_time = Cl.rel_size, Cl.rel_time
+        d.laycord, d.laygov, d.linchk, d.modscm, d.fric_switch = (Cl.laycord, Cl.laygov, Cl.linchk, Cl.modscm,
+                                                                  Cl.fric_switch)
+        d.dt, d.rx, d.ry, d.grx, d.gry, d.fric_coef = Cl.dt, Cl.rx, Cl.ry, Cl.grx, Cl.gry, Cl.fric_coef
+        keep = [np.ascontiguousarray(Cl.H, dtype=F32)]
+        d.h = _lib.fptr(keep[0])
+        if Cl.hp is not None and Cl.hq is not None:
+            keep += [np.ascontiguousarray(Cl.hp, dtype=F32), np.ascontiguousarray(Cl.hq, dtype=F32)]
+            d.hp, d.hq = _lib.fptr(keep[1]), _lib.fptr(keep[2])
+        if Cl.coefs is not None:
+            keep.append(np.ascontiguousarray(Cl.coefs.rows(), dtype=F32))
+            d.rows = _lib.fptr(keep[-1])
+        rc = self.lib.gc_engine_add_nested_class(self.h, pcls, C.byref(d))
+        if rc == -2:
+            raise MemoryError("engine budget exhausted")
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_add_nested_class failed: {rc}")
+        self.classes[key] = (rc, P.nx, P.ny)
+        return rc
+
+    def add(self, case: Case, z0=None, cls=None, nsteps=None, gauges=None, arrival_thr=None, child_z0=None) -> int:
+        """adds the case as a member; a two-layer case becomes a nested member.
+        Gauges are (layer_id, KI, KJ, CX, CY) with KI, KJ 1-based in that layer."""
         L = case.root
+        nested = len(case.layers) > 1
+        if len(case.layers) > 2:
+            raise ValueError("the engine runs at most one child layer per member")
         if cls is None:
-            cls = self.add_class(L)
+            cls = self.add_nested_class(L, case.layers[1]) if nested else self.add_class(L)
         z0 = np.ascontiguousarray(L.Z0 if z0 is None else z0, dtype=F32)
         g = case.gauges if gauges is None else gauges
         ng = len(g)
@@ -65,13 +101,23 @@ class Engine:
         gw = np.array([[x[3], x[4]] for x in g] or [[0, 0]], dtype=F32)
         n = case.nsteps if nsteps is None else nsteps
         thr = case.arrival_thr if arrival_thr is None else arrival_thr
-        rc = self.lib.gc_engine_add_member(self.h, cls, _lib.fptr(z0), int(n), ng, _lib.iptr(gij), _lib.fptr(gw),
-                                           C.c_float(thr))
+        if nested:
+            Cl = case.layers[1]
+            gl = np.array([0 if x[0] == L.id else 1 for x in g] or [0], dtype=np.int32)
+            cz = np.ascontiguousarray(Cl.Z0 if child_z0 is None else child_z0, dtype=F32)
+            rc = self.lib.gc_engine_add_nested_member(self.h, cls, _lib.fptr(z0), _lib.fptr(cz), int(n), ng,
+                                                      _lib.iptr(gl), _lib.iptr(gij), _lib.fptr(gw), C.c_float(thr))
+        else:
+            if any(x[0] != L.id for x in g):
+                raise ValueError("gauge on a layer the case does not have")
+            rc = self.lib.gc_engine_add_member(self.h, cls, _lib.fptr(z0), int(n), ng, _lib.iptr(gij),
+                                               _lib.fptr(gw), C.c_float(thr))
         if rc == -2:
             raise MemoryError("engine budget exhausted")
         if rc < 0:
             raise RuntimeError(f"gc_engine_add_member failed: {rc}")
-        self.members[rc] = (L.nx, L.ny, n, ng)
+        child = (case.layers[1].nx, case.layers[1].ny) if nested else None
+        self.members[rc] = (L.nx, L.ny, n, ng, child)
         return rc
 
     def step(self, n: int) -> int:
@@ -88,17 +134,36 @@ class Engine:
     def done(self, mid: int) -> bool:
         return self.lib.gc_engine_member_done(self.h, mid) == 1
 
-    def read(self, mid: int) -> dict:
-        nx, ny, n, ng = self.members[mid]
-        out = {k: np.zeros((ny, nx), F32) for k in ("z", "m", "n", "zmax")}
-        out["arrival"] = np.zeros((ny, nx), np.int32)
-        out["ts"] = np.zeros((n, max(ng, 1)), F32)
-        rc = self.lib.gc_engine_read(self.h, mid, _lib.fptr(out["z"]), _lib.fptr(out["m"]), _lib.fptr(out["n"]),
-                                     _lib.fptr(out["zmax"]), _lib.iptr(out["arrival"]),
-                                     _lib.fptr(out["ts"]) if ng else None)
+    def read(self, mid: int, fields=("z", "m", "n", "zmax", "arrival", "ts")) -> dict:
+        """results of a member (the named fields only); nested members also
+        give child_z/child_m/child_n when "child" is among the fields or the
+        default set is asked for"""
+        nx, ny, n, ng, child = self.members[mid]
+        want = set(fields)
+        out = {}
+        for k in ("z", "m", "n", "zmax"):
+            if k in want:
+                out[k] = np.zeros((ny, nx), F32)
+        if "arrival" in want:
+            out["arrival"] = np.zeros((ny, nx), np.int32)
+        if "ts" in want:
+            out["ts"] = np.zeros((n, max(ng, 1)), F32)
+        rc = self.lib.gc_engine_read(self.h, mid, _lib.fptr(out.get("z")), _lib.fptr(out.get("m")),
+                                     _lib.fptr(out.get("n")), _lib.fptr(out.get("zmax")),
+                                     _lib.iptr(out.get("arrival")), _lib.fptr(out["ts"]) if ng and "ts" in want
+                                     else None)
         if rc != 0:
             raise RuntimeError(f"gc_engine_read failed: {rc}")
-        out["ts"] = out["ts"][:, :ng]
+        if "ts" in out:
+            out["ts"] = out["ts"][:, :ng]
+        if child is not None and ("child" in want or "z" in want):
+            cnx, cny = child
+            for k in ("child_z", "child_m", "child_n"):
+                out[k] = np.zeros((cny, cnx), F32)
+            rc = self.lib.gc_engine_read_child(self.h, mid, _lib.fptr(out["child_z"]), _lib.fptr(out["child_m"]),
+                                               _lib.fptr(out["child_n"]))
+            if rc != 0:
+                raise RuntimeError(f"gc_engine_read_child failed: {rc}")
         return out
 
     def release(self, mid: int):

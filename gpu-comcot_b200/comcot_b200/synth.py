@@ -303,3 +303,57 @@ def poisson_trace(n=400, rate=2.0, seed=5, sizes=((481, 401), (961, 801), (1921,
         nsteps = int(round(minutes * 60.0 / dt))
         out.append((t, sz, nsteps, bool(rng.uniform() < nested_frac), int(rng.integers(0, 2 ** 31))))
     return out
+
+
+C5_SIZES = ((481, 401), (961, 801), (1921, 1601))
+
+
+def config_c5_templates(seed=50, sizes=C5_SIZES, dt=2.0):
+    """C5 grid classes: per outer size, a 2' linear spherical grid with an
+    east-side shelf and, under it, a 301x251 nonlinear Cartesian child at
+    ratio 5 (60 x 50 outer cells); un-nested requests of that size use the
+    outer grid alone."""
+    out = {}
+    for k, (nx, ny) in enumerate(sizes):
+        is_ = nx - 90
+        js = ny // 2 - 25
+        t = nested_case(f"C5t{nx}", nx, ny, 2.0, dt, [is_, is_ + 59, js, js + 49], 5, 0, seed=seed + k,
+                        n_seamounts=max(10, nx // 40))
+        out[(nx, ny)] = t
+    return out
+
+
+def child_wet_gauges(Cl: LayerSpec, n, rng):
+    out = []
+    tries = 0
+    while len(out) < n and tries < 100000:
+        tries += 1
+        i = int(rng.integers(3, Cl.nx - 3))
+        j = int(rng.integers(3, Cl.ny - 3))
+        if Cl.H[j, i] <= 5.0:
+            continue
+        x0 = float(Cl.x[i] + (Cl.x[i + 1] - Cl.x[i]) * rng.uniform(0.1, 0.9))
+        y0 = float(Cl.y[j] + (Cl.y[j + 1] - Cl.y[j]) * rng.uniform(0.1, 0.9))
+        ki, kj, cx, cy = pc.locate_gauge(Cl.x, Cl.y, x0, y0, first=2)
+        out.append((Cl.id, ki, kj, float(cx), float(cy)))
+    return out
+
+
+def c5_request_case(templates, size, nsteps, nested, seed, ngauges=16, child_gauges=4):
+    """one C5 forecast request: its own seeded dipole (amplitude U(0.5,5) m,
+    strike U(0,360)) in the western half of the outer grid and 16 gauges
+    (4 of them in the child when nested).  Layers are shared with the
+    template; only Z0 and the gauges are the request's own."""
+    t = templates[size]
+    P = t.layers[0]
+    rng = np.random.default_rng(seed)
+    lon_c = float(rng.uniform(P.x[P.nx // 8], P.x[P.nx // 2]))
+    lat_c = float(rng.uniform(P.y[P.ny // 4], P.y[3 * P.ny // 4]))
+    z0 = dipole(P.x, P.y, lon_c, lat_c, float(rng.uniform(0.5, 5.0)), float(rng.uniform(0.0, 360.0)))
+    Pr = LayerSpec(**{**P.__dict__, "Z0": z0})
+    layers = [Pr] + (list(t.layers[1:]) if nested else [])
+    case = Case(f"req{seed}", layers, nsteps)
+    ng_child = child_gauges if nested else 0
+    case.gauges = wet_gauges(P, ngauges - ng_child, rng) + (child_wet_gauges(t.layers[1], ng_child, rng)
+                                                           if nested else [])
+    return case

@@ -18,6 +18,17 @@
  * Member storage is taken with the stream-ordered allocator, so admitting a
  * request never waits for work in flight.  Admission is bounded by an HBM
  * budget counted by this engine.
+ *
+ * Nested members (an outer linear-spherical grid with one child layer, the
+ * ALL_GRID sub-cycle of all_grids.f90:4-312) step with the per-phase kernels
+ * in the order of comcot.f90:359-439: mass, open, the child's rel_time
+ * sub-steps (edge fluxes, mass, momentum, JNZ at the half step, UPDATE),
+ * momentum, then the step's outputs.  Each nested member's chain runs on its
+ * own forked stream, so the chains overlap one another and the fused launch
+ * of the single-grid members; in a captured chunk the fork and join become
+ * graph edges.  Their ping-pong parities are fixed when a chunk is captured,
+ * so chunks hold an even number of steps and a replay starts at the parity
+ * of the capture.
  */
 #include <string.h>
 
@@ -32,7 +43,17 @@ namespace {
 struct EngClass {
     int nx, ny, pitch;
     float *d_h = nullptr, *d_rows = nullptr;
+    void *block = nullptr; /* storage this class owns */
     size_t bytes = 0;
+    /* nested class: the outer grid of class `parent_cls` plus one child layer */
+    bool nested = false;
+    int parent_cls = -1;
+    int cnx = 0, cny = 0, cpitch = 0;
+    int corners[4] = {0, 0, 0, 0};
+    int rel_size = 1, rel_time = 1;
+    int laycord = 1, laygov = 1, linchk = 1, modscm = 1, fric_switch = 1;
+    float dt = 0, rx = 0, ry = 0, grx = 0, gry = 0, fric_coef = 0;
+    float *d_ch = nullptr, *d_chp = nullptr, *d_chq = nullptr, *d_crows = nullptr;
 };
 
 struct EngMember {
@@ -44,12 +65,50 @@ struct EngMember {
     float *z[2] = {nullptr, nullptr}, *m[2] = {nullptr, nullptr}, *n[2] = {nullptr, nullptr};
     float *zmax = nullptr, *ts = nullptr, *gw = nullptr;
     int *arrival = nullptr, *gij = nullptr;
+    /* nested members: the child's levels, DZ, the outer grid's NEWQ caches */
+    bool nested = false;
+    float *cz[2] = {nullptr, nullptr}, *cm[2] = {nullptr, nullptr}, *cn[2] = {nullptr, nullptr};
+    float *cdz2 = nullptr, *xflux = nullptr, *yflux = nullptr;
+    int *glayer = nullptr;
+    /* the last global step this member needs a launch at: single-grid
+     * members sample their last gauges in the launch after their last step */
+    int last_step() const { return nested ? step0 + nsteps - 1 : step0 + nsteps; }
 };
 
 size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 __global__ void k_advance(int *step, int by) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *step += by;
+}
+
+constexpr int kMaxAux = 8; /* forked streams for nested members */
+
+GcLayerDev outer_view(const EngClass &C, const EngMember &M, int cur) {
+    GcLayerDev d;
+    memset(&d, 0, sizeof d);
+    d.nx = C.nx; d.ny = C.ny; d.pitch = C.pitch;
+    d.root = 1; d.laycord = 0; d.laygov = 0; d.linchk = 1; d.modscm = 1; d.fric_switch = 1;
+    d.z1 = M.z[cur]; d.m1 = M.m[cur]; d.n1 = M.n[cur];
+    d.z1w = M.z[cur]; d.m1w = M.m[cur]; d.n1w = M.n[cur];
+    d.z2 = M.z[cur ^ 1]; d.m2 = M.m[cur ^ 1]; d.n2 = M.n[cur ^ 1];
+    d.h = C.d_h; d.rows = C.d_rows;
+    d.xflux = M.xflux; d.yflux = M.yflux;
+    d.zmax = M.zmax; d.arrival = M.arrival;
+    return d;
+}
+
+GcLayerDev child_view(const EngClass &C, const EngMember &M, int cur) {
+    GcLayerDev d;
+    memset(&d, 0, sizeof d);
+    d.nx = C.cnx; d.ny = C.cny; d.pitch = C.cpitch;
+    d.root = 0; d.laycord = C.laycord; d.laygov = C.laygov; d.linchk = C.linchk; d.modscm = C.modscm;
+    d.fric_switch = C.fric_switch;
+    d.rx = C.rx; d.ry = C.ry; d.grx = C.grx; d.gry = C.gry; d.dt = C.dt; d.fric_coef = C.fric_coef;
+    d.z1 = M.cz[cur]; d.m1 = M.cm[cur]; d.n1 = M.cn[cur];
+    d.z1w = M.cz[cur]; d.m1w = M.cm[cur]; d.n1w = M.cn[cur];
+    d.z2 = M.cz[cur ^ 1]; d.m2 = M.cm[cur ^ 1]; d.n2 = M.cn[cur ^ 1];
+    d.h = C.d_ch; d.hp = C.d_chp; d.hq = C.d_chq; d.rows = C.d_crows; d.dz2 = M.cdz2;
+    return d;
 }
 
 } // namespace
@@ -72,15 +131,104 @@ struct gc_engine {
     cudaGraphExec_t gexec = nullptr;
     long long launches = 0;
     int nctas = 0;
+    long long chunk_launches = 0; /* kernels in one replay of the chunk graph */
+    std::vector<int> nested_ids; /* active nested members */
+    cudaStream_t aux[kMaxAux] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kMaxAux] = {};
 };
+
+/* one outer step of a nested member whose 0-based step index is `local`
+ * (parities) and whose device step number is step_off + *d_base */
+static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_base, int step_off,
+                            cudaStream_t s) {
+    const EngClass &C = e->classes[M.cls];
+    const GcLayerDev P = outer_view(C, M, local & 1);
+    gc_launch_mass(P, s);
+    gc_launch_open(P, s);
+    int cc = (int)(((long long)local * C.rel_time) & 1);
+    const int nhalf = C.rel_time / 2 + 1;
+    for (int t = 1; t <= C.rel_time; t++) {
+        const GcLayerDev Cv = child_view(C, M, cc);
+        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
+        gc_launch_mass(Cv, s);
+        gc_launch_moment(Cv, s);
+        if (t == nhalf) { gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
+        gc_launch_update_edges(Cv, s);
+        cc ^= 1;
+        e->launches += 4;
+    }
+    gc_launch_moment(P, s);
+    const int flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
+    gc_launch_step_outputs(P, d_base, step_off, M.step0, flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc],
+                           C.cpitch, M.ts, M.nsteps, s);
+    e->launches += 4;
+}
+
+/* issues `count` consecutive steps, the first being host step e->gstep + 1
+ * and device step step_off0 + *d_base: the fused launch over the single-grid
+ * members on the engine stream, each nested member's chain on a forked
+ * stream, joined back before return */
+static cudaError_t eng_launch_steps(gc_engine *e, const int *d_base, int step_off0, int count) {
+    const int nn = (int)e->nested_ids.size();
+    const int naux = std::min(nn, kMaxAux);
+    if (naux > 0) {
+        cudaError_t err = cudaEventRecord(e->ev_fork, e->stream);
+        if (err != cudaSuccess) return err;
+        for (int a = 0; a < naux; a++) {
+            err = cudaStreamWaitEvent(e->aux[a], e->ev_fork, 0);
+            if (err != cudaSuccess) return err;
+        }
+    }
+    if (e->ntiles > 0) {
+        for (int k = 0; k < count; k++) {
+            cudaError_t err = gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, d_base,
+                                                    step_off0 + k, e->nctas, e->stream);
+            if (err != cudaSuccess) return err;
+            e->launches++;
+        }
+    }
+    for (int q = 0; q < nn; q++) {
+        EngMember &M = e->members[e->nested_ids[q]];
+        cudaStream_t s = e->aux[q % naux];
+        for (int k = 0; k < count; k++)
+            eng_nested_step(e, M, e->gstep + 1 + k - M.step0, d_base, step_off0 + k, s);
+    }
+    if (naux > 0) {
+        for (int a = 0; a < naux; a++) {
+            cudaError_t err = cudaEventRecord(e->ev_join[a], e->aux[a]);
+            if (err != cudaSuccess) return err;
+            err = cudaStreamWaitEvent(e->stream, e->ev_join[a], 0);
+            if (err != cudaSuccess) return err;
+        }
+    }
+    return cudaGetLastError();
+}
+
+/* forked streams and their events for up to kMaxAux nested chains; made
+ * here, outside any stream capture */
+static int eng_make_aux(gc_engine *e, int naux) {
+    if (naux > 0 && !e->ev_fork) GC_CUDA_OR_RET(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    for (int a = 0; a < naux && a < kMaxAux; a++) {
+        if (e->aux[a]) continue;
+        GC_CUDA_OR_RET(cudaStreamCreateWithFlags(&e->aux[a], cudaStreamNonBlocking));
+        GC_CUDA_OR_RET(cudaEventCreateWithFlags(&e->ev_join[a], cudaEventDisableTiming));
+    }
+    return GC_OK;
+}
 
 static int eng_rebuild(gc_engine *e) {
     std::vector<GcFusedGrid> grids;
     std::vector<int2> tiles;
     /* one tile height for the whole work list, chosen to fill whole waves */
     std::vector<int> anx, any;
-    for (auto &M : e->members)
-        if (M.used && !M.done) { anx.push_back(e->classes[M.cls].nx); any.push_back(e->classes[M.cls].ny); }
+    e->nested_ids.clear();
+    for (size_t k = 0; k < e->members.size(); k++) {
+        EngMember &M = e->members[k];
+        if (!M.used || M.done) continue;
+        if (M.nested) { e->nested_ids.push_back((int)k); continue; }
+        anx.push_back(e->classes[M.cls].nx);
+        any.push_back(e->classes[M.cls].ny);
+    }
     const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data());
     /* active members grouped by class */
     for (size_t c = 0; c < e->classes.size(); c++) {
@@ -88,7 +236,7 @@ static int eng_rebuild(gc_engine *e) {
         std::vector<int> idx;
         for (size_t k = 0; k < e->members.size(); k++) {
             EngMember &M = e->members[k];
-            if (!M.used || M.done || M.cls != (int)c) continue;
+            if (!M.used || M.done || M.nested || M.cls != (int)c) continue;
             idx.push_back((int)grids.size());
             GcFusedGrid g;
             memset(&g, 0, sizeof g);
@@ -104,10 +252,12 @@ static int eng_rebuild(gc_engine *e) {
             g.ng = M.ng; g.gij = M.gij; g.gw = M.gw; g.ts = M.ts; g.ts_len = M.nsteps;
             grids.push_back(g);
         }
+        if (idx.empty()) continue;
         int nt = gc_fused_tiles(C.nx, C.ny, ty, nullptr);
         for (int t = 0; t < nt; t++)
             for (int g : idx) tiles.push_back(make_int2(g, t));
     }
+    if (eng_make_aux(e, (int)e->nested_ids.size()) != GC_OK) return GC_ECUDA;
     e->ngrids = (int)grids.size();
     e->ntiles = (int)tiles.size();
     if (e->ngrids > e->grids_cap) {
@@ -136,7 +286,7 @@ static int eng_rebuild(gc_engine *e) {
 /* retire members whose last gauge sample has been issued */
 static void eng_retire(gc_engine *e) {
     for (auto &M : e->members)
-        if (M.used && !M.done && e->gstep >= M.step0 + M.nsteps) {
+        if (M.used && !M.done && e->gstep >= M.last_step()) {
             M.done = true;
             e->dirty = true;
         }
@@ -147,36 +297,36 @@ static int eng_issue(gc_engine *e, int nsteps) {
     while (issued < nsteps) {
         eng_retire(e);
         if (e->dirty && eng_rebuild(e) != GC_OK) return GC_ECUDA;
-        if (e->ntiles == 0) break;
+        if (e->ntiles == 0 && e->nested_ids.empty()) break;
         /* steps until the next member finishes: the member set is constant */
         int horizon = nsteps - issued;
         for (auto &M : e->members)
-            if (M.used && !M.done) horizon = std::min(horizon, M.step0 + M.nsteps - e->gstep);
+            if (M.used && !M.done) horizon = std::min(horizon, M.last_step() - e->gstep);
         if (horizon <= 0) horizon = 1;
         if (e->use_graphs && horizon >= e->chunk) {
+            /* the device counter must equal the host's step count */
+            GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_step, &e->gstep, sizeof(int), cudaMemcpyHostToDevice, e->stream));
             if (!e->gexec) {
-                GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_step, &e->gstep, sizeof(int), cudaMemcpyHostToDevice,
-                                               e->stream));
                 cudaGraph_t graph;
+                long long before = e->launches;
                 GC_CUDA_OR_RET(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-                for (int k = 1; k <= e->chunk; k++)
-                    gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, e->d_step, k,
-                                          e->nctas, e->stream);
-                k_advance<<<1, 32, 0, e->stream>>>(e->d_step, e->chunk);
-                GC_CUDA_OR_RET(cudaStreamEndCapture(e->stream, &graph));
+                cudaError_t lerr = eng_launch_steps(e, e->d_step, 1, e->chunk);
+                if (lerr == cudaSuccess)
+                    k_advance<<<1, 32, 0, e->stream>>>(e->d_step, e->chunk);
+                cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
+                GC_CUDA_OR_RET(lerr);
+                GC_CUDA_OR_RET(cerr);
+                e->chunk_launches = e->launches - before + 1; /* + k_advance */
+                e->launches = before;
                 GC_CUDA_OR_RET(cudaGraphInstantiate(&e->gexec, graph, 0));
                 cudaGraphDestroy(graph);
-            } else {
-                /* the device counter must equal the host's step count */
-                GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_step, &e->gstep, sizeof(int), cudaMemcpyHostToDevice,
-                                               e->stream));
             }
             int reps = horizon / e->chunk;
             if (reps * e->chunk > nsteps - issued) reps = (nsteps - issued) / e->chunk;
             if (reps <= 0) reps = 0;
             for (int r = 0; r < reps; r++) {
                 GC_CUDA_OR_RET(cudaGraphLaunch(e->gexec, e->stream));
-                e->launches += e->chunk;
+                e->launches += e->chunk_launches;
             }
             e->gstep += reps * e->chunk;
             issued += reps * e->chunk;
@@ -184,11 +334,8 @@ static int eng_issue(gc_engine *e, int nsteps) {
         }
         int n = std::min(horizon, nsteps - issued);
         for (int k = 0; k < n; k++) {
-            cudaError_t err = gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, nullptr,
-                                                    e->gstep + 1, e->nctas, e->stream);
-            if (err != cudaSuccess) return GC_ECUDA;
+            if (eng_launch_steps(e, nullptr, e->gstep + 1, 1) != cudaSuccess) return GC_ECUDA;
             e->gstep++;
-            e->launches++;
         }
         issued += n;
     }
@@ -230,13 +377,17 @@ int gc_engine_destroy(gc_engine *e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     for (auto &M : e->members)
         if (M.block) cudaFreeAsync(M.block, e->stream);
-    for (auto &C : e->classes) {
-        if (C.d_h) cudaFreeAsync(C.d_h, e->stream);
-    }
+    for (auto &C : e->classes)
+        if (C.block) cudaFreeAsync(C.block, e->stream);
     if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
     if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
     if (e->d_step) cudaFreeAsync(e->d_step, e->stream);
     cudaStreamSynchronize(e->stream);
+    for (int a = 0; a < kMaxAux; a++) {
+        if (e->aux[a]) cudaStreamDestroy(e->aux[a]);
+        if (e->ev_join[a]) cudaEventDestroy(e->ev_join[a]);
+    }
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     cudaStreamDestroy(e->stream);
     delete e;
     return GC_OK;
@@ -252,6 +403,7 @@ int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const floa
     if (e->in_use + (long long)C.bytes > e->budget) return GC_ENOMEM;
     void *blk = nullptr;
     GC_CUDA_OR_RET(cudaMallocAsync(&blk, C.bytes, e->stream));
+    C.block = blk;
     C.d_h = (float *)blk;
     C.d_rows = (float *)((char *)blk + field);
     GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_h, (size_t)C.pitch * sizeof(float), H, (size_t)nx * sizeof(float),
@@ -267,30 +419,43 @@ int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const floa
     return (int)e->classes.size() - 1;
 }
 
-long long gc_engine_member_bytes(gc_engine *e, int cls) {
-    if (!e || cls < 0 || cls >= (int)e->classes.size()) return GC_EINVAL;
-    EngClass &C = e->classes[cls];
-    size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
-    return (long long)(8 * field);
-}
+} /* extern "C" */
 
-int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int ngauges, const int *gij,
-                         const float *gw, float arrival_thr) {
-    if (!e || cls < 0 || cls >= (int)e->classes.size() || !z0 || nsteps < 1 || ngauges < 0) return GC_EINVAL;
-    if (ngauges > 0 && (!gij || !gw)) return GC_EINVAL;
-    EngClass &C = e->classes[cls];
-    for (int g = 0; g < ngauges; g++)
-        if (gij[2 * g] < 1 || gij[2 * g + 1] < 1 || gij[2 * g] >= C.nx || gij[2 * g + 1] >= C.ny) return GC_EINVAL;
+static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges) {
     size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
     size_t tsb = a256((size_t)nsteps * ngauges * sizeof(float));
     size_t gb = a256((size_t)2 * ngauges * sizeof(int)) + a256((size_t)2 * ngauges * sizeof(float));
     size_t bytes = 8 * field + tsb + gb;
+    if (C.nested) {
+        size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
+        bytes += 7 * cfield + a256((size_t)2 * C.nx * sizeof(float)) + a256((size_t)2 * C.ny * sizeof(float))
+                 + a256((size_t)ngauges * sizeof(int));
+    }
+    return bytes;
+}
+
+static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *cz0, int nsteps, int ngauges,
+                          const int *glayer, const int *gij, const float *gw, float arrival_thr) {
+    if (!e || cls < 0 || cls >= (int)e->classes.size() || !z0 || nsteps < 1 || ngauges < 0) return GC_EINVAL;
+    if (ngauges > 0 && (!gij || !gw)) return GC_EINVAL;
+    EngClass &C = e->classes[cls];
+    for (int g = 0; g < ngauges; g++) {
+        const bool child = glayer && glayer[g] != 0;
+        if (child && !C.nested) return GC_EINVAL;
+        if (glayer && (glayer[g] < 0 || glayer[g] > 1)) return GC_EINVAL;
+        const int nx = child ? C.cnx : C.nx, ny = child ? C.cny : C.ny;
+        if (gij[2 * g] < 1 || gij[2 * g + 1] < 1 || gij[2 * g] >= nx || gij[2 * g + 1] >= ny) return GC_EINVAL;
+    }
+    size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
+    size_t tsb = a256((size_t)nsteps * ngauges * sizeof(float));
+    size_t bytes = eng_member_bytes(C, nsteps, ngauges);
     if (e->in_use + (long long)bytes > e->budget) return GC_ENOMEM;
     EngMember M;
     M.used = true;
     M.cls = cls; M.nsteps = nsteps; M.ng = ngauges; M.thr = arrival_thr;
     M.step0 = e->gstep + 1;
     M.bytes = bytes;
+    M.nested = C.nested;
     GC_CUDA_OR_RET(cudaMallocAsync(&M.block, bytes, e->stream));
     char *p = (char *)M.block;
     for (int q = 0; q < 2; q++) {
@@ -302,7 +467,7 @@ int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int
     M.arrival = (int *)p; p += field;
     M.ts = (float *)p; p += tsb;
     M.gij = (int *)p; p += a256((size_t)2 * ngauges * sizeof(int));
-    M.gw = (float *)p;
+    M.gw = (float *)p; p += a256((size_t)2 * ngauges * sizeof(float));
     GC_CUDA_OR_RET(cudaMemsetAsync(M.block, 0, 6 * field, e->stream));
     GC_CUDA_OR_RET(cudaMemsetAsync(M.arrival, 0xff, field, e->stream));
     GC_CUDA_OR_RET(cudaMemcpy2DAsync(M.z[0], (size_t)C.pitch * sizeof(float), z0, (size_t)C.nx * sizeof(float),
@@ -314,6 +479,33 @@ int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int
         GC_CUDA_OR_RET(cudaMemcpyAsync(M.gw, gw, (size_t)2 * ngauges * sizeof(float), cudaMemcpyHostToDevice,
                                        e->stream));
     }
+    if (C.nested) {
+        size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
+        char *c0 = p;
+        for (int q = 0; q < 2; q++) {
+            M.cz[q] = (float *)p; p += cfield;
+            M.cm[q] = (float *)p; p += cfield;
+            M.cn[q] = (float *)p; p += cfield;
+        }
+        M.cdz2 = (float *)p; p += cfield;
+        M.xflux = (float *)p; p += a256((size_t)2 * C.nx * sizeof(float));
+        M.yflux = (float *)p; p += a256((size_t)2 * C.ny * sizeof(float));
+        M.glayer = (int *)p;
+        GC_CUDA_OR_RET(cudaMemsetAsync(c0, 0, (size_t)(p - c0), e->stream));
+        if (cz0)
+            GC_CUDA_OR_RET(cudaMemcpy2DAsync(M.cz[0], (size_t)C.cpitch * sizeof(float), cz0,
+                                             (size_t)C.cnx * sizeof(float), (size_t)C.cnx * sizeof(float),
+                                             (size_t)C.cny, cudaMemcpyHostToDevice, e->stream));
+        if (ngauges > 0) {
+            std::vector<int> gl((size_t)ngauges, 0);
+            if (glayer)
+                for (int g = 0; g < ngauges; g++) gl[g] = glayer[g];
+            GC_CUDA_OR_RET(cudaMemcpyAsync(M.glayer, gl.data(), gl.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                           e->stream));
+            /* the pageable copy is staged before return, but keep `gl` alive until it ran */
+            GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
+        }
+    }
     e->in_use += (long long)bytes;
     /* reuse a released slot id when there is one */
     int id = -1;
@@ -323,6 +515,95 @@ int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int
     else e->members[id] = M;
     e->dirty = true;
     return id;
+}
+
+extern "C" {
+
+long long gc_engine_member_bytes(gc_engine *e, int cls) {
+    if (!e || cls < 0 || cls >= (int)e->classes.size()) return GC_EINVAL;
+    return (long long)eng_member_bytes(e->classes[cls], 0, 0);
+}
+
+int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int ngauges, const int *gij,
+                         const float *gw, float arrival_thr) {
+    return eng_add_member(e, cls, z0, nullptr, nsteps, ngauges, nullptr, gij, gw, arrival_thr);
+}
+
+int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const float *child_z0, int nsteps,
+                                int ngauges, const int *glayer, const int *gij, const float *gw,
+                                float arrival_thr) {
+    return eng_add_member(e, cls, z0, child_z0, nsteps, ngauges, glayer, gij, gw, arrival_thr);
+}
+
+int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc *d) {
+    if (!e || !d || parent_cls < 0 || parent_cls >= (int)e->classes.size()) return GC_EINVAL;
+    const EngClass &Pc = e->classes[parent_cls];
+    if (Pc.nested || !d->h) return GC_EINVAL;
+    const int is = d->corners[0], ie = d->corners[1], js = d->corners[2], je = d->corners[3];
+    /* the NEWQ forecast reads outer rows JS-3 and columns IS-3
+     * (all_grids.f90:692-700,765-772), and the edge fluxes reach IE+2 / JE+2 */
+    if (d->rel_size < 1 || d->rel_time < 1 || is < 4 || js < 4 || ie > Pc.nx - 2 || je > Pc.ny - 2 || ie < is
+        || je < js || d->nx != (ie - is + 1) * d->rel_size + 1 || d->ny != (je - js + 1) * d->rel_size + 1)
+        return GC_EINVAL;
+    if ((d->laycord != 0 && d->laycord != 1) || (d->laygov != 0 && d->laygov != 1)) return GC_EINVAL;
+    if (d->laycord == 0 && (d->laygov != 0 || !d->rows)) return GC_ENOTSUP;
+    if (d->fric_switch != 0 && d->fric_switch != 1) return GC_EINVAL;
+    EngClass C = Pc;
+    C.block = nullptr;
+    C.nested = true;
+    C.parent_cls = parent_cls;
+    C.cnx = d->nx; C.cny = d->ny; C.cpitch = (d->nx + 31) & ~31;
+    memcpy(C.corners, d->corners, sizeof C.corners);
+    C.rel_size = d->rel_size; C.rel_time = d->rel_time;
+    C.laycord = d->laycord; C.laygov = d->laygov; C.linchk = d->linchk; C.modscm = d->modscm;
+    C.fric_switch = d->fric_switch;
+    C.dt = d->dt; C.rx = d->rx; C.ry = d->ry; C.grx = d->grx; C.gry = d->gry; C.fric_coef = d->fric_coef;
+    const size_t cells = (size_t)d->nx * d->ny;
+    const size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
+    const size_t rb = a256((size_t)GC_ROWW * C.cny * sizeof(float));
+    C.bytes = 3 * cfield + rb;
+    if (e->in_use + (long long)C.bytes > e->budget) return GC_ENOMEM;
+    /* HP/HQ from the caller, else PQ_DEPTH (initialization.f90:2501-2526) */
+    std::vector<float> hp(cells, 0.0f), hq(cells, 0.0f);
+    if (d->hp && d->hq) {
+        hp.assign(d->hp, d->hp + cells);
+        hq.assign(d->hq, d->hq + cells);
+    } else {
+        for (int j = 0; j < d->ny; j++)
+            for (int i = 0; i < d->nx; i++) {
+                size_t c = (size_t)j * d->nx + i;
+                if (d->h[c] > CC_GX) {
+                    hp[c] = 0.5f * (d->h[c] + d->h[(size_t)j * d->nx + std::min(i + 1, d->nx - 1)]);
+                    hq[c] = 0.5f * (d->h[c] + d->h[(size_t)std::min(j + 1, d->ny - 1) * d->nx + i]);
+                }
+            }
+    }
+    std::vector<float> rec((size_t)GC_ROWW * C.cny, 0.0f);
+    if (d->rows)
+        for (int k = 0; k < GC_NROW; k++)
+            for (int j = 0; j < C.cny; j++) rec[(size_t)j * GC_ROWW + k] = d->rows[(size_t)k * C.cny + j];
+    void *blk = nullptr;
+    GC_CUDA_OR_RET(cudaMallocAsync(&blk, C.bytes, e->stream));
+    C.block = blk;
+    char *p = (char *)blk;
+    C.d_ch = (float *)p; p += cfield;
+    C.d_chp = (float *)p; p += cfield;
+    C.d_chq = (float *)p; p += cfield;
+    C.d_crows = (float *)p;
+    GC_CUDA_OR_RET(cudaMemsetAsync(blk, 0, C.bytes, e->stream));
+    const size_t sp = (size_t)C.cpitch * sizeof(float), hpitch = (size_t)d->nx * sizeof(float);
+    GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_ch, sp, d->h, hpitch, hpitch, (size_t)d->ny, cudaMemcpyHostToDevice,
+                                     e->stream));
+    GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_chp, sp, hp.data(), hpitch, hpitch, (size_t)d->ny,
+                                     cudaMemcpyHostToDevice, e->stream));
+    GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_chq, sp, hq.data(), hpitch, hpitch, (size_t)d->ny,
+                                     cudaMemcpyHostToDevice, e->stream));
+    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_crows, rec.data(), rec.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                   e->stream));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream)); /* the host vectors end here */
+    e->in_use += (long long)C.bytes;
+    e->classes.push_back(C);
+    return (int)e->classes.size() - 1;
 }
 
 int gc_engine_step(gc_engine *e, int nsteps) {
@@ -367,6 +648,24 @@ int gc_engine_read(gc_engine *e, int id, float *z, float *m, float *n, float *zm
     return GC_OK;
 }
 
+int gc_engine_read_child(gc_engine *e, int id, float *z, float *m, float *n) {
+    if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used || !e->members[id].nested)
+        return GC_EINVAL;
+    EngMember &M = e->members[id];
+    EngClass &C = e->classes[M.cls];
+    int done_steps = std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
+    int cur = (int)(((long long)done_steps * C.rel_time) & 1);
+    size_t sp = (size_t)C.cpitch * sizeof(float), dp = (size_t)C.cnx * sizeof(float);
+    auto dl = [&](void *dst, const void *src) {
+        return cudaMemcpy2DAsync(dst, dp, src, sp, dp, (size_t)C.cny, cudaMemcpyDeviceToHost, e->stream);
+    };
+    if (z) GC_CUDA_OR_RET(dl(z, M.cz[cur]));
+    if (m) GC_CUDA_OR_RET(dl(m, M.cm[cur]));
+    if (n) GC_CUDA_OR_RET(dl(n, M.cn[cur]));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
+    return GC_OK;
+}
+
 int gc_engine_release(gc_engine *e, int id) {
     if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used) return GC_EINVAL;
     EngMember &M = e->members[id];
@@ -387,7 +686,8 @@ int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk)
         e->tuned = true;
     }
     e->use_graphs = use_graphs ? 1 : 0;
-    if (graph_chunk > 0) e->chunk = graph_chunk;
+    /* even, so a replayed chunk starts at the ping-pong parity it was captured at */
+    if (graph_chunk > 0) e->chunk = (graph_chunk + 1) & ~1;
     e->dirty = true;
     return GC_OK;
 }

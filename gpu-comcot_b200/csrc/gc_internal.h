@@ -98,6 +98,11 @@ void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int r
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s);
+/* max-eta (flags & 1), arrival (flags & 2) and gauge samples after one outer
+ * step of a batched nested member; step = step_off + *step_base */
+void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
+                            float thr, int ng, const int *gij, const float *gw, const int *glayer,
+                            const float *cz, int cpitch, float *ts, int ts_len, cudaStream_t s);
 
 /* ---- fused step (kernels_fused.cu) ---- */
 struct GcFusedGrid;

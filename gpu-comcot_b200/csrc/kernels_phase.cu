@@ -695,6 +695,44 @@ __global__ void k_gauges(GcLayerDev L, int ng, const int *ij, float *out) {
     out[4 * g + 3] = L.z2[c + L.pitch + 1];
 }
 
+/* outputs of one finished outer step of a batched nested member: running
+ * maximum and arrival step over the outer layer (L.z2 is the new surface)
+ * and the step's gauge samples (GET_TS bilinear weights, output.f90:1078-1090)
+ * from the outer layer or the child (cz, pitch cpitch).  The step number is
+ * step_off + *step_base (step_base may be NULL), so a replayed graph numbers
+ * the steps correctly; step - step0 is the member's 0-based step index. */
+__global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off, int step0, int flags,
+                               float thr, int ng, const int *gij, const float *gw, const int *glayer,
+                               const float *cz, int cpitch, float *ts, int ts_len) {
+    const int local = step_off + (step_base ? *step_base : 0) - step0;
+    if (local < 0 || local >= ts_len) return;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && ng > 0) {
+        for (int g = threadIdx.y * BX + threadIdx.x; g < ng; g += BX * BY) {
+            const bool child = glayer && glayer[g] != 0;
+            const float *z = child ? cz : L.z2;
+            const size_t P = child ? (size_t)cpitch : (size_t)L.pitch;
+            size_t c = (size_t)(gij[2 * g + 1] - 1) * P + (size_t)(gij[2 * g] - 1);
+            float l1 = z[c], l2 = z[c + 1], l3 = z[c + P], l4 = z[c + P + 1];
+            float cx = gw[2 * g], cy = gw[2 * g + 1];
+            float a = l1 * (1.0f - cx) * (1.0f - cy);
+            float b = l2 * (cx) * (1.0f - cy);
+            float d = l3 * (1.0f - cx) * (cy);
+            float e = l4 * (cx) * (cy);
+            ts[(size_t)local * ng + g] = a + b + d + e;
+        }
+    }
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    float z = L.z2[c];
+    if (flags & 1) {
+        float m = L.zmax[c];
+        if (!(m >= z)) L.zmax[c] = z;
+    }
+    if ((flags & 2) && L.arrival[c] < 0 && L.h[c] > CC_GX && z > thr) L.arrival[c] = local + 1;
+}
+
 inline dim3 grid2(const GcLayerDev &L) {
     return dim3((unsigned)((L.nx + BX - 1) / BX), (unsigned)((L.ny + BY - 1) / BY), 1);
 }
@@ -749,4 +787,11 @@ void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s)
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s) {
     if (ng <= 0) return;
     k_gauges<<<(ng + 127) / 128, 128, 0, s>>>(L, ng, d_ij, d_out);
+}
+
+void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
+                            float thr, int ng, const int *gij, const float *gw, const int *glayer,
+                            const float *cz, int cpitch, float *ts, int ts_len, cudaStream_t s) {
+    k_step_outputs<<<grid2(L), dim3(BX, BY), 0, s>>>(L, step_base, step_off, step0, flags, thr, ng, gij, gw,
+                                                     glayer, cz, cpitch, ts, ts_len);
 }

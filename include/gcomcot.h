@@ -116,6 +116,32 @@ int gc_engine_sync(gc_engine *e);
 int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
                    int *arrival, float *ts);
 int gc_engine_release(gc_engine *e, int member);
+
+/* A nested grid class: the outer grid of class `parent_cls` with one child
+ * layer (ALL_GRID sub-cycle, all_grids.f90:4-312; SC_OPTION = 0 coupling).
+ * corners = IS, IE, JS, JE in the outer grid (1-based, at least 4 cells from
+ * its edge); nx = (IE-IS+1)*rel_size+1, ny likewise.  laycord/laygov select
+ * the child's solver: (1,1) CONMASS/CONMOME with wet/dry and Manning
+ * friction, (1,0) MASS_C/MOMT_C, (0,0) MASS_S/MOMT_S (then `rows` is the
+ * child's [7][ny] block).  hp/hq may be NULL (then PQ_DEPTH of h).  Members
+ * of a nested class step with the per-phase kernels. */
+typedef struct {
+    int nx, ny;
+    int corners[4];
+    int rel_size, rel_time;
+    int laycord, laygov, linchk, modscm, fric_switch;
+    float dt, rx, ry, grx, gry, fric_coef;
+    const float *h, *hp, *hq, *rows;
+} gc_child_desc;
+int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc *child);
+/* a member of a nested class: child_z0 may be NULL (still water); gauge g
+ * reads layer glayer[g] (0 outer grid, 1 child; NULL = all outer) at
+ * 1-based gij of that layer */
+int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const float *child_z0, int nsteps,
+                                int ngauges, const int *glayer, const int *gij, const float *gw,
+                                float arrival_thr);
+/* the child's Z, M, N (level 1 after the member's completed steps) */
+int gc_engine_read_child(gc_engine *e, int member, float *z, float *m, float *n);
 long long gc_engine_bytes_in_use(gc_engine *e);
 long long gc_engine_member_bytes(gc_engine *e, int cls);
 /* tile variant (autotuned when < 0) and use of CUDA graphs for step chunks */

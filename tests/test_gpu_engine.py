@@ -63,3 +63,68 @@ def test_engine_budget_refuses():
         assert eng.member_bytes(cls) > (200 << 10) - eng.bytes_in_use()
         with pytest.raises(MemoryError):
             eng.add(c, cls=cls)
+
+
+def _nested(seed, rel_time, nsteps, child_gauges=3):
+    case = synth.nested_case("n", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, nsteps, seed=seed, rel_time=rel_time,
+                             ngauges=3)
+    Cl = case.layers[1]
+    rng = np.random.default_rng(seed + 100)
+    got = 0
+    while got < child_gauges:
+        i = int(rng.integers(3, Cl.nx - 3))
+        j = int(rng.integers(3, Cl.ny - 3))
+        if Cl.H[j, i] <= 5.0:
+            continue
+        x0 = float(Cl.x[i] + 0.4 * (Cl.x[i + 1] - Cl.x[i]))
+        y0 = float(Cl.y[j] + 0.7 * (Cl.y[j + 1] - Cl.y[j]))
+        ki, kj, cx, cy = synth.pc.locate_gauge(Cl.x, Cl.y, x0, y0, first=2)
+        case.gauges.append((Cl.id, ki, kj, float(cx), float(cy)))
+        got += 1
+    return case
+
+
+def _check_nested(got, case, oracle_mod):
+    o = oracle_mod.OracleRun(case)
+    ts = o.run(case.nsteps)
+    ref, rc = o.layer(0), o.layer(1)
+    for k in ("z", "m", "n", "zmax"):
+        assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), k
+    assert np.array_equal(got["arrival"], ref["arrival"])
+    for k in ("z", "m", "n"):
+        assert np.array_equal(got["child_" + k].view(np.uint32), rc[k].view(np.uint32)), "child " + k
+    H = case.layers[1].H
+    assert np.array_equal(got["child_z"] + H > 1e-5, rc["z"] + H > 1e-5)
+    assert np.array_equal(got["ts"].view(np.uint32), ts.view(np.uint32))
+
+
+@pytest.mark.parametrize("rel_time,graphs", [(None, 1), (2, 0), (3, 1)])
+def test_engine_nested_member_matches_oracle(oracle_mod, rel_time, graphs):
+    case = _nested(51, rel_time, 40)
+    with Engine(budget=2 << 30) as eng:
+        eng.config(variant=-1, use_graphs=graphs, chunk=8)
+        mid = eng.add(case)
+        eng.step(45)
+        eng.sync()
+        assert eng.done(mid)
+        _check_nested(eng.read(mid), case, oracle_mod)
+
+
+def test_engine_nested_and_single_members_in_one_mix(oracle_mod):
+    nest = [_nested(61, 2, 34), _nested(62, None, 50)]
+    single = [_case(97, 81, 63, 41), _case(70, 60, 64, 66)]
+    with Engine(budget=2 << 30) as eng:
+        eng.config(variant=-1, use_graphs=1, chunk=6)
+        ids = [eng.add(single[0]), eng.add(nest[0])]
+        eng.step(5)                                  # later arrivals join a running batch
+        ids += [eng.add(nest[1]), eng.add(single[1])]
+        eng.step(80)
+        eng.sync()
+        got = [eng.read(i) for i in ids]
+    _check_nested(got[1], nest[0], oracle_mod)
+    _check_nested(got[2], nest[1], oracle_mod)
+    for g, c in ((got[0], single[0]), (got[3], single[1])):
+        ref, ts = _oracle(c, oracle_mod)
+        for k in ("z", "m", "n", "zmax"):
+            assert np.array_equal(g[k].view(np.uint32), ref[k].view(np.uint32)), k
+        assert np.array_equal(g["ts"].view(np.uint32), ts.view(np.uint32))
