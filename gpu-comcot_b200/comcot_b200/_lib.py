@@ -80,6 +80,7 @@ SIGNATURES = {
     "gc_engine_add_nested_member": (C.c_int, [VP, C.c_int, P_F, P_F, C.c_int, C.c_int, P_I, P_I, P_F,
                                               C.c_float]),
     "gc_engine_read_child": (C.c_int, [VP, C.c_int, P_F, P_F, P_F]),
+    "gcomcot_fused_step_noalloc": (C.c_int, [C.c_int, VP, VP]),
 }
 
 

@@ -152,6 +152,32 @@ long long gc_engine_launches(gc_engine *e);
 /* the cudaStream_t the engine issues its kernels on */
 void *gc_engine_stream(gc_engine *e);
 
+/* ---- one fused step without any allocation (noalloc.cu) ---- */
+
+/* one grid of gcomcot_fused_step_noalloc: device arrays the caller owns,
+ * row-pitched (element (i,j) at p[j*pitch + i], pitch a multiple of 32 floats,
+ * every array 16-byte aligned).  rows is [ny][8]: R1(1,J), R11(1,J), R6(J),
+ * R3(1,J), R5(1,J), CX(J), CY(J), unused -- R2 = CX*max(HP,0), R4 = CY*max(HQ,0). */
+typedef struct {
+    int nx, ny, pitch;
+    const float *z1, *m1, *n1; /* time level 1, read */
+    float *z2, *m2, *n2;       /* time level 2, written */
+    const float *h;            /* still-water depth */
+    const float *rows;         /* per-row coefficient records */
+    float *zmax;               /* running maximum, updated in place; NULL to skip */
+} gc_grid_step_io;
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (codes that own all device memory, pipelines with a fixed reserved
+ * budget, loops where an allocation's device synchronisation is not
+ * acceptable): one outer step (MASS_S + OPEN + MOMT_S + max) of every grid in
+ * one launch on `stream`, with its work list in a fixed array built into the
+ * library (at most 64 grids and 24576 tiles of 128 columns; larger requests
+ * return -1).  Calls share that array: calls that overlap on the GPU race.
+ * The first call on a device does a one-time set-up and should come before any
+ * stream capture.  Returns 0 or a negative status. */
+int gcomcot_fused_step_noalloc(int ngrids, const gc_grid_step_io *grids, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
