@@ -39,9 +39,11 @@ os.environ.setdefault("GCOMCOT_QUIET", "1")  # the JSON line is the only stdout
 
 import numpy as np  # noqa: E402
 
-from comcot_b200 import synth  # noqa: E402
+from comcot_b200 import replicas, synth  # noqa: E402
 
 METRIC = "cell-updates/s"
+WORKLOADS = {"c1": "C1: 361x301 2' linear spherical, Gaussian hump, OPEN, max-eta, dt 2 s",
+             "c2": "C2: 2401x2001 1' linear spherical, OPEN, max-eta, 32 gauges, dt 1 s"}
 FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_CELL = 36  # Z1,M1,N1,H in + Z2,M2,N2 out (28 B) + max-eta read/write (8 B)
 
@@ -154,7 +156,8 @@ def run_reference(args):
     import oracle
 
     threads = os.cpu_count() or 1
-    case = synth.config_c2(nsteps=args.warmup + args.steps)
+    make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
+    case = make_case(nsteps=args.warmup + args.steps)
     o = oracle.OracleRun(case)
     o.run(max(1, min(args.warmup, 3)), threads=threads)
     t0 = time.perf_counter()
@@ -169,7 +172,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus, "steps": k,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "C2: 2401x2001 1' linear spherical, OPEN, max-eta, 32 gauges, dt 1 s"},
+            "config": {"workload": WORKLOADS.get(args.workload, WORKLOADS["c2"])},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
                              "sample": f"{k} outer steps of the full grid (of {args.steps} requested; "
@@ -217,10 +220,7 @@ def run_c4(args, torch, dist, rank, world, local):
     ck = clocks.stop()
     launches = eng.launches() - l0
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.reduce_max(ms, dist, 'cuda')
     cells = L.nx * L.ny
     value_cells = cells * nscen * run_steps * world / (ms * 1e-3)
     scen_per_hour = nscen * world * 3600.0 / (ms * 1e-3)
@@ -307,10 +307,7 @@ def run_c3(args, torch, dist, rank, world, local):
     ck = clocks.stop()
     launches = eng.launches() - l0
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.reduce_max(ms, dist, 'cuda')
     eng.close()
     value = cells * args.steps * world / (ms * 1e-3)
     e2e = None
@@ -390,7 +387,8 @@ def run_c5(args, torch, dist, rank, world, local):
     from comcot_b200.engine import Engine
 
     tpl = synth.config_c5_templates()
-    trace = synth.poisson_trace(n=args.requests, rate=args.rate, seed=5 + rank)
+    # one trace for the whole job; each rank serves its round-robin share
+    trace = replicas.shard(synth.poisson_trace(n=args.requests, rate=args.rate, seed=5), rank, world)
 
     def make_requests():
         return [serving.Request(k, t, synth.c5_request_case(tpl, size, nsteps, nested, seed))
@@ -508,7 +506,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed tile variant (skips the autotuner)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2: the headline single grid; c3: the nested run; c4: the 64-scenario ensemble; "
                          "c5: the forecast-serving load")
     ap.add_argument("--requests", type=int, default=400, help="C5: requests in the trace")
@@ -550,13 +548,23 @@ def main():
     if args.workload == "c5":
         return run_c5(args, torch, dist, rank, world, local)
 
+    return run_single(args, torch, dist, rank, world, local)
+
+
+def run_single(args, torch, dist, rank, world, local):
+    """C1 / C2: one linear spherical grid (value: the engine, device-resident;
+    e2e: the reference C ABI with host buffers; cpu_baseline: the serial oracle)."""
+    from comcot_b200.abi import ReferenceSession
+    from comcot_b200.engine import Engine
+
     tune_reps = 3
     from comcot_b200 import _lib
 
     lib = _lib.load()
-    nvar = 6
+    nvar = 16  # room for the autotuner's steps (the library compiles 8 tile variants)
     total = nvar * (tune_reps + 1) + args.warmup + args.steps + 8
-    case = synth.config_c2(nsteps=total)
+    make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
+    case = make_case(nsteps=total)
     cells = case.root.nx * case.root.ny
 
     # ---------------- device-resident throughput (engine) ----------------
@@ -585,17 +593,14 @@ def main():
         dist.barrier()
     launches = eng.launches() - l0  # fused steps + the graphs' step-counter kernels
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.reduce_max(ms, dist, 'cuda')
     value = cells * args.steps * world / (ms * 1e-3)
     eng.close()
 
     # ---------------- end to end through the reference C ABI ----------------
     e2e = None
     if not args.no_e2e:
-        case_e = synth.config_c2(nsteps=args.steps)
+        case_e = make_case(nsteps=args.steps)
         s = ReferenceSession(case_e, fusion=True, init_layers=False)
         st = torch.cuda.ExternalStream(s.stream())
         a = torch.cuda.Event(enable_timing=True)
@@ -609,10 +614,7 @@ def main():
         b.record(st)
         b.synchronize()
         e2e_ms = a.elapsed_time(b)
-        if dist:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = replicas.reduce_max(e2e_ms, dist, 'cuda')
         nx, ny = case_e.root.nx, case_e.root.ny
         field = nx * ny * 4
         h2d = (9 * field + ny * 4) / args.steps        # H, Z, R1..R5, R2, R4, R11 fields + R6
@@ -633,9 +635,10 @@ def main():
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "C2: 2401x2001 1' linear spherical, OPEN, max-eta, 32 gauges, dt 1 s",
+        "config": {"workload": WORKLOADS[args.workload],
                    "cells": cells, "parallelism": f"replicas x{world}",
-                   "l2": "working set 156 MB per step (8 fields x 19.5 MB) > 126 MB L2; no flush",
+                   "l2": ("working set 156 MB per step (8 fields x 19.5 MB) > 126 MB L2; no flush"
+                          if args.workload == "c2" else "working set 3.5 MB: L2 resident (no flush)"),
                    "tile_variant": variant, "graph_chunk": 64},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -647,7 +650,7 @@ def main():
     if e2e:
         line["e2e"] = e2e
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(synth.config_c2(nsteps=total))
+        line["cpu_baseline"] = cpu_baseline(make_case(nsteps=total))
     if dist:
         dist.barrier()
         dist.destroy_process_group()

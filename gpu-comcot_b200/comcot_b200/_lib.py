@@ -74,6 +74,7 @@ SIGNATURES = {
     "gc_engine_config": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),
     "gc_engine_autotune": (C.c_int, [VP, C.c_int]),
     "gc_engine_variant": (C.c_int, [VP]),
+    "gc_engine_num_variants": (C.c_int, []),
     "gc_engine_launches": (C.c_longlong, [VP]),
     "gc_engine_stream": (VP, [VP]),
     "gc_engine_add_nested_class": (C.c_int, [VP, C.c_int, C.POINTER(ChildDesc)]),
@@ -81,6 +82,7 @@ SIGNATURES = {
                                               C.c_float]),
     "gc_engine_read_child": (C.c_int, [VP, C.c_int, P_F, P_F, P_F]),
     "gcomcot_fused_step_noalloc": (C.c_int, [C.c_int, VP, VP]),
+    "gc_engine_member_health": (C.c_int, [VP, C.c_int, C.c_float]),
 }
 
 

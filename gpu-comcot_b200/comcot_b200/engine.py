@@ -172,6 +172,13 @@ class Engine:
             raise RuntimeError(f"gc_engine_release failed: {rc}")
         self.members.pop(mid, None)
 
+    def health(self, mid: int, bound: float = 100.0) -> int:
+        """0 healthy; bit 0: a NaN/Inf appeared; bit 1: |eta| > bound metres"""
+        rc = self.lib.gc_engine_member_health(self.h, mid, C.c_float(bound))
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_member_health failed: {rc}")
+        return rc
+
     def autotune(self, reps=5) -> int:
         return self.lib.gc_engine_autotune(self.h, int(reps))
 

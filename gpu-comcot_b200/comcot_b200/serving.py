@@ -12,6 +12,14 @@ and write only that member's state.
 
 Time-to-forecast is measured per request from its arrival to the moment its
 products are in host memory.
+
+Failure handling (all on the host; nothing faults a GPU): a request the
+engine refuses as malformed, or one larger than the whole budget, is marked
+"rejected" and the loop goes on; a
+request can be cancelled (``cancel_at`` seconds after its arrival, or
+``cancel(rid)``) and its memory is freed at the next harvest; a finished
+request whose surface held a NaN/Inf or exceeded ``blowup_m`` metres is
+marked "diverged" and its products are not returned as a forecast.
 """
 from __future__ import annotations
 
@@ -32,7 +40,9 @@ class Request:
     t_admit: float = -1.0
     t_done: float = -1.0
     result: dict = field(default_factory=dict)
-
+    cancel_at: float = float("inf")   # seconds after arrival (wall) to cancel it
+    status: str = "pending"           # done | rejected | cancelled | diverged
+    error: str = ""
     t_arrival_wall: float = 0.0
 
     @property
@@ -44,7 +54,7 @@ class ForecastServer:
     """Continuous-batching request loop on one GPU."""
 
     def __init__(self, budget_bytes: int, chunk: int = 32, variant: int = -1, keep_fields=("zmax", "arrival", "ts"),
-                 engine=None):
+                 engine=None, blowup_m: float = 100.0):
         """engine: an object with Engine's add/step/sync/done/read/release
         (default: a new Engine with this budget)"""
         self.eng = engine if engine is not None else Engine(budget=budget_bytes)
@@ -54,6 +64,9 @@ class ForecastServer:
         self.keep = keep_fields
         self.max_active = 0
         self.refused = 0      # admission attempts that found no room
+        self.blowup_m = blowup_m
+        self.idle_retries = 20   # refusals with nothing running before a request is rejected
+        self._cancel = set()
 
     def close(self):
         self.eng.close()
@@ -64,19 +77,33 @@ class ForecastServer:
     def __exit__(self, *a):
         self.close()
 
+    def cancel(self, rid: int):
+        """cancels request rid (waiting or running) at the next harvest"""
+        self._cancel.add(rid)
+
     def _try_admit(self, r: Request) -> bool:
+        """True when the request left the queue (admitted or rejected)"""
         try:
             mid = self.eng.add(r.case)
         except MemoryError:
             self.refused += 1
             return False
+        except (RuntimeError, ValueError) as exc:
+            r.status, r.error = "rejected", str(exc)
+            return True
         r._mid = mid
+        r.status = "running"
         return True
 
     def _harvest(self, r: Request):
-        out = self.eng.read(r._mid, fields=self.keep)
+        h = self.eng.health(r._mid, self.blowup_m)
+        if h:
+            r.status = "diverged"
+            r.error = ("non-finite surface" if h & 1 else "") + (" |eta| above %g m" % self.blowup_m if h & 2 else "")
+        else:
+            r.result = self.eng.read(r._mid, fields=self.keep)
+            r.status = "done"
         self.eng.release(r._mid)
-        r.result = out
 
     def serve(self, requests, speed: float = 1.0, clock=time.perf_counter):
         """Runs the trace.  Request k arrives t_arrival / speed wall seconds
@@ -87,27 +114,50 @@ class ForecastServer:
         pending = deque(sorted(requests, key=lambda r: r.t_arrival_wall))
         waiting: deque = deque()
         active = []
+        idle_refusals = 0
         t0 = clock()
         while pending or waiting or active:
             t = clock() - t0
             while pending and pending[0].t_arrival_wall <= t:
                 waiting.append(pending.popleft())
+            # cancellations of queued requests
+            for r in list(waiting):
+                if r.rid in self._cancel or t >= r.t_arrival_wall + r.cancel_at:
+                    waiting.remove(r)
+                    r.status, r.t_done = "cancelled", t
             while waiting and self._try_admit(waiting[0]):
                 r = waiting.popleft()
                 r.t_admit = clock() - t0
-                active.append(r)
+                idle_refusals = 0
+                if r.status == "rejected":
+                    r.t_done = r.t_admit
+                else:
+                    active.append(r)
             self.max_active = max(self.max_active, len(active))
             if not active:
                 if waiting:
-                    raise RuntimeError(f"request {waiting[0].rid} does not fit the engine budget alone")
+                    # nothing runs, so nothing will free memory: retry a few times
+                    # (an allocator can refuse transiently), then give the head up
+                    idle_refusals += 1
+                    if idle_refusals > self.idle_retries:
+                        r = waiting.popleft()
+                        r.status, r.error, r.t_done = "rejected", "does not fit the HBM budget", clock() - t0
+                        idle_refusals = 0
+                    else:
+                        time.sleep(0.001)
+                    continue
                 if pending:
                     time.sleep(max(0.0, min(0.002, pending[0].t_arrival_wall - (clock() - t0))))
                 continue
             self.eng.step(self.chunk)
             self.eng.sync()
             still = []
+            t = clock() - t0
             for r in active:
-                if self.eng.done(r._mid):
+                if r.rid in self._cancel or t >= r.t_arrival_wall + r.cancel_at:
+                    self.eng.release(r._mid)
+                    r.status, r.t_done = "cancelled", clock() - t0
+                elif self.eng.done(r._mid):
                     self._harvest(r)
                     r.t_done = clock() - t0
                 else:

@@ -200,9 +200,10 @@ def config_c2(nsteps=7200, ngauges=32):
 
 
 def nested_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel_time=None,
-                n_seamounts=40, fric=0.025, lon0=140.0, lat0=20.0, child_laygov=1, ngauges=0):
-    """Linear spherical parent with one Cartesian child (nonlinear by default)
-    over an east-side shelf window."""
+                n_seamounts=40, fric=0.025, lon0=140.0, lat0=20.0, child_laygov=1, ngauges=0, child_laycord=1):
+    """Linear spherical parent with one child over an east-side shelf window:
+    Cartesian (nonlinear by default, linear with child_laygov=0) or, with
+    child_laycord=0, linear spherical (the reference GPU path's only kind)."""
     rng = np.random.default_rng(seed)
     x, y = pc.axes(lon0, lat0, pnx, pny, dx_min)
     is_, ie, js, je = corners
@@ -245,6 +246,17 @@ def nested_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel
     if rel_time is not None:
         rt, dtc = rel_time, float(F32(dt) / F32(rel_time))
     Zc = dipole(cxd, cyd, lon_c, lat_c, 2.0, 0.0) * 0.0
+    if child_laycord == 0:
+        sx, sy = pc.child_axes_spherical(x, y, corners, rel_size, dx_min)
+        rt, dtc = pc.rel_time(dt, dxm, dym, float(Hc.max()), nonlinear=False)
+        if rel_time is not None:
+            rt, dtc = rel_time, float(F32(dt) / F32(rel_time))
+        C = spherical_layer(2, sx, sy, Hc, np.zeros_like(Hc), dtc, dx_min / rel_size, parent=1, level=2)
+        C.rel_size, C.rel_time, C.corners = rel_size, rt, list(corners)
+        case = Case(name, [P, C], nsteps)
+        if ngauges:
+            case.gauges = wet_gauges(P, ngauges, rng)
+        return case
     rx, ry = F32(dtc) / F32(dxm), F32(dtc) / F32(dym)
     C = LayerSpec(id=2, parent=1, level=2, nx=cnx, ny=cny, H=Hc, Z0=Zc.astype(np.float32), x=cxd, y=cyd,
                   dt=dtc, dx=dxm, dy=dym, laycord=1, laygov=child_laygov, rel_size=rel_size, rel_time=rt,

@@ -70,6 +70,7 @@ struct EngMember {
     float *cz[2] = {nullptr, nullptr}, *cm[2] = {nullptr, nullptr}, *cn[2] = {nullptr, nullptr};
     float *cdz2 = nullptr, *xflux = nullptr, *yflux = nullptr;
     int *glayer = nullptr;
+    int fty = 16; /* tile height of the outer grid's fused launch */
     /* the last global step this member needs a launch at: single-grid
      * members sample their last gauges in the launch after their last step */
     int last_step() const { return nested ? step0 + nsteps - 1 : step0 + nsteps; }
@@ -82,6 +83,21 @@ __global__ void k_advance(int *step, int by) {
 }
 
 constexpr int kMaxAux = 8; /* forked streams for nested members */
+
+/* health of one field: bit 0 = a NaN or Inf, bit 1 = |value| > bound */
+__global__ void k_health(const float *a, int nx, int ny, int pitch, float bound, int *flag) {
+    int bits = 0;
+    const long long n = (long long)nx * ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / nx), i = (int)(k - (long long)j * nx);
+        const float v = a[(size_t)j * pitch + i];
+        if (!isfinite(v)) bits |= 1;
+        else if (fabsf(v) > bound) bits |= 2;
+    }
+    bits = __reduce_or_sync(0xffffffffu, bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicOr(flag, bits);
+}
 
 GcLayerDev outer_view(const EngClass &C, const EngMember &M, int cur) {
     GcLayerDev d;
@@ -118,7 +134,7 @@ struct gc_engine {
     cudaStream_t stream = nullptr;
     std::vector<EngClass> classes;
     std::vector<EngMember> members;
-    int variant = 1;
+    int variant = 15; /* until tuned: the fastest single-grid variant on B200 */
     bool tuned = false;
     int use_graphs = 1, chunk = 32;
     int gstep = 0; /* steps issued */
@@ -132,19 +148,50 @@ struct gc_engine {
     long long launches = 0;
     int nctas = 0;
     long long chunk_launches = 0; /* kernels in one replay of the chunk graph */
+    int *d_health = nullptr;      /* one int for gc_engine_member_health */
     std::vector<int> nested_ids; /* active nested members */
     cudaStream_t aux[kMaxAux] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxAux] = {};
 };
 
-/* one outer step of a nested member whose 0-based step index is `local`
- * (parities) and whose device step number is step_off + *d_base */
+/* One outer step of a nested member whose 0-based step index is `local`
+ * (it fixes the ping-pong parities) and whose device step number is
+ * step_off + *d_base.
+ *
+ * The outer grid takes its whole step (MASS_S + OPEN + MOMT_S) in one fused
+ * launch before the child runs, and its momentum is then recomputed where
+ * JNZ changed the surface.  That gives the bits of the reference order
+ * (mass, open, child sub-cycle with JNZ, momentum): JNZ writes the outer
+ * Z(:,:,2) only inside IS..IE x JS..JE (all_grids.f90:378-411); outer M at
+ * (I,J) reads Z(I,J) and Z(I+1,J), N reads Z(I,J) and Z(I,J+1), and both
+ * read otherwise only level-1 fields, which nothing in the sub-cycle
+ * writes; so only M on [IS-1,IE] x [JS,JE] and N on [IS,IE] x [JS-1,JE] can
+ * differ, and the rectangle [IS-1,IE] x [JS-1,JE] is recomputed.  The child
+ * reads the outer Z(:,:,2), M(:,:,1) and N(:,:,1) only.  Max-eta, arrival
+ * and gauges follow in the outputs kernel, after the feedback. */
 static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_base, int step_off,
                             cudaStream_t s) {
     const EngClass &C = e->classes[M.cls];
-    const GcLayerDev P = outer_view(C, M, local & 1);
-    gc_launch_mass(P, s);
-    gc_launch_open(P, s);
+    const int cur = local & 1;
+    GcFusedGrid g;
+    memset(&g, 0, sizeof g);
+    g.nx = C.nx; g.ny = C.ny; g.pitch = C.pitch; g.root = 1; g.explicit_r24 = 0;
+    g.ty = M.fty;
+    gc_fused_tiles(C.nx, C.ny, g.ty, &g.tiles_x);
+    /* the fused launch records max-eta and arrival outside the JNZ window
+     * (IS..IE x JS..JE, 0-based IS-1..IE-1); the outputs kernel does the window */
+    const int win[4] = {C.corners[0] - 1, C.corners[1] - 1, C.corners[2] - 1, C.corners[3] - 1};
+    const int flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
+    /* the step number comes from the device counter (arrival steps); the
+     * member's level-1 buffer is 0 at its first step, so the kernel's parity
+     * equals `cur` */
+    g.step0 = M.step0; g.cur0 = 0; g.nsteps = M.nsteps; g.flags = flags; g.thr = M.thr;
+    g.has_win = 1; g.wi0 = win[0]; g.wi1 = win[1]; g.wj0 = win[2]; g.wj1 = win[3];
+    for (int q = 0; q < 2; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
+    g.h = C.d_h; g.rows = C.d_rows;
+    g.zmax = M.zmax; g.arrival = M.arrival;
+    gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
+    const GcLayerDev P = outer_view(C, M, cur);
     int cc = (int)(((long long)local * C.rel_time) & 1);
     const int nhalf = C.rel_time / 2 + 1;
     for (int t = 1; t <= C.rel_time; t++) {
@@ -157,11 +204,11 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
         cc ^= 1;
         e->launches += 4;
     }
-    gc_launch_moment(P, s);
-    const int flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
+    /* Fortran (IS-1 .. IE, JS-1 .. JE) -> 0-based (IS-2 .. IE-1, JS-2 .. JE-1) */
+    gc_launch_momt_s_window(P, C.corners[0] - 2, C.corners[1] - 1, C.corners[2] - 2, C.corners[3] - 1, s);
     gc_launch_step_outputs(P, d_base, step_off, M.step0, flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc],
-                           C.cpitch, M.ts, M.nsteps, s);
-    e->launches += 4;
+                           C.cpitch, M.ts, M.nsteps, win, s);
+    e->launches += 3;
 }
 
 /* issues `count` consecutive steps, the first being host step e->gstep + 1
@@ -258,6 +305,11 @@ static int eng_rebuild(gc_engine *e) {
             for (int g : idx) tiles.push_back(make_int2(g, t));
     }
     if (eng_make_aux(e, (int)e->nested_ids.size()) != GC_OK) return GC_ECUDA;
+    /* the outer grid of a nested member is stepped alone on its own stream */
+    for (int id : e->nested_ids) {
+        EngMember &M = e->members[id];
+        M.fty = gc_fused_pick_ty(e->variant, 1, &e->classes[M.cls].nx, &e->classes[M.cls].ny);
+    }
     e->ngrids = (int)grids.size();
     e->ntiles = (int)tiles.size();
     if (e->ngrids > e->grids_cap) {
@@ -333,10 +385,8 @@ static int eng_issue(gc_engine *e, int nsteps) {
             if (reps > 0) continue;
         }
         int n = std::min(horizon, nsteps - issued);
-        for (int k = 0; k < n; k++) {
-            if (eng_launch_steps(e, nullptr, e->gstep + 1, 1) != cudaSuccess) return GC_ECUDA;
-            e->gstep++;
-        }
+        if (eng_launch_steps(e, nullptr, e->gstep + 1, n) != cudaSuccess) return GC_ECUDA;
+        e->gstep += n;
         issued += n;
     }
     eng_retire(e);
@@ -382,6 +432,7 @@ int gc_engine_destroy(gc_engine *e) {
     if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
     if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
     if (e->d_step) cudaFreeAsync(e->d_step, e->stream);
+    if (e->d_health) cudaFreeAsync(e->d_health, e->stream);
     cudaStreamSynchronize(e->stream);
     for (int a = 0; a < kMaxAux; a++) {
         if (e->aux[a]) cudaStreamDestroy(e->aux[a]);
@@ -666,6 +717,33 @@ int gc_engine_read_child(gc_engine *e, int id, float *z, float *m, float *n) {
     return GC_OK;
 }
 
+/* Scans the member's max-eta and current surfaces (outer grid and child).
+ * The running maximum keeps a NaN once one appeared, so a NaN or Inf at any
+ * past step shows.  Returns 0 (healthy), a bit set (1: a NaN or Inf,
+ * 2: |eta| above `bound` metres) or a negative status. */
+int gc_engine_member_health(gc_engine *e, int id, float bound) {
+    if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used || !(bound > 0.0f))
+        return GC_EINVAL;
+    EngMember &M = e->members[id];
+    EngClass &C = e->classes[M.cls];
+    if (!e->d_health) GC_CUDA_OR_RET(cudaMallocAsync((void **)&e->d_health, sizeof(int), e->stream));
+    GC_CUDA_OR_RET(cudaMemsetAsync(e->d_health, 0, sizeof(int), e->stream));
+    const int done_steps = std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
+    const int cur = done_steps & 1;
+    k_health<<<256, 256, 0, e->stream>>>(M.zmax, C.nx, C.ny, C.pitch, bound, e->d_health);
+    k_health<<<256, 256, 0, e->stream>>>(M.z[cur], C.nx, C.ny, C.pitch, bound, e->d_health);
+    e->launches += 2;
+    if (M.nested) {
+        const int ccur = (int)(((long long)done_steps * C.rel_time) & 1);
+        k_health<<<64, 256, 0, e->stream>>>(M.cz[ccur], C.cnx, C.cny, C.cpitch, bound, e->d_health);
+        e->launches++;
+    }
+    int h = 0;
+    GC_CUDA_OR_RET(cudaMemcpyAsync(&h, e->d_health, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
+    return h;
+}
+
 int gc_engine_release(gc_engine *e, int id) {
     if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used) return GC_EINVAL;
     EngMember &M = e->members[id];
@@ -727,6 +805,8 @@ int gc_engine_autotune(gc_engine *e, int reps) {
 }
 
 int gc_engine_variant(gc_engine *e) { return e ? e->variant : GC_EINVAL; }
+int gc_engine_num_variants(void) { return gc_fused_num_variants(); }
+
 void *gc_engine_stream(gc_engine *e) { return e ? (void *)e->stream : nullptr; }
 long long gc_engine_launches(gc_engine *e) { return e ? e->launches : GC_EINVAL; }
 

@@ -29,6 +29,10 @@ struct GcFusedGrid {
     const float *gw;    /* [2*ng] (CX, CY) */
     float *ts;
     int ts_len;         /* steps the ts buffer can hold */
+    /* when has_win: cells [wi0,wi1] x [wj0,wj1] (0-based, inclusive) get no
+     * max-eta or arrival update, since a nested child's feedback rewrites
+     * their surface after this launch (zero-filled descriptors have none) */
+    int has_win, wi0, wi1, wj0, wj1;
 };
 
 /* one launch variant: warps per CTA and pipeline stages per warp */
@@ -51,6 +55,9 @@ int gc_fused_max_ctas(int variant);
 int gc_fused_take_error();
 /* single grid, descriptor by value */
 cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s);
+/* single grid at step step_off + *d_step_base (d_step_base may be NULL) */
+cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
+                                   cudaStream_t s);
 int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x);
 
 #endif

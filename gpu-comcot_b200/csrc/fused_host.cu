@@ -12,7 +12,9 @@ static int g_variant = -1;
 int gc_default_variant() {
     if (g_variant >= 0) return g_variant;
     const char *v = getenv("GCOMCOT_FUSED_VARIANT");
-    g_variant = v ? atoi(v) : 0;
+    /* 15: 4 warps x 4 stages, one copy issuer, Z1/max-eta in registers (the
+     * fastest on the 2401x2001 single grid on B200) */
+    g_variant = v ? atoi(v) : 15;
     if (g_variant < 0 || g_variant >= gc_fused_num_variants()) g_variant = 0;
     return g_variant;
 }

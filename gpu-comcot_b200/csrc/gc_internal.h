@@ -90,6 +90,8 @@ const char *gc_status_str(int code);
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_open(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s);
+/* linear spherical momentum over the 0-based cells [i0,i1] x [j0,j1] only */
+void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1, cudaStream_t s);
 void gc_launch_update_edges(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                      const int *corners, int t, cudaStream_t s);
@@ -99,10 +101,11 @@ void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s);
 /* max-eta (flags & 1), arrival (flags & 2) and gauge samples after one outer
- * step of a batched nested member; step = step_off + *step_base */
+ * step of a batched nested member; step = step_off + *step_base; max/arrival
+ * over the 0-based window win = {i0, i1, j0, j1} (NULL: the whole layer) */
 void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
                             float thr, int ng, const int *gij, const float *gw, const int *glayer,
-                            const float *cz, int cpitch, float *ts, int ts_len, cudaStream_t s);
+                            const float *cz, int cpitch, float *ts, int ts_len, const int *win, cudaStream_t s);
 
 /* ---- fused step (kernels_fused.cu) ---- */
 struct GcFusedGrid;

@@ -10,18 +10,23 @@
  *
  * Work decomposition: a warp owns a 128 x TY tile (I x J); lane l owns the
  * four consecutive cells I = i0+4l .. i0+4l+3 and moves them as float4.  The
- * warp marches up the tile's rows keeping rows r-2..r of N, r-1..r of M, H
- * and of the new surface in registers; the I+1 / I-1 neighbours come from
- * the adjacent lane by warp shuffle, and lanes 31 / 0 load the one-column
- * halos.  At row r the warp computes the new surface Z2 of row r (plus the
- * halo column), then the momentum of row r-1, which needs Z2 of rows r-1 and
- * r; the loads of row r+1 are issued before that arithmetic.  No shared
- * memory and no block barrier: warps of a CTA work on independent tiles.
- * The halo row/column of Z2 is recomputed by both neighbouring tiles from the
- * same inputs, bit-identically.  Per cell the
- * kernel streams Z1, M1, N1, H in and Z2, M2, N2 out (28 bytes) plus the
- * 8-byte max-amplitude read/write; R2 and R4 are rebuilt from H and the
- * per-row factors instead of being streamed.
+ * warp marches down the tile's rows.  Each row's M (with a west halo), N, H
+ * and per-row coefficient record arrive by 1-D bulk copies
+ * (cp.async.bulk, completing on an mbarrier) into an S-stage shared-memory
+ * ring private to the warp; Z1 and max-eta are either staged the same way or
+ * loaded straight into registers one row ahead (variant flag FL_ZD).  At row
+ * r the warp computes the new surface Z2 of row r (plus the east halo
+ * column, kept in a two-row shared ring), then the momentum of row r-1,
+ * which needs Z2 of rows r-1 and r; the copies for row r+S-2 are issued as
+ * soon as row r-2's stage is free.  There is no block barrier: warps of a
+ * CTA work on independent tiles.  The halo row/column of Z2 is recomputed by
+ * both neighbouring tiles from the same inputs, bit-identically.
+ *
+ * Per cell the kernel streams Z1, M1, N1, H in and Z2, M2, N2 out (28 bytes)
+ * plus the 8-byte max-amplitude read/write; R2 and R4 are rebuilt from H and
+ * the per-row factors instead of being streamed.  Every pipeline wait is
+ * bounded: a wait that gives up sets g_pipe_error and the warp leaves after
+ * its copies in flight have landed (or a second bounded wait expired).
  *
  * Arithmetic is evaluated in the Fortran order with separately rounded
  * float operations (the library is built with -fmad=false).
@@ -146,17 +151,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int lim
 
 constexpr int WAIT_LIMIT = 1 << 22;
 
+
+/* Variant flags.  FL_ONE: lane 0 issues all of a row's copies after one
+ * proxy fence (else lanes 0..5 issue one field each).  FL_ZD: Z1 and max-eta
+ * are not staged; each lane loads its own float4 of them from global memory
+ * one row ahead into registers (the stage then holds M, N, H and the row
+ * record only, 40 % less shared memory, so more warps fit on an SM). */
+constexpr int FL_ONE = 1, FL_ZD = 2;
+
 /* one pipeline stage holds one grid row of a warp tile (byte offsets) */
-constexpr int ST_M = 0;                /* M: 136 floats, cols i0-4 .. i0+131 (index c+4) */
-constexpr int ST_N = ST_M + 136 * 4;   /* N: 132 floats, cols i0 .. i0+131 */
-constexpr int ST_H = ST_N + 132 * 4;
-constexpr int ST_Z = ST_H + 132 * 4;   /* Z1 */
-constexpr int ST_X = ST_Z + 132 * 4;   /* max-eta, 128 floats */
-constexpr int ST_C = ST_X + 128 * 4;   /* row coefficient record, 8 floats */
-constexpr int STAGE_BYTES = ((ST_C + 32) + 127) / 128 * 128;
+template <int FL>
+struct Stage {
+    static constexpr int M = 0;                 /* M: 136 floats, cols i0-4 .. i0+131 (index c+4) */
+    static constexpr int N = M + 136 * 4;       /* N: 132 floats, cols i0 .. i0+131 */
+    static constexpr int H = N + 132 * 4;
+    static constexpr int Z = H + 132 * 4;       /* Z1 (staged variants) */
+    static constexpr int X = Z + ((FL & FL_ZD) ? 0 : 132 * 4);   /* max-eta, 128 floats */
+    static constexpr int C = X + ((FL & FL_ZD) ? 0 : 128 * 4);   /* row coefficient record, 8 floats */
+    static constexpr int BYTES = ((C + 32) + 127) / 128 * 128;
+};
 constexpr int ZR_FLOATS = 136;         /* new-surface ring row: cols i0 .. i0+128 */
 
-__host__ __device__ constexpr int warp_smem_bytes(int S) { return ((S * STAGE_BYTES + 2 * ZR_FLOATS * 4 + S * 8) + 127) / 128 * 128; }
+template <int FL>
+__host__ __device__ constexpr int warp_smem_bytes(int S) {
+    return ((S * Stage<FL>::BYTES + 2 * ZR_FLOATS * 4 + S * 8) + 127) / 128 * 128;
+}
 
 enum { F_M = 1, F_N = 2, F_H = 4, F_Z = 8, F_X = 16, F_C = 32 };
 
@@ -175,8 +194,12 @@ __device__ __forceinline__ void st4p(float *p, int i, int nx, const float v[4]) 
     }
 }
 
-template <int S, bool XR24>
+template <int S, bool XR24, int FL>
 __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int step, char *wsm, int &seq) {
+    using ST = Stage<FL>;
+    constexpr bool ZD = (FL & FL_ZD) != 0;
+    constexpr bool ONE = (FL & FL_ONE) != 0;
+    constexpr int SB_ = ST::BYTES;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     /* descriptor fields in registers (stores could alias a descriptor in global memory) */
@@ -202,8 +225,10 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     const int txi = lt % tiles_x, tyi = lt / tiles_x;
     const int i0 = txi * TXW, j0 = tyi * TY;
 
-    /* gauges: sample the surface the previous step left (its Z2 is our Z1) */
-    if (lt == 0 && Gref.ng > 0) {
+    /* gauges: the tile holding a gauge's base cell (KI,KJ) samples the surface
+     * the previous step left (its Z2 is our Z1); the 2x2 stencil reaches at
+     * most into the east / south neighbour tiles, finished with that step */
+    if (Gref.ng > 0) {
         const int ng = Gref.ng;
         int prev = local - 1;
         if (prev >= 0 && prev < Gref.ts_len) {
@@ -212,6 +237,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
             float *ts = Gref.ts;
             for (int g = lane; g < ng; g += 32) {
                 int ki = gij[2 * g] - 1, kj = gij[2 * g + 1] - 1;
+                if (ki < i0 || ki >= i0 + TXW || kj < j0 || kj >= j0 + TY) continue;
                 size_t c = (size_t)kj * P + ki;
                 float l1 = z1[c], l2 = z1[c + 1], l3 = z1[c + P], l4 = z1[c + P + 1];
                 float cx = gw[2 * g], cy = gw[2 * g + 1];
@@ -230,44 +256,62 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     const int K = 1 + min(TY + 1, ny - j0);
     const int jr0 = j0 > 0 ? j0 - 1 : 0;
     const uint32_t wbase = smem_u32(wsm);
-    const uint32_t bars = wbase + S * STAGE_BYTES + 2 * ZR_FLOATS * 4;
-    float *zr = reinterpret_cast<float *>(wsm + S * STAGE_BYTES);
+    const uint32_t bars = wbase + S * SB_ + 2 * ZR_FLOATS * 4;
+    float *zr = reinterpret_cast<float *>(wsm + S * SB_);
     const int seq0 = seq;
 
-    /* lanes 0..5 each own one field's copy: M, N, H, Z1, max-eta, coefficients;
-     * source column, byte count and stage offset are fixed for the tile */
+    /* copies of one row: M (with a 4-column west halo), N, H[, Z1, max-eta]
+     * and the row record; source columns and byte counts are fixed per tile */
+    const int ms = i0 >= 4 ? i0 - 4 : 0;
+    const uint32_t bm = 4u * (i0 >= 4 ? min(136, pitch - ms) : min(132, pitch));
+    const uint32_t bn = 4u * min(132, pitch - i0), bx = 4u * min(128, pitch - i0);
+    const uint32_t m_dst = ST::M + (i0 >= 4 ? 0 : 16);
+    const int mk_pro = F_N | F_H | F_C;
+    const int mk_halo = F_M | F_N | F_H | F_C | (ZD ? 0 : F_Z);
+    const int mk_mid = mk_halo | ((!ZD && do_max) ? F_X : 0);
+    const uint32_t by_pro = 2 * bn + 32u, by_halo = bm + (ZD ? 2 : 3) * bn + 32u;
+    const uint32_t by_mid = by_halo + ((!ZD && do_max) ? bx : 0u);
+    /* per-lane issuer (lanes 0..5 own one field each) */
     const char *cp_src = nullptr;
     size_t cp_stride = P * 4;
     uint32_t cp_dst = 0, cp_bytes = 0;
     int cp_bit = 0;
-    const int ms = i0 >= 4 ? i0 - 4 : 0;
-    const uint32_t bm = 4u * (i0 >= 4 ? min(136, pitch - ms) : min(132, pitch));
-    const uint32_t bn = 4u * min(132, pitch - i0), bx = 4u * min(128, pitch - i0);
-    if (lane == 0) { cp_src = (const char *)(m1 + ms); cp_dst = ST_M + (i0 >= 4 ? 0 : 16); cp_bytes = bm; cp_bit = F_M; }
-    if (lane == 1) { cp_src = (const char *)(n1 + i0); cp_dst = ST_N; cp_bytes = bn; cp_bit = F_N; }
-    if (lane == 2) { cp_src = (const char *)(Gref.h + i0); cp_dst = ST_H; cp_bytes = bn; cp_bit = F_H; }
-    if (lane == 3) { cp_src = (const char *)(z1 + i0); cp_dst = ST_Z; cp_bytes = bn; cp_bit = F_Z; }
-    if (lane == 4) { cp_src = (const char *)(zmax + i0); cp_dst = ST_X; cp_bytes = bx; cp_bit = F_X; }
-    if (lane == 5) { cp_src = (const char *)Gref.rows; cp_dst = ST_C; cp_bytes = 32u; cp_bit = F_C; cp_stride = GC_ROWW * 4; }
-    /* the three row kinds: the row above the tile, owned rows, the halo row below */
-    const int mk_pro = F_N | F_H | F_C;
-    const int mk_halo = F_M | F_N | F_H | F_Z | F_C;
-    const int mk_mid = mk_halo | (do_max ? F_X : 0);
-    const uint32_t by_pro = 2 * bn + 32u, by_halo = bm + 3 * bn + 32u;
-    const uint32_t by_mid = by_halo + (do_max ? bx : 0u);
+    if (!ONE) {
+        if (lane == 0) { cp_src = (const char *)(m1 + ms); cp_dst = m_dst; cp_bytes = bm; cp_bit = F_M; }
+        if (lane == 1) { cp_src = (const char *)(n1 + i0); cp_dst = ST::N; cp_bytes = bn; cp_bit = F_N; }
+        if (lane == 2) { cp_src = (const char *)(Gref.h + i0); cp_dst = ST::H; cp_bytes = bn; cp_bit = F_H; }
+        if (!ZD && lane == 3) { cp_src = (const char *)(z1 + i0); cp_dst = ST::Z; cp_bytes = bn; cp_bit = F_Z; }
+        if (!ZD && lane == 4) { cp_src = (const char *)(zmax + i0); cp_dst = ST::X; cp_bytes = bx; cp_bit = F_X; }
+        if (lane == 5) { cp_src = (const char *)Gref.rows; cp_dst = ST::C; cp_bytes = 32u; cp_bit = F_C; cp_stride = GC_ROWW * 4; }
+    }
     auto issue = [&](int k, int st) {
         const int mask = k == 0 ? mk_pro : (k <= TY ? mk_mid : mk_halo);
         const uint32_t bytes = k == 0 ? by_pro : (k <= TY ? by_mid : by_halo);
         const int jr = k == 0 ? jr0 : j0 + k - 1;
         const uint32_t bar = bars + 8 * st;
-        if (lane == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(bar, bytes);
-        }
-        __syncwarp();
-        if (cp_bit & mask) {
-            fence_proxy_async(); /* this stage's earlier generic reads come first */
-            bulk_g2s(wbase + st * STAGE_BYTES + cp_dst, cp_src + (size_t)jr * cp_stride, cp_bytes, bar);
+        const uint32_t sb = wbase + st * SB_;
+        if constexpr (ONE) {
+            if (lane == 0) {
+                fence_proxy_async(); /* the warp's earlier reads of this stage come first */
+                mbar_expect_tx(bar, bytes);
+                const size_t ro = (size_t)jr * P;
+                if (mask & F_M) bulk_g2s(sb + m_dst, m1 + ms + ro, bm, bar);
+                bulk_g2s(sb + ST::N, n1 + i0 + ro, bn, bar);
+                bulk_g2s(sb + ST::H, Gref.h + i0 + ro, bn, bar);
+                if (!ZD && (mask & F_Z)) bulk_g2s(sb + ST::Z, z1 + i0 + ro, bn, bar);
+                if (!ZD && (mask & F_X)) bulk_g2s(sb + ST::X, zmax + i0 + ro, bx, bar);
+                bulk_g2s(sb + ST::C, Gref.rows + (size_t)jr * GC_ROWW, 32u, bar);
+            }
+        } else {
+            if (lane == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(bar, bytes);
+            }
+            __syncwarp();
+            if (cp_bit & mask) {
+                fence_proxy_async(); /* this stage's earlier generic reads come first */
+                bulk_g2s(sb + cp_dst, cp_src + (size_t)jr * cp_stride, cp_bytes, bar);
+            }
         }
     };
     __syncwarp();
@@ -286,12 +330,27 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     /* stages and phase parities tracked incrementally: row k+1 follows row k */
     int stB = seq0 % S, stC = 0;
     uint32_t parB = (uint32_t)((seq0 / S) & 1);
-    bool ok = wait(stB, parB);
     const int c0 = 4 * lane;             /* this lane's first cell within the tile */
     const int ib = i0 + c0;
     const bool own = ib < nx;
     const int ih = i0 + TXW;
     const bool hasR = (lane == 31) && (ih < nx);
+    /* unstaged Z1 / max-eta: this lane's float4 of row r, loaded one row ahead */
+    float4 zq = make_float4(0.f, 0.f, 0.f, 0.f), xq = zq;
+    float zqh = 0.0f;
+    auto load_direct = [&](int k, float4 &zo, float4 &xo, float &zh) {
+        if constexpr (ZD) {
+            const int rr = j0 + k - 1;
+            if (k < K) {
+                const size_t ro = (size_t)rr * P;
+                if (own) zo = __ldg(reinterpret_cast<const float4 *>(z1 + ro + ib));
+                if (hasR) zh = __ldg(z1 + ro + ih);
+                if (own && do_max && k <= TY) xo = *reinterpret_cast<const float4 *>(zmax + ro + ib);
+            }
+        }
+    };
+    load_direct(1, zq, xq, zqh);
+    bool ok = wait(stB, parB);
     /* output row pointers at this lane's first cell: surface/max rows r, flux rows j = r-1 */
     float *z2p = z2 + (size_t)j0 * P + ib;
     float *zxp = zmax + (size_t)j0 * P + ib;
@@ -299,32 +358,49 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     float *n2p = n2 + (size_t)j0 * P + ib;
 
     /* a tile none of whose cells (halo row and column included) lies on a
-     * grid edge runs a body compiled without any boundary logic */
-    const bool edge = !(i0 >= 1 && i0 + TXW <= nx - 2 && j0 >= 1 && j0 + TY <= ny - 2);
+     * grid edge or in the max/arrival exclusion window runs a body compiled
+     * without any boundary logic */
+    const int wi0 = Gref.wi0, wi1 = Gref.wi1, wj0 = Gref.wj0, wj1 = Gref.wj1;
+    const bool inwin = Gref.has_win && i0 <= wi1 && i0 + TXW - 1 >= wi0 && j0 <= wj1 && j0 + TY - 1 >= wj0;
+    const bool edge = inwin || !(i0 >= 1 && i0 + TXW <= nx - 2 && j0 >= 1 && j0 + TY <= ny - 2);
     for (int k = 1; k <= TY + 1 && ok; k++) {
         const int r = j0 + k - 1;
         const bool rv = k < K;
         const int stA = (stB + 1 == S) ? 0 : stB + 1;
         const uint32_t parA = (stA == 0) ? (parB ^ 1u) : parB;
-        float *SA = reinterpret_cast<float *>(wsm + stA * STAGE_BYTES);
-        float *SB = reinterpret_cast<float *>(wsm + stB * STAGE_BYTES);
-        float *SC = reinterpret_cast<float *>(wsm + stC * STAGE_BYTES);
+        float *SA = reinterpret_cast<float *>(wsm + stA * SB_);
+        float *SB = reinterpret_cast<float *>(wsm + stB * SB_);
+        float *SC = reinterpret_cast<float *>(wsm + stC * SB_);
+        /* this row's unstaged values, and the next row's loads in flight */
+        const float4 zcur = zq, xcur = xq;
+        const float zhcur = zqh;
+        load_direct(k + 1, zq, xq, zqh);
         if (rv) {
             ok = wait(stA, parA);
             if (!ok) break;
-            if (i0 == 0 && lane == 0) SA[ST_M / 4 + 3] = SA[ST_M / 4 + 4]; /* IM1 = max(I-1,1) */
+            if (i0 == 0 && lane == 0) SA[ST::M / 4 + 3] = SA[ST::M / 4 + 4]; /* IM1 = max(I-1,1) */
         }
         __syncwarp();
         float *zA = zr + (k & 1) * ZR_FLOATS, *zB = zr + ((k - 1) & 1) * ZR_FLOATS;
         auto body = [&](auto edge_tag) {
             constexpr bool EDGE = decltype(edge_tag)::value;
             if (rv) {
-                const float *mA = SA + ST_M / 4 + 4, *nA = SA + ST_N / 4, *hA = SA + ST_H / 4, *z1A = SA + ST_Z / 4;
-                const float *nB = SB + ST_N / 4, *hB = SB + ST_H / 4;
-                const float r1 = SA[ST_C / 4 + GC_R1], r11 = SA[ST_C / 4 + GC_R11], r6 = SA[ST_C / 4 + GC_R6];
-                const float r6m = (r > 0) ? SB[ST_C / 4 + GC_R6] : 0.0f;
+                const float *mA = SA + ST::M / 4 + 4, *nA = SA + ST::N / 4, *hA = SA + ST::H / 4;
+                const float *nB = SB + ST::N / 4, *hB = SB + ST::H / 4;
+                const float r1 = SA[ST::C / 4 + GC_R1], r11 = SA[ST::C / 4 + GC_R11], r6 = SA[ST::C / 4 + GC_R6];
+                const float r6m = (r > 0) ? SB[ST::C / 4 + GC_R6] : 0.0f;
                 const float4 m4 = lds4(mA + c0), n4 = lds4(nA + c0), nb4 = lds4(nB + c0);
-                const float4 h4 = lds4(hA + c0), hb4 = lds4(hB + c0), z4 = lds4(z1A + c0);
+                const float4 h4 = lds4(hA + c0), hb4 = lds4(hB + c0);
+                float4 z4;
+                float z1h;
+                if constexpr (ZD) {
+                    z4 = zcur;
+                    z1h = zhcur;
+                } else {
+                    const float *z1A = SA + ST::Z / 4;
+                    z4 = lds4(z1A + c0);
+                    z1h = z1A[TXW];
+                }
                 const float mv[4] = {m4.x, m4.y, m4.z, m4.w}, nv[4] = {n4.x, n4.y, n4.z, n4.w};
                 const float nbv[4] = {nb4.x, nb4.y, nb4.z, nb4.w}, hv[4] = {h4.x, h4.y, h4.z, h4.w};
                 const float hbv[4] = {hb4.x, hb4.y, hb4.z, hb4.w}, zv[4] = {z4.x, z4.y, z4.z, z4.w};
@@ -348,11 +424,11 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                 *reinterpret_cast<float4 *>(zA + c0) = make_float4(zn[0], zn[1], zn[2], zn[3]);
                 if (lane == 31 && (!EDGE || hasR)) {
                     if constexpr (EDGE) {
-                        zA[TXW] = z2_cell(root, ih, r, nx, ny, z1A[TXW], hA[TXW], hB[TXW], mA[TXW], mA[TXW - 1],
+                        zA[TXW] = z2_cell(root, ih, r, nx, ny, z1h, hA[TXW], hB[TXW], mA[TXW], mA[TXW - 1],
                                           nA[TXW], nB[TXW], r1, r11, r6, r6m);
                     } else {
                         const float h = hA[TXW];
-                        float zz = z1A[TXW] - r1 * (mA[TXW] - mA[TXW - 1]) - r11 * (nA[TXW] * r6 - nB[TXW] * r6m);
+                        float zz = z1h - r1 * (mA[TXW] - mA[TXW - 1]) - r11 * (nA[TXW] * r6 - nB[TXW] * r6m);
                         zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
                         zz = ((zz + h) <= CC_EPS) ? -h : zz;
                         zA[TXW] = (h > CC_GX) ? zz : 0.0f;
@@ -361,11 +437,20 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                 if (k <= TY && own) {
                     if constexpr (EDGE) st4p(z2p, ib, nx, zn);
                     else *reinterpret_cast<float4 *>(z2p) = make_float4(zn[0], zn[1], zn[2], zn[3]);
+                    /* cells whose surface a child's feedback rewrites later */
+                    bool skip[4] = {false, false, false, false};
+                    if constexpr (EDGE) {
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            skip[q] = inwin && r >= wj0 && r <= wj1 && ib + q >= wi0 && ib + q <= wi1;
+                    }
                     if (do_max) {
-                        const float4 x4 = lds4(SA + ST_X / 4 + c0);
+                        float4 x4;
+                        if constexpr (ZD) x4 = xcur;
+                        else x4 = lds4(SA + ST::X / 4 + c0);
                         float zx[4] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
-                        for (int q = 0; q < 4; q++) zx[q] = (zx[q] >= zn[q]) ? zx[q] : zn[q];
+                        for (int q = 0; q < 4; q++) zx[q] = (zx[q] >= zn[q] || skip[q]) ? zx[q] : zn[q];
                         if constexpr (EDGE) st4p(zxp, ib, nx, zx);
                         else *reinterpret_cast<float4 *>(zxp) = make_float4(zx[0], zx[1], zx[2], zx[3]);
                     }
@@ -374,7 +459,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                         if (zhi > thr) {
 #pragma unroll
                             for (int q = 0; q < 4; q++) {
-                                if (ib + q < nx && zn[q] > thr && hv[q] > CC_GX) {
+                                if (ib + q < nx && zn[q] > thr && hv[q] > CC_GX && !skip[q]) {
                                     int *a = arrival + (size_t)r * P + ib + q;
                                     if (*a < 0) *a = local + 1;
                                 }
@@ -387,11 +472,12 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
             /* momentum of row j = r-1 (MOMT_S, moment.f90:86-145) */
             const int j = r - 1;
             if (k >= 2 && j < ny && own) {
-                const float *mB = SB + ST_M / 4 + 4, *mA = SA + ST_M / 4 + 4;
-                const float *nB = SB + ST_N / 4, *nC = SC + ST_N / 4;
-                const float *hB = SB + ST_H / 4, *hA = SA + ST_H / 4;
-                const float cx = SB[ST_C / 4 + GC_CX], r3 = SB[ST_C / 4 + GC_R3];
-                const float cy = SB[ST_C / 4 + GC_CY], r5 = SB[ST_C / 4 + GC_R5];
+                const float *mB = SB + ST::M / 4 + 4, *mA = SA + ST::M / 4 + 4;
+                const float *nB = SB + ST::N / 4, *nC = SC + ST::N / 4;
+                const float *hB = SB + ST::H / 4, *hA = SA + ST::H / 4;
+                float cx = 0.0f, cy = 0.0f;
+                if constexpr (!XR24) { cx = SB[ST::C / 4 + GC_CX]; cy = SB[ST::C / 4 + GC_CY]; }
+                const float r3 = SB[ST::C / 4 + GC_R3], r5 = SB[ST::C / 4 + GC_R5];
                 /* columns c0..c0+4 of H, N(j), N(j-1), Z2(j); c0-1..c0+3 of M(j), M(j+1) */
                 float hb[5], nb[5], nc[5], zb[5], mb[5], ma[5], ha[4], za[4];
                 {
@@ -468,15 +554,15 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     return true;
 }
 
-template <int W, int S, bool MULTI>
+template <int W, int S, int FL, bool MULTI>
 __global__ void __launch_bounds__(32 * W) k_fused(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
                                                    const int2 *__restrict__ tiles, int ntiles,
                                                    const int *__restrict__ step_base, int step_off) {
     extern __shared__ __align__(128) char smem[];
     const int step = step_off + (step_base ? *step_base : 0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    char *wsm = smem + warp * warp_smem_bytes(S);
-    const uint32_t bars = smem_u32(wsm) + S * STAGE_BYTES + 2 * ZR_FLOATS * 4;
+    char *wsm = smem + warp * warp_smem_bytes<FL>(S);
+    const uint32_t bars = smem_u32(wsm) + S * Stage<FL>::BYTES + 2 * ZR_FLOATS * 4;
     if (lane == 0) {
         for (int s = 0; s < S; s++) mbar_init(bars + 8 * s, 1);
         fence_mbar_init();
@@ -488,34 +574,40 @@ __global__ void __launch_bounds__(32 * W) k_fused(GcFusedGrid one, const GcFused
         if (MULTI) {
             const int2 w = tiles[tile];
             const GcFusedGrid &G = grids[w.x];
-            ok = G.explicit_r24 ? warp_tile<S, true>(G, w.y, step, wsm, seq)
-                                : warp_tile<S, false>(G, w.y, step, wsm, seq);
+            ok = G.explicit_r24 ? warp_tile<S, true, FL>(G, w.y, step, wsm, seq)
+                                : warp_tile<S, false, FL>(G, w.y, step, wsm, seq);
         } else {
-            ok = one.explicit_r24 ? warp_tile<S, true>(one, tile, step, wsm, seq)
-                                  : warp_tile<S, false>(one, tile, step, wsm, seq);
+            ok = one.explicit_r24 ? warp_tile<S, true, FL>(one, tile, step, wsm, seq)
+                                  : warp_tile<S, false, FL>(one, tile, step, wsm, seq);
         }
         if (!ok) return;
     }
 }
 
 struct Variant {
-    int w, s;
+    int w, s, fl;
     void (*one)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int);
     void (*multi)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int);
 };
 
-#define GC_VARIANT(W, S) {W, S, k_fused<W, S, false>, k_fused<W, S, true>}
+#define GC_VARIANT(W, S, FL) {W, S, FL, k_fused<W, S, FL, false>, k_fused<W, S, FL, true>}
 const Variant kVariants[] = {
-    GC_VARIANT(4, 6), GC_VARIANT(2, 8), GC_VARIANT(4, 8), GC_VARIANT(8, 5),
-    GC_VARIANT(1, 8), GC_VARIANT(2, 6), GC_VARIANT(4, 5), GC_VARIANT(8, 4),
+    GC_VARIANT(4, 6, 0), GC_VARIANT(2, 8, 0), GC_VARIANT(4, 8, 0), GC_VARIANT(8, 5, 0),
+    GC_VARIANT(1, 8, 0), GC_VARIANT(2, 6, 0), GC_VARIANT(4, 5, 0), GC_VARIANT(8, 4, 0),
+    GC_VARIANT(4, 6, FL_ONE), GC_VARIANT(8, 4, FL_ONE),
+    GC_VARIANT(4, 6, FL_ZD), GC_VARIANT(8, 4, FL_ZD), GC_VARIANT(4, 4, FL_ZD),
+    GC_VARIANT(4, 6, FL_ONE | FL_ZD), GC_VARIANT(8, 4, FL_ONE | FL_ZD), GC_VARIANT(4, 4, FL_ONE | FL_ZD),
 };
 #undef GC_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-int variant_smem(const Variant &v) { return v.w * warp_smem_bytes(v.s); }
+int variant_smem(const Variant &v) {
+    return v.w * ((v.fl & FL_ZD) ? (v.fl & FL_ONE ? warp_smem_bytes<FL_ONE | FL_ZD>(v.s) : warp_smem_bytes<FL_ZD>(v.s))
+                                 : (v.fl & FL_ONE ? warp_smem_bytes<FL_ONE>(v.s) : warp_smem_bytes<0>(v.s)));
+}
 
 void prepare(const Variant &v) {
-    static bool done[16] = {false};
+    static bool done[32] = {false};
     int idx = (int)(&v - kVariants);
     if (done[idx]) return;
     cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
@@ -567,6 +659,17 @@ cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cud
     int ntiles = gc_fused_tiles(g.nx, g.ny, g.ty, nullptr);
     prepare(v);
     v.one<<<(ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s>>>(g, nullptr, nullptr, ntiles, nullptr, step);
+    return cudaGetLastError();
+}
+
+cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
+                                   cudaStream_t s) {
+    if (variant < 0 || variant >= kNumVariants) variant = 0;
+    const Variant &v = kVariants[variant];
+    int ntiles = gc_fused_tiles(g.nx, g.ny, g.ty, nullptr);
+    prepare(v);
+    v.one<<<(ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s>>>(g, nullptr, nullptr, ntiles, d_step_base,
+                                                                        step_off);
     return cudaGetLastError();
 }
 

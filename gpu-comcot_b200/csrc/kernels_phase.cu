@@ -105,10 +105,12 @@ __device__ __forceinline__ float r4_at(const GcLayerDev &L, int i, int j, size_t
     return GC_ROW(L, GC_CY, j) * (0.5f * (h + hq1));
 }
 
-__global__ void k_momt_s(GcLayerDev L) {
-    int i = blockIdx.x * BX + threadIdx.x;
-    int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
+/* over the cells i0 <= i < i0+ni, j0 <= j < j0+nj (the whole layer, or a
+ * window whose level-2 surface changed after the layer's step) */
+__global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
+    int i = i0 + blockIdx.x * BX + threadIdx.x;
+    int j = j0 + blockIdx.y * BY + threadIdx.y;
+    if (i >= i0 + ni || j >= j0 + nj || i >= L.nx || j >= L.ny) return;
     const int P = L.pitch;
     size_t c = (size_t)j * P + i;
     int lo = L.root ? 0 : 1;
@@ -703,7 +705,8 @@ __global__ void k_gauges(GcLayerDev L, int ng, const int *ij, float *out) {
  * the steps correctly; step - step0 is the member's 0-based step index. */
 __global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off, int step0, int flags,
                                float thr, int ng, const int *gij, const float *gw, const int *glayer,
-                               const float *cz, int cpitch, float *ts, int ts_len) {
+                               const float *cz, int cpitch, float *ts, int ts_len, int wi0, int wj0, int wni,
+                               int wnj) {
     const int local = step_off + (step_base ? *step_base : 0) - step0;
     if (local < 0 || local >= ts_len) return;
     if (blockIdx.x == 0 && blockIdx.y == 0 && ng > 0) {
@@ -721,9 +724,9 @@ __global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off,
             ts[(size_t)local * ng + g] = a + b + d + e;
         }
     }
-    int i = blockIdx.x * BX + threadIdx.x;
-    int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
+    int i = wi0 + blockIdx.x * BX + threadIdx.x;
+    int j = wj0 + blockIdx.y * BY + threadIdx.y;
+    if (i >= wi0 + wni || j >= wj0 + wnj || i >= L.nx || j >= L.ny) return;
     size_t c = (size_t)j * L.pitch + i;
     float z = L.z2[c];
     if (flags & 1) {
@@ -746,9 +749,20 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
 }
 
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0) k_momt_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    if (L.laycord == 0) k_momt_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L, 0, 0, L.nx, L.ny);
     else if (L.laygov == 1) k_conmome<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
     else k_momt_c<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+}
+
+void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1, cudaStream_t s) {
+    i0 = i0 < 0 ? 0 : i0;
+    j0 = j0 < 0 ? 0 : j0;
+    i1 = i1 > L.nx - 1 ? L.nx - 1 : i1;
+    j1 = j1 > L.ny - 1 ? L.ny - 1 : j1;
+    if (i1 < i0 || j1 < j0) return;
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
+    dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
+    k_momt_s<<<grid, dim3(BX, BY), 0, s>>>(L, i0, j0, ni, nj);
 }
 
 void gc_launch_open(const GcLayerDev &L, cudaStream_t s) {
@@ -791,7 +805,10 @@ void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out
 
 void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
                             float thr, int ng, const int *gij, const float *gw, const int *glayer,
-                            const float *cz, int cpitch, float *ts, int ts_len, cudaStream_t s) {
-    k_step_outputs<<<grid2(L), dim3(BX, BY), 0, s>>>(L, step_base, step_off, step0, flags, thr, ng, gij, gw,
-                                                     glayer, cz, cpitch, ts, ts_len);
+                            const float *cz, int cpitch, float *ts, int ts_len, const int *win, cudaStream_t s) {
+    int i0 = 0, j0 = 0, ni = L.nx, nj = L.ny;
+    if (win) { i0 = win[0]; ni = win[1] - win[0] + 1; j0 = win[2]; nj = win[3] - win[2] + 1; }
+    dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
+    k_step_outputs<<<grid, dim3(BX, BY), 0, s>>>(L, step_base, step_off, step0, flags, thr, ng, gij, gw, glayer,
+                                                 cz, cpitch, ts, ts_len, i0, j0, ni, nj);
 }

@@ -142,12 +142,18 @@ int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const fl
                                 float arrival_thr);
 /* the child's Z, M, N (level 1 after the member's completed steps) */
 int gc_engine_read_child(gc_engine *e, int member, float *z, float *m, float *n);
+/* no counterpart in the reference (which has no failure detection): scans
+ * the member's max-eta and current surfaces; 0 = healthy, bit 0 = a NaN or
+ * Inf appeared, bit 1 = |eta| exceeded `bound` metres, < 0 = error */
+int gc_engine_member_health(gc_engine *e, int member, float bound);
 long long gc_engine_bytes_in_use(gc_engine *e);
 long long gc_engine_member_bytes(gc_engine *e, int cls);
 /* tile variant (autotuned when < 0) and use of CUDA graphs for step chunks */
 int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk);
 int gc_engine_autotune(gc_engine *e, int reps);
 int gc_engine_variant(gc_engine *e);
+/* number of compiled tile variants (all compute identical results) */
+int gc_engine_num_variants(void);
 long long gc_engine_launches(gc_engine *e);
 /* the cudaStream_t the engine issues its kernels on */
 void *gc_engine_stream(gc_engine *e);

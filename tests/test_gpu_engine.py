@@ -128,3 +128,48 @@ def test_engine_nested_and_single_members_in_one_mix(oracle_mod):
         for k in ("z", "m", "n", "zmax"):
             assert np.array_equal(g[k].view(np.uint32), ref[k].view(np.uint32)), k
         assert np.array_equal(g["ts"].view(np.uint32), ts.view(np.uint32))
+
+
+def test_every_tile_variant_matches_oracle(oracle_mod):
+    """the tile variants (warps, stages, copy issue, staged or direct Z1/max)
+    differ only in data movement: each must give the oracle's bits"""
+    from comcot_b200 import _lib
+
+    nvar = _lib.load().gc_engine_num_variants()
+    assert nvar >= 8
+    cases = [_case(97, 81, 81, 30), _case(130, 70, 82, 30), _case(33, 17, 83, 30), _case(300, 140, 84, 30)]
+    refs = [_oracle(c, oracle_mod) for c in cases]
+    for v in range(nvar):
+        with Engine(budget=1 << 30) as eng:
+            eng.config(variant=v, use_graphs=v % 2, chunk=8)
+            ids = [eng.add(c) for c in cases]
+            eng.step(31)
+            eng.sync()
+            for c, mid, (ref, ts) in zip(cases, ids, refs):
+                got = eng.read(mid)
+                for k in ("z", "m", "n", "zmax"):
+                    assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), (v, c.root.nx, k)
+                assert np.array_equal(got["arrival"], ref["arrival"]), v
+                assert np.array_equal(got["ts"].view(np.uint32), ts.view(np.uint32)), v
+
+
+def test_members_joining_mid_run(oracle_mod):
+    """members of different sizes, start steps and lengths, captured in
+    graphs and stepped eagerly, with the default tile variant"""
+    cases = [_case(257, 129, 91, 75), _case(97, 81, 92, 40), _case(500, 60, 93, 61)]
+    with Engine(budget=1 << 30) as eng:
+        eng.config(variant=15, use_graphs=1, chunk=10)
+        a = eng.add(cases[0])
+        eng.step(13)
+        b = eng.add(cases[1])
+        eng.step(9)
+        c = eng.add(cases[2])
+        eng.step(90)
+        eng.sync()
+        got = [eng.read(i) for i in (a, b, c)]
+    for g, cs in zip(got, cases):
+        ref, ts = _oracle(cs, oracle_mod)
+        for k in ("z", "m", "n", "zmax"):
+            assert np.array_equal(g[k].view(np.uint32), ref[k].view(np.uint32)), (cs.root.nx, k)
+        assert np.array_equal(g["arrival"], ref["arrival"])
+        assert np.array_equal(g["ts"].view(np.uint32), ts.view(np.uint32))

@@ -87,3 +87,18 @@ def test_nested_nonlinear_child(oracle_mod, rel_time):
     assert np.array_equal(cz + H > 1e-5, rc["z"] + H > 1e-5)
     assert np.array_equal(gpu["z"].view(np.uint32), ref["z"].view(np.uint32))
     assert np.array_equal(cz.view(np.uint32), rc["z"].view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["linear_cartesian", "linear_spherical"])
+def test_nested_linear_child(oracle_mod, kind):
+    """MASS_C/MOMT_C (LAYCORD 1, LAYGOV 0) and MASS_S/MOMT_S children"""
+    kw = {"child_laygov": 0} if kind == "linear_cartesian" else {"child_laycord": 0}
+    case = synth.nested_case("l", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 0, seed=5, rel_time=2, **kw)
+    gpu, _, o, _ = _run_both(case, 50, oracle_mod)
+    ref, rc = o.layer(0), o.layer(1)
+    cz, (cm, cn) = gpu["children"][0]
+    assert np.abs(rc["z"]).max() > 0 and np.abs(rc["m"]).max() > 0   # the child saw the wave
+    for a, b, what in ((gpu["z"], ref["z"], "parent eta"), (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"),
+                       (cn, rc["n"], "child N")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what

@@ -10,9 +10,10 @@ from comcot_b200.serving import ForecastServer, Request, fifo_latencies, percent
 
 
 class FakeCase:
-    def __init__(self, nsteps, nbytes):
+    def __init__(self, nsteps, nbytes, bad=0):
         self.nsteps = nsteps
         self.nbytes = nbytes
+        self.bad = bad            # health bits the fake device reports at the end
 
 
 class FakeEngine:
@@ -21,6 +22,7 @@ class FakeEngine:
     def __init__(self, budget, step_seconds=0.0):
         self.budget, self.used = budget, 0
         self.step_seconds = step_seconds
+        self.exhausted = 0        # the next n allocations fail as if the pool were exhausted
         self.members = {}
         self.next_id = 0
         self.log = []
@@ -30,7 +32,10 @@ class FakeEngine:
         pass
 
     def add(self, case):
-        if self.used + case.nbytes > self.budget:
+        if case.nbytes <= 0:
+            raise RuntimeError("gc_engine_add_member failed: -1")
+        if self.used + case.nbytes > self.budget or self.exhausted > 0:
+            self.exhausted = max(0, self.exhausted - 1)
             raise MemoryError
         mid = self.next_id
         self.next_id += 1
@@ -54,6 +59,9 @@ class FakeEngine:
 
     def read(self, mid, fields=()):
         return {"steps_run": self.members[mid][1]}
+
+    def health(self, mid, bound):
+        return self.members[mid][0].bad
 
     def release(self, mid):
         self.used -= self.members[mid][0].nbytes
@@ -82,10 +90,44 @@ def test_admission_by_footprint_and_fifo():
     assert eng.used == 0
 
 
-def test_request_larger_than_budget_is_an_error():
-    srv = ForecastServer(10, engine=FakeEngine(budget=10))
-    with pytest.raises(RuntimeError):
-        srv.serve([Request(0, 0.0, FakeCase(5, 11))], speed=float("inf"))
+def test_oversized_and_malformed_requests_are_rejected_and_the_rest_served():
+    eng = FakeEngine(budget=10)
+    reqs = [Request(0, 0.0, FakeCase(5, 11)), Request(1, 0.0, FakeCase(5, -1)), Request(2, 0.0, FakeCase(5, 4))]
+    ForecastServer(10, engine=eng).serve(reqs, speed=float("inf"))
+    assert [r.status for r in reqs] == ["rejected", "rejected", "done"]
+    assert "budget" in reqs[0].error and reqs[2].result["steps_run"] == 5
+    assert eng.used == 0
+
+
+def test_cancellation_frees_memory_for_waiting_requests():
+    eng = FakeEngine(budget=10, step_seconds=1e-3)
+    long_run = Request(0, 0.0, FakeCase(100000, 8), cancel_at=0.05)
+    queued = Request(1, 0.0, FakeCase(10, 8))
+    never = Request(2, 0.0, FakeCase(10, 8), cancel_at=0.0)
+    srv = ForecastServer(10, chunk=4, engine=eng)
+    srv.serve([long_run, never, queued], speed=float("inf"))
+    assert long_run.status == "cancelled" and never.status == "cancelled"
+    assert queued.status == "done" and queued.t_admit >= long_run.t_done
+    assert eng.used == 0
+
+
+def test_diverged_request_is_not_returned_as_a_forecast():
+    eng = FakeEngine(budget=100)
+    reqs = [Request(0, 0.0, FakeCase(8, 10, bad=1)), Request(1, 0.0, FakeCase(8, 10, bad=2)),
+            Request(2, 0.0, FakeCase(8, 10))]
+    ForecastServer(100, engine=eng).serve(reqs, speed=float("inf"))
+    assert [r.status for r in reqs] == ["diverged", "diverged", "done"]
+    assert reqs[0].result == {} and "non-finite" in reqs[0].error and "above" in reqs[1].error
+
+
+def test_allocator_exhaustion_is_retried_not_fatal():
+    eng = FakeEngine(budget=100, step_seconds=1e-4)
+    eng.exhausted = 3                            # the pool refuses the next three attempts
+    reqs = [Request(0, 0.0, FakeCase(20, 10)), Request(1, 0.0, FakeCase(20, 10))]
+    srv = ForecastServer(100, chunk=2, engine=eng)
+    srv.serve(reqs, speed=float("inf"))
+    assert [r.status for r in reqs] == ["done", "done"]
+    assert srv.refused == 3
 
 
 def test_arrivals_join_a_running_batch():
