@@ -197,7 +197,7 @@ def run_c4(args, torch, dist, rank, world, local):
     srcs = synth.ensemble_sources(L.x, L.y, nscen, seed=40 + rank)
     case = Case("C4", [L], run_steps)
     tune_reps = 2
-    extra = 8 * (tune_reps + 1) + args.warmup
+    extra = 40 * (tune_reps + 1) + args.warmup  # the autotuner's steps (32 candidates)
     eng = Engine(budget=120 << 30)
     eng.config(variant=args.variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
@@ -401,7 +401,7 @@ def run_c5(args, torch, dist, rank, world, local):
         big = [r for r in reqs if r.case.root.nx == 1921 and len(r.case.layers) == 1][:4]
         with Engine(budget=16 << 30) as eng:
             for r in big:
-                eng.add(r.case, nsteps=64)
+                eng.add(r.case, nsteps=200)
             variant = eng.autotune(2)
     budget = int(args.budget_gb * (1 << 30))
     # warm-up: a few requests through the server (module load, first graphs)
@@ -561,7 +561,7 @@ def run_single(args, torch, dist, rank, world, local):
     from comcot_b200 import _lib
 
     lib = _lib.load()
-    nvar = 16  # room for the autotuner's steps (the library compiles 8 tile variants)
+    nvar = 48  # room for the autotuner's steps (16 tile variants x 2 tile-height rules)
     total = nvar * (tune_reps + 1) + args.warmup + args.steps + 8
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)

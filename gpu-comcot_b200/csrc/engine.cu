@@ -148,6 +148,8 @@ struct gc_engine {
     long long launches = 0;
     int nctas = 0;
     long long chunk_launches = 0; /* kernels in one replay of the chunk graph */
+    int pdl = 1;                  /* programmatic dependent launch (GCOMCOT_PDL=0 turns it off) */
+    int ty_rule = 1;              /* tile-height rule (gc_fused_pick_ty), tuned with the variant */
     int *d_health = nullptr;      /* one int for gc_engine_member_health */
     std::vector<int> nested_ids; /* active nested members */
     cudaStream_t aux[kMaxAux] = {};
@@ -215,7 +217,19 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
  * and device step step_off0 + *d_base: the fused launch over the single-grid
  * members on the engine stream, each nested member's chain on a forked
  * stream, joined back before return */
+static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count);
+
+/* the engine's kernels go out with programmatic dependent launch: each one
+ * is scheduled while its predecessor in the stream runs and waits for it on
+ * the device, which hides the launch gap of a chain of short kernels */
 static cudaError_t eng_launch_steps(gc_engine *e, const int *d_base, int step_off0, int count) {
+    gc_set_pdl(e->pdl != 0);
+    cudaError_t err = eng_launch_steps_(e, d_base, step_off0, count);
+    gc_set_pdl(false);
+    return err;
+}
+
+static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count) {
     const int nn = (int)e->nested_ids.size();
     const int naux = std::min(nn, kMaxAux);
     if (naux > 0) {
@@ -276,7 +290,8 @@ static int eng_rebuild(gc_engine *e) {
         anx.push_back(e->classes[M.cls].nx);
         any.push_back(e->classes[M.cls].ny);
     }
-    const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data());
+    const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data(),
+                                                       e->ty_rule);
     /* active members grouped by class */
     for (size_t c = 0; c < e->classes.size(); c++) {
         EngClass &C = e->classes[c];
@@ -308,7 +323,7 @@ static int eng_rebuild(gc_engine *e) {
     /* the outer grid of a nested member is stepped alone on its own stream */
     for (int id : e->nested_ids) {
         EngMember &M = e->members[id];
-        M.fty = gc_fused_pick_ty(e->variant, 1, &e->classes[M.cls].nx, &e->classes[M.cls].ny);
+        M.fty = gc_fused_pick_ty(e->variant, 1, &e->classes[M.cls].nx, &e->classes[M.cls].ny, 1);
     }
     e->ngrids = (int)grids.size();
     e->ntiles = (int)tiles.size();
@@ -417,6 +432,8 @@ int gc_engine_create(long long hbm_budget_bytes, gc_engine **out) {
     }
     const char *v = getenv("GCOMCOT_FUSED_VARIANT");
     if (v) { e->variant = atoi(v); e->tuned = true; }
+    const char *pd = getenv("GCOMCOT_PDL");
+    if (pd && pd[0] == '0') e->pdl = 0;
     *out = e;
     return GC_OK;
 }
@@ -759,8 +776,11 @@ long long gc_engine_bytes_in_use(gc_engine *e) { return e ? e->in_use : GC_EINVA
 int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk) {
     if (!e) return GC_EINVAL;
     if (variant >= 0) {
-        if (variant >= gc_fused_num_variants()) return GC_EINVAL;
-        e->variant = variant;
+        /* variant + num_variants * rule selects a tile-height rule as well */
+        const int nv = gc_fused_num_variants();
+        if (variant >= nv * GC_TY_RULES) return GC_EINVAL;
+        e->variant = variant % nv;
+        e->ty_rule = variant / nv;
         e->tuned = true;
     }
     e->use_graphs = use_graphs ? 1 : 0;
@@ -778,24 +798,28 @@ int gc_engine_autotune(gc_engine *e, int reps) {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    int best = e->variant;
+    int best = e->variant, best_rule = e->ty_rule;
     float best_ms = 3.0e38f;
     int saved_graphs = e->use_graphs;
     e->use_graphs = 0;
     for (int v = 0; v < gc_fused_num_variants(); v++) {
-        e->variant = v;
-        e->dirty = true;
-        if (eng_issue(e, 1) < 0) return GC_ECUDA; /* warm */
-        cudaEventRecord(a, e->stream);
-        int got = eng_issue(e, reps);
-        cudaEventRecord(b, e->stream);
-        cudaEventSynchronize(b);
-        if (got < reps) break;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, a, b);
-        if (ms < best_ms) { best_ms = ms; best = v; }
+        for (int rule = 0; rule < GC_TY_RULES; rule++) {
+            e->variant = v;
+            e->ty_rule = rule;
+            e->dirty = true;
+            if (eng_issue(e, 1) < 0) return GC_ECUDA; /* warm */
+            cudaEventRecord(a, e->stream);
+            int got = eng_issue(e, reps);
+            cudaEventRecord(b, e->stream);
+            cudaEventSynchronize(b);
+            if (got < reps) break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best_ms) { best_ms = ms; best = v; best_rule = rule; }
+        }
     }
     e->variant = best;
+    e->ty_rule = best_rule;
     e->tuned = true;
     e->use_graphs = saved_graphs;
     e->dirty = true;
@@ -804,7 +828,7 @@ int gc_engine_autotune(gc_engine *e, int reps) {
     return best;
 }
 
-int gc_engine_variant(gc_engine *e) { return e ? e->variant : GC_EINVAL; }
+int gc_engine_variant(gc_engine *e) { return e ? e->variant + gc_fused_num_variants() * e->ty_rule : GC_EINVAL; }
 int gc_engine_num_variants(void) { return gc_fused_num_variants(); }
 
 void *gc_engine_stream(gc_engine *e) { return e ? (void *)e->stream : nullptr; }

@@ -42,9 +42,11 @@ struct GcTileCfg {
 
 int gc_fused_num_variants();
 GcTileCfg gc_fused_variant(int v);
-/* rows per tile for a work list of grids (nx[k], ny[k]) that fills whole
- * waves of the variant's resident warps */
-int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny);
+/* rows per tile for a work list of grids (nx[k], ny[k]); rule 0: the
+ * shortest tiles that keep the wave count of 16-row tiles, rule 1: the
+ * height that minimises the busiest warp's rows (the autotuner tries both) */
+constexpr int GC_TY_RULES = 2;
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule = 0);
 /* launches the fused step over a work list: tiles[t] = {grid, tile within
  * that grid}; step = *step_base + step_off (step_base may be NULL) */
 cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles,

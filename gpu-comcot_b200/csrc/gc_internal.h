@@ -87,6 +87,9 @@ const char *gc_status_str(int code);
     } while (0)
 
 /* ---- per-phase kernels (kernels_phase.cu) ---- */
+/* launches from this host thread use programmatic dependent launch */
+void gc_set_pdl(bool on);
+bool gc_pdl_on();
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_open(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s);

@@ -559,6 +559,10 @@ __global__ void __launch_bounds__(32 * W) k_fused(GcFusedGrid one, const GcFused
                                                    const int2 *__restrict__ tiles, int ntiles,
                                                    const int *__restrict__ step_base, int step_off) {
     extern __shared__ __align__(128) char smem[];
+    /* programmatic dependent launch: the previous step's kernel has finished
+     * and its writes are visible past this point (no-op for plain launches) */
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int step = step_off + (step_base ? *step_base : 0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *wsm = smem + warp * warp_smem_bytes<FL>(S);
@@ -619,6 +623,24 @@ void prepare(const Variant &v) {
 
 int gc_fused_num_variants() { return kNumVariants; }
 
+/* ordinary launch, or with programmatic stream serialization when the
+ * calling thread asked for it (gc_set_pdl) */
+static cudaError_t launch_fused(void (*kern)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int),
+                         int ctas, int threads, int smem, cudaStream_t s, const GcFusedGrid &g,
+                         const GcFusedGrid *grids, const int2 *tiles, int ntiles, const int *step_base, int step_off) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = gc_pdl_on() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, g, grids, tiles, ntiles, step_base, step_off);
+}
+
 /* 1 if a pipeline wait in the fused kernel gave up since the last call */
 int gc_fused_take_error() {
     int v = 0, z = 0;
@@ -638,19 +660,38 @@ int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x) {
     return tx * tyn;
 }
 
-int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny) {
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule) {
     const int slots = gc_fused_max_ctas(variant) * gc_fused_variant(variant).warps;
     auto tiles = [&](int ty) {
         long long t = 0;
         for (int g = 0; g < ngrids; g++) t += gc_fused_tiles(nx[g], ny[g], ty, nullptr);
         return t;
     };
-    /* waves at 16 rows per tile; then the shortest tiles that keep that many waves */
-    long long waves = (tiles(16) + slots - 1) / slots;
-    if (waves < 1) waves = 1;
-    for (int ty = 8; ty <= 256; ty++)
-        if (tiles(ty) <= waves * slots) return ty;
-    return 256;
+    if (rule == 0) {
+        /* the number of waves 16-row tiles need, then the shortest tiles
+         * that keep to it (short tiles interleave members' reads of a shared
+         * bathymetry tile closely in time) */
+        long long waves = (tiles(16) + slots - 1) / slots;
+        if (waves < 1) waves = 1;
+        for (int ty = 8; ty <= 256; ty++)
+            if (tiles(ty) <= waves * slots) return ty;
+        return 256;
+    }
+    /* a launch lasts as long as its busiest warp: waves x (rows per tile plus
+     * the row above, the halo row below and about one row of pipeline fill);
+     * the height that minimises it, ties to fewer waves */
+    int best = 16;
+    long long best_cost = -1, best_waves = 0;
+    for (int ty = 4; ty <= 256; ty++) {
+        const long long waves = (tiles(ty) + slots - 1) / slots;
+        const long long cost = waves * (ty + 3);
+        if (best_cost < 0 || cost < best_cost || (cost == best_cost && waves < best_waves)) {
+            best = ty;
+            best_cost = cost;
+            best_waves = waves;
+        }
+    }
+    return best;
 }
 
 cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s) {
@@ -658,8 +699,8 @@ cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cud
     const Variant &v = kVariants[variant];
     int ntiles = gc_fused_tiles(g.nx, g.ny, g.ty, nullptr);
     prepare(v);
-    v.one<<<(ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s>>>(g, nullptr, nullptr, ntiles, nullptr, step);
-    return cudaGetLastError();
+    return launch_fused(v.one, (ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s, g, nullptr, nullptr, ntiles,
+                        nullptr, step);
 }
 
 cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
@@ -668,9 +709,8 @@ cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int 
     const Variant &v = kVariants[variant];
     int ntiles = gc_fused_tiles(g.nx, g.ny, g.ty, nullptr);
     prepare(v);
-    v.one<<<(ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s>>>(g, nullptr, nullptr, ntiles, d_step_base,
-                                                                        step_off);
-    return cudaGetLastError();
+    return launch_fused(v.one, (ntiles + v.w - 1) / v.w, 32 * v.w, variant_smem(v), s, g, nullptr, nullptr, ntiles,
+                        d_step_base, step_off);
 }
 
 int gc_fused_max_ctas(int variant) {
@@ -695,6 +735,6 @@ cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const
     GcFusedGrid dummy;
     memset(&dummy, 0, sizeof dummy);
     prepare(v);
-    v.multi<<<nctas, 32 * v.w, variant_smem(v), s>>>(dummy, d_grids, d_tiles, ntiles, d_step_base, step_off);
-    return cudaGetLastError();
+    return launch_fused(v.multi, nctas, 32 * v.w, variant_smem(v), s, dummy, d_grids, d_tiles, ntiles, d_step_base,
+                        step_off);
 }

@@ -9,6 +9,7 @@
  * to the REAL arithmetic of the reference solvers cited per kernel.
  * Indices are 0-based: Fortran (I,J) = (i+1, j+1).
  */
+#include <utility>
 #include "gc_internal.h"
 
 namespace {
@@ -23,7 +24,18 @@ __device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 /* MASS_S (mass.f90:61-100).  Child edge rows i==0 / j==0 are not computed by
  * the reference; they keep the value of time level 1 (the UPDATE edge copy of
  * all_grids.f90:323-324 made them equal), so they are carried over here. */
+/* Programmatic dependent launch: a kernel launched with it may be scheduled
+ * while its predecessor still runs; griddepcontrol.wait then blocks until
+ * the predecessor has completed and its writes are visible, so it comes
+ * before any global access.  launch_dependents lets the next kernel in the
+ * stream be scheduled early.  Both are no-ops for an ordinary launch. */
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __global__ void k_mass_s(GcLayerDev L) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -53,6 +65,7 @@ __global__ void k_mass_s(GcLayerDev L) {
 /* MASS_C (mass.f90:103-157) and CONMASS (mass.f90:162-224) */
 template <bool NONLIN>
 __global__ void k_mass_c(GcLayerDev L) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -108,6 +121,7 @@ __device__ __forceinline__ float r4_at(const GcLayerDev &L, int i, int j, size_t
 /* over the cells i0 <= i < i0+ni, j0 <= j < j0+nj (the whole layer, or a
  * window whose level-2 surface changed after the layer's step) */
 __global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
+    pdl_enter();
     int i = i0 + blockIdx.x * BX + threadIdx.x;
     int j = j0 + blockIdx.y * BY + threadIdx.y;
     if (i >= i0 + ni || j >= j0 + nj || i >= L.nx || j >= L.ny) return;
@@ -146,6 +160,7 @@ __global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
 /* linear Cartesian momentum (moment.f90:152-277)                    */
 /* ---------------------------------------------------------------- */
 __global__ void k_momt_c(GcLayerDev L) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -263,6 +278,7 @@ __device__ __forceinline__ void wave_breaking(const GcLayerDev &L, size_t c, flo
 }
 
 __global__ void k_conmome(GcLayerDev L) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -520,6 +536,7 @@ __device__ float open_cell(const GcLayerDev &L, int i, int j) {
 
 /* one thread per perimeter cell: index k walks J=1 row, J=NY row, I=1, I=NX */
 __global__ void k_open(GcLayerDev L) {
+    pdl_enter();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int nx = L.nx, ny = L.ny;
     int i, j;
@@ -534,6 +551,7 @@ __global__ void k_open(GcLayerDev L) {
 /* UPDATE edge copy (all_grids.f90:323-324): Z2(1,:) = Z2(2,:), then
  * Z2(:,1) = Z2(:,2), so Z2(1,1) = Z2(2,2). */
 __global__ void k_update_edges(GcLayerDev L) {
+    pdl_enter();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t P = L.pitch;
     if (k < L.ny) {
@@ -555,6 +573,7 @@ constexpr int EDGE_THREADS = 256;
 
 __global__ void k_edges(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is, int ie,
                         int js, int je, int t, int smem_len) {
+    pdl_enter();
     extern __shared__ float prof[];
     const int side = blockIdx.x; /* 0 left(M), 1 right(M), 2 bottom(N), 3 top(N) */
     const bool vert = side < 2;
@@ -642,6 +661,7 @@ __global__ void k_edges(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int i
  * block, summed in the Fortran order (KI outer, KJ inner). */
 __global__ void k_jnz(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is, int ie, int js,
                       int je) {
+    pdl_enter();
     int I = is + blockIdx.x * blockDim.x + threadIdx.x;
     int J = js + blockIdx.y;
     if (I > ie || J > je) return;
@@ -668,6 +688,7 @@ __global__ void k_jnz(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is,
 /* outputs                                                           */
 /* ---------------------------------------------------------------- */
 __global__ void k_maxamp(GcLayerDev L) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -677,6 +698,7 @@ __global__ void k_maxamp(GcLayerDev L) {
 }
 
 __global__ void k_arrival(GcLayerDev L, int step, float thr) {
+    pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
@@ -687,6 +709,7 @@ __global__ void k_arrival(GcLayerDev L, int step, float thr) {
 /* gauge stencil: for each (ki,kj) 1-based, the four surface values the
  * reference's gcomcot_get_z_ returns (GPUOutput.cu:29-44) */
 __global__ void k_gauges(GcLayerDev L, int ng, const int *ij, float *out) {
+    pdl_enter();
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ng) return;
     int i = ij[2 * g] - 1, j = ij[2 * g + 1] - 1;
@@ -707,6 +730,7 @@ __global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off,
                                float thr, int ng, const int *gij, const float *gw, const int *glayer,
                                const float *cz, int cpitch, float *ts, int ts_len, int wi0, int wj0, int wni,
                                int wnj) {
+    pdl_enter();
     const int local = step_off + (step_base ? *step_base : 0) - step0;
     if (local < 0 || local >= ts_len) return;
     if (blockIdx.x == 0 && blockIdx.y == 0 && ng > 0) {
@@ -736,6 +760,28 @@ __global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off,
     if ((flags & 2) && L.arrival[c] < 0 && L.h[c] > CC_GX && z > thr) L.arrival[c] = local + 1;
 }
 
+thread_local bool t_pdl = false;
+
+/* ordinary launch, or one with programmatic stream serialization */
+template <typename... KArgs, typename... Args>
+void launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args) {
+    if (!t_pdl) {
+        kern<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 inline dim3 grid2(const GcLayerDev &L) {
     return dim3((unsigned)((L.nx + BX - 1) / BX), (unsigned)((L.ny + BY - 1) / BY), 1);
 }
@@ -743,15 +789,15 @@ inline dim3 grid2(const GcLayerDev &L) {
 } // namespace
 
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0) k_mass_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
-    else if (L.laygov == 1) k_mass_c<true><<<grid2(L), dim3(BX, BY), 0, s>>>(L);
-    else k_mass_c<false><<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    if (L.laycord == 0) launch(k_mass_s, grid2(L), dim3(BX, BY), 0, s, L);
+    else if (L.laygov == 1) launch(k_mass_c<true>, grid2(L), dim3(BX, BY), 0, s, L);
+    else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0) k_momt_s<<<grid2(L), dim3(BX, BY), 0, s>>>(L, 0, 0, L.nx, L.ny);
-    else if (L.laygov == 1) k_conmome<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
-    else k_momt_c<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
+    else if (L.laygov == 1) launch(k_conmome, grid2(L), dim3(BX, BY), 0, s, L);
+    else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
 void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1, cudaStream_t s) {
@@ -762,17 +808,17 @@ void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1
     if (i1 < i0 || j1 < j0) return;
     const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
     dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
-    k_momt_s<<<grid, dim3(BX, BY), 0, s>>>(L, i0, j0, ni, nj);
+    launch(k_momt_s, grid, dim3(BX, BY), 0, s, L, i0, j0, ni, nj);
 }
 
 void gc_launch_open(const GcLayerDev &L, cudaStream_t s) {
     int n = 2 * L.nx + 2 * (L.ny - 2);
-    k_open<<<(n + 127) / 128, 128, 0, s>>>(L);
+    launch(k_open, (n + 127) / 128, 128, 0, s, L);
 }
 
 void gc_launch_update_edges(const GcLayerDev &L, cudaStream_t s) {
     int n = L.ny + L.nx - 1;
-    k_update_edges<<<(n + 127) / 128, 128, 0, s>>>(L);
+    launch(k_update_edges, (n + 127) / 128, 128, 0, s, L);
 }
 
 void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
@@ -780,27 +826,27 @@ void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int
     int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
     int len = (ie - is + 5) > (je - js + 5) ? (ie - is + 5) : (je - js + 5);
     size_t smem = (size_t)len * sizeof(float);
-    k_edges<<<4, EDGE_THREADS, smem, s>>>(P, C, rel_size, rel_time, is, ie, js, je, t, len);
+    launch(k_edges, 4, EDGE_THREADS, smem, s, P, C, rel_size, rel_time, is, ie, js, je, t, len);
 }
 
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                    const int *corners, cudaStream_t s) {
     int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
     dim3 grid((unsigned)((ie - is + 1 + 127) / 128), (unsigned)(je - js + 1), 1);
-    k_jnz<<<grid, 128, 0, s>>>(P, C, rel_size, rel_time, is, ie, js, je);
+    launch(k_jnz, grid, 128, 0, s, P, C, rel_size, rel_time, is, ie, js, je);
 }
 
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s) {
-    k_maxamp<<<grid2(L), dim3(BX, BY), 0, s>>>(L);
+    launch(k_maxamp, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s) {
-    k_arrival<<<grid2(L), dim3(BX, BY), 0, s>>>(L, step, thr);
+    launch(k_arrival, grid2(L), dim3(BX, BY), 0, s, L, step, thr);
 }
 
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s) {
     if (ng <= 0) return;
-    k_gauges<<<(ng + 127) / 128, 128, 0, s>>>(L, ng, d_ij, d_out);
+    launch(k_gauges, (ng + 127) / 128, 128, 0, s, L, ng, d_ij, d_out);
 }
 
 void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
@@ -809,6 +855,9 @@ void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_
     int i0 = 0, j0 = 0, ni = L.nx, nj = L.ny;
     if (win) { i0 = win[0]; ni = win[1] - win[0] + 1; j0 = win[2]; nj = win[3] - win[2] + 1; }
     dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
-    k_step_outputs<<<grid, dim3(BX, BY), 0, s>>>(L, step_base, step_off, step0, flags, thr, ng, gij, gw, glayer,
+    launch(k_step_outputs, grid, dim3(BX, BY), 0, s, L, step_base, step_off, step0, flags, thr, ng, gij, gw, glayer,
                                                  cz, cpitch, ts, ts_len, i0, j0, ni, nj);
 }
+
+void gc_set_pdl(bool on) { t_pdl = on; }
+bool gc_pdl_on() { return t_pdl; }

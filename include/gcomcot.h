@@ -148,7 +148,8 @@ int gc_engine_read_child(gc_engine *e, int member, float *z, float *m, float *n)
 int gc_engine_member_health(gc_engine *e, int member, float bound);
 long long gc_engine_bytes_in_use(gc_engine *e);
 long long gc_engine_member_bytes(gc_engine *e, int cls);
-/* tile variant (autotuned when < 0) and use of CUDA graphs for step chunks */
+/* tile variant (autotuned when < 0; v + gc_engine_num_variants() * r also
+ * picks tile-height rule r) and use of CUDA graphs for step chunks */
 int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk);
 int gc_engine_autotune(gc_engine *e, int reps);
 int gc_engine_variant(gc_engine *e);
