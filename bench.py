@@ -64,13 +64,13 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per launch of the fused step from the committed ncu summary"""
-    f = ROOT / "profiles" / "fused_linear_step_c2.txt"
+def profiled_traffic(name="fused_linear_step_c2.txt", key="traffic_bytes_per_launch"):
+    """DRAM bytes (read + write) per launch of a kernel, from its committed ncu summary"""
+    f = ROOT / "profiles" / name
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -260,7 +260,11 @@ def run_c4(args, torch, dist, rank, world, local):
                        "l2": f"working set {nscen} x 7 fields x 4.9 MB >> 126 MB L2"},
             "cell_updates_per_s": value_cells,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                         "traffic": (None if profiled_traffic("fused_ensemble_step_c4.txt",
+                                                              "traffic_bytes_per_member_launch") is None
+                                     else nscen * profiled_traffic("fused_ensemble_step_c4.txt",
+                                                                   "traffic_bytes_per_member_launch")),
+                         "peak_kind": f"{peak_kind} (copy bandwidth)",
                          "algorithmic_bytes_per_launch": bpc * cells * nscen},
             "clocks": ck, "gpu_launches": launches}
     if plain:

@@ -17,6 +17,21 @@ P_F = C.POINTER(C.c_float)
 VP = C.c_void_p
 
 
+class Fault(C.Structure):
+    """gc_fault (include/gcomcot.h)"""
+    _fields_ = [(n, C.c_double) for n in ("hh", "l", "w", "d", "th", "dl", "rd", "x0", "y0", "xo", "yo")] + [
+        ("sw", C.c_int)]
+
+
+def faults_array(faults):
+    """list of dicts (keys of gc_fault; missing ones 0) -> ctypes array"""
+    arr = (Fault * max(1, len(faults)))()
+    for k, f in enumerate(faults):
+        for key, v in f.items():
+            setattr(arr[k], key, v)
+    return arr
+
+
 class ChildDesc(C.Structure):
     """gc_child_desc (include/gcomcot.h)"""
     _fields_ = ([("nx", C.c_int), ("ny", C.c_int), ("corners", C.c_int * 4), ("rel_size", C.c_int),
@@ -83,6 +98,10 @@ SIGNATURES = {
     "gc_engine_read_child": (C.c_int, [VP, C.c_int, P_F, P_F, P_F]),
     "gcomcot_fused_step_noalloc": (C.c_int, [C.c_int, VP, VP]),
     "gc_engine_member_health": (C.c_int, [VP, C.c_int, C.c_float]),
+    "gc_okada_apply": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP, VP, C.c_float, C.c_float, VP,
+                                 VP, VP]),
+    "gc_engine_set_class_axes": (C.c_int, [VP, C.c_int, P_F, P_F]),
+    "gc_engine_add_member_faults": (C.c_int, [VP, C.c_int, VP, C.c_int, C.c_int, C.c_int, P_I, P_F, C.c_float]),
 }
 
 

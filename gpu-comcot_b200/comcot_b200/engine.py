@@ -24,6 +24,7 @@ class Engine:
         self.h = h
         self.classes = {}
         self.members = {}
+        self._axes = set()
 
     def __enter__(self):
         return self
@@ -53,6 +54,34 @@ class Engine:
         if rc < 0:
             raise RuntimeError(f"gc_engine_add_class failed: {rc}")
         self.classes[key] = (rc, L.nx, L.ny)
+        return rc
+
+    def add_faults(self, case: Case, faults, nsteps=None, gauges=None, arrival_thr=None) -> int:
+        """a member whose initial state is generated on the device from fault
+        parameters (list of dicts with gc_fault's keys) on case.root's grid"""
+        L = case.root
+        cls = self.add_class(L)
+        if cls not in self._axes:
+            x = np.ascontiguousarray(L.x, dtype=F32)
+            y = np.ascontiguousarray(L.y, dtype=F32)
+            rc = self.lib.gc_engine_set_class_axes(self.h, cls, _lib.fptr(x), _lib.fptr(y))
+            if rc != 0:
+                raise RuntimeError(f"gc_engine_set_class_axes failed: {rc}")
+            self._axes.add(cls)
+        g = case.gauges if gauges is None else gauges
+        ng = len(g)
+        gij = np.array([[x[1], x[2]] for x in g] or [[0, 0]], dtype=np.int32)
+        gw = np.array([[x[3], x[4]] for x in g] or [[0, 0]], dtype=F32)
+        n = case.nsteps if nsteps is None else nsteps
+        thr = case.arrival_thr if arrival_thr is None else arrival_thr
+        arr = _lib.faults_array(faults)
+        rc = self.lib.gc_engine_add_member_faults(self.h, cls, C.cast(arr, C.c_void_p), len(faults), int(n), ng,
+                                                  _lib.iptr(gij), _lib.fptr(gw), C.c_float(thr))
+        if rc == -2:
+            raise MemoryError("engine budget exhausted")
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_add_member_faults failed: {rc}")
+        self.members[rc] = (L.nx, L.ny, n, ng, None)
         return rc
 
     def add_nested_class(self, P, Cl) -> int:

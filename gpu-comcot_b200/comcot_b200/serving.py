@@ -29,6 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import outputs
 from .engine import Engine
 
 
@@ -37,6 +38,7 @@ class Request:
     rid: int
     t_arrival: float          # seconds after the start of the trace
     case: object              # synth.Case: layers (shared per class), Z0, gauges, nsteps
+    faults: list | None = None  # fault planes: the initial state is generated on the device
     t_admit: float = -1.0
     t_done: float = -1.0
     result: dict = field(default_factory=dict)
@@ -54,7 +56,7 @@ class ForecastServer:
     """Continuous-batching request loop on one GPU."""
 
     def __init__(self, budget_bytes: int, chunk: int = 32, variant: int = -1, keep_fields=("zmax", "arrival", "ts"),
-                 engine=None, blowup_m: float = 100.0):
+                 engine=None, blowup_m: float = 100.0, out_dir: str | None = None):
         """engine: an object with Engine's add/step/sync/done/read/release
         (default: a new Engine with this budget)"""
         self.eng = engine if engine is not None else Engine(budget=budget_bytes)
@@ -67,8 +69,13 @@ class ForecastServer:
         self.blowup_m = blowup_m
         self.idle_retries = 20   # refusals with nothing running before a request is rejected
         self._cancel = set()
+        # products of finished requests go to out_dir/req_<rid>/ on a writer thread
+        self.out_dir = out_dir
+        self.writer = outputs.AsyncWriter() if out_dir else None
 
     def close(self):
+        if self.writer:
+            self.writer.close()
         self.eng.close()
 
     def __enter__(self):
@@ -84,7 +91,7 @@ class ForecastServer:
     def _try_admit(self, r: Request) -> bool:
         """True when the request left the queue (admitted or rejected)"""
         try:
-            mid = self.eng.add(r.case)
+            mid = self.eng.add_faults(r.case, r.faults) if r.faults else self.eng.add(r.case)
         except MemoryError:
             self.refused += 1
             return False
@@ -103,6 +110,9 @@ class ForecastServer:
         else:
             r.result = self.eng.read(r._mid, fields=self.keep)
             r.status = "done"
+            if self.writer:
+                L = r.case.root
+                self.writer.submit(outputs.write_forecast, f"{self.out_dir}/req_{r.rid:05d}", r.result, L.H, L.dt)
         self.eng.release(r._mid)
 
     def serve(self, requests, speed: float = 1.0, clock=time.perf_counter):

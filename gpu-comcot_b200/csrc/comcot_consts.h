@@ -32,5 +32,6 @@
 #define CC_RAD_DEG  0.01745329252
 #define CC_RAD_MIN  0.000290888208665721
 #define CC_CORI_W   7.2722e-5
+#define CC_PI       3.14159265358979
 
 #endif

@@ -54,6 +54,8 @@ struct EngClass {
     int laycord = 1, laygov = 1, linchk = 1, modscm = 1, fric_switch = 1;
     float dt = 0, rx = 0, ry = 0, grx = 0, gry = 0, fric_coef = 0;
     float *d_ch = nullptr, *d_chp = nullptr, *d_chq = nullptr, *d_crows = nullptr;
+    /* longitude / latitude axes (degrees), for members made from faults */
+    float *d_lon = nullptr, *d_lat = nullptr;
 };
 
 struct EngMember {
@@ -70,6 +72,7 @@ struct EngMember {
     float *cz[2] = {nullptr, nullptr}, *cm[2] = {nullptr, nullptr}, *cn[2] = {nullptr, nullptr};
     float *cdz2 = nullptr, *xflux = nullptr, *yflux = nullptr;
     int *glayer = nullptr;
+    float *h = nullptr; /* own depth (members made from faults), else the class's */
     int fty = 16; /* tile height of the outer grid's fused launch */
     /* the last global step this member needs a launch at: single-grid
      * members sample their last gauges in the launch after their last step */
@@ -309,7 +312,7 @@ static int eng_rebuild(gc_engine *e) {
             g.flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
             g.thr = M.thr;
             for (int q = 0; q < 2; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
-            g.h = C.d_h; g.rows = C.d_rows;
+            g.h = M.h ? M.h : C.d_h; g.rows = C.d_rows;
             g.zmax = M.zmax; g.arrival = M.arrival;
             g.ng = M.ng; g.gij = M.gij; g.gw = M.gw; g.ts = M.ts; g.ts_len = M.nsteps;
             grids.push_back(g);
@@ -444,8 +447,10 @@ int gc_engine_destroy(gc_engine *e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     for (auto &M : e->members)
         if (M.block) cudaFreeAsync(M.block, e->stream);
-    for (auto &C : e->classes)
+    for (auto &C : e->classes) {
         if (C.block) cudaFreeAsync(C.block, e->stream);
+        if (C.d_lon) cudaFreeAsync(C.d_lon, e->stream);
+    }
     if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
     if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
     if (e->d_step) cudaFreeAsync(e->d_step, e->stream);
@@ -489,11 +494,11 @@ int gc_engine_add_class(gc_engine *e, int nx, int ny, const float *H, const floa
 
 } /* extern "C" */
 
-static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges) {
+static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges, bool own_h = false) {
     size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
     size_t tsb = a256((size_t)nsteps * ngauges * sizeof(float));
     size_t gb = a256((size_t)2 * ngauges * sizeof(int)) + a256((size_t)2 * ngauges * sizeof(float));
-    size_t bytes = 8 * field + tsb + gb;
+    size_t bytes = (own_h ? 9 : 8) * field + tsb + gb;
     if (C.nested) {
         size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
         bytes += 7 * cfield + a256((size_t)2 * C.nx * sizeof(float)) + a256((size_t)2 * C.ny * sizeof(float))
@@ -503,8 +508,10 @@ static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges) {
 }
 
 static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *cz0, int nsteps, int ngauges,
-                          const int *glayer, const int *gij, const float *gw, float arrival_thr) {
-    if (!e || cls < 0 || cls >= (int)e->classes.size() || !z0 || nsteps < 1 || ngauges < 0) return GC_EINVAL;
+                          const int *glayer, const int *gij, const float *gw, float arrival_thr,
+                          const gc_fault *faults = nullptr, int nfaults = 0) {
+    if (!e || cls < 0 || cls >= (int)e->classes.size() || (!z0 && !faults) || nsteps < 1 || ngauges < 0)
+        return GC_EINVAL;
     if (ngauges > 0 && (!gij || !gw)) return GC_EINVAL;
     EngClass &C = e->classes[cls];
     for (int g = 0; g < ngauges; g++) {
@@ -516,7 +523,9 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
     }
     size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
     size_t tsb = a256((size_t)nsteps * ngauges * sizeof(float));
-    size_t bytes = eng_member_bytes(C, nsteps, ngauges);
+    const bool own_h = faults != nullptr;
+    if (own_h && (C.nested || !C.d_lon || nfaults < 1)) return C.nested ? GC_ENOTSUP : GC_EINVAL;
+    size_t bytes = eng_member_bytes(C, nsteps, ngauges, own_h);
     if (e->in_use + (long long)bytes > e->budget) return GC_ENOMEM;
     EngMember M;
     M.used = true;
@@ -538,8 +547,22 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
     M.gw = (float *)p; p += a256((size_t)2 * ngauges * sizeof(float));
     GC_CUDA_OR_RET(cudaMemsetAsync(M.block, 0, 6 * field, e->stream));
     GC_CUDA_OR_RET(cudaMemsetAsync(M.arrival, 0xff, field, e->stream));
-    GC_CUDA_OR_RET(cudaMemcpy2DAsync(M.z[0], (size_t)C.pitch * sizeof(float), z0, (size_t)C.nx * sizeof(float),
-                                     (size_t)C.nx * sizeof(float), (size_t)C.ny, cudaMemcpyHostToDevice, e->stream));
+    if (own_h) {
+        /* still water, then the faults' deformation on Z and on the member's own H */
+        M.h = (float *)p;
+        p += field;
+        GC_CUDA_OR_RET(cudaMemcpyAsync(M.h, C.d_h, field, cudaMemcpyDeviceToDevice, e->stream));
+        int rc = gc_okada_apply(faults, nfaults, 0, C.nx, C.ny, C.pitch, C.d_lon, C.d_lat, 0.0f, 0.0f, M.z[0], M.h,
+                                e->stream);
+        if (rc != GC_OK) {
+            cudaFreeAsync(M.block, e->stream);
+            return rc;
+        }
+    } else {
+        GC_CUDA_OR_RET(cudaMemcpy2DAsync(M.z[0], (size_t)C.pitch * sizeof(float), z0, (size_t)C.nx * sizeof(float),
+                                         (size_t)C.nx * sizeof(float), (size_t)C.ny, cudaMemcpyHostToDevice,
+                                         e->stream));
+    }
     GC_CUDA_OR_RET(cudaMemcpyAsync(M.zmax, M.z[0], field, cudaMemcpyDeviceToDevice, e->stream));
     if (ngauges > 0) {
         GC_CUDA_OR_RET(cudaMemcpyAsync(M.gij, gij, (size_t)2 * ngauges * sizeof(int), cudaMemcpyHostToDevice,
@@ -601,6 +624,30 @@ int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const fl
                                 int ngauges, const int *glayer, const int *gij, const float *gw,
                                 float arrival_thr) {
     return eng_add_member(e, cls, z0, child_z0, nsteps, ngauges, glayer, gij, gw, arrival_thr);
+}
+
+int gc_engine_set_class_axes(gc_engine *e, int cls, const float *lon, const float *lat) {
+    if (!e || cls < 0 || cls >= (int)e->classes.size() || !lon || !lat) return GC_EINVAL;
+    EngClass &C = e->classes[cls];
+    if (C.nested) return GC_ENOTSUP;
+    if (!C.d_lon) {
+        const size_t bytes = a256((size_t)C.nx * sizeof(float)) + a256((size_t)C.ny * sizeof(float));
+        if (e->in_use + (long long)bytes > e->budget) return GC_ENOMEM;
+        GC_CUDA_OR_RET(cudaMallocAsync((void **)&C.d_lon, bytes, e->stream));
+        C.d_lat = (float *)((char *)C.d_lon + a256((size_t)C.nx * sizeof(float)));
+        e->in_use += (long long)bytes;
+        C.bytes += bytes;
+    }
+    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_lon, lon, (size_t)C.nx * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_lat, lat, (size_t)C.ny * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
+    return GC_OK;
+}
+
+int gc_engine_add_member_faults(gc_engine *e, int cls, const gc_fault *faults, int nfaults, int nsteps, int ngauges,
+                                const int *gij, const float *gw, float arrival_thr) {
+    if (!faults || nfaults < 1) return GC_EINVAL;
+    return eng_add_member(e, cls, nullptr, nullptr, nsteps, ngauges, nullptr, gij, gw, arrival_thr, faults, nfaults);
 }
 
 int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc *d) {

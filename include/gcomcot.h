@@ -91,6 +91,30 @@ void *gcomcot_stream(void);
 int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const int *g_i,
                   const int *g_j, float *out4);
 
+/* ---- on-device source generation (source_okada.cu) ---- */
+
+/* One rectangular fault plane as the reference's FAULT type describes it
+ * (type_module.f90:130-147): focal depth to the top edge, length, width and
+ * dislocation in metres; strike, dip and slip (rake) in degrees; epicentre
+ * longitude/latitude; the origin of a Cartesian layer; sw = 0 puts the
+ * epicentre at the plane's centre, 9 at the centre of its top edge. */
+typedef struct {
+    double hh, l, w, d;
+    double th, dl, rd;
+    double x0, y0;
+    double xo, yo;
+    int sw;
+} gc_fault;
+
+/* replaces deform.f90:2-240 (GET_FLOOR_DEFORM with DEFORM_OKADA for
+ * instantaneous faults): adds each fault's seafloor deformation to the
+ * surface d_z and subtracts it from the depth d_h (device arrays, row pitch
+ * `pitch` floats; either may be NULL), in fault order.  laycord 0: cell
+ * positions from the device axes d_x[nx] (longitude) and d_y[ny] (latitude);
+ * 1: from the spacings dx, dy in metres.  Returns 0 or < 0. */
+int gc_okada_apply(const gc_fault *faults, int nf, int laycord, int nx, int ny, int pitch, const float *d_x,
+                   const float *d_y, float dx, float dy, float *d_z, float *d_h, void *stream);
+
 /* ---- batched ensemble / serving engine (engine.cu) ---- */
 typedef struct gc_engine gc_engine;
 
@@ -142,6 +166,14 @@ int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const fl
                                 float arrival_thr);
 /* the child's Z, M, N (level 1 after the member's completed steps) */
 int gc_engine_read_child(gc_engine *e, int member, float *z, float *m, float *n);
+/* longitude [nx] and latitude [ny] axes of a (non-nested) class, in degrees,
+ * needed by members created from fault parameters */
+int gc_engine_set_class_axes(gc_engine *e, int cls, const float *lon, const float *lat);
+/* a member whose initial state comes from faults on the device: still water
+ * plus the seafloor deformation (gc_okada_apply), with its own depth H minus
+ * the deformation (the reference's UPDATE_BATH, initialization.f90:2410-2434) */
+int gc_engine_add_member_faults(gc_engine *e, int cls, const gc_fault *faults, int nfaults, int nsteps,
+                                int ngauges, const int *gij, const float *gw, float arrival_thr);
 /* no counterpart in the reference (which has no failure detection): scans
  * the member's max-eta and current surfaces; 0 = healthy, bit 0 = a NaN or
  * Inf appeared, bit 1 = |eta| exceeded `bound` metres, < 0 = error */

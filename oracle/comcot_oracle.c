@@ -1036,6 +1036,160 @@ void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp, double 
     }
 }
 
+
+/* ------------------------------------------------------------------ */
+/* Okada (1985) seafloor deformation (deform.f90:74-240, 494-586)      */
+/* ------------------------------------------------------------------ */
+static inline REAL r_sin(REAL x) { return sizeof(REAL) == sizeof(float) ? (REAL)sinf((float)x) : (REAL)sin((double)x); }
+static inline REAL r_cos(REAL x) { return sizeof(REAL) == sizeof(float) ? (REAL)cosf((float)x) : (REAL)cos((double)x); }
+static inline REAL r_log(REAL x) { return sizeof(REAL) == sizeof(float) ? (REAL)logf((float)x) : (REAL)log((double)x); }
+static inline REAL r_atan(REAL x) { return sizeof(REAL) == sizeof(float) ? (REAL)atanf((float)x) : (REAL)atan((double)x); }
+static inline REAL r_asin(REAL x) { return sizeof(REAL) == sizeof(float) ? (REAL)asinf((float)x) : (REAL)asin((double)x); }
+static inline REAL r_powr(REAL x, REAL y) {
+    return sizeof(REAL) == sizeof(float) ? (REAL)powf((float)x, (float)y) : (REAL)pow((double)x, (double)y);
+}
+static inline int r_isnan(REAL x) { return x != x; }
+static inline int r_isbig(REAL x) {
+    REAL a = o_abs(x);
+    return sizeof(REAL) == sizeof(float) ? (float)a >= 3.40282347e38f : (double)a >= 1.7976931348623157e308;
+}
+
+/* oblique stereographic projection on the WGS84 ellipsoid (Snyder 1987),
+ * metres east / north of (lon0, lat0) */
+void ocl_stereo(REAL lonin, REAL latin, REAL lon0, REAL lat0, REAL *xo, REAL *yo) {
+    const REAL rad = R(CC_RAD_DEG);
+    const REAL pole = R(CC_PI) / R(2.0) - R(CC_EPS);
+    REAL lat = latin * rad, lon = lonin * rad, lt0 = lat0 * rad, ln0 = lon0 * rad;
+    if (lat > pole) lat = pole;
+    if (lat < -pole) lat = -pole;
+    if (lt0 > pole) lt0 = pole;
+    if (lt0 < -pole) lt0 = -pole;
+    const REAL cs = r_cos(lat), sn = r_sin(lat), cs0 = r_cos(lt0), sn0 = r_sin(lt0);
+    const REAL a = R(6378137.0), e = R(0.08181919092891), f2 = R(0.00669438000426), k0 = R(0.9996);
+    const REAL tmp0 = o_sqrt(R(1.0) - f2 * (sn0 * sn0));
+    (void)cs;
+    const REAL rho0 = a * (R(1.0) - f2) / (tmp0 * tmp0 * tmp0);
+    /* NU0 is not declared REAL in the reference (deform.f90:515-518, no
+     * IMPLICIT NONE), so Fortran's implicit typing makes it an INTEGER and
+     * the assignment truncates */
+    const REAL nu0 = (REAL)(int)(a / tmp0);
+    const REAL rr = o_sqrt(rho0 * nu0);
+    const REAL c04 = (cs0 * cs0) * (cs0 * cs0);
+    const REAL n = o_sqrt(R(1.0) + f2 * c04 / (R(1.0) - f2));
+    const REAL s1 = (R(1.0) + sn0) / (R(1.0) - sn0);
+    const REAL s2 = (R(1.0) - e * sn0) / (R(1.0) + e * sn0);
+    const REAL w1 = r_powr(s1 * r_powr(s2, e), n);
+    const REAL sn_xi0 = (w1 - R(1.0)) / (w1 + R(1.0));
+    const REAL c = (n + sn0) * (R(1.0) - sn_xi0) / (n - sn0) / (R(1.0) + sn_xi0);
+    const REAL w2 = c * w1;
+    const REAL sa = (R(1.0) + sn) / (R(1.0) - sn);
+    const REAL sb = (R(1.0) - e * sn) / (R(1.0) + e * sn);
+    const REAL w = c * r_powr(sa * r_powr(sb, e), n);
+    const REAL xi0 = r_asin((w2 - R(1.0)) / (w2 + R(1.0)));
+    const REAL lm0 = ln0;
+    const REAL lm = n * (lon - lm0) + lm0;
+    const REAL xi = r_asin((w - R(1.0)) / (w + R(1.0)));
+    const REAL beta = R(1.0) + r_sin(xi) * r_sin(xi0) + r_cos(xi) * r_cos(xi0) * r_cos(lm - lm0);
+    *yo = R(0.0) + R(2.0) * rr * k0 * (r_sin(xi) * r_cos(xi0) - r_cos(xi) * r_sin(xi0) * r_cos(lm - lm0)) / beta;
+    *xo = R(0.0) + R(2.0) * rr * k0 * r_cos(xi) * r_sin(lm - lm0) / beta;
+}
+
+/* STRIKE_SLIP (deform.f90:190-215) */
+static REAL okada_ss(REAL y1, REAL y2, REAL q_x2, REAL dp, REAL dd) {
+    const REAL sn = r_sin(dp), cs = r_cos(dp);
+    const REAL q = q_x2 * sn - dd * cs;
+    const REAL d_bar = y2 * sn - q * cs;
+    const REAL r = o_sqrt(y1 * y1 + y2 * y2 + q * q);
+    REAL t1 = r + d_bar, t2 = r + y2;
+    if (t1 <= R(CC_EPS)) t1 = R(CC_EPS);
+    if (t2 <= R(CC_EPS)) t2 = R(CC_EPS);
+    const REAL a4 = R(0.5) / cs * (r_log(t1) - sn * r_log(t2));
+    return -(d_bar * q / r / (r + y2) + q * sn / (r + y2) + a4 * sn) / R(2.0) / R(3.14159);
+}
+
+/* DIP_SLIP (deform.f90:218-236) */
+static REAL okada_ds(REAL y1, REAL y2, REAL q_x2, REAL dp, REAL dd) {
+    const REAL sn = r_sin(dp), cs = r_cos(dp);
+    const REAL q = q_x2 * sn - dd * cs;
+    const REAL d_bar = y2 * sn - q * cs;
+    const REAL r = o_sqrt(y1 * y1 + y2 * y2 + q * q);
+    const REAL xx = o_sqrt(y1 * y1 + q * q);
+    const REAL a5 = R(1.0) / cs * r_atan((y2 * (xx + q * cs) + xx * (r + xx) * sn) / y1 / (r + xx) / cs);
+    return -(d_bar * q / r / (r + y1) + sn * r_atan(y1 * y2 / q / r) - a5 * sn * cs) / R(2.0) / R(3.14159);
+}
+
+void ocl_okada(const ocl_fault *f, int laycord, int nx, int ny, const double *x, const double *y, double dx,
+               double dy, REAL *deform) {
+    const REAL rad = R(CC_RAD_DEG);
+    const REAL ang_l = rad * R(f->dl), ang_r = rad * R(f->rd), ang_t = rad * R(f->th);
+    const REAL halfl = R(0.5) * R(f->l), w = R(f->w);
+    REAL hh = R(f->hh) + R(0.5) * w * r_sin(ang_l);
+    REAL del_x = R(0.5) * w * r_cos(ang_l) * r_cos(ang_t);
+    REAL del_y = R(0.5) * w * r_cos(ang_l) * r_sin(ang_t);
+    if (f->sw == 9) {
+        hh = R(f->hh) + w * r_sin(ang_l);
+        del_x = w * r_cos(ang_l) * r_cos(ang_t);
+        del_y = w * r_cos(ang_l) * r_sin(ang_t);
+    }
+    const REAL ds = R(f->d) * r_cos(ang_r), dd = R(f->d) * r_sin(ang_r);
+    const REAL sn = r_sin(ang_l), cs = r_cos(ang_l);
+    const REAL st = r_sin(ang_t), ct = r_cos(ang_t);
+    REAL xl = 0, yl = 0;
+    if (laycord != 0) ocl_stereo(R(f->xo), R(f->yo), R(f->x0), R(f->y0), &xl, &yl);
+    for (int i = 1; i <= nx; i++) {
+        for (int j = 1; j <= ny; j++) {
+            REAL xs, ys;
+            if (laycord == 0) {
+                ocl_stereo(R(x[i - 1]), R(y[j - 1]), R(f->x0), R(f->y0), &xs, &ys);
+                xs = xs - del_x;
+                ys = ys + del_y;
+            } else {
+                /* deform.f90:150-154 as written: X = DX*(I-1) - XL, where XL is the
+                 * layer origin's projected offset from the epicentre */
+                const REAL yy = R(dy) * (R(j) - R(1.0)), xx = R(dx) * (R(i) - R(1.0));
+                xs = xx - xl - del_x;
+                ys = yy - yl + del_y;
+            }
+            const REAL x1 = xs * st + ys * ct;
+            REAL x2 = xs * ct - ys * st;
+            x2 = -x2;
+            const REAL p = x2 * cs + hh * sn;
+            const REAL f1 = okada_ss(x1 + halfl, p, x2, ang_l, hh);
+            const REAL f2 = okada_ss(x1 + halfl, p - w, x2, ang_l, hh);
+            const REAL f3 = okada_ss(x1 - halfl, p, x2, ang_l, hh);
+            const REAL f4 = okada_ss(x1 - halfl, p - w, x2, ang_l, hh);
+            const REAL g1 = okada_ds(x1 + halfl, p, x2, ang_l, hh);
+            const REAL g2 = okada_ds(x1 + halfl, p - w, x2, ang_l, hh);
+            const REAL g3 = okada_ds(x1 - halfl, p, x2, ang_l, hh);
+            const REAL g4 = okada_ds(x1 - halfl, p - w, x2, ang_l, hh);
+            REAL us = (f1 - f2 - f3 + f4) * ds;
+            REAL ud = (g1 - g2 - g3 + g4) * dd;
+            if (r_isbig(us)) us = 0;
+            if (r_isbig(ud)) ud = 0;
+            if (r_isnan(us)) us = 0;
+            if (r_isnan(ud)) ud = 0;
+            if (o_abs(us) <= R(CC_GX)) us = 0;
+            if (o_abs(ud) <= R(CC_GX)) ud = 0;
+            deform[(size_t)(j - 1) * nx + (i - 1)] = us + ud;
+        }
+    }
+}
+
+void ocl_okada_apply(const ocl_fault *f, int nf, int laycord, int nx, int ny, const double *x, const double *y,
+                     double dx, double dy, REAL *z, REAL *h) {
+    size_t n = (size_t)nx * ny;
+    REAL *d = (REAL *)malloc(n * sizeof(REAL));
+    if (!d) return;
+    for (int k = 0; k < nf; k++) {
+        ocl_okada(&f[k], laycord, nx, ny, x, y, dx, dy, d);
+        for (size_t c = 0; c < n; c++) {
+            z[c] = z[c] + d[c];
+            h[c] = h[c] - d[c];
+        }
+    }
+    free(d);
+}
+
 /* the shared deterministic elementary functions, exposed for their tests */
 float ocl_expf(float x) { return cc_expf(x); }
 float ocl_powf(float x, float y) { return cc_powf(x, y); }

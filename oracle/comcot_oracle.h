@@ -73,6 +73,26 @@ int  ocl_rel_time(double dt_parent, double dx_m, double dy_m, double hmax, int n
 void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp,
                  double xs, double xe, double ys, double ye, int *corners);
 
+/* one rectangular fault plane (type_module.f90:130-147); angles in degrees,
+ * lengths in metres, positions in degrees */
+typedef struct {
+    double hh, l, w, d;       /* focal depth to the top edge, length, width, dislocation */
+    double th, dl, rd;        /* strike, dip, slip (rake) */
+    double x0, y0;            /* epicentre longitude, latitude */
+    double xo, yo;            /* domain origin (Cartesian layers) */
+    int sw;                   /* 0: epicentre at the plane's centre; 9: at its top edge's centre */
+} ocl_fault;
+
+/* DEFORM_OKADA (deform.f90:74-187) for every cell of a layer: laycord 0 uses
+ * the longitudes x[nx] / latitudes y[ny], laycord 1 the spacings dx, dy */
+void ocl_okada(const ocl_fault *f, int laycord, int nx, int ny, const double *x, const double *y, double dx,
+               double dy, REAL *deform);
+/* GET_FLOOR_DEFORM (deform.f90:2-72) for instantaneous faults: per fault,
+ * Z += DEFORM and H -= DEFORM, in fault order */
+void ocl_okada_apply(const ocl_fault *f, int nf, int laycord, int nx, int ny, const double *x, const double *y,
+                     double dx, double dy, REAL *z, REAL *h);
+void ocl_stereo(REAL lonin, REAL latin, REAL lon0, REAL lat0, REAL *xo, REAL *yo);
+
 float ocl_expf(float x);
 float ocl_powf(float x, float y);
 

@@ -55,12 +55,38 @@ def load(dtype=np.float32):
     lib.ocl_rel_time.restype = C.c_int
     lib.ocl_corners.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double,
                                 C.c_double, C.c_double, C.c_void_p]
+    lib.ocl_okada.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                              C.c_double, C.c_void_p]
+    lib.ocl_okada_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     lib.ocl_expf.argtypes = [C.c_float]
     lib.ocl_expf.restype = C.c_float
     lib.ocl_powf.argtypes = [C.c_float, C.c_float]
     lib.ocl_powf.restype = C.c_float
     _libs[key] = lib
     return lib
+
+
+class OFault(C.Structure):
+    """ocl_fault (comcot_oracle.h)"""
+    _fields_ = [(n, C.c_double) for n in ("hh", "l", "w", "d", "th", "dl", "rd", "x0", "y0", "xo", "yo")] + [
+        ("sw", C.c_int)]
+
+
+def okada_apply(faults, laycord, nx, ny, x=None, y=None, dx=0.0, dy=0.0, z=None, h=None, dtype=np.float32):
+    """GET_FLOOR_DEFORM restated: returns (z + sum of deformations, h - sum)"""
+    lib = load(dtype)
+    arr = (OFault * max(1, len(faults)))()
+    for k, f in enumerate(faults):
+        for key, v in f.items():
+            setattr(arr[k], key, v)
+    zz = np.array(np.zeros((ny, nx)) if z is None else z, dtype=dtype, order="C", copy=True)
+    hh = np.array(np.zeros((ny, nx)) if h is None else h, dtype=dtype, order="C", copy=True)
+    xa = np.ascontiguousarray(np.zeros(nx) if x is None else x, dtype=np.float64)
+    ya = np.ascontiguousarray(np.zeros(ny) if y is None else y, dtype=np.float64)
+    lib.ocl_okada_apply(C.addressof(arr), len(faults), laycord, nx, ny, xa.ctypes.data, ya.ctypes.data, dx, dy,
+                        zz.ctypes.data, hh.ctypes.data)
+    return zz, hh
 
 
 class OLayer(C.Structure):

@@ -146,3 +146,20 @@ def test_fifo_model_and_percentiles():
     assert np.allclose(lat, [1.0, 1.5, 2.4]) and end == 3.0
     p = percentiles(np.arange(101))
     assert p["p50"] == 50.0 and p["p99"] == 99.0
+
+
+def test_finished_requests_products_written_in_background(tmp_path):
+    import types
+
+    class Eng(FakeEngine):
+        def read(self, mid, fields=()):
+            return {"zmax": np.full((2, 3), 0.25, np.float32), "ts": np.zeros((2, 1), np.float32),
+                    "arrival": np.full((2, 3), -1, np.int32)}
+
+    case = FakeCase(4, 10)
+    case.root = types.SimpleNamespace(H=np.ones((2, 3), np.float32), dt=2.0)
+    with ForecastServer(100, engine=Eng(budget=100), out_dir=str(tmp_path)) as srv:
+        srv.serve([Request(7, 0.0, case)], speed=float("inf"))
+    import os
+    assert sorted(os.listdir(tmp_path / "req_00007")) == ["arrival_layer01.dat", "ts_record0001.dat",
+                                                          "zmax_layer01.dat"]
