@@ -58,6 +58,12 @@ class ReferenceSession:
                                           _f(L.grx), _f(L.gry), _i(L.fric_switch), _f(L.fric_coef),
                                           _i(L.linchk), _i(L.modscm), _i(nx), _i(ny), _lib.fptr(hp),
                                           _lib.fptr(hq))
+        if L.laycord == 0 and L.laygov == 1:
+            c = L.coefs
+            full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)
+            r0, r21, r22 = full(c.r0), full(c.r1), full(c.r22)
+            self._keep += [r0, r21, r22]
+            lib.gcomcot_set_layer_coefs_(_i(L.id), _lib.fptr(r0), _lib.fptr(r21), _lib.fptr(r22), _i(nx), _i(ny))
         if L.coefs is not None:
             c = L.coefs
             full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)

@@ -67,6 +67,8 @@ class Coefs:
     cy: np.ndarray   # [ny]  R4 = CY * max(HQ,0)
     r2: np.ndarray = field(default=None)  # [ny, nx]
     r4: np.ndarray = field(default=None)
+    r0: np.ndarray = field(default=None)  # [ny] RR/(DEL_Y*RAD_MIN), nonlinear advection (comcot.f90:727)
+    r22: np.ndarray = field(default=None)  # [ny] RR/COS_N/(DX*RAD_MIN) (comcot.f90:733)
 
     def rows(self) -> np.ndarray:
         return np.stack([self.r1, self.r11, self.r6, self.r3, self.r5, self.cx, self.cy]).astype(np.float32)
@@ -90,6 +92,8 @@ def para(h: np.ndarray, lat: np.ndarray, dx_min: float, dt: float, del_y_min=Non
     r3 = (rt * sin_m).astype(np.float32)
     r5 = (rt * sin_n).astype(np.float32)
     r6 = cos_n.astype(np.float32)
+    r0 = (rr / (dely * RAD_MIN)).astype(np.float32)
+    r22 = (rr / cos_n / (dx_min * RAD_MIN)).astype(np.float32)
     hp, hq = pq_depth(h)
     if laygov == 0:
         r2 = (cx[:, None] * np.maximum(hp, F32(0))).astype(np.float32)
@@ -97,7 +101,7 @@ def para(h: np.ndarray, lat: np.ndarray, dx_min: float, dt: float, del_y_min=Non
     else:
         r2 = np.repeat(cx[:, None], nx, axis=1).astype(np.float32)
         r4 = np.repeat(cy[:, None], nx, axis=1).astype(np.float32)
-    return Coefs(r1, r11, r6, r3, r5, cx, cy, r2, r4)
+    return Coefs(r1, r11, r6, r3, r5, cx, cy, r2, r4, r0, r22)
 
 
 def rel_time(dt_parent: float, dx_m: float, dy_m: float, hmax: float, nonlinear: bool):

@@ -168,7 +168,9 @@ def wet_gauges(L: LayerSpec, n, rng, first=1, margin=5):
 
 
 def single_layer_case(name, nx, ny, dx_min, dt, nsteps, seed, n_seamounts, shelf_cols, land_cols,
-                      source="hump", ngauges=0, lon0=140.0, lat0=20.0, amp=None):
+                      source="hump", ngauges=0, lon0=140.0, lat0=20.0, amp=None, laygov=0, fric=0.025):
+    """One spherical layer, linear (laygov 0) or nonlinear with Manning
+    friction (laygov 1, CONMASS_S / CONMOME_S)."""
     rng = np.random.default_rng(seed)
     x, y = pc.axes(lon0, lat0, nx, ny, dx_min)
     H = bathymetry(x, y, rng, n_seamounts=n_seamounts, shelf_cols=shelf_cols, land_cols=land_cols)
@@ -179,7 +181,9 @@ def single_layer_case(name, nx, ny, dx_min, dt, nsteps, seed, n_seamounts, shelf
     else:
         a = float(rng.uniform(0.5, 5.0)) if amp is None else amp
         Z0 = dipole(x, y, lon_c, lat_c, a, float(rng.uniform(0.0, 360.0)))
-    L = spherical_layer(1, x, y, H, Z0, dt, dx_min)
+    L = spherical_layer(1, x, y, H, Z0, dt, dx_min, laygov=laygov)
+    if laygov == 1:
+        L.fric_switch, L.fric_coef, L.linchk = 0, fric, 1
     case = Case(name, [L], nsteps)
     if ngauges:
         case.gauges = wet_gauges(L, ngauges, rng)
@@ -248,11 +252,14 @@ def nested_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel
     Zc = dipole(cxd, cyd, lon_c, lat_c, 2.0, 0.0) * 0.0
     if child_laycord == 0:
         sx, sy = pc.child_axes_spherical(x, y, corners, rel_size, dx_min)
-        rt, dtc = pc.rel_time(dt, dxm, dym, float(Hc.max()), nonlinear=False)
+        rt, dtc = pc.rel_time(dt, dxm, dym, float(Hc.max()), nonlinear=(child_laygov == 1))
         if rel_time is not None:
             rt, dtc = rel_time, float(F32(dt) / F32(rel_time))
-        C = spherical_layer(2, sx, sy, Hc, np.zeros_like(Hc), dtc, dx_min / rel_size, parent=1, level=2)
+        C = spherical_layer(2, sx, sy, Hc, np.zeros_like(Hc), dtc, dx_min / rel_size, parent=1, level=2,
+                            laygov=child_laygov)
         C.rel_size, C.rel_time, C.corners = rel_size, rt, list(corners)
+        if child_laygov == 1:
+            C.fric_switch, C.fric_coef, C.linchk = 0, fric, 1
         case = Case(name, [P, C], nsteps)
         if ngauges:
             case.gauges = wet_gauges(P, ngauges, rng)

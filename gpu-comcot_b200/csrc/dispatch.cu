@@ -32,7 +32,7 @@ void gc_flush() {
     if (!(rt.pend_mass | rt.pend_open | rt.pend_momt | rt.pend_maxamp)) return;
     GcLayer &L = rt.layers[rt.root];
     bool done = false;
-    if (rt.fuse_enabled && rt.pend_mass && rt.pend_open && rt.pend_momt && L.laycord == 0) {
+    if (rt.fuse_enabled && rt.pend_mass && rt.pend_open && rt.pend_momt && L.laycord == 0 && L.laygov == 0) {
         done = gc_fused_step(L, rt.pend_maxamp != 0, false, 0, 0.0f, 0, nullptr, nullptr, rt.stream);
         if (done) rt.launches++;
     }

@@ -45,6 +45,7 @@ struct GcLayerDev {
     const float *h, *hp, *hq;
     const float *r2, *r4;        /* only when explicit_r24 */
     const float *rows;           /* [ny][GC_ROWW] */
+    const float *rows2;          /* [ny][2] R0, R22 (nonlinear spherical layers) */
     float *dz2;                  /* nonlinear layers */
     float *xflux, *yflux;        /* [2*nx], [2*ny] forecast caches */
     float *zmax;

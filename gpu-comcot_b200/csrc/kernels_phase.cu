@@ -21,9 +21,6 @@ __device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 /* ---------------------------------------------------------------- */
 /* continuity                                                        */
 /* ---------------------------------------------------------------- */
-/* MASS_S (mass.f90:61-100).  Child edge rows i==0 / j==0 are not computed by
- * the reference; they keep the value of time level 1 (the UPDATE edge copy of
- * all_grids.f90:323-324 made them equal), so they are carried over here. */
 /* Programmatic dependent launch: a kernel launched with it may be scheduled
  * while its predecessor still runs; griddepcontrol.wait then blocks until
  * the predecessor has completed and its writes are visible, so it comes
@@ -34,6 +31,11 @@ __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+/* MASS_S (mass.f90:61-100) and, NONLIN, CONMASS_S (mass.f90:226-278).  Child
+ * edge rows i==0 / j==0 are not computed by the reference; they keep the
+ * value of time level 1 (the UPDATE edge copy of all_grids.f90:323-324 made
+ * them equal), so they are carried over here. */
+template <bool NONLIN>
 __global__ void k_mass_s(GcLayerDev L) {
     pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
@@ -47,6 +49,24 @@ __global__ void k_mass_s(GcLayerDev L) {
         return;
     }
     float h = L.h[c];
+    if (NONLIN) {
+        float dz, z;
+        if (h >= CC_ELMAX) {
+            float r1 = GC_ROW(L, GC_R1, j), r11 = GC_ROW(L, GC_R11, j);
+            float r6 = GC_ROW(L, GC_R6, j), r6m = GC_ROW(L, GC_R6, j - 1);
+            float zz = L.z1[c] - r1 * (L.m1[c] - L.m1[c - 1])
+                       - r11 * (L.n1[c] * r6 - L.n1[c - L.pitch] * r6m);
+            if (fabs_(zz) < CC_EPS) zz = 0.0f;
+            float dd = zz + h;
+            if (dd >= CC_GX) { dz = dd; z = zz; }
+            else { dz = 0.0f; z = -h; }
+        } else {
+            dz = 0.0f; z = -h;
+        }
+        L.dz2[c] = dz;
+        L.z2[c] = z;
+        return;
+    }
     float out;
     if (h > CC_GX) {
         float r1 = GC_ROW(L, GC_R1, j), r11 = GC_ROW(L, GC_R11, j);
@@ -277,6 +297,13 @@ __device__ __forceinline__ void wave_breaking(const GcLayerDev &L, size_t c, flo
     }
 }
 
+/* CONMOME (moment.f90:280-780) and, SPH, CONMOME_S (moment.f90:783-1268):
+ * the same structure; the spherical form takes the wet/dry face depth as
+ * HP + (Z + Z(I+1))/2, the pressure coefficient R2 / R4 of its row, Coriolis
+ * +4 R3 XQQ / -4 R5 XPP, advection coefficients R21 (= R1) / R0 / R22 per
+ * row, and applies the y friction to XQ (the Cartesian routine subtracts it
+ * from XP, moment.f90:672). */
+template <bool SPH>
 __global__ void k_conmome(GcLayerDev L) {
     pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
@@ -310,9 +337,9 @@ __global__ void k_conmome(GcLayerDev L) {
                 if (dzc > CC_GX && dzp > CC_GX) {
                     dd = D.dp2(i, j); df = D.dp1(i, j);
                 } else if (dzc > CC_GX && dzp <= CC_GX && hz[cp] + z[c] > CC_GX) {
-                    dd = 0.5f * dzc; df = dd;
+                    dd = SPH ? L.hp[c] + 0.5f * (z[c] + z[cp]) : 0.5f * dzc; df = dd;
                 } else if (dzc <= CC_GX && dzp > CC_GX && hz[c] + z[cp] > CC_GX) {
-                    dd = 0.5f * dzp; df = dd;
+                    dd = SPH ? L.hp[c] + 0.5f * (z[c] + z[cp]) : 0.5f * dzp; df = dd;
                 } else {
                     noflux = true;
                 }
@@ -325,49 +352,53 @@ __global__ void k_conmome(GcLayerDev L) {
                     ff = konst * fm * fm * sqrtf(p[c] * p[c] + xqq * xqq) / cc_powf(df, CC_MANNEXP);
                 else
                     ff = 0.0f;
-                float xp = p[c] - L.grx * dd * (z[cp] - z[c]);
+                const float cpx = SPH ? GC_ROW(L, GC_CX, j) : L.grx;
+                float xp = p[c] - cpx * dd * (z[cp] - z[c]);
                 if (L.modscm == 0 && j + 1 < jy) {
-                    float scm = L.grx * dd / 12.0f
+                    float scm = cpx * dd / 12.0f
                                 * ((AT(z, ip1, jp1) - 2.0f * z[cp] + AT(z, ip1, jm1))
                                    - (AT(z, i, jp1) - 2.0f * z[c] + AT(z, i, jm1)));
                     xp = xp - scm;
                 }
                 if (L.fric_switch != 1) xp = xp - ff * p[c];
+                if (SPH) xp = xp + 4.0f * GC_ROW(L, GC_R3, j) * xqq;
+                const float ax = SPH ? GC_ROW(L, GC_R1, j) : L.rx;   /* R21 = R1 */
+                const float ay = SPH ? L.rows2[2 * (size_t)j] : L.ry;   /* R0 */
                 float dp1c = D.dp1(i, j);
                 if (L.linchk == 1 && dp1c >= CC_GX && span) {
                     float advx, advy;
                     if (p[c] < 0.0f) {
                         float dp1p = D.dp1(ip1, j);
                         if (dp1p < CC_GX || D.d(ip1, j) < CC_GX)
-                            advx = L.rx * (-(p[c] * p[c] / dp1c));
+                            advx = ax * (-(p[c] * p[c] / dp1c));
                         else
-                            advx = L.rx * (p[cp] * p[cp] / dp1p - p[c] * p[c] / dp1c);
+                            advx = ax * (p[cp] * p[cp] / dp1p - p[c] * p[c] / dp1c);
                     } else {
                         float dp1m = D.dp1(im1, j);
                         float pm = AT(p, im1, j);
                         if (dp1m < CC_GX || D.d(i, j) < CC_GX)
-                            advx = L.rx * (p[c] * p[c] / dp1c);
+                            advx = ax * (p[c] * p[c] / dp1c);
                         else
-                            advx = L.rx * (p[c] * p[c] / dp1c - pm * pm / dp1m);
+                            advx = ax * (p[c] * p[c] / dp1c - pm * pm / dp1m);
                     }
                     if (xqq < 0.0f) {
                         if (D.d(i, jp1) < CC_GX || D.d(ip1, jp1) < CC_GX) {
-                            advy = L.ry * (-(p[c] * xqq / dp1c));
+                            advy = ay * (-(p[c] * xqq / dp1c));
                         } else if (D.dp1(i, jp1) < CC_GX) {
-                            advy = L.ry * (-(p[c] * xqq / dp1c));
+                            advy = ay * (-(p[c] * xqq / dp1c));
                         } else {
                             float xqe = 0.25f * (AT(q, i, jp1) + AT(q, ip1, jp1) + q[c] + q[cp]);
-                            advy = L.ry * (AT(p, i, jp1) * xqe / D.dp1(i, jp1) - p[c] * xqq / dp1c);
+                            advy = ay * (AT(p, i, jp1) * xqe / D.dp1(i, jp1) - p[c] * xqq / dp1c);
                         }
                     } else {
                         if (D.d(i, jm1) < CC_GX || D.d(ip1, jm1) < CC_GX) {
-                            advy = L.ry * (p[c] * xqq / dp1c);
+                            advy = ay * (p[c] * xqq / dp1c);
                         } else if (D.dp1(i, jm1) < CC_GX) {
-                            advy = L.ry * (p[c] * xqq / dp1c);
+                            advy = ay * (p[c] * xqq / dp1c);
                         } else {
                             float xqe = 0.25f * (AT(q, i, jm1) + AT(q, ip1, jm1) + AT(q, i, j - 2)
                                                  + AT(q, ip1, j - 2));
-                            advy = L.ry * (p[c] * xqq / dp1c - AT(p, i, jm1) * xqe / D.dp1(i, jm1));
+                            advy = ay * (p[c] * xqq / dp1c - AT(p, i, jm1) * xqe / D.dp1(i, jm1));
                         }
                     }
                     wave_breaking(L, c, advx, advy);
@@ -398,9 +429,9 @@ __global__ void k_conmome(GcLayerDev L) {
                 if (dzc > CC_GX && dzq > CC_GX) {
                     dd = D.dq2(i, j); df = D.dq1(i, j);
                 } else if (dzc > CC_GX && dzq <= CC_GX && hz[cq] + z[c] > CC_GX) {
-                    dd = 0.5f * dzc; df = dd;
+                    dd = SPH ? L.hq[c] + 0.5f * (z[c] + z[cq]) : 0.5f * dzc; df = dd;
                 } else if (dzc <= CC_GX && dzq > CC_GX && hz[c] + z[cq] > CC_GX) {
-                    dd = 0.5f * dzq; df = dd;
+                    dd = SPH ? L.hq[c] + 0.5f * (z[c] + z[cq]) : 0.5f * dzq; df = dd;
                 } else {
                     noflux = true;
                 }
@@ -413,49 +444,55 @@ __global__ void k_conmome(GcLayerDev L) {
                     ff = konst * fm * fm * sqrtf(q[c] * q[c] + xpp * xpp) / cc_powf(df, CC_MANNEXP);
                 else
                     ff = 0.0f;
-                float xq = q[c] - L.gry * dd * (z[cq] - z[c]);
+                const float cqy = SPH ? GC_ROW(L, GC_CY, j) : L.gry;
+                float xq = q[c] - cqy * dd * (z[cq] - z[c]);
                 if (L.modscm == 0 && i + 1 < ix) {
-                    float scm = L.gry * dd / 12.0f
+                    float scm = cqy * dd / 12.0f
                                 * ((AT(z, ip1, jp1) - 2.0f * z[cq] + AT(z, im1, jp1))
                                    - (AT(z, ip1, j) - 2.0f * z[c] + AT(z, im1, j)));
                     xq = xq - scm;
                 }
-                /* moment.f90:672 applies -FF*Q to XP, which is unused: no term on XQ */
+                /* CONMOME applies -FF*Q to XP, which is unused (moment.f90:672):
+                 * no term on XQ; CONMOME_S applies it to XQ (moment.f90:1150) */
+                if (SPH && L.fric_switch != 1) xq = xq - ff * q[c];
+                if (SPH) xq = xq - 4.0f * GC_ROW(L, GC_R5, j) * xpp;
+                const float by = SPH ? L.rows2[2 * (size_t)j] : L.ry;        /* R0 */
+                const float bx = SPH ? L.rows2[2 * (size_t)j + 1] : L.rx;    /* R22 */
                 float dq1c = D.dq1(i, j);
                 if (L.linchk == 1 && dq1c >= CC_GX && span) {
                     float advx, advy;
                     if (q[c] < 0.0f) {
                         float dq1q = D.dq1(i, jp1);
                         if (dq1q < CC_GX || D.d(i, jp1) < CC_GX)
-                            advy = L.ry * (-(q[c] * q[c] / dq1c));
+                            advy = by * (-(q[c] * q[c] / dq1c));
                         else
-                            advy = L.ry * (q[cq] * q[cq] / dq1q - q[c] * q[c] / dq1c);
+                            advy = by * (q[cq] * q[cq] / dq1q - q[c] * q[c] / dq1c);
                     } else {
                         float dq1m = D.dq1(i, jm1);
                         float qm = AT(q, i, jm1);
                         if (dq1m < CC_GX || D.d(i, j) < CC_GX)
-                            advy = L.ry * (q[c] * q[c] / dq1c);
+                            advy = by * (q[c] * q[c] / dq1c);
                         else
-                            advy = L.ry * (q[c] * q[c] / dq1c - qm * qm / dq1m);
+                            advy = by * (q[c] * q[c] / dq1c - qm * qm / dq1m);
                     }
                     if (xpp < 0.0f) {
                         if (D.d(ip1, j) < CC_GX || D.d(ip1, jp1) < CC_GX) {
-                            advx = L.rx * (-(q[c] * xpp / dq1c));
+                            advx = bx * (-(q[c] * xpp / dq1c));
                         } else if (D.dq1(ip1, j) < CC_GX) {
-                            advx = L.rx * (-(q[c] * xpp / dq1c));
+                            advx = bx * (-(q[c] * xpp / dq1c));
                         } else {
                             float xpe = 0.25f * (AT(p, ip1, j) + AT(p, ip1, jp1) + p[c] + p[cq]);
-                            advx = L.rx * (AT(q, ip1, j) * xpe / D.dq1(ip1, j) - q[c] * xpp / dq1c);
+                            advx = bx * (AT(q, ip1, j) * xpe / D.dq1(ip1, j) - q[c] * xpp / dq1c);
                         }
                     } else {
                         if (D.d(im1, j) < CC_GX || D.d(im1, jp1) < CC_GX) {
-                            advx = L.rx * (q[c] * xpp / dq1c);
+                            advx = bx * (q[c] * xpp / dq1c);
                         } else if (D.dq1(i - 1, j) < CC_GX) {
-                            advx = L.rx * (q[c] * xpp / dq1c);
+                            advx = bx * (q[c] * xpp / dq1c);
                         } else {
                             float xpe = 0.25f * (AT(p, im1, j) + AT(p, im1, jp1) + AT(p, i - 2, j)
                                                  + AT(p, i - 2, jp1));
-                            advx = L.rx * (q[c] * xpp / dq1c - AT(q, im1, j) * xpe / D.dq1(im1, j));
+                            advx = bx * (q[c] * xpp / dq1c - AT(q, im1, j) * xpe / D.dq1(im1, j));
                         }
                     }
                     wave_breaking(L, c, advx, advy);
@@ -789,14 +826,16 @@ inline dim3 grid2(const GcLayerDev &L) {
 } // namespace
 
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0) launch(k_mass_s, grid2(L), dim3(BX, BY), 0, s, L);
+    if (L.laycord == 0 && L.laygov == 1) launch(k_mass_s<true>, grid2(L), dim3(BX, BY), 0, s, L);
+    else if (L.laycord == 0) launch(k_mass_s<false>, grid2(L), dim3(BX, BY), 0, s, L);
     else if (L.laygov == 1) launch(k_mass_c<true>, grid2(L), dim3(BX, BY), 0, s, L);
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
-    else if (L.laygov == 1) launch(k_conmome, grid2(L), dim3(BX, BY), 0, s, L);
+    if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, grid2(L), dim3(BX, BY), 0, s, L);
+    else if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
+    else if (L.laygov == 1) launch(k_conmome<false>, grid2(L), dim3(BX, BY), 0, s, L);
     else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);
 }
 

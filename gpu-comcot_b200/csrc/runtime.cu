@@ -73,7 +73,7 @@ GcLayerDev GcLayer::view() const {
     d.z1 = z[cur]; d.m1 = m[cur]; d.n1 = n[cur];
     d.z1w = z[cur]; d.m1w = m[cur]; d.n1w = n[cur];
     d.z2 = z[o]; d.m2 = m[o]; d.n2 = n[o];
-    d.h = h; d.hp = hp; d.hq = hq; d.r2 = r2; d.r4 = r4; d.rows = rows; d.dz2 = dz2;
+    d.h = h; d.hp = hp; d.hq = hq; d.r2 = r2; d.r4 = r4; d.rows = rows; d.dz2 = dz2; d.rows2 = rows2;
     d.xflux = xflux; d.yflux = yflux; d.zmax = zmax; d.arrival = arrival;
     return d;
 }
@@ -88,12 +88,14 @@ int gc_layer_alloc(GcLayer &L) {
     size_t field = align256((size_t)L.pitch * L.ny * sizeof(float));
     size_t rows = align256((size_t)GC_ROWW * L.ny * sizeof(float));
     size_t nfield = 6 /* z,m,n x2 */ + 1 /* h */ + 1 /* zmax */ + 1 /* arrival */;
-    bool cart = L.laycord == 1;
+    bool cart = L.laycord == 1 || L.laygov == 1; /* layers that read HP, HQ */
+    bool nls = L.laycord == 0 && L.laygov == 1;  /* nonlinear spherical: R0, R22 rows */
     if (cart) nfield += 2;           /* hp, hq */
     if (L.laygov == 1) nfield += 1;  /* dz2 */
     if (L.explicit_r24) nfield += 2; /* r2, r4 */
     size_t flux = align256((size_t)2 * L.nx * sizeof(float)) + align256((size_t)2 * L.ny * sizeof(float));
-    size_t total = nfield * field + rows + flux;
+    size_t rows2b = nls ? align256((size_t)2 * L.ny * sizeof(float)) : 0;
+    size_t total = nfield * field + rows + flux + rows2b;
     void *blk = nullptr;
     cudaError_t e = cudaMalloc(&blk, total);
     if (e != cudaSuccess) {
@@ -119,6 +121,7 @@ int gc_layer_alloc(GcLayer &L) {
     L.rows = (float *)take(rows);
     L.xflux = (float *)take(align256((size_t)2 * L.nx * sizeof(float)));
     L.yflux = (float *)take(align256((size_t)2 * L.ny * sizeof(float)));
+    L.rows2 = nls ? (float *)take(rows2b) : nullptr;
     L.block = blk;
     L.block_bytes = total;
     /* arrival starts at -1 (no arrival yet) */
@@ -249,6 +252,26 @@ void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, fl
     p.hq.assign(HQ ? HQ : (const float *)nullptr, HQ ? HQ + cells : (const float *)nullptr);
 }
 
+/* extension: the nonlinear spherical advection coefficients of PARA
+ * (comcot.f90:727-733): R0, R21 (= R1) and R22, NX x NY arrays read at row
+ * I = 1 like R1.  Call before gcomcot_init_layer_ for a layer with
+ * LAYCORD = 0, LAYGOV = 1, after gcomcot_set_layer_params_. */
+void gcomcot_set_layer_coefs_(int *id, float *R0, float *R21, float *R22, int *nx, int *ny) {
+    init_runtime();
+    (void)R21;
+    if (*id < 0 || *id >= GC_MAX_LAYERS || *nx < 1 || *ny < 1 || !R0 || !R22) {
+        fprintf(stderr, "ERROR: invalid layerid or coefficient arrays\n");
+        exit(EXIT_FAILURE);
+    }
+    GcPendingParams &p = g_rt.pending[*id];
+    p.r0.resize((size_t)*ny);
+    p.r22.resize((size_t)*ny);
+    for (int j = 0; j < *ny; j++) {
+        p.r0[j] = R0[(size_t)j * *nx];
+        p.r22[j] = R22[(size_t)j * *nx];
+    }
+}
+
 /* GPUcomcot.cu:214-251 */
 void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, int *rel_time,
                          int *corners, float *grx, float *gry, float *R1_f, float *R2_f,
@@ -310,9 +333,23 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
     std::vector<float> rowblk((size_t)GC_ROWW * L.ny, 0.0f);
     if (L.laycord == 0) {
         std::vector<float> cx((size_t)L.ny, 0.0f), cy((size_t)L.ny, 0.0f);
-        bool f2 = factor_rows(L.nx, L.ny, H_f, R2_f, true, cx.data());
-        bool f4 = factor_rows(L.nx, L.ny, H_f, R4_f, false, cy.data());
-        L.explicit_r24 = !(f2 && f4);
+        if (L.laygov == 1) {
+            /* nonlinear spherical: R2, R4 carry no depth factor (comcot.f90:736-738,
+             * 745-747), one value per row */
+            for (int j = 0; j < L.ny; j++) {
+                cx[j] = R2_f[(size_t)j * L.nx];
+                cy[j] = R4_f[(size_t)j * L.nx];
+            }
+            L.explicit_r24 = false;
+            if (!pp.set || pp.r0.size() != (size_t)L.ny || pp.r22.size() != (size_t)L.ny) {
+                fprintf(stderr, "gcomcot: nonlinear spherical layer %d needs gcomcot_set_layer_coefs_ first\n", L.id);
+                exit(EXIT_FAILURE);
+            }
+        } else {
+            bool f2 = factor_rows(L.nx, L.ny, H_f, R2_f, true, cx.data());
+            bool f4 = factor_rows(L.nx, L.ny, H_f, R4_f, false, cy.data());
+            L.explicit_r24 = !(f2 && f4);
+        }
         for (int j = 0; j < L.ny; j++) {
             float *rw = &rowblk[(size_t)j * GC_ROWW];
             rw[GC_R1] = R1_f[(size_t)j * L.nx];
@@ -334,7 +371,14 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
         if (gc_layer_upload_field(L, L.r2, R2_f) != GC_OK) exit(EXIT_FAILURE);
         if (gc_layer_upload_field(L, L.r4, R4_f) != GC_OK) exit(EXIT_FAILURE);
     }
-    if (L.laycord == 1) {
+    if (L.rows2) {
+        std::vector<float> r2b((size_t)2 * L.ny);
+        for (int j = 0; j < L.ny; j++) { r2b[2 * j] = pp.r0[j]; r2b[2 * j + 1] = pp.r22[j]; }
+        GC_CUDA_OR_DIE(cudaMemcpyAsync(L.rows2, r2b.data(), r2b.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                       g_rt.stream));
+        GC_CUDA_OR_DIE(cudaStreamSynchronize(g_rt.stream));
+    }
+    if (L.hp) {
         /* HP/HQ from the caller, else PQ_DEPTH (initialization.f90:2501-2526) */
         std::vector<float> hp(cells, 0.0f), hq(cells, 0.0f);
         if (pp.set && pp.hp.size() == cells && pp.hq.size() == cells) {

@@ -23,6 +23,7 @@ struct GcLayer {
     float *z[2] = {nullptr, nullptr}, *m[2] = {nullptr, nullptr}, *n[2] = {nullptr, nullptr};
     float *h = nullptr, *hp = nullptr, *hq = nullptr, *r2 = nullptr, *r4 = nullptr;
     float *rows = nullptr, *dz2 = nullptr, *xflux = nullptr, *yflux = nullptr, *zmax = nullptr;
+    float *rows2 = nullptr; /* [ny][2] R0, R22 of nonlinear spherical layers */
     int *arrival = nullptr;
     int cur = 0;          /* buffer index holding time level 1 */
     bool z2_valid = false; /* level-2 buffer holds the reference's Z(:,:,2) */
@@ -36,6 +37,7 @@ struct GcPendingParams {
     int laycord = 0, laygov = 0, linchk = 1, modscm = 1, fric_switch = 1;
     float dt = 0, rx = 0, ry = 0, grx = 0, gry = 0, fric_coef = 0;
     std::vector<float> hp, hq;
+    std::vector<float> r0, r22; /* per row, from gcomcot_set_layer_coefs_ */
 };
 
 struct GcRuntime {

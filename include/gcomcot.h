@@ -69,6 +69,12 @@ void jnz_dbglaunch_(float *Z_f, int *outid, int *inid);
 void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, float *rx, float *ry,
                                float *grx, float *gry, int *fric_switch, float *fric_coef,
                                int *linchk, int *modscm, int *nx, int *ny, float *HP, float *HQ);
+/* no counterpart in the reference, whose device path has no nonlinear
+ * spherical solver: R0, R21, R22 of PARA (comcot.f90:727-733) for a layer
+ * with LAYCORD 0, LAYGOV 1 (CONMASS_S / CONMOME_S); NX x NY arrays read at
+ * row I = 1.  Call after gcomcot_set_layer_params_, before
+ * gcomcot_init_layer_. */
+void gcomcot_set_layer_coefs_(int *id, float *R0, float *R21, float *R22, int *nx, int *ny);
 /* no counterpart in the reference: arrival-step tracking on the outer layer */
 void gcomcot_set_arrival_(int *id, float *thr);
 void gcomcot_get_arrival_(int *arrival, int *id);

@@ -157,11 +157,42 @@ static void conmass_rows(void *ctx, int js, int je) {
     }
 }
 
+/* CONMASS_S (mass.f90:226-278) nonlinear continuity, spherical, moving shoreline */
+static void conmass_s_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int is = 2, ie = (L->id == 1) ? L->nx - 1 : L->nx;
+    for (int j = js; j <= je; j++) {
+        int jm1 = j - 1;
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(L, i, j);
+            REAL h = L->h[c];
+            if (h >= R(CC_ELMAX)) {
+                REAL zz = L->z1[c] - L->r1[j - 1] * (L->m1[c] - L->m1[IDX(L, i - 1, j)])
+                          - L->r11[j - 1] * (L->n1[c] * L->r6[j - 1]
+                                             - L->n1[IDX(L, i, jm1)] * L->r6[jm1 - 1]);
+                if (o_abs(zz) < R(CC_EPS)) zz = R(0);
+                REAL dd = zz + h;
+                if (dd >= R(CC_GX)) {
+                    L->dz2[c] = dd;
+                    L->z2[c] = zz;
+                } else {
+                    L->dz2[c] = R(0);
+                    L->z2[c] = -h;
+                }
+            } else {
+                L->dz2[c] = R(0);
+                L->z2[c] = -h;
+            }
+        }
+    }
+}
+
 void ocl_mass(ocl_layer *L) {
     /* dispatcher: mass.f90:18-52.  Edge rows: I=2.., J=2.. (mass.f90:70-78) */
     int je = (L->id == 1) ? L->ny - 1 : L->ny;
     if (L->laycord == 0) {
-        par_rows(mass_s_rows, L, 2, je);
+        if (L->laygov == 1) par_rows(conmass_s_rows, L, 2, je);
+        else par_rows(mass_s_rows, L, 2, je);
     } else if (L->laygov == 1) {
         par_rows(conmass_rows, L, 2, je);
     } else {
@@ -537,6 +568,213 @@ static void conmome_y_rows(void *vctx, int js, int je) {
     }
 }
 
+
+/* CONMOME_S (moment.f90:783-1268), nonlinear momentum in spherical
+ * coordinates.  As CONMOME but: the face depth on a wet/dry face is
+ * HP + (Z + Z(I+1))/2 (:906-915), the pressure term uses R2 / R4 of PARA
+ * (per row for LAYGOV 1), Coriolis enters as +4 R3 XQQ / -4 R5 XPP
+ * (:952, :1154), the advection coefficients are R21 (= R1), R0 and R22, and
+ * the y friction is applied to XQ. */
+static void conmome_s_x_rows(void *vctx, int js, int je) {
+    conmome_ctx *x = (conmome_ctx *)vctx;
+    ocl_layer *L = x->L;
+    int ix = L->nx, jy = L->ny;
+    int is = 2, ie = ix - 1;
+    if (L->id == 1) is = 1;
+    REAL konst = (L->fric_switch != 1) ? R(0.5) * R(L->dt) * R(CC_GRAV) : R(0);
+    REAL fm = R(L->fric_coef);
+    int ispans = CC_SPAN, ispane = ix - CC_SPAN, jspans = CC_SPAN, jspane = jy - CC_SPAN;
+    const REAL *dp1 = x->dp1, *dp2 = x->dp2, *dz = L->dz2, *z = L->z2, *hz = L->h;
+    const REAL *p = L->m1, *q = L->n1;
+    for (int j = js; j <= je; j++) {
+        int jp1 = MIN(j + 1, jy), jm1 = MAX(j - 1, 1);
+        REAL r2 = L->r2[IDX(L, 1, j)], r3 = L->r3[j - 1], r21 = L->r1[j - 1], r0 = L->r0[j - 1];
+        for (int i = is; i <= ie; i++) {
+            int ip1 = MIN(i + 1, ix), im1 = MAX(i - 1, 1);
+            size_t c = IDX(L, i, j), cp = IDX(L, ip1, j);
+            REAL dd = R(0), df = R(0), ff = R(0);
+            int noflux = 0;
+            if (hz[c] <= R(CC_ELMAX) || L->hp[c] <= R(CC_ELMAX)) {
+                noflux = 1;
+            } else {
+                if (dz[c] > R(CC_GX) && dz[cp] > R(CC_GX)) {
+                    dd = dp2[c]; df = dp1[c];
+                } else if (dz[c] > R(CC_GX) && dz[cp] <= R(CC_GX) && hz[cp] + z[c] > R(CC_GX)) {
+                    dd = L->hp[c] + R(0.5) * (z[c] + z[cp]); df = dd;
+                } else if (dz[c] <= R(CC_GX) && dz[cp] > R(CC_GX) && hz[c] + z[cp] > R(CC_GX)) {
+                    dd = L->hp[c] + R(0.5) * (z[c] + z[cp]); df = dd;
+                } else {
+                    noflux = 1;
+                }
+                if (!noflux && dd < R(CC_GX)) noflux = 1;
+            }
+            if (noflux) { L->m2[c] = R(0); continue; }
+            if (df < R(CC_DFMIN)) df = R(CC_DFMIN);
+            REAL xqq = R(0.25) * (q[c] + q[cp] + q[IDX(L, i, jm1)] + q[IDX(L, ip1, jm1)]);
+            if (L->fric_switch != 1)
+                ff = konst * fm * fm * o_sqrt(p[c] * p[c] + xqq * xqq) / o_pow(df, R(CC_MANNEXP));
+            else
+                ff = R(0);
+            REAL xp;
+            if (L->modscm == 0 && j < jy)
+                xp = p[c] - r2 * dd * (z[cp] - z[c])
+                     - r2 * dd / R(12)
+                           * ((z[IDX(L, ip1, jp1)] - R(2) * z[cp] + z[IDX(L, ip1, jm1)])
+                              - (z[IDX(L, i, jp1)] - R(2) * z[c] + z[IDX(L, i, jm1)]));
+            else
+                xp = p[c] - r2 * dd * (z[cp] - z[c]);
+            if (L->fric_switch != 1) xp = xp - ff * p[c];
+            xp = xp + R(4.0) * r3 * xqq;
+            if (L->linchk == 1 && dp1[c] >= R(CC_GX) && i > ispans && i < ispane && j > jspans
+                && j < jspane) {
+                REAL advx = R(0), advy = R(0);
+                if (p[c] < R(0)) {
+                    if (dp1[cp] < R(CC_GX) || dz[cp] < R(CC_GX))
+                        advx = r21 * (-(p[c] * p[c] / dp1[c]));
+                    else
+                        advx = r21 * (p[cp] * p[cp] / dp1[cp] - p[c] * p[c] / dp1[c]);
+                } else {
+                    size_t cm = IDX(L, im1, j);
+                    if (dp1[cm] < R(CC_GX) || dz[c] < R(CC_GX))
+                        advx = r21 * (p[c] * p[c] / dp1[c]);
+                    else
+                        advx = r21 * (p[c] * p[c] / dp1[c] - p[cm] * p[cm] / dp1[cm]);
+                }
+                if (xqq < R(0)) {
+                    size_t cj = IDX(L, i, jp1);
+                    if (dz[cj] < R(CC_GX) || dz[IDX(L, ip1, jp1)] < R(CC_GX)) {
+                        advy = r0 * (-(p[c] * xqq / dp1[c]));
+                    } else if (dp1[cj] < R(CC_GX)) {
+                        advy = r0 * (-(p[c] * xqq / dp1[c]));
+                    } else {
+                        REAL xqe = R(0.25) * (q[cj] + q[IDX(L, ip1, jp1)] + q[c] + q[cp]);
+                        advy = r0 * (p[cj] * xqe / dp1[cj] - p[c] * xqq / dp1[c]);
+                    }
+                } else {
+                    size_t cj = IDX(L, i, jm1);
+                    if (dz[cj] < R(CC_GX) || dz[IDX(L, ip1, jm1)] < R(CC_GX)) {
+                        advy = r0 * (p[c] * xqq / dp1[c]);
+                    } else if (dp1[cj] < R(CC_GX)) {
+                        advy = r0 * (p[c] * xqq / dp1[c]);
+                    } else {
+                        REAL xqe = R(0.25) * (q[cj] + q[IDX(L, ip1, jm1)] + q[IDX(L, i, j - 2)]
+                                              + q[IDX(L, ip1, j - 2)]);
+                        advy = r0 * (p[c] * xqq / dp1[c] - p[cj] * xqe / dp1[cj]);
+                    }
+                }
+                wave_breaking(L, c, &advx, &advy);
+                xp = xp - advx - advy;
+            }
+            if (L->fric_switch != 1) xp = xp / (R(1) + ff);
+            if (o_abs(xp) < R(CC_EPS)) xp = R(0);
+            REAL lim = R(CC_VLIMIT) * dd;
+            if (xp > lim) xp = lim;
+            if (xp < -lim) xp = -lim;
+            L->m2[c] = xp;
+        }
+    }
+}
+
+static void conmome_s_y_rows(void *vctx, int js, int je) {
+    conmome_ctx *x = (conmome_ctx *)vctx;
+    ocl_layer *L = x->L;
+    int ix = L->nx, jy = L->ny;
+    int is = 2, ie = ix;
+    if (L->id == 1) { is = 1; ie = ix - 1; }
+    REAL konst = (L->fric_switch != 1) ? R(0.5) * R(L->dt) * R(CC_GRAV) : R(0);
+    REAL fm = R(L->fric_coef);
+    int ispans = CC_SPAN, ispane = ix - CC_SPAN, jspans = CC_SPAN, jspane = jy - CC_SPAN;
+    const REAL *dq1 = x->dq1, *dq2 = x->dq2, *dz = L->dz2, *z = L->z2, *hz = L->h;
+    const REAL *p = L->m1, *q = L->n1;
+    for (int j = js; j <= je; j++) {
+        int jp1 = MIN(j + 1, jy), jm1 = MAX(j - 1, 1);
+        REAL r4 = L->r4[IDX(L, 1, j)], r5 = L->r5[j - 1], r0 = L->r0[j - 1], r22 = L->r22[j - 1];
+        for (int i = is; i <= ie; i++) {
+            int ip1 = MIN(i + 1, ix), im1 = MAX(i - 1, 1);
+            size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+            REAL dd = R(0), df = R(0), ff = R(0);
+            int noflux = 0;
+            if (hz[c] <= R(CC_ELMAX) || L->hq[c] <= R(CC_ELMAX)) {
+                noflux = 1;
+            } else {
+                if (dz[c] > R(CC_GX) && dz[cq] > R(CC_GX)) {
+                    dd = dq2[c]; df = dq1[c];
+                } else if (dz[c] > R(CC_GX) && dz[cq] <= R(CC_GX) && hz[cq] + z[c] > R(CC_GX)) {
+                    dd = L->hq[c] + R(0.5) * (z[c] + z[cq]); df = dd;
+                } else if (dz[c] <= R(CC_GX) && dz[cq] > R(CC_GX) && hz[c] + z[cq] > R(CC_GX)) {
+                    dd = L->hq[c] + R(0.5) * (z[c] + z[cq]); df = dd;
+                } else {
+                    noflux = 1;
+                }
+                if (!noflux && dd < R(CC_GX)) noflux = 1;
+            }
+            if (noflux) { L->n2[c] = R(0); continue; }
+            if (df < R(CC_DFMIN)) df = R(CC_DFMIN);
+            REAL xpp = R(0.25) * (p[c] + p[cq] + p[IDX(L, im1, j)] + p[IDX(L, im1, jp1)]);
+            if (L->fric_switch != 1)
+                ff = konst * fm * fm * o_sqrt(q[c] * q[c] + xpp * xpp) / o_pow(df, R(CC_MANNEXP));
+            else
+                ff = R(0);
+            REAL xq;
+            if (L->modscm == 0 && i < ix)
+                xq = q[c] - r4 * dd * (z[cq] - z[c])
+                     - r4 * dd / R(12)
+                           * ((z[IDX(L, ip1, jp1)] - R(2) * z[cq] + z[IDX(L, im1, jp1)])
+                              - (z[IDX(L, ip1, j)] - R(2) * z[c] + z[IDX(L, im1, j)]));
+            else
+                xq = q[c] - r4 * dd * (z[cq] - z[c]);
+            if (L->fric_switch != 1) xq = xq - ff * q[c];
+            xq = xq - R(4.0) * r5 * xpp;
+            if (L->linchk == 1 && dq1[c] >= R(CC_GX) && i > ispans && i < ispane && j > jspans
+                && j < jspane) {
+                REAL advx = R(0), advy = R(0);
+                if (q[c] < R(0)) {
+                    if (dq1[cq] < R(CC_GX) || dz[cq] < R(CC_GX))
+                        advy = r0 * (-(q[c] * q[c] / dq1[c]));
+                    else
+                        advy = r0 * (q[cq] * q[cq] / dq1[cq] - q[c] * q[c] / dq1[c]);
+                } else {
+                    size_t cm = IDX(L, i, jm1);
+                    if (dq1[cm] < R(CC_GX) || dz[c] < R(CC_GX))
+                        advy = r0 * (q[c] * q[c] / dq1[c]);
+                    else
+                        advy = r0 * (q[c] * q[c] / dq1[c] - q[cm] * q[cm] / dq1[cm]);
+                }
+                if (xpp < R(0)) {
+                    size_t ci = IDX(L, ip1, j);
+                    if (dz[ci] < R(CC_GX) || dz[IDX(L, ip1, jp1)] < R(CC_GX)) {
+                        advx = r22 * (-(q[c] * xpp / dq1[c]));
+                    } else if (dq1[ci] < R(CC_GX)) {
+                        advx = r22 * (-(q[c] * xpp / dq1[c]));
+                    } else {
+                        REAL xpe = R(0.25) * (p[ci] + p[IDX(L, ip1, jp1)] + p[c] + p[cq]);
+                        advx = r22 * (q[ci] * xpe / dq1[ci] - q[c] * xpp / dq1[c]);
+                    }
+                } else {
+                    size_t ci = IDX(L, im1, j);
+                    if (dz[ci] < R(CC_GX) || dz[IDX(L, im1, jp1)] < R(CC_GX)) {
+                        advx = r22 * (q[c] * xpp / dq1[c]);
+                    } else if (dq1[IDX(L, i - 1, j)] < R(CC_GX)) {
+                        advx = r22 * (q[c] * xpp / dq1[c]);
+                    } else {
+                        REAL xpe = R(0.25) * (p[ci] + p[IDX(L, im1, jp1)] + p[IDX(L, i - 2, j)]
+                                              + p[IDX(L, i - 2, jp1)]);
+                        advx = r22 * (q[c] * xpp / dq1[c] - q[ci] * xpe / dq1[ci]);
+                    }
+                }
+                wave_breaking(L, c, &advx, &advy);
+                xq = xq - advx - advy;
+            }
+            if (L->fric_switch != 1) xq = xq / (R(1) + ff);
+            if (o_abs(xq) < R(CC_EPS)) xq = R(0);
+            REAL lim = R(CC_VLIMIT) * dd;
+            if (xq > lim) xq = lim;
+            if (xq < -lim) xq = -lim;
+            L->n2[c] = xq;
+        }
+    }
+}
+
 static void conmome(ocl_layer *L) {
     size_t n = (size_t)L->nx * L->ny;
     conmome_ctx x;
@@ -544,19 +782,23 @@ static void conmome(ocl_layer *L) {
     x.dp1 = (REAL *)malloc(4 * n * sizeof(REAL));
     x.dp2 = x.dp1 + n; x.dq1 = x.dp2 + n; x.dq2 = x.dq1 + n;
     par_rows(conmome_pre_rows, &x, 1, L->ny);
-    /* x: children I=2..NX-1, J=2..NY; root I=1..NX-1, J=1..NY-1 (moment.f90:376-389) */
-    if (L->id == 1) par_rows(conmome_x_rows, &x, 1, L->ny - 1);
-    else par_rows(conmome_x_rows, &x, 2, L->ny);
+    /* x: children I=2..NX-1, J=2..NY; root I=1..NX-1, J=1..NY-1 (moment.f90:376-389,
+     * the same ranges in CONMOME_S, :867-878,1052-1063) */
+    rowfn gx = L->laycord == 0 ? conmome_s_x_rows : conmome_x_rows;
+    if (L->id == 1) par_rows(gx, &x, 1, L->ny - 1);
+    else par_rows(gx, &x, 2, L->ny);
     /* y: children I=2..NX, J=2..NY-1; root I=1..NX-1, J=1..NY-1 (moment.f90:586-599) */
-    if (L->id == 1) par_rows(conmome_y_rows, &x, 1, L->ny - 1);
-    else par_rows(conmome_y_rows, &x, 2, L->ny - 1);
+    rowfn fy = L->laycord == 0 ? conmome_s_y_rows : conmome_y_rows;
+    if (L->id == 1) par_rows(fy, &x, 1, L->ny - 1);
+    else par_rows(fy, &x, 2, L->ny - 1);
     free(x.dp1);
 }
 
 void ocl_moment(ocl_layer *L) {
     /* dispatcher moment.f90:21-54 */
     int js = (L->id == 1) ? 1 : 2;
-    if (L->laycord == 0) par_rows(momt_s_rows, L, js, L->ny);
+    if (L->laycord == 0 && L->laygov == 1) conmome(L);
+    else if (L->laycord == 0) par_rows(momt_s_rows, L, js, L->ny);
     else if (L->laygov == 1) conmome(L);
     else par_rows(momt_c_rows, L, js, L->ny);
 }
@@ -1001,6 +1243,21 @@ void ocl_para(int nx, int ny, int laygov, double dt, double dx_min, const double
                 r4[c] = rs / (dely * rad_min);
             }
         }
+    }
+}
+
+void ocl_para_nl(int ny, double dt, double dx_min, const double *lat, const double *del_y_min, REAL *r0,
+                 REAL *r22) {
+    /* R0 = RR/(DEL_Y*RAD_MIN), R22 = RR/COS_N/(DX*RAD_MIN) (comcot.f90:727,733) */
+    REAL rr = R(dt) / R(CC_R_EARTH);
+    REAL osixty = R(0.016666666667);
+    REAL rad_deg = R(CC_RAD_DEG), rad_min = R(CC_RAD_MIN);
+    for (int j = 1; j <= ny; j++) {
+        REAL y = R(lat[j - 1]), dely = R(del_y_min[j - 1]);
+        REAL ang_n = (y + R(0.5) * dely * osixty) * rad_deg;
+        REAL cos_n = sizeof(REAL) == sizeof(float) ? (REAL)cosf((float)ang_n) : (REAL)cos((double)ang_n);
+        r0[j - 1] = rr / (dely * rad_min);
+        r22[j - 1] = rr / cos_n / (R(dx_min) * rad_min);
     }
 }
 

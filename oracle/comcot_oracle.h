@@ -35,6 +35,7 @@ typedef struct {
     int corners[4];   /* IS, IE, JS, JE in the parent           (type_module.f90:99) */
     double dt, rx, ry, grx, gry, fric_coef;
     REAL *r1, *r11, *r6, *r3, *r5;        /* [ny] per-row spherical coefficients */
+    REAL *r0, *r22;                       /* [ny] nonlinear spherical advection (PARA, comcot.f90:727-733) */
     REAL *r2, *r4;                        /* [nx*ny] */
     REAL *h, *hp, *hq;                    /* [nx*ny] */
     REAL *z1, *z2, *m1, *m2, *n1, *n2;    /* [nx*ny] time levels 1 and 2 */
@@ -68,6 +69,9 @@ void ocl_pq_depth(int nx, int ny, const REAL *h, REAL *hp, REAL *hq);
 void ocl_para(int nx, int ny, int laygov, double dt, double dx_min,
               const double *lat, const double *del_y_min, const REAL *hp, const REAL *hq,
               REAL *r1, REAL *r11, REAL *r2, REAL *r3, REAL *r4, REAL *r5, REAL *r6);
+/* R0 and R22 of PARA (comcot.f90:727,733) per row */
+void ocl_para_nl(int ny, double dt, double dx_min, const double *lat, const double *del_y_min, REAL *r0,
+                 REAL *r22);
 int  ocl_rel_time(double dt_parent, double dx_m, double dy_m, double hmax, int nonlinear,
                   double *dt_child);
 void ocl_corners(int nx_p, const double *xp, int ny_p, const double *yp,

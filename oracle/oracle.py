@@ -94,7 +94,7 @@ class OLayer(C.Structure):
                                         "modscm", "fric_switch", "rel_size", "rel_time")]
                 + [("corners", C.c_int * 4)]
                 + [(n, C.c_double) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
-                + [(n, C.c_void_p) for n in ("r1", "r11", "r6", "r3", "r5", "r2", "r4", "h", "hp", "hq",
+                + [(n, C.c_void_p) for n in ("r1", "r11", "r6", "r3", "r5", "r0", "r22", "r2", "r4", "h", "hp", "hq",
                                              "z1", "z2", "m1", "m2", "n1", "n2", "dz2", "xflux", "yflux",
                                              "zmax", "arrival")])
 
@@ -132,8 +132,11 @@ class OracleRun:
         if c is not None:
             for nm in ("r1", "r11", "r6", "r3", "r5", "r2", "r4"):
                 f[nm] = self._a(getattr(c, nm))
+            for nm in ("r0", "r22"):
+                v = getattr(c, nm, None)
+                f[nm] = self._a(v if v is not None else np.zeros(ny))
         else:
-            for nm in ("r1", "r11", "r6", "r3", "r5"):
+            for nm in ("r1", "r11", "r6", "r3", "r5", "r0", "r22"):
                 f[nm] = self._a(np.zeros(ny))
             f["r2"] = self._a(np.zeros((ny, nx)))
             f["r4"] = self._a(np.zeros((ny, nx)))

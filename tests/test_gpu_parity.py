@@ -89,10 +89,12 @@ def test_nested_nonlinear_child(oracle_mod, rel_time):
     assert np.array_equal(cz.view(np.uint32), rc["z"].view(np.uint32))
 
 
-@pytest.mark.parametrize("kind", ["linear_cartesian", "linear_spherical"])
+@pytest.mark.parametrize("kind", ["linear_cartesian", "linear_spherical", "nonlinear_spherical"])
 def test_nested_linear_child(oracle_mod, kind):
-    """MASS_C/MOMT_C (LAYCORD 1, LAYGOV 0) and MASS_S/MOMT_S children"""
-    kw = {"child_laygov": 0} if kind == "linear_cartesian" else {"child_laycord": 0}
+    """MASS_C/MOMT_C (LAYCORD 1, LAYGOV 0), MASS_S/MOMT_S and
+    CONMASS_S/CONMOME_S (LAYCORD 0, LAYGOV 1) children"""
+    kw = {"linear_cartesian": {"child_laygov": 0}, "linear_spherical": {"child_laycord": 0},
+          "nonlinear_spherical": {"child_laycord": 0, "child_laygov": 1}}[kind]
     case = synth.nested_case("l", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 0, seed=5, rel_time=2, **kw)
     gpu, _, o, _ = _run_both(case, 50, oracle_mod)
     ref, rc = o.layer(0), o.layer(1)
@@ -102,3 +104,19 @@ def test_nested_linear_child(oracle_mod, kind):
                        (cn, rc["n"], "child N")):
         _cmp(a, b, what)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
+@pytest.mark.parametrize("shape", [(97, 81), (130, 7)])
+def test_nonlinear_spherical_root(oracle_mod, shape):
+    """CONMASS_S / CONMOME_S on the outermost layer, with land (wet/dry) and
+    Manning friction; the fused linear kernel must not take it"""
+    nx, ny = shape
+    case = synth.single_layer_case("ns", nx, ny, 2.0, 2.0, 0, seed=13, n_seamounts=5, shelf_cols=min(10, nx // 4),
+                                   land_cols=min(4, nx // 8), ngauges=0, laygov=1, amp=3.0)
+    gpu, _, o, _ = _run_both(case, 80, oracle_mod)
+    ref = o.layer(0)
+    for a, b, what in ((gpu["z"], ref["z"], "eta"), (gpu["mn"][0], ref["m"], "M"), (gpu["mn"][1], ref["n"], "N"),
+                       (gpu["zmax"], ref["zmax"], "zmax")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+    assert np.array_equal(gpu["arrival"], ref["arrival"])
