@@ -197,13 +197,16 @@ def run_c4(args, torch, dist, rank, world, local):
     srcs = synth.ensemble_sources(L.x, L.y, nscen, seed=40 + rank)
     case = Case("C4", [L], run_steps)
     tune_reps = 2
-    extra = 40 * (tune_reps + 1) + args.warmup  # the autotuner's steps (32 candidates)
+    from comcot_b200 import _lib
+    ncand = 2 * _lib.load().gc_engine_num_variants()  # tile variants x tile-height rules
+    extra = ncand * (tune_reps + 1) + args.warmup  # the autotuner's steps
     eng = Engine(budget=120 << 30)
     eng.config(variant=args.variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
     ids = [eng.add(case, z0=z, cls=cls, nsteps=run_steps + extra, gauges=[], arrival_thr=0.05) for z in srcs]
     variant = eng.autotune(tune_reps) if args.variant < 0 else args.variant
     eng.step(args.warmup)
+    eng.prepare()  # step-chunk graph built before the timed region
     eng.sync()
     stream = torch.cuda.ExternalStream(eng.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -295,6 +298,7 @@ def run_c3(args, torch, dist, rank, world, local):
     eng.config(variant=args.variant, use_graphs=1, chunk=64)
     eng.add(case)
     eng.step(args.warmup)
+    eng.prepare()  # step-chunk graph built before the timed region
     eng.sync()
     stream = torch.cuda.ExternalStream(eng.stream())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -565,8 +569,8 @@ def run_single(args, torch, dist, rank, world, local):
     from comcot_b200 import _lib
 
     lib = _lib.load()
-    nvar = 48  # room for the autotuner's steps (16 tile variants x 2 tile-height rules)
-    total = nvar * (tune_reps + 1) + args.warmup + args.steps + 8
+    ncand = 2 * lib.gc_engine_num_variants()  # the autotuner's candidates: tile variants x tile-height rules
+    total = ncand * (tune_reps + 1) + args.warmup + args.steps + 8
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)
     cells = case.root.nx * case.root.ny
@@ -577,6 +581,7 @@ def run_single(args, torch, dist, rank, world, local):
     eng.add(case)
     variant = eng.autotune(tune_reps) if args.variant < 0 else args.variant
     eng.step(args.warmup)
+    eng.prepare()  # step-chunk graph built before the timed region
     eng.sync()
     stream = torch.cuda.ExternalStream(eng.stream())
     ev0 = torch.cuda.Event(enable_timing=True)

@@ -211,6 +211,13 @@ class Engine:
     def autotune(self, reps=5) -> int:
         return self.lib.gc_engine_autotune(self.h, int(reps))
 
+    def prepare(self):
+        """builds the work list and the step-chunk graph now, so that the
+        next step() does not pay for them"""
+        rc = self.lib.gc_engine_prepare(self.h)
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_prepare failed: {rc}")
+
     def variant(self) -> int:
         return self.lib.gc_engine_variant(self.h)
 

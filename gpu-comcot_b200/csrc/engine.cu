@@ -150,6 +150,10 @@ struct gc_engine {
     cudaGraphExec_t gexec = nullptr;
     long long launches = 0;
     int nctas = 0;
+    /* a work list of one grid launches the single-grid kernel with this
+     * descriptor by value (no descriptor loads, fewer registers) */
+    bool single = false;
+    GcFusedGrid one_grid;
     long long chunk_launches = 0; /* kernels in one replay of the chunk graph */
     int pdl = 1;                  /* programmatic dependent launch (GCOMCOT_PDL=0 turns it off) */
     int ty_rule = 1;              /* tile-height rule (gc_fused_pick_ty), tuned with the variant */
@@ -245,8 +249,9 @@ static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_o
     }
     if (e->ntiles > 0) {
         for (int k = 0; k < count; k++) {
-            cudaError_t err = gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, d_base,
-                                                    step_off0 + k, e->nctas, e->stream);
+            cudaError_t err = e->single ? gc_fused_launch_one_at(e->variant, e->one_grid, d_base, step_off0 + k, e->stream)
+                                        : gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, d_base,
+                                                                step_off0 + k, e->nctas, e->stream);
             if (err != cudaSuccess) return err;
             e->launches++;
         }
@@ -293,8 +298,9 @@ static int eng_rebuild(gc_engine *e) {
         anx.push_back(e->classes[M.cls].nx);
         any.push_back(e->classes[M.cls].ny);
     }
+    const bool single = anx.size() == 1;
     const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data(),
-                                                       e->ty_rule);
+                                                       e->ty_rule, !single);
     /* active members grouped by class */
     for (size_t c = 0; c < e->classes.size(); c++) {
         EngClass &C = e->classes[c];
@@ -326,10 +332,12 @@ static int eng_rebuild(gc_engine *e) {
     /* the outer grid of a nested member is stepped alone on its own stream */
     for (int id : e->nested_ids) {
         EngMember &M = e->members[id];
-        M.fty = gc_fused_pick_ty(e->variant, 1, &e->classes[M.cls].nx, &e->classes[M.cls].ny, 1);
+        M.fty = gc_fused_pick_ty(e->variant, 1, &e->classes[M.cls].nx, &e->classes[M.cls].ny, 1, false);
     }
     e->ngrids = (int)grids.size();
     e->ntiles = (int)tiles.size();
+    e->single = single && e->ngrids == 1;
+    if (e->single) e->one_grid = grids[0];
     if (e->ngrids > e->grids_cap) {
         if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
         e->grids_cap = std::max(e->ngrids, 2 * e->grids_cap);
@@ -362,6 +370,26 @@ static void eng_retire(gc_engine *e) {
         }
 }
 
+/* captures and uploads the graph of one chunk of steps for the current work
+ * list */
+static cudaError_t eng_build_graph(gc_engine *e) {
+    cudaGraph_t graph;
+    long long before = e->launches;
+    cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return err;
+    cudaError_t lerr = eng_launch_steps(e, e->d_step, 1, e->chunk);
+    if (lerr == cudaSuccess) k_advance<<<1, 32, 0, e->stream>>>(e->d_step, e->chunk);
+    cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
+    e->chunk_launches = e->launches - before + 1; /* + k_advance */
+    e->launches = before;
+    if (lerr != cudaSuccess) return lerr;
+    if (cerr != cudaSuccess) return cerr;
+    err = cudaGraphInstantiate(&e->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return err;
+    return cudaGraphUpload(e->gexec, e->stream);
+}
+
 static int eng_issue(gc_engine *e, int nsteps) {
     int issued = 0;
     while (issued < nsteps) {
@@ -376,21 +404,7 @@ static int eng_issue(gc_engine *e, int nsteps) {
         if (e->use_graphs && horizon >= e->chunk) {
             /* the device counter must equal the host's step count */
             GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_step, &e->gstep, sizeof(int), cudaMemcpyHostToDevice, e->stream));
-            if (!e->gexec) {
-                cudaGraph_t graph;
-                long long before = e->launches;
-                GC_CUDA_OR_RET(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-                cudaError_t lerr = eng_launch_steps(e, e->d_step, 1, e->chunk);
-                if (lerr == cudaSuccess)
-                    k_advance<<<1, 32, 0, e->stream>>>(e->d_step, e->chunk);
-                cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
-                GC_CUDA_OR_RET(lerr);
-                GC_CUDA_OR_RET(cerr);
-                e->chunk_launches = e->launches - before + 1; /* + k_advance */
-                e->launches = before;
-                GC_CUDA_OR_RET(cudaGraphInstantiate(&e->gexec, graph, 0));
-                cudaGraphDestroy(graph);
-            }
+            if (!e->gexec) GC_CUDA_OR_RET(eng_build_graph(e));
             int reps = horizon / e->chunk;
             if (reps * e->chunk > nsteps - issued) reps = (nsteps - issued) / e->chunk;
             if (reps <= 0) reps = 0;
@@ -873,6 +887,16 @@ int gc_engine_autotune(gc_engine *e, int reps) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return best;
+}
+
+int gc_engine_prepare(gc_engine *e) {
+    if (!e) return GC_EINVAL;
+    eng_retire(e);
+    if (e->dirty && eng_rebuild(e) != GC_OK) return GC_ECUDA;
+    if (e->use_graphs && !e->gexec && (e->ntiles > 0 || !e->nested_ids.empty()))
+        GC_CUDA_OR_RET(eng_build_graph(e));
+    GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
+    return GC_OK;
 }
 
 int gc_engine_variant(gc_engine *e) { return e ? e->variant + gc_fused_num_variants() * e->ty_rule : GC_EINVAL; }

@@ -46,13 +46,15 @@ GcTileCfg gc_fused_variant(int v);
  * shortest tiles that keep the wave count of 16-row tiles, rule 1: the
  * height that minimises the busiest warp's rows (the autotuner tries both) */
 constexpr int GC_TY_RULES = 2;
-int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule = 0);
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule = 0, bool multi = true);
 /* launches the fused step over a work list: tiles[t] = {grid, tile within
  * that grid}; step = *step_base + step_off (step_base may be NULL) */
 cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles,
                                   int ntiles, const int *d_step_base, int step_off, int nctas,
                                   cudaStream_t s);
-int gc_fused_max_ctas(int variant);
+/* resident CTAs on the device: of the work-list kernel (multi) or of the
+ * single-grid kernel */
+int gc_fused_max_ctas(int variant, bool multi = true);
 /* 1 if a pipeline wait in the fused kernel gave up since the last call (clears it) */
 int gc_fused_take_error();
 /* single grid, descriptor by value */

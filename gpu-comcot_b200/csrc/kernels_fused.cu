@@ -660,8 +660,8 @@ int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x) {
     return tx * tyn;
 }
 
-int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule) {
-    const int slots = gc_fused_max_ctas(variant) * gc_fused_variant(variant).warps;
+int gc_fused_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule, bool multi) {
+    const int slots = gc_fused_max_ctas(variant, multi) * gc_fused_variant(variant).warps;
     auto tiles = [&](int ty) {
         long long t = 0;
         for (int g = 0; g < ngrids; g++) t += gc_fused_tiles(nx[g], ny[g], ty, nullptr);
@@ -713,14 +713,14 @@ cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int 
                         d_step_base, step_off);
 }
 
-int gc_fused_max_ctas(int variant) {
+int gc_fused_max_ctas(int variant, bool multi) {
     if (variant < 0 || variant >= kNumVariants) variant = 0;
     const Variant &v = kVariants[variant];
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     prepare(v);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v.multi, 32 * v.w, variant_smem(v));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, multi ? v.multi : v.one, 32 * v.w, variant_smem(v));
     return sms * (per > 0 ? per : 1);
 }
 

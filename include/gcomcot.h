@@ -190,6 +190,9 @@ long long gc_engine_member_bytes(gc_engine *e, int cls);
  * picks tile-height rule r) and use of CUDA graphs for step chunks */
 int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk);
 int gc_engine_autotune(gc_engine *e, int reps);
+/* builds the work list and the step-chunk graph for the current members
+ * ahead of the next gc_engine_step (otherwise the first chunk pays for them) */
+int gc_engine_prepare(gc_engine *e);
 int gc_engine_variant(gc_engine *e);
 /* number of compiled tile variants (all compute identical results) */
 int gc_engine_num_variants(void);
