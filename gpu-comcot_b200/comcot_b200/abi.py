@@ -82,6 +82,12 @@ class ReferenceSession:
                                 _lib.iptr(corners), _f(L.grx), _f(L.gry), _lib.fptr(R1), _lib.fptr(R2),
                                 _lib.fptr(R3), _lib.fptr(R4), _lib.fptr(R5), _lib.fptr(R6), _lib.fptr(R11),
                                 _lib.fptr(H), _lib.fptr(Z), _i(nx), _i(ny))
+        if L.sponge is not None:
+            # BC_TYPE 1: SPONGE_COEF's fields (comcot.f90:220)
+            cx = np.ascontiguousarray(L.sponge[0], dtype=F32)
+            cy = np.ascontiguousarray(L.sponge[1], dtype=F32)
+            self._keep += [cx, cy]
+            lib.gcomcot_set_sponge_(_i(L.id), _lib.fptr(cx), _lib.fptr(cy), _f(L.dt), _i(nx), _i(ny))
 
     # ---- one outer step exactly as comcot.f90:359-439 ----
     def step(self, maxamp: bool = True):
@@ -91,6 +97,8 @@ class ReferenceSession:
         if len(self.case.layers) > 1:
             lib.all_grid_launch_()
         lib.momt_launch_(None, None, None, _i(rid))
+        if self.case.root.sponge is not None:
+            lib.sponge_launch_(_i(rid))
         if maxamp:
             lib.maxamp_launch_(_i(rid))
         ts = [self.get_ts(g) for g in self.case.gauges]

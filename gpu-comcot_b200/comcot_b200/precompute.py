@@ -25,6 +25,7 @@ import numpy as np
 
 GRAV = np.float32(9.807)
 GX = np.float32(1.0e-5)
+EPS = np.float32(1.0e-10)
 R_EARTH = 6378000.0
 RAD_DEG = 0.01745329252
 RAD_MIN = 0.000290888208665721
@@ -187,3 +188,81 @@ def child_cartesian_spacing(yp, corners_, rel_size, dx_min_parent):
     dx = R_EARTH * math.cos(lat * RAD_DEG) * dlon / rel_size
     dy = R_EARTH * dlon / rel_size
     return dx, dy
+
+
+def h_mean(h: np.ndarray) -> np.float32:
+    """H_CALC (boundaries.f90:351-385): mean of the wet depths (H > GX),
+    accumulated in float with I outermost, as the Fortran loops run"""
+    hw = np.ascontiguousarray(h, dtype=F32).T.ravel()   # I outer, J inner
+    wet = hw[hw > F32(GX)]
+    if wet.size == 0:
+        return F32(0.0)
+    s = np.cumsum(wet, dtype=F32)[-1]                   # sequential float additions
+    return F32(s / F32(wet.size))
+
+
+def sponge_coef(x: np.ndarray, y: np.ndarray, h: np.ndarray, laycord: int):
+    """SPONGE_COEF (boundaries.f90:250-345), in float arithmetic: damping
+    coefficients [ny, nx] for X and Y over a band of twice the characteristic
+    wavelength (20 x mean wet depth) along the edges.  COEFX depends on I only
+    and COEFY on J only.  On a spherical layer the band width is converted to
+    degrees but the ramp is still divided by the width in metres, so every
+    coefficient falls below EPS and is 0, as in the reference."""
+    depth = h_mean(h)
+    if depth <= F32(GX):
+        depth = F32(GX)
+    pi, grav = F32(math.pi), F32(9.807)
+    wavelength = F32(20.0) * depth
+    width = F32(2.0) * wavelength
+    alpha_c = F32(10.0)
+    t = F32(wavelength / F32(math.sqrt(float(F32(grav * depth)))))
+    omega = F32(F32(F32(2.0) * pi) / t)
+    if laycord == 0:
+        sw = F32(F32(F32(width / F32(6378000.0)) * F32(180.0)) / pi)
+    else:
+        sw = width
+    r_max = width
+    xa = np.asarray(x, dtype=F32)
+    ya = np.asarray(y, dtype=F32)
+    xs, ys = F32(xa[0] + sw), F32(ya[0] + sw)
+    xe, ye = F32(xa[-1] - sw), F32(ya[-1] - sw)
+    em1 = F32(F32(math.exp(1.0)) - F32(1.0))
+
+    def ramp(v, lo, hi):
+        r = np.where(v <= lo, -(v - lo), np.where(v >= hi, v - hi, F32(0.0))).astype(F32)
+        r = np.clip(r, F32(0.0), r_max).astype(F32)
+        a = (r / r_max).astype(F32)
+        e = np.exp((a * a).astype(np.float64)).astype(F32)
+        c = ((alpha_c * omega) * (e - F32(1.0))).astype(F32) / em1
+        c = c.astype(F32)
+        return np.where(c <= F32(EPS), F32(0.0), c).astype(F32)
+
+    cxv = ramp(xa, xs, xe)
+    cyv = ramp(ya, ys, ye)
+    ny, nx = len(ya), len(xa)
+    return (np.ascontiguousarray(np.broadcast_to(cxv[None, :], (ny, nx))),
+            np.ascontiguousarray(np.broadcast_to(cyv[:, None], (ny, nx))))
+
+
+def bc_wall(h: np.ndarray, ini_switch: int = 0, incident: int = 0) -> np.ndarray:
+    """BC_WALL (boundaries.f90:388-428): a copy of H with the two outermost
+    rows / columns set to -999 m (land), all four sides unless a wave maker
+    (INI_SWITCH 2) enters through side INCIDENT (1 top, 2 bottom, 3 left,
+    4 right), which stays open"""
+    out = np.array(h, dtype=F32, copy=True)
+    sides = {"w": True, "s": True, "e": True, "n": True}
+    if ini_switch == 2:
+        # the Fortran leaves one side commented out per incident direction
+        open_side = {1: "n", 2: "s", 3: "w", 4: "e"}.get(incident)
+        if open_side is None:
+            return out
+        sides[open_side] = False
+    if sides["w"]:
+        out[:, 0:2] = -999.0
+    if sides["s"]:
+        out[0:2, :] = -999.0
+    if sides["e"]:
+        out[:, -2:] = -999.0
+    if sides["n"]:
+        out[-2:, :] = -999.0
+    return out

@@ -57,6 +57,7 @@ class LayerSpec:
     modscm: int = 1
     hp: np.ndarray | None = None
     hq: np.ndarray | None = None
+    sponge: tuple | None = None  # (COEFX, COEFY) [ny, nx] of SPONGE_COEF, outer layer only
 
 
 @dataclass

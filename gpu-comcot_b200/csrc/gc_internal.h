@@ -102,6 +102,7 @@ void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                    const int *corners, cudaStream_t s);
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
+void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s);
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s);
 /* max-eta (flags & 1), arrival (flags & 2) and gauge samples after one outer

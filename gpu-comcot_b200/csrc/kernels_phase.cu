@@ -734,6 +734,22 @@ __global__ void k_maxamp(GcLayerDev L) {
     if (!(m >= z)) L.zmax[c] = z;
 }
 
+/* SPONGE_LAYER (boundaries.f90:229-244) with separable coefficients,
+ * COEFX(I,J) = spx[I] and COEFY(I,J) = spy[J]: where either is positive,
+ * M2 += CX*DT*M1 and N2 += CY*DT*N1 */
+__global__ void k_sponge(GcLayerDev L, const float *__restrict__ spx, const float *__restrict__ spy, float dt) {
+    pdl_enter();
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const float cx = spx[i], cy = spy[j];
+    if (cx > 0.0f || cy > 0.0f) {
+        size_t c = (size_t)j * L.pitch + i;
+        L.m2[c] = L.m2[c] + cx * dt * L.m1[c];
+        L.n2[c] = L.n2[c] + cy * dt * L.n1[c];
+    }
+}
+
 __global__ void k_arrival(GcLayerDev L, int step, float thr) {
     pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
@@ -877,6 +893,10 @@ void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int r
 
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s) {
     launch(k_maxamp, grid2(L), dim3(BX, BY), 0, s, L);
+}
+
+void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s) {
+    launch(k_sponge, grid2(L), dim3(BX, BY), 0, s, L, spx, spy, dt);
 }
 
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s) {

@@ -288,6 +288,8 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
     }
     GcLayer &L = g_rt.layers[*layerid];
     if (L.used && L.block) cudaFree(L.block);
+    if (L.spx) cudaFree(L.spx);
+    if (L.spy) cudaFree(L.spy);
     L = GcLayer();
     L.used = true;
     L.id = *layerid; L.parent = *parent; L.level = *level;
@@ -462,6 +464,50 @@ void maxamp_launch_(const int *lid) {
     g_rt.launches++;
 }
 
+/* extension: the sponge layer of SPONGE_COEF / SPONGE_LAYER
+ * (boundaries.f90:206-345), whose device path the reference lacks (it
+ * applies it to host arrays the GPU run never reads back).  COEFX, COEFY are
+ * the NX x NY fields SPONGE_COEF makes; COEFX must depend on I only and
+ * COEFY on J only, as SPONGE_COEF's always do.  DT is the layer's time step.
+ * Call after gcomcot_init_layer_. */
+void gcomcot_set_sponge_(int *id, float *coefx, float *coefy, float *dt, int *nx, int *ny) {
+    GcLayer &L = layer_or_die(*id);
+    if (*nx != L.nx || *ny != L.ny || !coefx || !coefy) {
+        fprintf(stderr, "gcomcot: sponge coefficients of layer %d must be %dx%d\n", L.id, L.nx, L.ny);
+        exit(EXIT_FAILURE);
+    }
+    std::vector<float> vx((size_t)L.nx), vy((size_t)L.ny);
+    for (int i = 0; i < L.nx; i++) vx[i] = coefx[i];
+    for (int j = 0; j < L.ny; j++) vy[j] = coefy[(size_t)j * L.nx];
+    for (int j = 0; j < L.ny; j++)
+        for (int i = 0; i < L.nx; i++) {
+            const size_t c = (size_t)j * L.nx + i;
+            if (memcmp(&coefx[c], &vx[i], sizeof(float)) != 0 || memcmp(&coefy[c], &vy[j], sizeof(float)) != 0) {
+                fprintf(stderr, "gcomcot: sponge coefficients of layer %d are not COEFX(I) x COEFY(J)\n", L.id);
+                exit(EXIT_FAILURE);
+            }
+        }
+    if (!L.spx) GC_CUDA_OR_DIE(cudaMalloc((void **)&L.spx, (size_t)L.nx * sizeof(float)));
+    if (!L.spy) GC_CUDA_OR_DIE(cudaMalloc((void **)&L.spy, (size_t)L.ny * sizeof(float)));
+    GC_CUDA_OR_DIE(cudaMemcpy(L.spx, vx.data(), vx.size() * sizeof(float), cudaMemcpyHostToDevice));
+    GC_CUDA_OR_DIE(cudaMemcpy(L.spy, vy.data(), vy.size() * sizeof(float), cudaMemcpyHostToDevice));
+    L.sp_dt = *dt;
+}
+
+/* extension: SPONGE_LAYER (boundaries.f90:206-247) on the device, called
+ * where comcot.f90:403-406 calls it, after MOMT_LAUNCH */
+void sponge_launch_(const int *lid) {
+    gc_gauge_invalidate();
+    GcLayer &L = layer_or_die(*lid);
+    if (!L.spx || !L.spy) {
+        fprintf(stderr, "gcomcot: layer %d has no sponge coefficients (gcomcot_set_sponge_)\n", L.id);
+        exit(EXIT_FAILURE);
+    }
+    gc_flush();
+    gc_launch_sponge(L.view(), L.spx, L.spy, L.sp_dt, g_rt.stream);
+    g_rt.launches++;
+}
+
 /* GPUall_grids.cu:701-705: the nested sub-cycle of every child of layer 1 */
 void all_grid_launch_(void) {
     gc_gauge_invalidate();
@@ -572,6 +618,8 @@ void cuda_shutdown_(void) {
     cudaStreamSynchronize(g_rt.stream);
     for (int k = 0; k < GC_MAX_LAYERS; k++) {
         if (g_rt.layers[k].block) cudaFree(g_rt.layers[k].block);
+        if (g_rt.layers[k].spx) cudaFree(g_rt.layers[k].spx);
+        if (g_rt.layers[k].spy) cudaFree(g_rt.layers[k].spy);
         g_rt.layers[k] = GcLayer();
         g_rt.pending[k] = GcPendingParams();
     }

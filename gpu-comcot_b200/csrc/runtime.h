@@ -25,6 +25,8 @@ struct GcLayer {
     float *rows = nullptr, *dz2 = nullptr, *xflux = nullptr, *yflux = nullptr, *zmax = nullptr;
     float *rows2 = nullptr; /* [ny][2] R0, R22 of nonlinear spherical layers */
     int *arrival = nullptr;
+    float *spx = nullptr, *spy = nullptr; /* sponge coefficients per column / per row */
+    float sp_dt = 0.0f;
     int cur = 0;          /* buffer index holding time level 1 */
     bool z2_valid = false; /* level-2 buffer holds the reference's Z(:,:,2) */
     bool mn2_valid = false;

@@ -75,6 +75,14 @@ void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, fl
  * row I = 1.  Call after gcomcot_set_layer_params_, before
  * gcomcot_init_layer_. */
 void gcomcot_set_layer_coefs_(int *id, float *R0, float *R21, float *R22, int *nx, int *ny);
+/* no device counterpart in the reference (comcot.f90:403-406 applies
+ * SPONGE_LAYER to host arrays): the sponge band of SPONGE_COEF
+ * (boundaries.f90:250-345).  COEFX, COEFY are NX x NY fields, COEFX a
+ * function of I only and COEFY of J only; DT the layer's step.  Call after
+ * gcomcot_init_layer_. */
+void gcomcot_set_sponge_(int *id, float *coefx, float *coefy, float *dt, int *nx, int *ny);
+/* SPONGE_LAYER (boundaries.f90:206-247) on the device; call after momt_launch_ */
+void sponge_launch_(const int *lid);
 /* no counterpart in the reference: arrival-step tracking on the outer layer */
 void gcomcot_set_arrival_(int *id, float *thr);
 void gcomcot_get_arrival_(int *arrival, int *id);

@@ -1154,6 +1154,68 @@ static void all_grid_rec(ocl_layer *layers, int n, int parent_idx) {
 
 void ocl_all_grid(ocl_layer *layers, int n) { all_grid_rec(layers, n, 0); }
 
+void ocl_sponge(ocl_layer *L) {
+    /* SPONGE_LAYER (boundaries.f90:229-244): where either coefficient is
+     * positive, M2 += CX*DT*M1 and N2 += CY*DT*N1 */
+    const REAL dt = R(L->dt);
+    for (int j = 1; j <= L->ny; j++)
+        for (int i = 1; i <= L->nx; i++) {
+            size_t c = IDX(L, i, j);
+            REAL cx = L->spx[c], cy = L->spy[c];
+            if (cx > R(0) || cy > R(0)) {
+                L->m2[c] = L->m2[c] + cx * dt * L->m1[c];
+                L->n2[c] = L->n2[c] + cy * dt * L->n1[c];
+            }
+        }
+}
+
+void ocl_sponge_coef(int nx, int ny, int laycord, const REAL *x, const REAL *y, const REAL *h, REAL *coefx,
+                     REAL *coefy) {
+    /* H_CALC (boundaries.f90:351-385): mean wet depth, summed with I
+     * outermost as the Fortran loops run */
+    REAL hsum = R(0);
+    int k = 0;
+    for (int i = 1; i <= nx; i++)
+        for (int j = 1; j <= ny; j++) {
+            REAL hv = h[(size_t)(j - 1) * nx + (i - 1)];
+            if (hv > R(CC_GX)) {
+                hsum = hsum + hv;
+                k = k + 1;
+            }
+        }
+    REAL depth = k > 0 ? hsum / (REAL)k : R(0);
+    if (depth <= R(CC_GX)) depth = R(CC_GX);
+    /* SPONGE_COEF (boundaries.f90:271-345) */
+    const REAL pi = R(CC_PI), grav = R(CC_GRAV);
+    const REAL wavelength = R(20.0) * depth;
+    const REAL width = R(2.0) * wavelength;
+    const REAL alpha_c = R(10.0);
+    const REAL t = wavelength / o_sqrt(grav * depth);
+    const REAL omega = R(2.0) * pi / t;
+    const REAL sw = laycord == 0 ? width / R(CC_R_EARTH) * R(180.0) / pi : width;
+    const REAL r_max = width;
+    const REAL xs = x[0] + sw, ys = y[0] + sw, xe = x[nx - 1] - sw, ye = y[ny - 1] - sw;
+    const REAL em1 = o_exp(R(1.0)) - R(1.0);
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            const REAL x0 = x[i - 1], y0 = y[j - 1];
+            REAL rx = x0 <= xs ? -(x0 - xs) : (x0 >= xe ? x0 - xe : R(0));
+            REAL ry = y0 <= ys ? -(y0 - ys) : (y0 >= ye ? y0 - ye : R(0));
+            REAL xr = rx, yr = ry;
+            if (xr <= R(0)) xr = R(0);
+            if (yr <= R(0)) yr = R(0);
+            if (xr >= r_max) xr = r_max;
+            if (yr >= r_max) yr = r_max;
+            const REAL ax = xr / r_max, ay = yr / r_max;
+            REAL cx = alpha_c * omega * (o_exp(ax * ax) - R(1.0)) / em1;
+            REAL cy = alpha_c * omega * (o_exp(ay * ay) - R(1.0)) / em1;
+            if (cx <= R(CC_EPS)) cx = R(0);
+            if (cy <= R(CC_EPS)) cy = R(0);
+            coefx[(size_t)(j - 1) * nx + (i - 1)] = cx;
+            coefy[(size_t)(j - 1) * nx + (i - 1)] = cy;
+        }
+}
+
 void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr) {
     /* one outer step in the GPU driver's order (comcot.f90:359-439) */
     ocl_layer *L = &layers[0];
@@ -1161,6 +1223,7 @@ void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr) {
     ocl_open(L);
     ocl_all_grid(layers, n);
     ocl_moment(L);
+    if (L->spx && L->spy) ocl_sponge(L);
     if (L->zmax) ocl_maxamp(L);
     if (L->arrival) ocl_arrival(L, step, arrival_thr);
 }

@@ -43,6 +43,7 @@ typedef struct {
     REAL *xflux, *yflux;                  /* [2*nx], [2*ny] nesting forecast caches */
     REAL *zmax;                           /* [nx*ny] or NULL */
     int  *arrival;                        /* [nx*ny] or NULL */
+    REAL *spx, *spy;                      /* [nx*ny] SPONGE_COEFX/Y of the outer layer, or NULL */
 } ocl_layer;
 
 void ocl_set_threads(int n);
@@ -57,6 +58,12 @@ void ocl_jnq(ocl_layer *P, ocl_layer *C);
 void ocl_newq(ocl_layer *P, ocl_layer *C, int t);
 void ocl_jnz(ocl_layer *P, ocl_layer *C);
 void ocl_maxamp(ocl_layer *L);
+/* SPONGE_LAYER (boundaries.f90:206-247): after the momentum step */
+void ocl_sponge(ocl_layer *L);
+/* SPONGE_COEF with H_CALC (boundaries.f90:250-385): coefficient fields of a
+ * layer with axes x[nx], y[ny] (degrees, or metres for laycord 1) */
+void ocl_sponge_coef(int nx, int ny, int laycord, const REAL *x, const REAL *y, const REAL *h, REAL *coefx,
+                     REAL *coefy);
 void ocl_arrival(ocl_layer *L, int step, double thr);
 void ocl_all_grid(ocl_layer *layers, int n);
 void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr);

@@ -59,6 +59,9 @@ def load(dtype=np.float32):
                               C.c_double, C.c_void_p]
     lib.ocl_okada_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+    lib.ocl_sponge.argtypes = [C.c_void_p]
+    lib.ocl_sponge_coef.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
     lib.ocl_expf.argtypes = [C.c_float]
     lib.ocl_expf.restype = C.c_float
     lib.ocl_powf.argtypes = [C.c_float, C.c_float]
@@ -96,7 +99,7 @@ class OLayer(C.Structure):
                 + [(n, C.c_double) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
                 + [(n, C.c_void_p) for n in ("r1", "r11", "r6", "r3", "r5", "r0", "r22", "r2", "r4", "h", "hp", "hq",
                                              "z1", "z2", "m1", "m2", "n1", "n2", "dz2", "xflux", "yflux",
-                                             "zmax", "arrival")])
+                                             "zmax", "arrival", "spx", "spy")])
 
 
 class OracleRun:
@@ -150,6 +153,9 @@ class OracleRun:
         f["yflux"] = self._a(np.zeros(2 * ny))
         f["zmax"] = self._a(L.Z0.astype(np.float32).copy()) if is_root else None
         f["arrival"] = self._a(np.full((ny, nx), -1), np.int32) if is_root else None
+        sp = getattr(L, "sponge", None)
+        f["spx"] = self._a(sp[0]) if (is_root and sp is not None) else None
+        f["spy"] = self._a(sp[1]) if (is_root and sp is not None) else None
         for nm, a in f.items():
             setattr(o, nm, a.ctypes.data if a is not None else None)
         return f
@@ -185,3 +191,17 @@ class OracleRun:
         # after CHANGE / UPDATE the levels are equal; level 1 is the latest
         return {"z": f["z1"], "m": f["m1"], "n": f["n1"], "zmax": f["zmax"], "arrival": f["arrival"],
                 "dz": f["dz2"]}
+
+
+def sponge_coef(laycord, x, y, h, dtype=np.float32):
+    """SPONGE_COEF (boundaries.f90:250-345): coefficient fields [ny, nx]"""
+    lib = load(dtype)
+    ny, nx = h.shape
+    xa = np.ascontiguousarray(x, dtype=dtype)
+    ya = np.ascontiguousarray(y, dtype=dtype)
+    ha = np.ascontiguousarray(h, dtype=dtype)
+    cx = np.zeros((ny, nx), dtype)
+    cy = np.zeros((ny, nx), dtype)
+    lib.ocl_sponge_coef(nx, ny, laycord, xa.ctypes.data, ya.ctypes.data, ha.ctypes.data, cx.ctypes.data,
+                        cy.ctypes.data)
+    return cx, cy

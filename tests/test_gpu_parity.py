@@ -120,3 +120,29 @@ def test_nonlinear_spherical_root(oracle_mod, shape):
         _cmp(a, b, what)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
     assert np.array_equal(gpu["arrival"], ref["arrival"])
+
+
+@pytest.mark.parametrize("kind", ["sponge", "sponge_wall"])
+def test_sponge_and_wall_outer_layer(oracle_mod, kind):
+    """SPONGE_LAYER after the momentum step (boundaries.f90:206-247) and the
+    BC_WALL bathymetry (boundaries.f90:388-428).  The coefficients are
+    SPONGE_COEF's on metre axes (on degree axes they are all 0, as in the
+    reference), here a band of about 7 cells along every edge."""
+    from comcot_b200 import precompute as pc
+    case = synth.single_layer_case("sp", 97, 81, 2.0, 2.0, 0, seed=21, n_seamounts=5, shelf_cols=10,
+                                   land_cols=0, ngauges=0, amp=2.0)
+    L = case.root
+    if kind == "sponge_wall":
+        L.H = pc.bc_wall(L.H)
+        L.hp, L.hq = pc.pq_depth(L.H)
+    L.sponge = pc.sponge_coef(np.arange(L.nx) * 20000.0, np.arange(L.ny) * 20000.0, L.H, 1)
+    assert L.sponge[0].max() > 0
+    gpu, _, o, _ = _run_both(case, 60, oracle_mod)
+    ref = o.layer(0)
+    assert np.isfinite(ref["m"]).all()
+    band = (L.sponge[0] > 0) | (L.sponge[1] > 0)
+    assert np.abs(ref["m"][band]).max() > 0   # the wave reached the band
+    for a, b, what in ((gpu["z"], ref["z"], "eta"), (gpu["mn"][0], ref["m"], "M"), (gpu["mn"][1], ref["n"], "N"),
+                       (gpu["zmax"], ref["zmax"], "zmax")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what

@@ -76,3 +76,38 @@ def test_c3_geometry():
     assert C_.rel_size == 5 and C_.laycord == 1 and C_.laygov == 1
     assert C_.rel_time == 1  # 200 m shelf, CR 0.35
     assert C_.H.min() >= -20.0 - 1e-3 and C_.H.max() <= 200.0 + 1e-3
+
+
+def test_sponge_coef_bitwise_and_separable(oracle_mod):
+    """SPONGE_COEF + H_CALC (boundaries.f90:250-385) against the oracle's
+    REAL restatement, on spherical and Cartesian axes"""
+    for seed, (nx, ny) in enumerate([(97, 81), (160, 45), (33, 200)]):
+        case = synth.single_layer_case("s", nx, ny, 2.0, 2.0, 0, seed=seed, n_seamounts=4, shelf_cols=8,
+                                       land_cols=3)
+        L = case.root
+        for laycord, x, y in ((0, L.x, L.y), (1, np.arange(nx) * 20000.0, np.arange(ny) * 18000.0)):
+            cx, cy = pc.sponge_coef(x, y, L.H, laycord)
+            ox, oy = oracle_mod.sponge_coef(laycord, x, y, L.H)
+            assert np.array_equal(cx.view(np.uint32), ox.view(np.uint32))
+            assert np.array_equal(cy.view(np.uint32), oy.view(np.uint32))
+            assert (cx == cx[:1, :]).all() and (cy == cy[:, :1]).all()
+            if laycord == 0:
+                # the band is converted to degrees but divided by metres: no damping at all
+                assert not cx.any() and not cy.any()
+            else:
+                assert cx[:, 0] .max() > 0 and cy[0, :].max() > 0 and cx[:, nx // 2].max() == 0
+
+
+def test_bc_wall_sides():
+    H = np.full((10, 12), 100.0, np.float32)
+    w = pc.bc_wall(H)
+    assert (w[:, :2] == -999).all() and (w[:, -2:] == -999).all() and (w[:2, :] == -999).all()
+    assert (w[-2:, :] == -999).all() and (w[2:-2, 2:-2] == 100).all()
+    # a wave maker entering from side INCIDENT keeps that side open (boundaries.f90:395-419)
+    for inc, open_view in ((1, lambda a: a[-2:, 2:-2]), (2, lambda a: a[:2, 2:-2]), (3, lambda a: a[2:-2, :2]),
+                           (4, lambda a: a[2:-2, -2:])):
+        w = pc.bc_wall(H, ini_switch=2, incident=inc)
+        assert (open_view(w) == 100).all()
+        assert (w == -999).sum() == H.size - 6 * 8 - open_view(w).size
+    assert (pc.bc_wall(H, ini_switch=2, incident=5) == H).all()
+    assert (H == 100).all()   # the input is not modified
