@@ -71,6 +71,7 @@ SIGNATURES = {
     "gcomcot_set_layer_coefs_": (None, [P_I, P_F, P_F, P_F, P_I, P_I]),
     "gcomcot_set_sponge_": (None, [P_I, P_F, P_F, P_F, P_I, P_I]),
     "sponge_launch_": (None, [P_I]),
+    "gcomcot_set_sc_tables_": (None, [P_I, P_I, P_F, P_I, P_I, P_I, P_I]),
     "gcomcot_set_arrival_": (None, [P_I, P_F]),
     "gcomcot_get_arrival_": (None, [P_I, P_I]),
     "gcomcot_launch_count": (C.c_longlong, []),

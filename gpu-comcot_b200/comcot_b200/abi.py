@@ -58,6 +58,14 @@ class ReferenceSession:
                                           _f(L.grx), _f(L.gry), _i(L.fric_switch), _f(L.fric_coef),
                                           _i(L.linchk), _i(L.modscm), _i(nx), _i(ny), _lib.fptr(hp),
                                           _lib.fptr(hq))
+        if L.sc is not None:
+            # SC_OPTION = 1 tables in Fortran order POS(NX,NY,2), CXY(NX,NY,4)
+            pos = np.ascontiguousarray(np.moveaxis(L.sc.pos, -1, 0), dtype=np.int32)
+            cxy = np.ascontiguousarray(np.moveaxis(L.sc.cxy, -1, 0), dtype=F32)
+            self._keep += [pos, cxy]
+            parent = next(Q for Q in self.case.layers if Q.id == L.parent)
+            lib.gcomcot_set_sc_tables_(_i(L.id), _lib.iptr(pos), _lib.fptr(cxy), _i(nx), _i(ny),
+                                       _i(parent.modscm), _i(1 if L.sc.fix_top else 0))
         if L.laycord == 0 and L.laygov == 1:
             c = L.coefs
             full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)

@@ -266,3 +266,155 @@ def bc_wall(h: np.ndarray, ini_switch: int = 0, incident: int = 0) -> np.ndarray
     if sides["n"]:
         out[-2:, :] = -999.0
     return out
+
+
+# ---------------------------------------------------------------------
+# SC_OPTION = 1: Cartesian child of a spherical parent (UTM coupling)
+# ---------------------------------------------------------------------
+# WGS84 constants as initialization.f90:1410-1420 / 1520-1530 state them
+_UTM_A, _UTM_K0 = 6378137.0, 0.9996
+_UTM_ES = 0.006739496756587
+_UTM_F2, _UTM_F4, _UTM_F6 = 0.006694380004261, 0.00004481472364144701, 0.0000003000067898417773
+
+
+def _meridian_arc(lat):
+    a, f2, f4, f6 = _UTM_A, _UTM_F2, _UTM_F4, _UTM_F6
+    return a * ((1.0 - f2 / 4.0 - 3.0 * f4 / 64.0 - 5.0 * f6 / 256.0) * lat
+                - (3.0 * f2 / 8.0 + 3.0 * f4 / 32.0 + 45.0 * f6 / 1024.0) * np.sin(2.0 * lat)
+                + (15.0 * f4 / 256.0 + 45.0 * f6 / 1024.0) * np.sin(4.0 * lat)
+                - (35.0 * f6 / 3072.0) * np.sin(6.0 * lat))
+
+
+def _pole():
+    return math.pi / 2.0 - 1.0e-10
+
+
+def sph_to_utm(lon, lat, lon0):
+    """SPH_TO_UTM (initialization.f90:1490-1590): transverse Mercator on
+    WGS84 about central meridian lon0 (degrees), natural origin on the
+    equator, no false easting / northing; double precision"""
+    lat = np.clip(np.asarray(lat, np.float64) * RAD_DEG, -_pole(), _pole())
+    lon = np.asarray(lon, np.float64) * RAD_DEG
+    ln0 = lon0 * RAD_DEG
+    cs, sn = np.cos(lat), np.sin(lat)
+    tn = sn / cs
+    nu = _UTM_A / np.sqrt(1.0 - _UTM_F2 * sn ** 2)
+    t = tn ** 2
+    c = _UTM_ES * cs ** 2
+    p = (lon - ln0) * cs
+    s = _meridian_arc(lat)
+    es = _UTM_ES
+    x = _UTM_K0 * nu * (p + (1.0 - t + c) * p ** 3 / 6.0 + (5.0 - 18.0 * t + t ** 2 + 72.0 * c - 58.0 * es) * p ** 5 / 120.0)
+    y = _UTM_K0 * (s + nu * tn * (p ** 2 / 2.0 + (5.0 - t + 9.0 * c + 4.0 * c ** 2) * p ** 4 / 24.0
+                                  + (61.0 - 58.0 * t + t ** 2 + 600.0 * c - 330.0 * es) * p ** 6 / 720.0))
+    return x, y
+
+
+def utm_to_sph(x, y, lon0):
+    """UTM_TO_SPH (initialization.f90:1390-1487): the inverse, with the
+    footpoint latitude series; double precision"""
+    a, f2, es, k0 = _UTM_A, _UTM_F2, _UTM_ES, _UTM_K0
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    mu1 = (y / k0) / a / (1.0 - f2 / 4.0 - 3.0 * _UTM_F4 / 64.0 - 5.0 * _UTM_F6 / 256.0)
+    e1 = (1.0 - math.sqrt(1.0 - f2)) / (1.0 + math.sqrt(1.0 - f2))
+    lt1 = (mu1 + (3.0 * e1 / 2.0 - 27.0 * e1 ** 3 / 32.0) * np.sin(2.0 * mu1)
+           + (21.0 * e1 ** 2 / 16.0 - 55.0 * e1 ** 4 / 32.0) * np.sin(4.0 * mu1)
+           + (151.0 * e1 ** 3 / 96.0) * np.sin(6.0 * mu1) + (1097.0 * e1 ** 4 / 512.0) * np.sin(8.0 * mu1))
+    lt1 = np.clip(lt1, -_pole(), _pole())
+    tmp1 = np.sqrt(1.0 - f2 * np.sin(lt1) ** 2)
+    nu1 = a / tmp1
+    rho1 = a * (1.0 - f2) / tmp1 ** 3
+    t1 = np.tan(lt1) ** 2
+    c1 = es * np.cos(lt1) ** 2
+    d = x / nu1 / k0
+    lat = lt1 - nu1 * np.tan(lt1) / rho1 * (d ** 2 / 2.0 - (5.0 + 3.0 * t1 + 10.0 * c1 - 4.0 * c1 ** 2 - 9.0 * es)
+                                            * d ** 4 / 24.0 + (61.0 + 90.0 * t1 + 298.0 * c1 + 45.0 * t1 ** 2
+                                                               - 252 * es - 3.0 * c1 ** 2) * d ** 6 / 720.0)
+    lon = lon0 * RAD_DEG + 1.0 / np.cos(lt1) * (d - (1.0 + 2.0 * t1 + c1) * d ** 3 / 6.0
+                                               + (5.0 - 2.0 * c1 + 28.0 * t1 - 3.0 * c1 ** 2 + 8.0 * es
+                                                  + 24.0 * t1 ** 2) * d ** 5 / 120.0)
+    return lon * 180.0 / math.pi, lat * 180.0 / math.pi
+
+
+def utm_zone_meridian(olon: float) -> float:
+    """COORD_CONVERT (initialization.f90:1340-1350): central meridian of the
+    6-degree zone holding olon, zones numbered from 0 E; 0 when none does"""
+    lon0 = 0.0
+    for i in range(60):
+        zc = 3.0 + i * 6.0
+        if zc - 3.0 <= olon < zc + 3.0:
+            lon0 = zc
+    return lon0
+
+
+def coord_convert_to_utm(lon, lat, olon, olat):
+    """COORD_CONVERT option 0: easting / northing with the false offsets"""
+    x, y = sph_to_utm(lon, lat, utm_zone_meridian(olon))
+    return x + 500000.0, y + (10000000.0 if olat < 0.0 else 0.0)
+
+
+def coord_convert_to_sph(x, y, olon, olat):
+    """COORD_CONVERT option 1"""
+    return utm_to_sph(np.asarray(x) - 500000.0, np.asarray(y) - (10000000.0 if olat < 0.0 else 0.0),
+                      utm_zone_meridian(olon))
+
+
+@dataclass
+class ScGeometry:
+    """a Cartesian child of a spherical parent under SC_OPTION = 1"""
+    x: np.ndarray          # [nx] easting (m)
+    y: np.ndarray          # [ny] northing (m)
+    dx: float
+    dy: float
+    pos: np.ndarray        # [ny, nx, 2] int32, 1-based (KI, KJ) of the parent cell holding each child node
+    cxy: np.ndarray        # [ny, nx, 4] float32 bilinear weights of (KI,KJ),(KI+1,KJ),(KI,KJ+1),(KI+1,KJ+1)
+    corners: list          # [IMIN, IMAX, JMIN, JMAX] of pos (the child's corners after matching)
+    xs: float
+    ys: float
+
+
+def sc_child_geometry(xp, yp, corners_, rel_size, dx_min_parent, del_y_parent=None) -> ScGeometry:
+    """SUBGRID_MATCHING for LAYCORD 0 -> 1 (initialization.f90:996-1123):
+    the child's UTM axes from the projected window corners, then the
+    position and weight tables of every child node in the parent grid"""
+    xp = np.asarray(xp, np.float64)
+    yp = np.asarray(yp, np.float64)
+    c1, c2, c3, c4 = corners_
+    dely = dx_min_parent if del_y_parent is None else del_y_parent[c3 - 1]
+    dx = dx_min_parent / 60.0 / rel_size
+    dy = dely / 60.0 / rel_size
+    xs = 0.5 * (xp[c1 - 1] + xp[c1 - 2]) - dx / 2.0
+    xe = 0.5 * (xp[c2 - 1] + xp[c2]) - dx / 2.0
+    ys = 0.5 * (yp[c3 - 1] + yp[c3 - 2]) - dy / 2.0
+    ye = 0.5 * (yp[c4 - 1] + yp[c4]) - dy / 2.0
+    nx = (c2 - c1 + 1) * rel_size + 1
+    ny = (c4 - c3 + 1) * rel_size + 1
+    x_end, _ = coord_convert_to_utm(xe, ys, xs, ys)
+    _, y_end = coord_convert_to_utm(xs, ye, xs, ys)
+    x0, y0 = coord_convert_to_utm(xs, ys, xs, ys)
+    dxm = (float(x_end) - float(x0)) / (nx - 1)
+    dym = (float(y_end) - float(y0)) / (ny - 1)
+    x = float(x0) + np.arange(nx) * dxm
+    y = float(y0) + np.arange(ny) * dym
+    X, Y = np.meshgrid(x, y)
+    lon, lat = coord_convert_to_sph(X, Y, xs, ys)
+    npx, npy = len(xp), len(yp)
+    # KI: the K in 2..NX-1 with X(K) <= lon < X(K+1), else 0 (1-based)
+    ki = np.searchsorted(xp, lon, side="right")          # first index with xp > lon -> K+1 (1-based K)
+    ok_i = (ki >= 2) & (ki <= npx - 1)
+    ki = np.where(ok_i, ki, 0)
+    kj = np.searchsorted(yp, lat, side="right")
+    ok_j = (kj >= 2) & (kj <= npy - 1)
+    kj = np.where(ok_j, kj, 0)
+    pos = np.stack([ki, kj], axis=-1).astype(np.int32)
+    cxy = np.zeros((ny, nx, 4), np.float32)
+    good = ok_i & ok_j
+    kk = np.where(good, ki, 1) - 1
+    jj = np.where(good, kj, 1) - 1
+    cx = (lon - xp[kk]) / (xp[kk + 1] - xp[kk])
+    cy = (lat - yp[jj]) / (yp[jj + 1] - yp[jj])
+    w = np.stack([(1.0 - cx) * (1.0 - cy), cx * (1.0 - cy), (1.0 - cx) * cy, cx * cy], axis=-1)
+    cxy[good] = w[good].astype(np.float32)
+    corners_sc = [int(ki.min()), int(ki.max()), int(kj.min()), int(kj.max())]
+    return ScGeometry(x=x, y=y, dx=dxm, dy=dym, pos=pos, cxy=cxy, corners=corners_sc, xs=xs, ys=ys)

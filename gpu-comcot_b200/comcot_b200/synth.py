@@ -58,6 +58,14 @@ class LayerSpec:
     hp: np.ndarray | None = None
     hq: np.ndarray | None = None
     sponge: tuple | None = None  # (COEFX, COEFY) [ny, nx] of SPONGE_COEF, outer layer only
+    sc: "ScSpec | None" = None  # SC_OPTION = 1 coupling tables of a Cartesian child of a spherical parent
+
+
+@dataclass
+class ScSpec:
+    pos: np.ndarray      # [ny, nx, 2] int32, 1-based (KI, KJ) in the parent
+    cxy: np.ndarray      # [ny, nx, 4] float32 bilinear weights
+    fix_top: bool = False
 
 
 @dataclass
@@ -274,6 +282,27 @@ def nested_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel
     case = Case(name, [P, C], nsteps)
     if ngauges:
         case.gauges = wet_gauges(P, ngauges, rng)
+    return case
+
+
+def nested_sc_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel_time=None, child_laygov=1,
+                   fix_top=False, **kw):
+    """nested_case's spherical parent with a Cartesian child coupled by
+    SC_OPTION = 1: the child's axes are UTM eastings / northings of its
+    window's corners and every child node carries its parent cell and
+    bilinear weights (SUBGRID_MATCHING, initialization.f90:996-1123)"""
+    case = nested_case(name, pnx, pny, dx_min, dt, corners, rel_size, nsteps, seed, rel_time=rel_time,
+                       child_laygov=child_laygov, **kw)
+    P, C = case.layers
+    g = pc.sc_child_geometry(P.x, P.y, corners, rel_size, dx_min)
+    assert (C.ny, C.nx) == g.pos.shape[:2]
+    C.x, C.y = g.x.astype(np.float32), g.y.astype(np.float32)
+    C.dx, C.dy = g.dx, g.dy
+    C.corners = list(g.corners)
+    rx, ry = F32(C.dt) / F32(g.dx), F32(C.dt) / F32(g.dy)
+    C.rx, C.ry = float(rx), float(ry)
+    C.grx, C.gry = float(F32(9.807) * rx), float(F32(9.807) * ry)
+    C.sc = ScSpec(pos=g.pos, cxy=g.cxy, fix_top=fix_top)
     return case
 
 

@@ -101,6 +101,25 @@ void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int
                      const int *corners, int t, cudaStream_t s);
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                    const int *corners, cudaStream_t s);
+/* SC_OPTION = 1 coupling of a Cartesian child to a spherical parent: the
+ * parent cell (KI, KJ) and bilinear weights of every child edge node, and
+ * for JNZ_SC, per parent cell of the child's window, the child nodes that
+ * fall in it (CSR, in the reference's summation order) */
+struct GcScView {
+    const int2 *epos;    /* [2*ny + 2*nx] 1-based (KI, KJ): left, right, bottom, top edge nodes */
+    const float4 *ew;    /* [2*ny + 2*nx] weights of (KI,KJ), (KI+1,KJ), (KI,KJ+1), (KI+1,KJ+1) */
+    const int *start;    /* [(wi1-wi0+1)*(wj1-wj0+1) + 1] */
+    const int *cell;     /* child offsets j*pitch + i */
+    int wi0, wi1, wj0, wj1; /* parent window, 0-based inclusive */
+    int band[4][4];      /* forecast bands i0, i1, j0, j1 (0-based): left M, right M, top N, bottom N */
+    int fix_top;         /* 1: top edge blends C2*YN1 (the reference uses C1*YN1) */
+    int modscm;          /* the parent's MODSCM (0 adds the modified-scheme term) */
+    float half;          /* REL_SIZE**2 / 2 */
+};
+void gc_launch_sc_edges(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, int t, int rel_time,
+                        const float *zwet, cudaStream_t s);
+void gc_launch_sc_forecast(const GcLayerDev &P, const GcScView &sv, cudaStream_t s);
+void gc_launch_sc_jnz(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, cudaStream_t s);
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s);
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);

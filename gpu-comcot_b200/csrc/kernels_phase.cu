@@ -10,6 +10,8 @@
  * Indices are 0-based: Fortran (I,J) = (i+1, j+1).
  */
 #include <utility>
+#include <algorithm>
+
 #include "gc_internal.h"
 
 namespace {
@@ -734,6 +736,126 @@ __global__ void k_maxamp(GcLayerDev L) {
     if (!(m >= z)) L.zmax[c] = z;
 }
 
+/* ---------------------------------------------------------------- */
+/* SC_OPTION = 1 coupling (all_grids.f90:996-1425)                   */
+/* ---------------------------------------------------------------- */
+/* Z1+Z2+Z3+Z4 of the four weighted parent values (all_grids.f90:1030-1034) */
+__device__ __forceinline__ float sc_bilin(const float *f, int pitch, int2 ps, float4 w) {
+    const size_t c = (size_t)(ps.y - 1) * pitch + (ps.x - 1);
+    float z1 = f[c] * w.x;
+    float z2 = f[c + 1] * w.y;
+    float z3 = f[c + pitch] * w.z;
+    float z4 = f[c + pitch + 1] * w.w;
+    return z1 + z2 + z3 + z4;
+}
+
+/* EDGE_INTERP_SC (t = 1) and the edge blend of NEWQ_SC (t >= 2,
+ * all_grids.f90:1268-1362), one thread per child edge node.  The wet test
+ * is at the edge node itself on the child's level-2 surface as the
+ * reference holds it (zwet); EDGE_INTERP_SC's own test reads indices left
+ * over from elsewhere, which no implementation can reproduce. */
+__global__ void k_sc_edges(GcLayerDev P, GcLayerDev C, GcScView sv, int t, float c1, float c2, const float *zwet) {
+    pdl_enter();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = C.nx, ny = C.ny;
+    if (k >= 2 * ny + 2 * nx) return;
+    int side, i, j;
+    if (k < ny) { side = 0; i = 0; j = k; }
+    else if (k < 2 * ny) { side = 1; i = nx - 1; j = k - ny; }
+    else if (k < 2 * ny + nx) { side = 2; i = k - 2 * ny; j = 0; }
+    else { side = 3; i = k - 2 * ny - nx; j = ny - 1; }
+    const bool vert = side < 2;
+    const size_t cc = (size_t)j * C.pitch + i;
+    float v = 0.0f;
+    if (C.h[cc] + zwet[cc] > CC_GX) {
+        const int2 ps = sv.epos[k];
+        const float4 w = sv.ew[k];
+        const float x1 = sc_bilin(vert ? P.m1 : P.n1, P.pitch, ps, w);
+        if (t == 1) {
+            v = x1;
+        } else {
+            const float x2 = sc_bilin(vert ? P.m2 : P.n2, P.pitch, ps, w);
+            /* the reference's top edge weights YN1 by C1 (all_grids.f90:1357) */
+            const float w1 = (side == 3 && !sv.fix_top) ? c1 : c2;
+            v = c1 * x2 + w1 * x1;
+        }
+    }
+    if (vert) C.m1w[cc] = v;
+    else C.n1w[cc] = v;
+}
+
+/* NEWQ_SC forecast of the parent fluxes at the end of its step on four
+ * bands around the child (all_grids.f90:1130-1266), into the parent's
+ * level 2, which its own momentum step overwrites afterwards */
+__global__ void k_sc_forecast(GcLayerDev P, GcScView sv) {
+    pdl_enter();
+    const int b = blockIdx.z;
+    const int i = sv.band[b][0] + blockIdx.x * BX + threadIdx.x;
+    const int j = sv.band[b][2] + blockIdx.y * BY + threadIdx.y;
+    if (i > sv.band[b][1] || j > sv.band[b][3]) return;
+    const int Pp = P.pitch;
+    const size_t c = (size_t)j * Pp + i;
+    const float twlvth = 0.08333333333333f;
+    if (b < 2) {
+        const size_t cp = c + 1;
+        float out = 0.0f;
+        if (P.h[c] > CC_GX && P.h[cp] > CC_GX) {
+            const int jm1 = j - 1 < 0 ? 0 : j - 1, jp1 = j + 1 > P.ny - 1 ? P.ny - 1 : j + 1;
+            const size_t cm = (size_t)jm1 * Pp + i, cq = (size_t)jp1 * Pp + i;
+            const float tot_n = P.n1[c] + P.n1[cp] + P.n1[cm] + P.n1[cm + 1];
+            const float r2 = r2_at(P, i, j, c, P.h[c], P.h[cp]);
+            float xm = P.m1[c] - r2 * (P.z2[cp] - P.z2[c]) + GC_ROW(P, GC_R3, j) * tot_n;
+            if (sv.modscm == 0) {
+                const float scm = r2 * twlvth * ((P.z2[cq + 1] - 2.0f * P.z2[cp] + P.z2[cm + 1]) -
+                                                 (P.z2[cq] - 2.0f * P.z2[c] + P.z2[cm]));
+                xm = xm - scm;
+            }
+            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            out = xm;
+        }
+        P.m2[c] = out;
+    } else {
+        const size_t cq = c + Pp;
+        float out = 0.0f;
+        if (P.h[c] > CC_GX && P.h[cq] > CC_GX) {
+            const size_t cw = (size_t)j * Pp + (i - 1 < 0 ? 0 : i - 1);
+            const size_t ce = (size_t)j * Pp + (i + 1 > P.nx - 1 ? P.nx - 1 : i + 1);
+            const float tot_m = P.m1[cw] + P.m1[cw + Pp] + P.m1[c] + P.m1[cq];
+            const float r4 = r4_at(P, i, j, c, P.h[c], P.h[cq]);
+            float xn = P.n1[c] - r4 * (P.z2[cq] - P.z2[c]) - GC_ROW(P, GC_R5, j) * tot_m;
+            if (sv.modscm == 0) {
+                const float scm = r4 * twlvth * ((P.z2[ce + Pp] - 2.0f * P.z2[cq] + P.z2[cw + Pp]) -
+                                                 (P.z2[ce] - 2.0f * P.z2[c] + P.z2[cw]));
+                xn = xn - scm;
+            }
+            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            out = xn;
+        }
+        P.n2[c] = out;
+    }
+}
+
+/* JNZ_SC (all_grids.f90:1367-1425) as a gather: each parent cell of the
+ * window sums the wet child surfaces that fall in it, in the reference's
+ * order, and takes their mean where more than half of r*r nodes
+ * contributed (elsewhere it keeps its value) */
+__global__ void k_sc_jnz(GcLayerDev P, GcLayerDev C, GcScView sv) {
+    pdl_enter();
+    const int i = sv.wi0 + blockIdx.x * BX + threadIdx.x;
+    const int j = sv.wj0 + blockIdx.y * BY + threadIdx.y;
+    if (i > sv.wi1 || j > sv.wj1) return;
+    const int q = (j - sv.wj0) * (sv.wi1 - sv.wi0 + 1) + (i - sv.wi0);
+    float sum = 0.0f, cnt = 0.0f;
+    for (int k = sv.start[q]; k < sv.start[q + 1]; k++) {
+        const int cc = sv.cell[k];
+        if (C.h[cc] + C.z2[cc] > CC_GX) {
+            sum = sum + C.z2[cc];
+            cnt = cnt + 1.0f;
+        }
+    }
+    if (cnt > sv.half) P.z2[(size_t)j * P.pitch + i] = sum / cnt;
+}
+
 /* SPONGE_LAYER (boundaries.f90:229-244) with separable coefficients,
  * COEFX(I,J) = spx[I] and COEFY(I,J) = spy[J]: where either is positive,
  * M2 += CX*DT*M1 and N2 += CY*DT*N1 */
@@ -893,6 +1015,29 @@ void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int r
 
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s) {
     launch(k_maxamp, grid2(L), dim3(BX, BY), 0, s, L);
+}
+
+void gc_launch_sc_edges(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, int t, int rel_time,
+                        const float *zwet, cudaStream_t s) {
+    const int n = 2 * C.ny + 2 * C.nx;
+    const float c1 = ((float)t - 1.0f) / (float)rel_time;
+    const float c2 = 1.0f - c1;
+    launch(k_sc_edges, (n + 127) / 128, 128, 0, s, P, C, sv, t, c1, c2, zwet);
+}
+
+void gc_launch_sc_forecast(const GcLayerDev &P, const GcScView &sv, cudaStream_t s) {
+    int wmax = 1, hmax = 1;
+    for (int b = 0; b < 4; b++) {
+        wmax = std::max(wmax, sv.band[b][1] - sv.band[b][0] + 1);
+        hmax = std::max(hmax, sv.band[b][3] - sv.band[b][2] + 1);
+    }
+    dim3 grid((unsigned)((wmax + BX - 1) / BX), (unsigned)((hmax + BY - 1) / BY), 4);
+    launch(k_sc_forecast, grid, dim3(BX, BY), 0, s, P, sv);
+}
+
+void gc_launch_sc_jnz(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, cudaStream_t s) {
+    dim3 grid((unsigned)((sv.wi1 - sv.wi0 + 1 + BX - 1) / BX), (unsigned)((sv.wj1 - sv.wj0 + 1 + BY - 1) / BY), 1);
+    launch(k_sc_jnz, grid, dim3(BX, BY), 0, s, P, C, sv);
 }
 
 void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s) {

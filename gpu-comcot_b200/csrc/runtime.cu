@@ -272,6 +272,117 @@ void gcomcot_set_layer_coefs_(int *id, float *R0, float *R21, float *R22, int *n
     }
 }
 
+/* extension: the SC_OPTION = 1 tables of a Cartesian child of a spherical
+ * parent, POS(NX,NY,2) and CXY(NX,NY,4) as SUBGRID_MATCHING builds them
+ * (initialization.f90:1065-1124), the parent's MODSCM (the band forecast of
+ * NEWQ_SC adds the modified-scheme term when it is 0) and FIX_TOP (1: the
+ * top edge blends C2*YN1; 0: C1*YN1 as all_grids.f90:1357 does).  Call
+ * before gcomcot_init_layer_ of that child, whose corners are then the
+ * extent of POS. */
+void gcomcot_set_sc_tables_(int *id, int *pos, float *cxy, int *nx, int *ny, int *parent_modscm, int *fix_top) {
+    init_runtime();
+    if (*id < 0 || *id >= GC_MAX_LAYERS || *nx < 3 || *ny < 3 || !pos || !cxy) {
+        fprintf(stderr, "ERROR: invalid layerid or SC tables\n");
+        exit(EXIT_FAILURE);
+    }
+    GcPendingParams &p = g_rt.pending[*id];
+    const size_t n = (size_t)(*nx) * (*ny);
+    p.sc = true;
+    p.sc_fix_top = *fix_top != 0;
+    p.sc_modscm = *parent_modscm;
+    p.sc_pos.assign(2 * n, 0);
+    p.sc_cxy.assign(4 * n, 0.0f);
+    for (size_t c = 0; c < n; c++) {
+        for (int k = 0; k < 2; k++) p.sc_pos[2 * c + k] = pos[(size_t)k * n + c];
+        for (int k = 0; k < 4; k++) p.sc_cxy[4 * c + k] = cxy[(size_t)k * n + c];
+    }
+}
+
+/* device tables of an SC_OPTION = 1 child (see GcScView) */
+static void sc_build(GcLayer &L, const GcLayer &P, const GcPendingParams &pp) {
+    const int nx = L.nx, ny = L.ny;
+    auto fail = [&](const char *what) {
+        fprintf(stderr, "gcomcot: SC tables of layer %d: %s\n", L.id, what);
+        exit(EXIT_FAILURE);
+    };
+    if (pp.sc_pos.size() != (size_t)2 * nx * ny) fail("sized for another layer");
+    auto ki = [&](int i, int j) { return pp.sc_pos[2 * ((size_t)j * nx + i)]; };
+    auto kj = [&](int i, int j) { return pp.sc_pos[2 * ((size_t)j * nx + i) + 1]; };
+    /* every node inside the parent with its whole 2x2 stencil */
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+            if (ki(i, j) < 1 || kj(i, j) < 1 || ki(i, j) > P.nx - 1 || kj(i, j) > P.ny - 1)
+                fail("a node lies outside the parent's interior");
+    const int ne = 2 * ny + 2 * nx;
+    std::vector<int2> epos(ne);
+    std::vector<float4> ew(ne);
+    auto put = [&](int k, int i, int j) {
+        const size_t c = (size_t)j * nx + i;
+        epos[k] = make_int2(ki(i, j), kj(i, j));
+        ew[k] = make_float4(pp.sc_cxy[4 * c], pp.sc_cxy[4 * c + 1], pp.sc_cxy[4 * c + 2], pp.sc_cxy[4 * c + 3]);
+    };
+    for (int j = 0; j < ny; j++) { put(j, 0, j); put(ny + j, nx - 1, j); }
+    for (int i = 0; i < nx; i++) { put(2 * ny + i, i, 0); put(2 * ny + nx + i, i, ny - 1); }
+    /* the parent window and, per parent cell, the child nodes in it, child
+     * I outermost as JNZ_SC sums them */
+    const int c0 = L.corners[0], c1 = L.corners[1], c2 = L.corners[2], c3 = L.corners[3];
+    const int ww = c1 - c0 + 1, wh = c3 - c2 + 1;
+    std::vector<int> start((size_t)ww * wh + 1, 0), cell;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            const int a = ki(i, j), b = kj(i, j);
+            if (a >= c0 && a <= c1 && b >= c2 && b <= c3) start[(size_t)(b - c2) * ww + (a - c0) + 1]++;
+        }
+    for (size_t q = 0; q < (size_t)ww * wh; q++) start[q + 1] += start[q];
+    cell.resize((size_t)start.back());
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            const int a = ki(i, j), b = kj(i, j);
+            if (a >= c0 && a <= c1 && b >= c2 && b <= c3) cell[fill[(size_t)(b - c2) * ww + (a - c0)]++] = j * L.pitch + i;
+        }
+    /* forecast bands (all_grids.f90:1131-1134, 1165-1168, 1199-1202, 1233-1236), 0-based */
+    GcScView v{};
+    auto band = [&](int b, int i0, int i1, int j0, int j1, bool xflux) {
+        /* the M band reads column I+1, the N band row J+1 */
+        if (i0 < 1 || j0 < 1 || (xflux ? i1 + 1 > P.nx || j1 > P.ny : i1 > P.nx || j1 + 1 > P.ny))
+            fail("a forecast band reaches past the parent's edge");
+        v.band[b][0] = i0 - 1; v.band[b][1] = i1 - 1; v.band[b][2] = j0 - 1; v.band[b][3] = j1 - 1;
+    };
+    int a = ki(0, 0), b = ki(0, ny - 1);
+    band(0, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
+    a = ki(nx - 1, 0); b = ki(nx - 1, ny - 1);
+    band(1, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
+    a = kj(0, ny - 1); b = kj(nx - 1, ny - 1);
+    band(2, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
+    a = kj(0, 0); b = kj(nx - 1, 0);
+    band(3, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
+    const size_t b_epos = ((size_t)ne * sizeof(int2) + 255) & ~(size_t)255;
+    const size_t b_ew = ((size_t)ne * sizeof(float4) + 255) & ~(size_t)255;
+    const size_t b_start = (start.size() * sizeof(int) + 255) & ~(size_t)255;
+    const size_t b_cell = ((cell.size() + 1) * sizeof(int) + 255) & ~(size_t)255;
+    char *blk = nullptr;
+    GC_CUDA_OR_DIE(cudaMalloc((void **)&blk, b_epos + b_ew + b_start + b_cell));
+    L.sc_block = blk;
+    GC_CUDA_OR_DIE(cudaMemcpy(blk, epos.data(), ne * sizeof(int2), cudaMemcpyHostToDevice));
+    GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos, ew.data(), ne * sizeof(float4), cudaMemcpyHostToDevice));
+    GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos + b_ew, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!cell.empty())
+        GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos + b_ew + b_start, cell.data(), cell.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice));
+    v.epos = (const int2 *)blk;
+    v.ew = (const float4 *)(blk + b_epos);
+    v.start = (const int *)(blk + b_epos + b_ew);
+    v.cell = (const int *)(blk + b_epos + b_ew + b_start);
+    v.wi0 = c0 - 1; v.wi1 = c1 - 1; v.wj0 = c2 - 1; v.wj1 = c3 - 1;
+    v.fix_top = pp.sc_fix_top;
+    v.modscm = pp.sc_modscm;
+    v.half = (float)(L.rel_size * L.rel_size) / 2.0f;
+    L.sc = v;
+    L.has_sc = true;
+    L.sc_stepped = false;
+}
+
 /* GPUcomcot.cu:214-251 */
 void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, int *rel_time,
                          int *corners, float *grx, float *gry, float *R1_f, float *R2_f,
@@ -290,6 +401,7 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
     if (L.used && L.block) cudaFree(L.block);
     if (L.spx) cudaFree(L.spx);
     if (L.spy) cudaFree(L.spy);
+    if (L.sc_block) cudaFree(L.sc_block);
     L = GcLayer();
     L.used = true;
     L.id = *layerid; L.parent = *parent; L.level = *level;
@@ -317,8 +429,10 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
         int is = L.corners[0], ie = L.corners[1], js = L.corners[2], je = L.corners[3];
         /* the NEWQ forecast reads parent rows JS-3 and columns IS-3
          * (all_grids.f90:692-700,765-772), so the window must start at 4 */
-        if (is < 4 || js < 4 || ie > P->nx - 2 || je > P->ny - 2 || ie < is || je < js
-            || L.nx != (ie - is + 1) * L.rel_size + 1 || L.ny != (je - js + 1) * L.rel_size + 1
+        /* an SC_OPTION = 1 child keeps the size of its original window; its
+         * corners are the extent of its nodes' positions (initialization.f90:1120-1123) */
+        const bool sized = pp.sc || (L.nx == (ie - is + 1) * L.rel_size + 1 && L.ny == (je - js + 1) * L.rel_size + 1);
+        if (is < 4 || js < 4 || ie > P->nx - 2 || je > P->ny - 2 || ie < is || je < js || !sized
             || L.rel_size < 1 || L.rel_time < 1) {
             fprintf(stderr,
                     "gcomcot: layer %d corners (%d,%d,%d,%d) ratio %d do not match %dx%d inside "
@@ -398,6 +512,7 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
         if (gc_layer_upload_field(L, L.hp, hp.data()) != GC_OK) exit(EXIT_FAILURE);
         if (gc_layer_upload_field(L, L.hq, hq.data()) != GC_OK) exit(EXIT_FAILURE);
     }
+    if (pp.sc) sc_build(L, *gc_layer(L.parent), pp);
     GC_CUDA_OR_DIE(cudaStreamSynchronize(g_rt.stream));
     if (!getenv("GCOMCOT_QUIET")) printf("Initializing layer id %d\n", L.id);
 }
@@ -620,6 +735,7 @@ void cuda_shutdown_(void) {
         if (g_rt.layers[k].block) cudaFree(g_rt.layers[k].block);
         if (g_rt.layers[k].spx) cudaFree(g_rt.layers[k].spx);
         if (g_rt.layers[k].spy) cudaFree(g_rt.layers[k].spy);
+        if (g_rt.layers[k].sc_block) cudaFree(g_rt.layers[k].sc_block);
         g_rt.layers[k] = GcLayer();
         g_rt.pending[k] = GcPendingParams();
     }
@@ -648,18 +764,27 @@ void gc_subcycle(int parent_id) {
         GcLayer &C = g_rt.layers[cid];
         int nhalf = C.rel_time / 2 + 1;
         for (int k = 1; k <= C.rel_time; k++) {
-            gc_launch_edges(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, k, g_rt.stream);
+            if (C.has_sc) {
+                /* EDGE_INTERP_SC / NEWQ_SC (all_grids.f90:996-1364) */
+                const GcLayerDev cv = C.view();
+                if (k > 1) { gc_launch_sc_forecast(P.view(), C.sc, g_rt.stream); g_rt.launches++; }
+                gc_launch_sc_edges(P.view(), cv, C.sc, k, C.rel_time, C.sc_stepped ? cv.z1 : cv.z2, g_rt.stream);
+            } else {
+                gc_launch_edges(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, k, g_rt.stream);
+            }
             gc_launch_mass(C.view(), g_rt.stream);
             C.z2_valid = true;
             gc_subcycle(cid);
             gc_launch_moment(C.view(), g_rt.stream);
             C.mn2_valid = true;
             if (k == nhalf) {
-                gc_launch_jnz(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, g_rt.stream);
+                if (C.has_sc) gc_launch_sc_jnz(P.view(), C.view(), C.sc, g_rt.stream);
+                else gc_launch_jnz(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, g_rt.stream);
                 g_rt.launches++;
             }
             gc_launch_update_edges(C.view(), g_rt.stream);
             gc_swap(C);
+            C.sc_stepped = true;
             g_rt.launches += 4;
         }
     }

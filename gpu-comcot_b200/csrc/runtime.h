@@ -26,6 +26,10 @@ struct GcLayer {
     float *rows2 = nullptr; /* [ny][2] R0, R22 of nonlinear spherical layers */
     int *arrival = nullptr;
     float *spx = nullptr, *spy = nullptr; /* sponge coefficients per column / per row */
+    bool has_sc = false;      /* SC_OPTION = 1 child */
+    GcScView sc{};            /* its device tables (in sc_block) */
+    void *sc_block = nullptr;
+    bool sc_stepped = false;  /* after its first sub-step the level-1 buffer holds the reference's Z(:,:,2) */
     float sp_dt = 0.0f;
     int cur = 0;          /* buffer index holding time level 1 */
     bool z2_valid = false; /* level-2 buffer holds the reference's Z(:,:,2) */
@@ -40,6 +44,11 @@ struct GcPendingParams {
     float dt = 0, rx = 0, ry = 0, grx = 0, gry = 0, fric_coef = 0;
     std::vector<float> hp, hq;
     std::vector<float> r0, r22; /* per row, from gcomcot_set_layer_coefs_ */
+    /* SC_OPTION = 1 tables from gcomcot_set_sc_tables_, [ny][nx][2] and [ny][nx][4] */
+    bool sc = false;
+    int sc_fix_top = 0, sc_modscm = 1;
+    std::vector<int> sc_pos;
+    std::vector<float> sc_cxy;
 };
 
 struct GcRuntime {

@@ -83,6 +83,13 @@ void gcomcot_set_layer_coefs_(int *id, float *R0, float *R21, float *R22, int *n
 void gcomcot_set_sponge_(int *id, float *coefx, float *coefy, float *dt, int *nx, int *ny);
 /* SPONGE_LAYER (boundaries.f90:206-247) on the device; call after momt_launch_ */
 void sponge_launch_(const int *lid);
+/* no device counterpart in the reference (its device path couples every
+ * child as linear spherical): the SC_OPTION = 1 tables of a Cartesian child
+ * of a spherical parent, POS(NX,NY,2) and CXY(NX,NY,4) from
+ * SUBGRID_MATCHING (initialization.f90:1065-1124), the parent's MODSCM, and
+ * FIX_TOP (1: the top edge blends C2*YN1 instead of the C1*YN1 of
+ * all_grids.f90:1357).  Call before gcomcot_init_layer_ of that child. */
+void gcomcot_set_sc_tables_(int *id, int *pos, float *cxy, int *nx, int *ny, int *parent_modscm, int *fix_top);
 /* no counterpart in the reference: arrival-step tracking on the outer layer */
 void gcomcot_set_arrival_(int *id, float *thr);
 void gcomcot_get_arrival_(int *arrival, int *id);

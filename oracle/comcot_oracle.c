@@ -1099,6 +1099,170 @@ void ocl_jnz(ocl_layer *P, ocl_layer *C) {
 }
 
 /* ------------------------------------------------------------------ */
+/* SC_OPTION = 1: Cartesian child of a spherical parent, coupled through */
+/* the child nodes' positions POS and bilinear weights CXY in the parent */
+/* ------------------------------------------------------------------ */
+static inline const int *sc_pos(ocl_layer *C, int i, int j) { return C->pos + 2 * IDX(C, i, j); }
+static inline const REAL *sc_w(ocl_layer *C, int i, int j) { return C->cxy + 4 * IDX(C, i, j); }
+
+/* Z1+Z2+Z3+Z4 of the four weighted parent values (all_grids.f90:1030-1034) */
+static REAL sc_bilin(const REAL *f, ocl_layer *P, const int *ps, const REAL *w) {
+    int ki = ps[0], kj = ps[1];
+    REAL z1 = f[IDX(P, ki, kj)] * w[0];
+    REAL z2 = f[IDX(P, ki + 1, kj)] * w[1];
+    REAL z3 = f[IDX(P, ki, kj + 1)] * w[2];
+    REAL z4 = f[IDX(P, ki + 1, kj + 1)] * w[3];
+    return z1 + z2 + z3 + z4;
+}
+
+/* EDGE_INTERP_SC (all_grids.f90:996-1087).  The reference tests wetness at
+ * LA%H(I,J)+LA%Z(I,J,2) with I (left/right edges) and J (bottom/top edges)
+ * left over from elsewhere: an undefined value on entry and NY+1 after the
+ * J loops, outside the array.  That read cannot be reproduced; the test
+ * here is at the edge node itself, as NEWQ_SC (:1268-1362) makes it. */
+void ocl_edge_sc(ocl_layer *P, ocl_layer *C) {
+    for (int j = 1; j <= C->ny; j++)
+        for (int s = 0; s < 2; s++) {
+            int i = s == 0 ? 1 : C->nx;
+            size_t c = IDX(C, i, j);
+            C->m1[c] = (C->h[c] + C->z2[c] > R(CC_GX)) ? sc_bilin(P->m1, P, sc_pos(C, i, j), sc_w(C, i, j)) : R(0);
+        }
+    for (int i = 1; i <= C->nx; i++)
+        for (int s = 0; s < 2; s++) {
+            int j = s == 0 ? 1 : C->ny;
+            size_t c = IDX(C, i, j);
+            C->n1[c] = (C->h[c] + C->z2[c] > R(CC_GX)) ? sc_bilin(P->n1, P, sc_pos(C, i, j), sc_w(C, i, j)) : R(0);
+        }
+}
+
+/* NEWQ_SC forecast of the parent X flux on one band (all_grids.f90:1130-1163) */
+static void sc_forecast_m(ocl_layer *P, int is, int ie, int js, int je) {
+    const REAL twlvth = R(0.08333333333333);
+    for (int i = is; i <= ie; i++) {
+        int ip1 = i + 1;
+        for (int j = js; j <= je; j++) {
+            size_t c = IDX(P, i, j), cp = IDX(P, ip1, j);
+            if (P->h[c] > R(CC_GX) && P->h[cp] > R(CC_GX)) {
+                int jm1 = MAX(j - 1, 1), jp1 = MIN(j + 1, P->ny);
+                REAL tot_n = P->n1[c] + P->n1[cp] + P->n1[IDX(P, i, jm1)] + P->n1[IDX(P, ip1, jm1)];
+                REAL xm = P->m1[c] - P->r2[c] * (P->z2[cp] - P->z2[c]) + P->r3[j - 1] * tot_n;
+                if (P->modscm == 0) {
+                    REAL scm = P->r2[c] * twlvth *
+                               ((P->z2[IDX(P, ip1, jp1)] - R(2) * P->z2[cp] + P->z2[IDX(P, ip1, jm1)]) -
+                                (P->z2[IDX(P, i, jp1)] - R(2) * P->z2[c] + P->z2[IDX(P, i, jm1)]));
+                    xm = xm - scm;
+                }
+                if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                P->m2[c] = xm;
+            } else {
+                P->m2[c] = R(0);
+            }
+        }
+    }
+}
+
+/* the Y flux on one band (all_grids.f90:1198-1231) */
+static void sc_forecast_n(ocl_layer *P, int is, int ie, int js, int je) {
+    const REAL twlvth = R(0.08333333333333);
+    for (int j = js; j <= je; j++) {
+        int jp1 = j + 1;
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(P, i, j), cq = IDX(P, i, jp1);
+            if (P->h[c] > R(CC_GX) && P->h[cq] > R(CC_GX)) {
+                int im1 = MAX(i - 1, 1), ip1 = MIN(i + 1, P->nx);
+                REAL tot_m = P->m1[IDX(P, im1, j)] + P->m1[IDX(P, im1, jp1)] + P->m1[c] + P->m1[cq];
+                REAL xn = P->n1[c] - P->r4[c] * (P->z2[cq] - P->z2[c]) - P->r5[j - 1] * tot_m;
+                if (P->modscm == 0) {
+                    REAL scm = P->r4[c] * twlvth *
+                               ((P->z2[IDX(P, ip1, jp1)] - R(2) * P->z2[cq] + P->z2[IDX(P, im1, jp1)]) -
+                                (P->z2[IDX(P, ip1, j)] - R(2) * P->z2[c] + P->z2[IDX(P, im1, j)]));
+                    xn = xn - scm;
+                }
+                if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                P->n2[c] = xn;
+            } else {
+                P->n2[c] = R(0);
+            }
+        }
+    }
+}
+
+void ocl_newq_sc(ocl_layer *P, ocl_layer *C, int t) {
+    /* NEWQ_SC (all_grids.f90:1090-1364): forecast the parent fluxes at the
+     * end of its step on four bands around the child's edges, written into
+     * the parent's level 2 (its momentum step overwrites them later), then
+     * blend the two levels at the edge nodes */
+    const int nx = C->nx, ny = C->ny;
+    int a = sc_pos(C, 1, 1)[0], b = sc_pos(C, 1, ny)[0];
+    sc_forecast_m(P, MIN(a, b) - 2, MAX(a, b) + 2, C->corners[2] - 2, C->corners[3] + 2);
+    a = sc_pos(C, nx, 1)[0]; b = sc_pos(C, nx, ny)[0];
+    sc_forecast_m(P, MIN(a, b) - 2, MAX(a, b) + 2, C->corners[2] - 2, C->corners[3] + 2);
+    a = sc_pos(C, 1, ny)[1]; b = sc_pos(C, nx, ny)[1];
+    sc_forecast_n(P, C->corners[0] - 2, C->corners[1] + 2, MIN(a, b) - 2, MAX(a, b) + 2);
+    a = sc_pos(C, 1, 1)[1]; b = sc_pos(C, nx, 1)[1];
+    sc_forecast_n(P, C->corners[0] - 2, C->corners[1] + 2, MIN(a, b) - 2, MAX(a, b) + 2);
+    const REAL c1 = (R(t) - R(1)) / R(C->rel_time);
+    const REAL c2 = R(1) - c1;
+    for (int j = 1; j <= ny; j++)
+        for (int s = 0; s < 2; s++) {
+            int i = s == 0 ? 1 : nx;
+            size_t c = IDX(C, i, j);
+            if (C->h[c] + C->z2[c] > R(CC_GX)) {
+                REAL x1 = sc_bilin(P->m1, P, sc_pos(C, i, j), sc_w(C, i, j));
+                REAL x2 = sc_bilin(P->m2, P, sc_pos(C, i, j), sc_w(C, i, j));
+                C->m1[c] = c1 * x2 + c2 * x1;
+            } else {
+                C->m1[c] = R(0);
+            }
+        }
+    for (int i = 1; i <= nx; i++)
+        for (int s = 0; s < 2; s++) {
+            int j = s == 0 ? 1 : ny;
+            size_t c = IDX(C, i, j);
+            if (C->h[c] + C->z2[c] > R(CC_GX)) {
+                REAL y1 = sc_bilin(P->n1, P, sc_pos(C, i, j), sc_w(C, i, j));
+                REAL y2 = sc_bilin(P->n2, P, sc_pos(C, i, j), sc_w(C, i, j));
+                /* the reference's top edge weights YN1 by C1 (all_grids.f90:1357) */
+                REAL w1 = (s == 1 && !C->sc_fix_top) ? c1 : c2;
+                C->n1[c] = c1 * y2 + w1 * y1;
+            } else {
+                C->n1[c] = R(0);
+            }
+        }
+}
+
+void ocl_jnz_sc(ocl_layer *P, ocl_layer *C) {
+    /* JNZ_SC (all_grids.f90:1367-1425): sum of the wet child surfaces that
+     * fall in each parent cell, in the reference's loop order (child I
+     * outermost); the parent surface takes their mean where more than half
+     * of r*r nodes contributed and is left as it is elsewhere.  Child nodes
+     * outside the parent interior (KI or KJ = 0) are skipped: the reference
+     * would index its sums at 0 there. */
+    size_t np = (size_t)P->nx * P->ny;
+    REAL *zs = (REAL *)calloc(np, sizeof(REAL));
+    REAL *cs = (REAL *)calloc(np, sizeof(REAL));
+    const REAL half = R(C->rel_size * C->rel_size) / R(2);
+    for (int i = 1; i <= C->nx; i++)
+        for (int j = 1; j <= C->ny; j++) {
+            size_t c = IDX(C, i, j);
+            if (C->h[c] + C->z2[c] > R(CC_GX)) {
+                const int *ps = sc_pos(C, i, j);
+                if (ps[0] < 1 || ps[1] < 1) continue;
+                size_t q = IDX(P, ps[0], ps[1]);
+                zs[q] = zs[q] + C->z2[c];
+                cs[q] = cs[q] + R(1);
+            }
+        }
+    for (int i = C->corners[0]; i <= C->corners[1]; i++)
+        for (int j = C->corners[2]; j <= C->corners[3]; j++) {
+            size_t q = IDX(P, i, j);
+            if (cs[q] > half) P->z2[q] = zs[q] / cs[q];
+        }
+    free(zs);
+    free(cs);
+}
+
+/* ------------------------------------------------------------------ */
 /* outputs: running maximum, arrival step, gauges                      */
 /* ------------------------------------------------------------------ */
 void ocl_maxamp(ocl_layer *L) {
@@ -1141,12 +1305,20 @@ static void all_grid_rec(ocl_layer *layers, int n, int parent_idx) {
         if (c == parent_idx || C->parent != P->id) continue;
         int nhalf = C->rel_time / 2 + 1;
         for (int k = 1; k <= C->rel_time; k++) {
-            if (k == 1) ocl_jnq(P, C);
-            else ocl_newq(P, C, k);
+            if (C->sc_option == 1) {
+                if (k == 1) ocl_edge_sc(P, C);
+                else ocl_newq_sc(P, C, k);
+            } else {
+                if (k == 1) ocl_jnq(P, C);
+                else ocl_newq(P, C, k);
+            }
             ocl_mass(C);
             all_grid_rec(layers, n, c);
             ocl_moment(C);
-            if (k == nhalf) ocl_jnz(P, C);
+            if (k == nhalf) {
+                if (C->sc_option == 1) ocl_jnz_sc(P, C);
+                else ocl_jnz(P, C);
+            }
             ocl_update(C);
         }
     }

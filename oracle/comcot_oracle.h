@@ -44,6 +44,10 @@ typedef struct {
     REAL *zmax;                           /* [nx*ny] or NULL */
     int  *arrival;                        /* [nx*ny] or NULL */
     REAL *spx, *spy;                      /* [nx*ny] SPONGE_COEFX/Y of the outer layer, or NULL */
+    int sc_option;                        /* 1: Cartesian child coupled through POS/CXY (SC_OPTION = 1) */
+    int sc_fix_top;                       /* 1: top edge blends C2*YN1 instead of the reference's C1*YN1 */
+    int *pos;                             /* [ny][nx][2] 1-based (KI, KJ) in the parent, SC_OPTION = 1 */
+    REAL *cxy;                            /* [ny][nx][4] bilinear weights, SC_OPTION = 1 */
 } ocl_layer;
 
 void ocl_set_threads(int n);
@@ -57,6 +61,10 @@ void ocl_update(ocl_layer *L);
 void ocl_jnq(ocl_layer *P, ocl_layer *C);
 void ocl_newq(ocl_layer *P, ocl_layer *C, int t);
 void ocl_jnz(ocl_layer *P, ocl_layer *C);
+/* SC_OPTION = 1 coupling (all_grids.f90:996-1425) */
+void ocl_edge_sc(ocl_layer *P, ocl_layer *C);
+void ocl_newq_sc(ocl_layer *P, ocl_layer *C, int t);
+void ocl_jnz_sc(ocl_layer *P, ocl_layer *C);
 void ocl_maxamp(ocl_layer *L);
 /* SPONGE_LAYER (boundaries.f90:206-247): after the momentum step */
 void ocl_sponge(ocl_layer *L);

@@ -99,7 +99,8 @@ class OLayer(C.Structure):
                 + [(n, C.c_double) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
                 + [(n, C.c_void_p) for n in ("r1", "r11", "r6", "r3", "r5", "r0", "r22", "r2", "r4", "h", "hp", "hq",
                                              "z1", "z2", "m1", "m2", "n1", "n2", "dz2", "xflux", "yflux",
-                                             "zmax", "arrival", "spx", "spy")])
+                                             "zmax", "arrival", "spx", "spy")]
+                + [("sc_option", C.c_int), ("sc_fix_top", C.c_int), ("pos", C.c_void_p), ("cxy", C.c_void_p)])
 
 
 class OracleRun:
@@ -156,6 +157,11 @@ class OracleRun:
         sp = getattr(L, "sponge", None)
         f["spx"] = self._a(sp[0]) if (is_root and sp is not None) else None
         f["spy"] = self._a(sp[1]) if (is_root and sp is not None) else None
+        sc = getattr(L, "sc", None)
+        o.sc_option = 1 if sc is not None else 0
+        o.sc_fix_top = int(sc.fix_top) if sc is not None else 0
+        f["pos"] = self._a(sc.pos, np.int32) if sc is not None else None
+        f["cxy"] = self._a(sc.cxy) if sc is not None else None
         for nm, a in f.items():
             setattr(o, nm, a.ctypes.data if a is not None else None)
         return f

@@ -146,3 +146,21 @@ def test_sponge_and_wall_outer_layer(oracle_mod, kind):
                        (gpu["zmax"], ref["zmax"], "zmax")):
         _cmp(a, b, what)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
+@pytest.mark.parametrize("rel_time,fix_top,laygov", [(None, False, 1), (2, False, 1), (3, True, 1), (2, False, 0)])
+def test_nested_sc_option_1_child(oracle_mod, rel_time, fix_top, laygov):
+    """SC_OPTION = 1 (all_grids.f90:996-1425): a Cartesian child coupled to
+    its spherical parent through per-node positions and bilinear weights;
+    EDGE_INTERP_SC at the first sub-step, NEWQ_SC's band forecast and blend
+    after it, JNZ_SC at the half step; bitwise against the oracle"""
+    case = synth.nested_sc_case("sc", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 0, seed=3, rel_time=rel_time,
+                                fix_top=fix_top, child_laygov=laygov)
+    gpu, _, o, _ = _run_both(case, 50, oracle_mod)
+    ref, rc = o.layer(0), o.layer(1)
+    cz, (cm, cn) = gpu["children"][0]
+    assert np.abs(rc["m"]).max() > 0
+    for a, b, what in ((gpu["z"], ref["z"], "parent eta"), (gpu["mn"][0], ref["m"], "parent M"),
+                       (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"), (cn, rc["n"], "child N")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what

@@ -111,3 +111,28 @@ def test_bc_wall_sides():
         assert (w == -999).sum() == H.size - 6 * 8 - open_view(w).size
     assert (pc.bc_wall(H, ini_switch=2, incident=5) == H).all()
     assert (H == 100).all()   # the input is not modified
+
+
+def test_utm_round_trip_and_sc_tables():
+    """SPH_TO_UTM / UTM_TO_SPH (initialization.f90:1390-1590) invert each
+    other, and the SC_OPTION = 1 tables place every child node inside the
+    parent cell they name, with weights summing to 1"""
+    rng = np.random.default_rng(4)
+    for _ in range(20):
+        lon0 = float(rng.uniform(3.0, 357.0))
+        lon = lon0 + rng.uniform(-2.5, 2.5, 50)
+        lat = rng.uniform(-70.0, 70.0, 50)
+        x, y = pc.sph_to_utm(lon, lat, lon0)
+        lo, la = pc.utm_to_sph(x, y, lon0)
+        assert np.abs(lo - lon).max() < 1e-6 and np.abs(la - lat).max() < 1e-6
+    assert pc.utm_zone_meridian(140.2) == 141.0 and pc.utm_zone_meridian(-10.0) == 0.0
+    xp, yp = pc.axes(140.0, 20.0, 97, 81, 2.0)
+    g = pc.sc_child_geometry(xp, yp, [60, 79, 30, 49], 3, 2.0)
+    assert g.pos.shape == (61, 61, 2) and (g.pos >= 2).all()
+    lon, lat = pc.coord_convert_to_sph(*np.meshgrid(g.x, g.y), g.xs, g.ys)
+    ki, kj = g.pos[..., 0] - 1, g.pos[..., 1] - 1
+    assert (xp[ki] <= lon).all() and (lon < xp[ki + 1]).all()
+    assert (yp[kj] <= lat).all() and (lat < yp[kj + 1]).all()
+    assert np.abs(g.cxy.sum(-1) - 1.0).max() < 1e-6 and (g.cxy >= 0).all()
+    assert g.corners == [int(g.pos[..., 0].min()), int(g.pos[..., 0].max()), int(g.pos[..., 1].min()),
+                         int(g.pos[..., 1].max())]
