@@ -161,6 +161,10 @@ struct gc_engine {
     std::vector<int> nested_ids; /* active nested members */
     cudaStream_t aux[kMaxAux] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kMaxAux] = {};
+    /* per aux stream, a second stream for the child's first sub-step, which
+     * runs beside the outer grid's fused step */
+    cudaStream_t caux[kMaxAux] = {};
+    cudaEvent_t ev_cfork[kMaxAux] = {}, ev_cjoin[kMaxAux] = {};
 };
 
 /* One outer step of a nested member whose 0-based step index is `local`
@@ -178,8 +182,8 @@ struct gc_engine {
  * differ, and the rectangle [IS-1,IE] x [JS-1,JE] is recomputed.  The child
  * reads the outer Z(:,:,2), M(:,:,1) and N(:,:,1) only.  Max-eta, arrival
  * and gauges follow in the outputs kernel, after the feedback. */
-static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_base, int step_off,
-                            cudaStream_t s) {
+static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_base, int step_off, int a) {
+    cudaStream_t s = e->aux[a];
     const EngClass &C = e->classes[M.cls];
     const int cur = local & 1;
     GcFusedGrid g;
@@ -199,15 +203,32 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     for (int q = 0; q < 2; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
     g.h = C.d_h; g.rows = C.d_rows;
     g.zmax = M.zmax; g.arrival = M.arrival;
-    gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
     const GcLayerDev P = outer_view(C, M, cur);
     int cc = (int)(((long long)local * C.rel_time) & 1);
     const int nhalf = C.rel_time / 2 + 1;
+    /* the child's first sub-step (JNQ, its mass and momentum) reads the
+     * outer grid's level-1 fluxes only, which the fused step does not write,
+     * and the fused step reads nothing of the child's: they run side by
+     * side, joined before JNZ */
+    {
+        const GcLayerDev Cv = child_view(C, M, cc);
+        cudaStream_t cs = e->caux[a];
+        cudaEventRecord(e->ev_cfork[a], s);
+        cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
+        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, 1, cs);
+        gc_launch_mass(Cv, cs);
+        gc_launch_moment(Cv, cs);
+        cudaEventRecord(e->ev_cjoin[a], cs);
+    }
+    gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
+    cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
     for (int t = 1; t <= C.rel_time; t++) {
         const GcLayerDev Cv = child_view(C, M, cc);
-        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
-        gc_launch_mass(Cv, s);
-        gc_launch_moment(Cv, s);
+        if (t > 1) {
+            gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
+            gc_launch_mass(Cv, s);
+            gc_launch_moment(Cv, s);
+        }
         if (t == nhalf) { gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
         gc_launch_update_edges(Cv, s);
         cc ^= 1;
@@ -258,9 +279,8 @@ static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_o
     }
     for (int q = 0; q < nn; q++) {
         EngMember &M = e->members[e->nested_ids[q]];
-        cudaStream_t s = e->aux[q % naux];
         for (int k = 0; k < count; k++)
-            eng_nested_step(e, M, e->gstep + 1 + k - M.step0, d_base, step_off0 + k, s);
+            eng_nested_step(e, M, e->gstep + 1 + k - M.step0, d_base, step_off0 + k, q % naux);
     }
     if (naux > 0) {
         for (int a = 0; a < naux; a++) {
@@ -281,6 +301,9 @@ static int eng_make_aux(gc_engine *e, int naux) {
         if (e->aux[a]) continue;
         GC_CUDA_OR_RET(cudaStreamCreateWithFlags(&e->aux[a], cudaStreamNonBlocking));
         GC_CUDA_OR_RET(cudaEventCreateWithFlags(&e->ev_join[a], cudaEventDisableTiming));
+        GC_CUDA_OR_RET(cudaStreamCreateWithFlags(&e->caux[a], cudaStreamNonBlocking));
+        GC_CUDA_OR_RET(cudaEventCreateWithFlags(&e->ev_cfork[a], cudaEventDisableTiming));
+        GC_CUDA_OR_RET(cudaEventCreateWithFlags(&e->ev_cjoin[a], cudaEventDisableTiming));
     }
     return GC_OK;
 }
@@ -473,6 +496,9 @@ int gc_engine_destroy(gc_engine *e) {
     for (int a = 0; a < kMaxAux; a++) {
         if (e->aux[a]) cudaStreamDestroy(e->aux[a]);
         if (e->ev_join[a]) cudaEventDestroy(e->ev_join[a]);
+        if (e->caux[a]) cudaStreamDestroy(e->caux[a]);
+        if (e->ev_cfork[a]) cudaEventDestroy(e->ev_cfork[a]);
+        if (e->ev_cjoin[a]) cudaEventDestroy(e->ev_cjoin[a]);
     }
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     cudaStreamDestroy(e->stream);
