@@ -206,39 +206,47 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     const GcLayerDev P = outer_view(C, M, cur);
     int cc = (int)(((long long)local * C.rel_time) & 1);
     const int nhalf = C.rel_time / 2 + 1;
-    /* the child's first sub-step (JNQ, its mass and momentum) reads the
-     * outer grid's level-1 fluxes only, which the fused step does not write,
-     * and the fused step reads nothing of the child's: they run side by
-     * side, joined before JNZ */
-    {
-        const GcLayerDev Cv = child_view(C, M, cc);
-        cudaStream_t cs = e->caux[a];
-        cudaEventRecord(e->ev_cfork[a], s);
-        cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
-        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, 1, cs);
-        gc_launch_mass(Cv, cs);
-        gc_launch_moment(Cv, cs);
-        cudaEventRecord(e->ev_cjoin[a], cs);
-    }
+    /* the child's first sub-step (JNQ, its mass and momentum, UPDATE's edge
+     * copy) reads the outer grid's level-1 fluxes only, which the fused step
+     * does not write, and the fused step reads nothing of the child's: they
+     * run side by side, joined before JNZ.  UPDATE writes the child's row and
+     * column 0 alone, which JNZ never reads, so it may precede JNZ. */
+    cudaStream_t cs = e->caux[a];
+    const GcLayerDev Cv1 = child_view(C, M, cc);
+    cudaEventRecord(e->ev_cfork[a], s);
+    cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
+    gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
+    gc_launch_mass(Cv1, cs);
+    gc_launch_moment(Cv1, cs);
+    gc_launch_update_edges(Cv1, cs);
+    cudaEventRecord(e->ev_cjoin[a], cs);
     gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
     cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
-    for (int t = 1; t <= C.rel_time; t++) {
+    if (nhalf == 1) { gc_launch_jnz(P, Cv1, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
+    cc ^= 1;
+    e->launches += 4;
+    for (int t = 2; t <= C.rel_time; t++) {
         const GcLayerDev Cv = child_view(C, M, cc);
-        if (t > 1) {
-            gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
-            gc_launch_mass(Cv, s);
-            gc_launch_moment(Cv, s);
-        }
+        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
+        gc_launch_mass(Cv, s);
+        gc_launch_moment(Cv, s);
         if (t == nhalf) { gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
         gc_launch_update_edges(Cv, s);
         cc ^= 1;
         e->launches += 4;
     }
-    /* Fortran (IS-1 .. IE, JS-1 .. JE) -> 0-based (IS-2 .. IE-1, JS-2 .. JE-1) */
-    gc_launch_momt_s_window(P, C.corners[0] - 2, C.corners[1] - 1, C.corners[2] - 2, C.corners[3] - 1, s);
+    /* the window's momentum (which the surface JNZ wrote changes) and its
+     * max-eta / arrival / gauges, side by side; both read the final surface,
+     * neither writes what the other reads.  Fortran (IS-1 .. IE, JS-1 .. JE)
+     * -> 0-based (IS-2 .. IE-1, JS-2 .. JE-1) */
+    cudaEventRecord(e->ev_cfork[a], s);
+    cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
     gc_launch_step_outputs(P, d_base, step_off, M.step0, flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc],
-                           C.cpitch, M.ts, M.nsteps, win, s);
-    e->launches += 3;
+                           C.cpitch, M.ts, M.nsteps, win, cs);
+    cudaEventRecord(e->ev_cjoin[a], cs);
+    gc_launch_momt_s_window(P, C.corners[0] - 2, C.corners[1] - 1, C.corners[2] - 2, C.corners[3] - 1, s);
+    cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
+    e->launches += 3; /* the fused step, the window's momentum, the outputs */
 }
 
 /* issues `count` consecutive steps, the first being host step e->gstep + 1

@@ -324,8 +324,8 @@ __global__ void k_conmome(GcLayerDev L) {
     const int jm1 = j > 0 ? j - 1 : 0, jp1 = j + 1 < jy ? j + 1 : jy - 1;
 #define AT(a, ii, jj) (a)[(size_t)(jj) * P + (ii)]
 
-    /* ---------------- x direction ---------------- */
-    {
+    /* ---------------- x direction (blockIdx.z = 0) ---------------- */
+    if (blockIdx.z == 0) {
         bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
         float out = 0.0f;
         if (inx) {
@@ -416,8 +416,8 @@ __global__ void k_conmome(GcLayerDev L) {
         }
         L.m2[c] = out;
     }
-    /* ---------------- y direction ---------------- */
-    {
+    /* ---------------- y direction (blockIdx.z = 1) ---------------- */
+    else {
         bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
         float out = 0.0f;
         if (iny) {
@@ -971,9 +971,11 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
 }
 
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, grid2(L), dim3(BX, BY), 0, s, L);
+    /* CONMOME's two directions are independent: one grid layer each */
+    const dim3 g2(grid2(L).x, grid2(L).y, 2);
+    if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L);
     else if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
-    else if (L.laygov == 1) launch(k_conmome<false>, grid2(L), dim3(BX, BY), 0, s, L);
+    else if (L.laygov == 1) launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L);
     else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
