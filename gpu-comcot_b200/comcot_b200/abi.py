@@ -34,6 +34,8 @@ class ReferenceSession:
         self.lib.gcomcot_init_gpu_()
         self.lib.gcomcot_set_fusion(1 if fusion else 0)
         self._keep = []
+        # the host arrays a Fortran caller already holds (LO%R1 ... LO%Z), built once
+        self._host = {L.id: self._host_arrays(L) for L in case.layers}
         if init_layers:
             self.init_layers()
         if arrival:
@@ -47,55 +49,65 @@ class ReferenceSession:
     def stream(self) -> int:
         return int(self.lib.gcomcot_stream() or 0)
 
+    @staticmethod
+    def _host_arrays(L: LayerSpec) -> dict:
+        """the NX x NY Fortran-order host arrays GCOMCOT_INIT_LAYER and the
+        extension calls read, as comcot.f90 holds them"""
+        ny, nx = L.ny, L.nx
+        full = lambda v: np.ascontiguousarray(np.repeat(np.asarray(v)[:, None], nx, axis=1), dtype=F32)
+        a = {}
+        if L.laycord == 1 or L.laygov != 0:
+            a["hp"] = np.ascontiguousarray(L.hp, dtype=F32)
+            a["hq"] = np.ascontiguousarray(L.hq, dtype=F32)
+        if L.sc is not None:
+            a["pos"] = np.ascontiguousarray(np.moveaxis(L.sc.pos, -1, 0), dtype=np.int32)
+            a["cxy"] = np.ascontiguousarray(np.moveaxis(L.sc.cxy, -1, 0), dtype=F32)
+        if L.laycord == 0 and L.laygov == 1:
+            c = L.coefs
+            a["r0"], a["r21"], a["r22"] = full(c.r0), full(c.r1), full(c.r22)
+        if L.coefs is not None:
+            c = L.coefs
+            a["R1"], a["R11"], a["R3"], a["R5"] = full(c.r1), full(c.r11), full(c.r3), full(c.r5)
+            a["R2"] = np.ascontiguousarray(c.r2, dtype=F32)
+            a["R4"] = np.ascontiguousarray(c.r4, dtype=F32)
+            a["R6"] = np.ascontiguousarray(c.r6, dtype=F32)
+        else:
+            z = np.zeros((ny, nx), F32)
+            a["R1"] = a["R11"] = a["R3"] = a["R5"] = a["R2"] = a["R4"] = z
+            a["R6"] = np.zeros(ny, F32)
+        a["H"] = np.ascontiguousarray(L.H, dtype=F32)
+        a["Z"] = np.ascontiguousarray(L.Z0, dtype=F32)
+        a["corners"] = np.array(L.corners, dtype=np.int32)
+        if L.sponge is not None:
+            a["spx"] = np.ascontiguousarray(L.sponge[0], dtype=F32)
+            a["spy"] = np.ascontiguousarray(L.sponge[1], dtype=F32)
+        return a
+
     def _init_layer(self, L: LayerSpec):
         lib = self.lib
         ny, nx = L.ny, L.nx
+        a = self._host[L.id]
         if L.laycord == 1 or L.laygov != 0:
-            hp = np.ascontiguousarray(L.hp, dtype=F32)
-            hq = np.ascontiguousarray(L.hq, dtype=F32)
-            self._keep += [hp, hq]
             lib.gcomcot_set_layer_params_(_i(L.id), _i(L.laycord), _i(L.laygov), _f(L.dt), _f(L.rx), _f(L.ry),
                                           _f(L.grx), _f(L.gry), _i(L.fric_switch), _f(L.fric_coef),
-                                          _i(L.linchk), _i(L.modscm), _i(nx), _i(ny), _lib.fptr(hp),
-                                          _lib.fptr(hq))
+                                          _i(L.linchk), _i(L.modscm), _i(nx), _i(ny), _lib.fptr(a["hp"]),
+                                          _lib.fptr(a["hq"]))
         if L.sc is not None:
             # SC_OPTION = 1 tables in Fortran order POS(NX,NY,2), CXY(NX,NY,4)
-            pos = np.ascontiguousarray(np.moveaxis(L.sc.pos, -1, 0), dtype=np.int32)
-            cxy = np.ascontiguousarray(np.moveaxis(L.sc.cxy, -1, 0), dtype=F32)
-            self._keep += [pos, cxy]
             parent = next(Q for Q in self.case.layers if Q.id == L.parent)
-            lib.gcomcot_set_sc_tables_(_i(L.id), _lib.iptr(pos), _lib.fptr(cxy), _i(nx), _i(ny),
+            lib.gcomcot_set_sc_tables_(_i(L.id), _lib.iptr(a["pos"]), _lib.fptr(a["cxy"]), _i(nx), _i(ny),
                                        _i(parent.modscm), _i(1 if L.sc.fix_top else 0))
         if L.laycord == 0 and L.laygov == 1:
-            c = L.coefs
-            full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)
-            r0, r21, r22 = full(c.r0), full(c.r1), full(c.r22)
-            self._keep += [r0, r21, r22]
-            lib.gcomcot_set_layer_coefs_(_i(L.id), _lib.fptr(r0), _lib.fptr(r21), _lib.fptr(r22), _i(nx), _i(ny))
-        if L.coefs is not None:
-            c = L.coefs
-            full = lambda v: np.ascontiguousarray(np.repeat(v[:, None], nx, axis=1), dtype=F32)
-            R1, R11, R3, R5 = full(c.r1), full(c.r11), full(c.r3), full(c.r5)
-            R2 = np.ascontiguousarray(c.r2, dtype=F32)
-            R4 = np.ascontiguousarray(c.r4, dtype=F32)
-            R6 = np.ascontiguousarray(c.r6, dtype=F32)
-        else:
-            z = np.zeros((ny, nx), F32)
-            R1 = R11 = R3 = R5 = R2 = R4 = z
-            R6 = np.zeros(ny, F32)
-        H = np.ascontiguousarray(L.H, dtype=F32)
-        Z = np.ascontiguousarray(L.Z0, dtype=F32)
-        corners = np.array(L.corners, dtype=np.int32)
+            lib.gcomcot_set_layer_coefs_(_i(L.id), _lib.fptr(a["r0"]), _lib.fptr(a["r21"]), _lib.fptr(a["r22"]),
+                                         _i(nx), _i(ny))
         lib.gcomcot_init_layer_(_i(L.id), _i(L.parent), _i(L.level), _i(L.rel_size), _i(L.rel_time),
-                                _lib.iptr(corners), _f(L.grx), _f(L.gry), _lib.fptr(R1), _lib.fptr(R2),
-                                _lib.fptr(R3), _lib.fptr(R4), _lib.fptr(R5), _lib.fptr(R6), _lib.fptr(R11),
-                                _lib.fptr(H), _lib.fptr(Z), _i(nx), _i(ny))
+                                _lib.iptr(a["corners"]), _f(L.grx), _f(L.gry), _lib.fptr(a["R1"]),
+                                _lib.fptr(a["R2"]), _lib.fptr(a["R3"]), _lib.fptr(a["R4"]), _lib.fptr(a["R5"]),
+                                _lib.fptr(a["R6"]), _lib.fptr(a["R11"]), _lib.fptr(a["H"]), _lib.fptr(a["Z"]),
+                                _i(nx), _i(ny))
         if L.sponge is not None:
             # BC_TYPE 1: SPONGE_COEF's fields (comcot.f90:220)
-            cx = np.ascontiguousarray(L.sponge[0], dtype=F32)
-            cy = np.ascontiguousarray(L.sponge[1], dtype=F32)
-            self._keep += [cx, cy]
-            lib.gcomcot_set_sponge_(_i(L.id), _lib.fptr(cx), _lib.fptr(cy), _f(L.dt), _i(nx), _i(ny))
+            lib.gcomcot_set_sponge_(_i(L.id), _lib.fptr(a["spx"]), _lib.fptr(a["spy"]), _f(L.dt), _i(nx), _i(ny))
 
     # ---- one outer step exactly as comcot.f90:359-439 ----
     def step(self, maxamp: bool = True):

@@ -29,6 +29,9 @@ static GcArrivalCfg g_arr;
 
 void gc_flush() {
     GcRuntime &rt = gc_rt();
+    /* each step's kernels are scheduled while the previous one runs and wait
+     * for it on the device */
+    GcPdlScope pdl(true);
     if (!(rt.pend_mass | rt.pend_open | rt.pend_momt | rt.pend_maxamp)) return;
     GcLayer &L = rt.layers[rt.root];
     bool done = false;

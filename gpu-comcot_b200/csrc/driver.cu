@@ -19,6 +19,7 @@ struct GaugeReg {
 };
 static std::vector<GaugeReg> g_reg;
 static bool g_snap_valid = false;
+static bool g_ij_stale = true;    /* the device copy of the stencil indices needs an upload */
 static int *g_d_ij = nullptr;     /* [2*cap] */
 static float *g_h_out = nullptr;  /* mapped pinned [4*cap] */
 static float *g_d_out = nullptr;  /* device alias of g_h_out */
@@ -31,6 +32,7 @@ static int ensure_cap(int n) {
     int cap = n < 64 ? 64 : 2 * n;
     if (g_d_ij) cudaFree(g_d_ij);
     if (g_h_out) cudaFreeHost(g_h_out);
+    g_ij_stale = true;
     GC_CUDA_OR_RET(cudaMalloc(&g_d_ij, (size_t)2 * cap * sizeof(int)));
     GC_CUDA_OR_RET(cudaHostAlloc((void **)&g_h_out, (size_t)4 * cap * sizeof(float), cudaHostAllocMapped));
     GC_CUDA_OR_RET(cudaHostGetDevicePointer((void **)&g_d_out, g_h_out, 0));
@@ -42,12 +44,17 @@ static int ensure_cap(int n) {
  * per layer that has gauges, then waits */
 static int snapshot() {
     GcRuntime &rt = gc_rt();
+    GcPdlScope pdl(true); /* the gauge kernel waits for the step on the device */
     int n = (int)g_reg.size();
     if (ensure_cap(n) != GC_OK) return GC_ECUDA;
-    std::vector<int> ij((size_t)2 * n);
-    for (int g = 0; g < n; g++) { ij[2 * g] = g_reg[g].i; ij[2 * g + 1] = g_reg[g].j; }
-    GC_CUDA_OR_RET(cudaMemcpyAsync(g_d_ij, ij.data(), ij.size() * sizeof(int), cudaMemcpyHostToDevice,
-                                   rt.stream));
+    if (g_ij_stale) {
+        /* only when the set of gauges changed: a copy from pageable memory
+         * waits for the stream, which would cost a second round trip a step */
+        std::vector<int> ij((size_t)2 * n);
+        for (int g = 0; g < n; g++) { ij[2 * g] = g_reg[g].i; ij[2 * g + 1] = g_reg[g].j; }
+        GC_CUDA_OR_RET(cudaMemcpy(g_d_ij, ij.data(), ij.size() * sizeof(int), cudaMemcpyHostToDevice));
+        g_ij_stale = false;
+    }
     /* gauges are registered grouped by first use; launch per run of equal lid */
     int g0 = 0;
     while (g0 < n) {
@@ -79,6 +86,7 @@ bool gc_gauge_lookup(int lid, int i, int j, float *out4) {
         g_reg.insert(g_reg.begin() + pos, GaugeReg{lid, i, j});
         found = (int)pos;
         g_snap_valid = false;
+        g_ij_stale = true;
     }
     if (!g_snap_valid) {
         gc_flush();
@@ -94,6 +102,7 @@ void gc_gauge_release() {
     g_d_ij = nullptr; g_h_out = nullptr; g_d_out = nullptr; g_cap = 0;
     g_reg.clear();
     g_snap_valid = false;
+    g_ij_stale = true;
 }
 
 extern "C" {

@@ -91,6 +91,12 @@ const char *gc_status_str(int code);
 /* launches from this host thread use programmatic dependent launch */
 void gc_set_pdl(bool on);
 bool gc_pdl_on();
+/* programmatic dependent launch for the launches in a scope */
+struct GcPdlScope {
+    bool prev;
+    explicit GcPdlScope(bool on) : prev(gc_pdl_on()) { gc_set_pdl(on); }
+    ~GcPdlScope() { gc_set_pdl(prev); }
+};
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_open(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s);

@@ -482,7 +482,9 @@ void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, i
                                    cudaMemcpyHostToDevice, g_rt.stream));
     if (gc_layer_upload_field(L, L.h, H_f) != GC_OK) exit(EXIT_FAILURE);
     if (gc_layer_upload_field(L, L.z[0], Z_f) != GC_OK) exit(EXIT_FAILURE);
-    if (gc_layer_upload_field(L, L.zmax, Z_f) != GC_OK) exit(EXIT_FAILURE);
+    /* Zmax starts from the initial Z (GPUcomcot.cu:79): a device copy */
+    GC_CUDA_OR_DIE(cudaMemcpyAsync(L.zmax, L.z[0], (size_t)L.pitch * L.ny * sizeof(float), cudaMemcpyDeviceToDevice,
+                                   g_rt.stream));
     if (L.explicit_r24) {
         if (gc_layer_upload_field(L, L.r2, R2_f) != GC_OK) exit(EXIT_FAILURE);
         if (gc_layer_upload_field(L, L.r4, R4_f) != GC_OK) exit(EXIT_FAILURE);
@@ -760,6 +762,7 @@ void cuda_shutdown_(void) {
 /* ------------------------------------------------------------------ */
 void gc_subcycle(int parent_id) {
     GcLayer &P = g_rt.layers[parent_id];
+    GcPdlScope pdl(true);
     for (int cid : P.children) {
         GcLayer &C = g_rt.layers[cid];
         int nhalf = C.rel_time / 2 + 1;
