@@ -96,7 +96,7 @@ def para(h: np.ndarray, lat: np.ndarray, dx_min: float, dt: float, del_y_min=Non
     r0 = (rr / (dely * RAD_MIN)).astype(np.float32)
     r22 = (rr / cos_n / (dx_min * RAD_MIN)).astype(np.float32)
     hp, hq = pq_depth(h)
-    if laygov == 0:
+    if laygov in (0, 2):   # LAYGOV 3 and the nonlinear forms carry no depth factor (comcot.f90:733-747,776-795)
         r2 = (cx[:, None] * np.maximum(hp, F32(0))).astype(np.float32)
         r4 = (cy[:, None] * np.maximum(hq, F32(0))).astype(np.float32)
     else:

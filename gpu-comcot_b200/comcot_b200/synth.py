@@ -178,8 +178,9 @@ def wet_gauges(L: LayerSpec, n, rng, first=1, margin=5):
 
 def single_layer_case(name, nx, ny, dx_min, dt, nsteps, seed, n_seamounts, shelf_cols, land_cols,
                       source="hump", ngauges=0, lon0=140.0, lat0=20.0, amp=None, laygov=0, fric=0.025):
-    """One spherical layer, linear (laygov 0) or nonlinear with Manning
-    friction (laygov 1, CONMASS_S / CONMOME_S)."""
+    """One spherical layer: linear (laygov 0), nonlinear with Manning
+    friction (laygov 1, CONMASS_S / CONMOME_S), or the dispersion-corrected
+    forms (laygov 2 and 3, MASS_S_D / MOMT_S_D)."""
     rng = np.random.default_rng(seed)
     x, y = pc.axes(lon0, lat0, nx, ny, dx_min)
     H = bathymetry(x, y, rng, n_seamounts=n_seamounts, shelf_cols=shelf_cols, land_cols=land_cols)
@@ -193,6 +194,8 @@ def single_layer_case(name, nx, ny, dx_min, dt, nsteps, seed, n_seamounts, shelf
     L = spherical_layer(1, x, y, H, Z0, dt, dx_min, laygov=laygov)
     if laygov == 1:
         L.fric_switch, L.fric_coef, L.linchk = 0, fric, 1
+    if laygov % 2 == 1:
+        L.modscm = 1   # comcot.f90:602
     case = Case(name, [L], nsteps)
     if ngauges:
         case.gauges = wet_gauges(L, ngauges, rng)

@@ -140,6 +140,143 @@ __device__ __forceinline__ float r4_at(const GcLayerDev &L, int i, int j, size_t
     return GC_ROW(L, GC_CY, j) * (0.5f * (h + hq1));
 }
 
+/* MASS_S_D / MASS_C_D (dispersion.f90:239-543), LAYGOV 2 and 3.  The
+ * reference's ALPHA clears its whole MASK inside the cell loop
+ * (dispersion.f90:125), so every cell takes the non-dispersive branch
+ * (:333-337, :460-462): linear continuity with the land clamp ZZ+H <= ZERO. */
+template <bool SPH>
+__global__ void k_mass_d(GcLayerDev L) {
+    pdl_enter();
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    size_t c = (size_t)j * L.pitch + i;
+    if (L.root) {
+        if (i < 1 || i > L.nx - 2 || j < 1 || j > L.ny - 2) return;
+    } else if (i == 0 || j == 0) {
+        L.z2[c] = L.z1[c];
+        return;
+    }
+    const float h = L.h[c];
+    float out = 0.0f;
+    if (h > CC_GX) {
+        float zz;
+        if (SPH)
+            zz = L.z1[c] - GC_ROW(L, GC_R1, j) * (L.m1[c] - L.m1[c - 1])
+                 - GC_ROW(L, GC_R11, j) * (L.n1[c] * GC_ROW(L, GC_R6, j) - L.n1[c - L.pitch] * GC_ROW(L, GC_R6, j - 1));
+        else
+            zz = L.z1[c] - L.rx * (L.m1[c] - L.m1[c - 1]) - L.ry * (L.n1[c] - L.n1[c - L.pitch]);
+        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if ((zz + h) <= 0.0f) zz = -h;
+        out = zz;
+    }
+    L.z2[c] = out;
+}
+
+/* MOMT_S_D / MOMT_C_D (dispersion.f90:544-1692), LAYGOV 2 and 3, with the
+ * reference's MASK = 0.  Spherical (:681-692, :812-823): MOMT_S plus the
+ * modified-scheme term when MODSCM = 0, the y wet test against ZERO (:706).
+ * Cartesian (:1225-1233, :1560-1568): face depth HM = HP + (Z + Z(I+1))/2,
+ * HN = (H + H(J+1) + Z + Z(J+1))/2, Manning friction, the modified-scheme
+ * term; a dry face is not written by the reference (:922, :1255), so it
+ * keeps its level-2 value, which equals level 1 after CHANGE / UPDATE. */
+template <bool SPH>
+__global__ void k_momt_d(GcLayerDev L) {
+    pdl_enter();
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    const int nx = L.nx, ny = L.ny, P = L.pitch;
+    if (i >= nx || j >= ny) return;
+    const size_t c = (size_t)j * P + i;
+    const int lo = L.root ? 0 : 1;
+    const float *z = L.z2;
+    const float konst = 0.5f * L.dt * CC_GRAV, fm = L.fric_coef;
+    /* x: I = IS..NX-1, J = JS..NY; cells outside are never written by the
+     * reference and stay 0 */
+    if (!(i >= lo && i <= nx - 2 && j >= lo)) {
+        L.m2[c] = 0.0f;
+    } else {
+        const size_t cp = c + 1;
+        const int jm1 = j > 0 ? j - 1 : 0, jp1 = j < ny - 1 ? j + 1 : ny - 1;
+        const size_t cm = (size_t)jm1 * P + i, cu = (size_t)jp1 * P + i;
+        const float h = L.h[c], hp1 = L.h[cp];
+        if (SPH) {
+            float xm = 0.0f;
+            if (h > CC_GX && hp1 > CC_GX) {
+                const float tot_n = L.n1[c] + L.n1[cp] + L.n1[cm] + L.n1[cm + 1];
+                const float r2 = r2_at(L, i, j, c, h, hp1);
+                xm = L.m1[c] - r2 * (z[cp] - z[c]) + GC_ROW(L, GC_R3, j) * tot_n;
+                if (L.modscm == 0) {
+                    const float scm = r2 * CC_TWLVTH * ((z[cu + 1] - 2.0f * z[cp] + z[cm + 1]) - (z[cu] - 2.0f * z[c] + z[cm]));
+                    xm = xm - scm;
+                }
+                if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            }
+            L.m2[c] = xm;
+        } else if (h > CC_GX && hp1 > CC_GX) {
+            const float hm = L.hp[c] + 0.5f * (z[c] + z[cp]);
+            float ff = 0.0f;
+            if (L.fric_switch != 1) {
+                const float xqq = 0.25f * (L.n1[c] + L.n1[cp] + L.n1[cm] + L.n1[cm + 1]);
+                if (hm >= 1.0e-3f)
+                    ff = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq) / cc_powf(hm, CC_MANNEXP);
+            }
+            float xm = (1.0f - ff) * L.m1[c] - L.grx * hm * (z[cp] - z[c]);
+            if (L.modscm == 0) {
+                const float scm = L.grx * CC_TWLVTH * hm * ((z[cu + 1] - 2.0f * z[cp] + z[cm + 1]) - (z[cu] - 2.0f * z[c] + z[cm]));
+                xm = xm - scm;
+            }
+            if (L.fric_switch != 1) xm = xm / (1.0f + ff);
+            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            L.m2[c] = xm;
+        } else {
+            L.m2[c] = L.m1[c];
+        }
+    }
+    /* y: J = JS..NY-1, I = IS..NX */
+    if (!(j >= lo && j <= ny - 2 && i >= lo)) {
+        L.n2[c] = 0.0f;
+    } else {
+        const size_t cq = c + P;
+        const int im1 = i > 0 ? i - 1 : 0, ip1 = i < nx - 1 ? i + 1 : nx - 1;
+        const size_t cw = (size_t)j * P + im1, ce = (size_t)j * P + ip1;
+        const float h = L.h[c], hq1 = L.h[cq];
+        if (SPH) {
+            float xn = 0.0f;
+            if (h > 0.0f && hq1 > 0.0f) {
+                const float tot_m = L.m1[cw] + L.m1[cw + P] + L.m1[c] + L.m1[cq];
+                /* R4 = C(J) * AMAX1(HQ,0), HQ = 0 where H <= GX (PQ_DEPTH) */
+                const float r4 = L.explicit_r24 ? L.r4[c] : (h > CC_GX ? r4_at(L, i, j, c, h, hq1) : 0.0f);
+                xn = L.n1[c] - r4 * (z[cq] - z[c]) - GC_ROW(L, GC_R5, j) * tot_m;
+                if (L.modscm == 0) {
+                    const float scm = r4 * CC_TWLVTH * ((z[ce + P] - 2.0f * z[cq] + z[cw + P]) - (z[ce] - 2.0f * z[c] + z[cw]));
+                    xn = xn - scm;
+                }
+                if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            }
+            L.n2[c] = xn;
+        } else if (h > CC_GX && hq1 > CC_GX) {
+            const float hn = 0.5f * (h + hq1 + z[c] + z[cq]);
+            float ff = 0.0f;
+            if (L.fric_switch != 1) {
+                const float xpp = 0.25f * (L.m1[c] + L.m1[cq] + L.m1[cw] + L.m1[cw + P]);
+                if (hn >= 1.0e-5f)
+                    ff = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp) / cc_powf(hn, CC_MANNEXP);
+            }
+            float xn = (1.0f - ff) * L.n1[c] - L.gry * hn * (z[cq] - z[c]);
+            if (L.modscm == 0) {
+                const float scm = L.gry * CC_TWLVTH * hn * ((z[ce + P] - 2.0f * z[cq] + z[cw + P]) - (z[ce] - 2.0f * z[c] + z[cw]));
+                xn = xn - scm;
+            }
+            if (L.fric_switch != 1) xn = xn / (1.0f + ff);
+            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            L.n2[c] = xn;
+        } else {
+            L.n2[c] = L.n1[c];
+        }
+    }
+}
+
 /* over the cells i0 <= i < i0+ni, j0 <= j < j0+nj (the whole layer, or a
  * window whose level-2 surface changed after the layer's step) */
 __global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
@@ -964,7 +1101,10 @@ inline dim3 grid2(const GcLayerDev &L) {
 } // namespace
 
 void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
-    if (L.laycord == 0 && L.laygov == 1) launch(k_mass_s<true>, grid2(L), dim3(BX, BY), 0, s, L);
+    if (L.laygov == 2 || L.laygov == 3) {
+        if (L.laycord == 0) launch(k_mass_d<true>, grid2(L), dim3(BX, BY), 0, s, L);
+        else launch(k_mass_d<false>, grid2(L), dim3(BX, BY), 0, s, L);
+    } else if (L.laycord == 0 && L.laygov == 1) launch(k_mass_s<true>, grid2(L), dim3(BX, BY), 0, s, L);
     else if (L.laycord == 0) launch(k_mass_s<false>, grid2(L), dim3(BX, BY), 0, s, L);
     else if (L.laygov == 1) launch(k_mass_c<true>, grid2(L), dim3(BX, BY), 0, s, L);
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
@@ -973,7 +1113,10 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
     /* CONMOME's two directions are independent: one grid layer each */
     const dim3 g2(grid2(L).x, grid2(L).y, 2);
-    if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L);
+    if (L.laygov == 2 || L.laygov == 3) {
+        if (L.laycord == 0) launch(k_momt_d<true>, grid2(L), dim3(BX, BY), 0, s, L);
+        else launch(k_momt_d<false>, grid2(L), dim3(BX, BY), 0, s, L);
+    } else if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L);
     else if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
     else if (L.laygov == 1) launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L);
     else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);

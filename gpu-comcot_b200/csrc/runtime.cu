@@ -238,6 +238,10 @@ void gcomcot_set_layer_params_(int *id, int *laycord, int *laygov, float *dt, fl
         fprintf(stderr, "ERROR: invalid layerid\n");
         exit(EXIT_FAILURE);
     }
+    if (*laycord < 0 || *laycord > 1 || *laygov < 0 || *laygov > 3) {
+        fprintf(stderr, "gcomcot: LAYCORD=%d LAYGOV=%d is not supported (0-1, 0-3)\n", *laycord, *laygov);
+        exit(EXIT_FAILURE);
+    }
     if (*fric_switch != 0 && *fric_switch != 1) {
         fprintf(stderr, "gcomcot: FRIC_SWITCH=%d is not supported (0 or 1)\n", *fric_switch);
         exit(EXIT_FAILURE);

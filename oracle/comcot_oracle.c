@@ -187,10 +187,44 @@ static void conmass_s_rows(void *ctx, int js, int je) {
     }
 }
 
+/* MASS_S_D / MASS_C_D (dispersion.f90:239-356, 357-543) for LAYGOV 2 and 3.
+ * ALPHA (dispersion.f90:36-165) clears the whole MASK inside its cell loop
+ * (:125), so MASK ends up 0 everywhere and every cell takes the
+ * non-dispersive branch (:333-337, :460-462): the linear continuity with the
+ * land clamp ZZ+H <= ZERO (MASS_S / MASS_C use EPS). */
+static void mass_d_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    REAL rx = R(L->rx), ry = R(L->ry);
+    int is = 2, ie = (L->id == 1) ? L->nx - 1 : L->nx;
+    for (int j = js; j <= je; j++) {
+        int jm1 = MAX(j - 1, 1);
+        for (int i = is; i <= ie; i++) {
+            size_t c = IDX(L, i, j);
+            REAL h = L->h[c];
+            int im1 = MAX(i - 1, 1);
+            if (h > R(CC_GX)) {
+                REAL zz;
+                if (L->laycord == 0)
+                    zz = L->z1[c] - L->r1[j - 1] * (L->m1[c] - L->m1[IDX(L, im1, j)])
+                         - L->r11[j - 1] * (L->n1[c] * L->r6[j - 1] - L->n1[IDX(L, i, jm1)] * L->r6[jm1 - 1]);
+                else
+                    zz = L->z1[c] - rx * (L->m1[c] - L->m1[IDX(L, im1, j)]) - ry * (L->n1[c] - L->n1[IDX(L, i, jm1)]);
+                if (o_abs(zz) < R(CC_EPS)) zz = R(0);
+                if ((zz + h) <= R(0)) zz = -h;
+                L->z2[c] = zz;
+            } else {
+                L->z2[c] = R(0);
+            }
+        }
+    }
+}
+
 void ocl_mass(ocl_layer *L) {
     /* dispatcher: mass.f90:18-52.  Edge rows: I=2.., J=2.. (mass.f90:70-78) */
     int je = (L->id == 1) ? L->ny - 1 : L->ny;
-    if (L->laycord == 0) {
+    if (L->laygov == 2 || L->laygov == 3) {
+        par_rows(mass_d_rows, L, 2, je);
+    } else if (L->laycord == 0) {
         if (L->laygov == 1) par_rows(conmass_s_rows, L, 2, je);
         else par_rows(mass_s_rows, L, 2, je);
     } else if (L->laygov == 1) {
@@ -794,9 +828,135 @@ static void conmome(ocl_layer *L) {
     free(x.dp1);
 }
 
+/* MOMT_S_D (dispersion.f90:544-838) with MASK = 0: MOMT_S plus the
+ * modified-scheme term when MODSCM = 0 (:686-692, :817-823), and the y wet
+ * test against ZERO (:706) */
+static void momt_s_d_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int nx = L->nx, ny = L->ny;
+    int is0 = (L->id == 1) ? 1 : 2, js0 = is0;
+    const REAL twlvth = R(0.08333333333333);
+    for (int j = js; j <= je; j++) {
+        if (j >= js0) {
+            int jm1 = MAX(j - 1, 1), jp1 = MIN(j + 1, ny);
+            for (int i = is0; i <= nx - 1; i++) {
+                int ip1 = i + 1;
+                size_t c = IDX(L, i, j), cp = IDX(L, ip1, j);
+                if (L->h[c] > R(CC_GX) && L->h[cp] > R(CC_GX)) {
+                    REAL tot_n = L->n1[c] + L->n1[cp] + L->n1[IDX(L, i, jm1)] + L->n1[IDX(L, ip1, jm1)];
+                    REAL xm = L->m1[c] - L->r2[c] * (L->z2[cp] - L->z2[c]) + L->r3[j - 1] * tot_n;
+                    if (L->modscm == 0) {
+                        REAL scm = L->r2[c] * twlvth *
+                                   ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cp] + L->z2[IDX(L, ip1, jm1)]) -
+                                    (L->z2[IDX(L, i, jp1)] - R(2) * L->z2[c] + L->z2[IDX(L, i, jm1)]));
+                        xm = xm - scm;
+                    }
+                    if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                    L->m2[c] = xm;
+                } else {
+                    L->m2[c] = R(0);
+                }
+            }
+        }
+        if (j >= js0 && j <= ny - 1) {
+            int jp1 = j + 1;
+            for (int i = is0; i <= nx; i++) {
+                size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+                if (L->h[c] > R(0) && L->h[cq] > R(0)) {
+                    int im1 = MAX(i - 1, 1), ip1 = MIN(i + 1, nx);
+                    REAL tot_m = L->m1[IDX(L, im1, j)] + L->m1[IDX(L, im1, jp1)] + L->m1[c] + L->m1[cq];
+                    REAL xn = L->n1[c] - L->r4[c] * (L->z2[cq] - L->z2[c]) - L->r5[j - 1] * tot_m;
+                    if (L->modscm == 0) {
+                        REAL scm = L->r4[c] * twlvth *
+                                   ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cq] + L->z2[IDX(L, im1, jp1)]) -
+                                    (L->z2[IDX(L, ip1, j)] - R(2) * L->z2[c] + L->z2[IDX(L, im1, j)]));
+                        xn = xn - scm;
+                    }
+                    if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                    L->n2[c] = xn;
+                } else {
+                    L->n2[c] = R(0);
+                }
+            }
+        }
+    }
+}
+
+/* MOMT_C_D (dispersion.f90:839-1692) with MASK = 0 (:1225-1233, :1560-1568): total face depth
+ * HM = HP + (Z + Z(I+1))/2 (x) and HN = (H + H(J+1) + Z + Z(J+1))/2 (y),
+ * Manning friction, the modified-scheme term when MODSCM = 0; the convection
+ * terms of LAYGOV 3 sit inside the MASK branch and never apply.  A dry face
+ * is not written (the IFs at :922 and :1255 have no ELSE), so it keeps its
+ * level-2 value, which after CHANGE / UPDATE equals level 1. */
+static void momt_c_d_rows(void *ctx, int js, int je) {
+    ocl_layer *L = (ocl_layer *)ctx;
+    int nx = L->nx, ny = L->ny;
+    int is0 = (L->id == 1) ? 1 : 2, js0 = is0;
+    const REAL twlvth = R(0.08333333333333);
+    const REAL konst = R(0.5) * R(L->dt) * R(CC_GRAV);
+    const REAL fm = R(L->fric_coef), grx = R(L->grx), gry = R(L->gry);
+    const REAL mexp = R(CC_MANNEXP);
+    for (int j = js; j <= je; j++) {
+        if (j >= js0) {
+            int jm1 = MAX(j - 1, 1), jp1 = MIN(j + 1, ny);
+            for (int i = is0; i <= nx - 1; i++) {
+                int ip1 = i + 1;
+                size_t c = IDX(L, i, j), cp = IDX(L, ip1, j);
+                if (!(L->h[c] > R(CC_GX) && L->h[cp] > R(CC_GX))) continue;
+                REAL hm = L->hp[c] + R(0.5) * (L->z2[c] + L->z2[cp]);
+                REAL ff = R(0);
+                if (L->fric_switch != 1) {
+                    REAL xqq = R(0.25) * (L->n1[c] + L->n1[cp] + L->n1[IDX(L, i, jm1)] + L->n1[IDX(L, ip1, jm1)]);
+                    if (hm >= R(1.0e-3))
+                        ff = konst * fm * fm * o_sqrt(L->m1[c] * L->m1[c] + xqq * xqq) / o_pow(hm, mexp);
+                }
+                REAL xm = (R(1) - ff) * L->m1[c] - grx * hm * (L->z2[cp] - L->z2[c]);
+                if (L->modscm == 0) {
+                    REAL scm = grx * twlvth * hm *
+                               ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cp] + L->z2[IDX(L, ip1, jm1)]) -
+                                (L->z2[IDX(L, i, jp1)] - R(2) * L->z2[c] + L->z2[IDX(L, i, jm1)]));
+                    xm = xm - scm;
+                }
+                if (L->fric_switch != 1) xm = xm / (R(1) + ff);
+                if (o_abs(xm) < R(CC_EPS)) xm = R(0);
+                L->m2[c] = xm;
+            }
+        }
+        if (j >= js0 && j <= ny - 1) {
+            int jp1 = j + 1;
+            for (int i = is0; i <= nx; i++) {
+                size_t c = IDX(L, i, j), cq = IDX(L, i, jp1);
+                if (!(L->h[c] > R(CC_GX) && L->h[cq] > R(CC_GX))) continue;
+                int im1 = MAX(i - 1, 1), ip1 = MIN(i + 1, nx);
+                REAL hn = R(0.5) * (L->h[c] + L->h[cq] + L->z2[c] + L->z2[cq]);
+                REAL ff = R(0);
+                if (L->fric_switch != 1) {
+                    REAL xpp = R(0.25) * (L->m1[c] + L->m1[cq] + L->m1[IDX(L, im1, j)] + L->m1[IDX(L, im1, jp1)]);
+                    if (hn >= R(1.0e-5))
+                        ff = konst * fm * fm * o_sqrt(L->n1[c] * L->n1[c] + xpp * xpp) / o_pow(hn, mexp);
+                }
+                REAL xn = (R(1) - ff) * L->n1[c] - gry * hn * (L->z2[cq] - L->z2[c]);
+                if (L->modscm == 0) {
+                    REAL scm = gry * twlvth * hn *
+                               ((L->z2[IDX(L, ip1, jp1)] - R(2) * L->z2[cq] + L->z2[IDX(L, im1, jp1)]) -
+                                (L->z2[IDX(L, ip1, j)] - R(2) * L->z2[c] + L->z2[IDX(L, im1, j)]));
+                    xn = xn - scm;
+                }
+                if (L->fric_switch != 1) xn = xn / (R(1) + ff);
+                if (o_abs(xn) < R(CC_EPS)) xn = R(0);
+                L->n2[c] = xn;
+            }
+        }
+    }
+}
+
 void ocl_moment(ocl_layer *L) {
     /* dispatcher moment.f90:21-54 */
     int js = (L->id == 1) ? 1 : 2;
+    if (L->laygov == 2 || L->laygov == 3) {
+        par_rows(L->laycord == 0 ? momt_s_d_rows : momt_c_d_rows, L, js, L->ny);
+        return;
+    }
     if (L->laycord == 0 && L->laygov == 1) conmome(L);
     else if (L->laycord == 0) par_rows(momt_s_rows, L, js, L->ny);
     else if (L->laygov == 1) conmome(L);

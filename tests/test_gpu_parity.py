@@ -164,3 +164,38 @@ def test_nested_sc_option_1_child(oracle_mod, rel_time, fix_top, laygov):
                        (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"), (cn, rc["n"], "child N")):
         _cmp(a, b, what)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
+@pytest.mark.parametrize("laygov", [2, 3])
+def test_dispersion_scheme_outer_layer(oracle_mod, laygov):
+    """MASS_S_D / MOMT_S_D (dispersion.f90:239-356, 544-838) as the reference
+    computes them (its MASK is all zero): the modified-scheme term for
+    LAYGOV 2 on the outer layer (MODSCM 0), the depth-free R2 / R4 of
+    LAYGOV 3 (comcot.f90:776-795); with land"""
+    case = synth.single_layer_case("d", 97, 81, 2.0, 2.0, 0, seed=13, n_seamounts=5, shelf_cols=10, land_cols=4,
+                                   ngauges=0, laygov=laygov, amp=3.0)
+    gpu, _, o, _ = _run_both(case, 80, oracle_mod)
+    ref = o.layer(0)
+    for a, b, what in ((gpu["z"], ref["z"], "eta"), (gpu["mn"][0], ref["m"], "M"), (gpu["mn"][1], ref["n"], "N"),
+                       (gpu["zmax"], ref["zmax"], "zmax")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
+@pytest.mark.parametrize("laygov,laycord,modscm", [(2, 1, 1), (3, 1, 0), (2, 0, 1)])
+def test_dispersion_scheme_child(oracle_mod, laygov, laycord, modscm):
+    """MASS_C_D / MOMT_C_D (dispersion.f90:357-543, 839-1692) and the
+    spherical forms on a child: total face depth, Manning friction, dry faces
+    keeping their flux; MODSCM 0 forced once to cover the modified-scheme term
+    of the Cartesian form"""
+    kw = {"child_laygov": laygov} if laycord == 1 else {"child_laycord": 0, "child_laygov": laygov}
+    case = synth.nested_case("d", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 0, seed=5, rel_time=2, **kw)
+    case.layers[1].modscm = modscm
+    gpu, _, o, _ = _run_both(case, 50, oracle_mod)
+    ref, rc = o.layer(0), o.layer(1)
+    cz, (cm, cn) = gpu["children"][0]
+    assert np.abs(rc["m"]).max() > 0
+    for a, b, what in ((gpu["z"], ref["z"], "parent eta"), (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"),
+                       (cn, rc["n"], "child N")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
