@@ -60,6 +60,9 @@ def load(dtype=np.float32):
     lib.ocl_okada_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     lib.ocl_sponge.argtypes = [C.c_void_p]
+    lib.ocl_edge_sc.argtypes = [C.c_void_p, C.c_void_p]
+    lib.ocl_newq_sc.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.ocl_jnz_sc.argtypes = [C.c_void_p, C.c_void_p]
     lib.ocl_sponge_coef.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]
     lib.ocl_expf.argtypes = [C.c_float]
