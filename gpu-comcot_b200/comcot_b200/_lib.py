@@ -38,7 +38,8 @@ class ChildDesc(C.Structure):
                  ("rel_time", C.c_int)]
                 + [(n, C.c_int) for n in ("laycord", "laygov", "linchk", "modscm", "fric_switch")]
                 + [(n, C.c_float) for n in ("dt", "rx", "ry", "grx", "gry", "fric_coef")]
-                + [(n, P_F) for n in ("h", "hp", "hq", "rows")])
+                + [(n, P_F) for n in ("h", "hp", "hq", "rows", "rows2")]
+                + [("sc_pos", P_I), ("sc_cxy", P_F), ("sc_fix_top", C.c_int), ("parent_modscm", C.c_int)])
 
 
 # name -> (restype, argtypes)

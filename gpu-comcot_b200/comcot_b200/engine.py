@@ -106,6 +106,15 @@ class Engine:
         if Cl.coefs is not None:
             keep.append(np.ascontiguousarray(Cl.coefs.rows(), dtype=F32))
             d.rows = _lib.fptr(keep[-1])
+            if Cl.laycord == 0 and Cl.laygov == 1:
+                keep.append(np.ascontiguousarray(np.stack([Cl.coefs.r0, Cl.coefs.r22]), dtype=F32))
+                d.rows2 = _lib.fptr(keep[-1])
+        if Cl.sc is not None:
+            # SC_OPTION = 1 tables, [ny][nx][2] and [ny][nx][4]
+            keep += [np.ascontiguousarray(Cl.sc.pos, dtype=np.int32), np.ascontiguousarray(Cl.sc.cxy, dtype=F32)]
+            d.sc_pos, d.sc_cxy = _lib.iptr(keep[-2]), _lib.fptr(keep[-1])
+            d.sc_fix_top = 1 if Cl.sc.fix_top else 0
+        d.parent_modscm = P.modscm
         rc = self.lib.gc_engine_add_nested_class(self.h, pcls, C.byref(d))
         if rc == -2:
             raise MemoryError("engine budget exhausted")

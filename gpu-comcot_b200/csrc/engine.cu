@@ -54,6 +54,11 @@ struct EngClass {
     int laycord = 1, laygov = 1, linchk = 1, modscm = 1, fric_switch = 1;
     float dt = 0, rx = 0, ry = 0, grx = 0, gry = 0, fric_coef = 0;
     float *d_ch = nullptr, *d_chp = nullptr, *d_chq = nullptr, *d_crows = nullptr;
+    float *d_crows2 = nullptr; /* [ny][2] R0, R22 of a nonlinear spherical child */
+    /* SC_OPTION = 1 child: position / weight tables */
+    bool has_sc = false;
+    GcScView sc{};
+    void *sc_block = nullptr;
     /* longitude / latitude axes (degrees), for members made from faults */
     float *d_lon = nullptr, *d_lat = nullptr;
 };
@@ -72,6 +77,9 @@ struct EngMember {
     float *cz[2] = {nullptr, nullptr}, *cm[2] = {nullptr, nullptr}, *cn[2] = {nullptr, nullptr};
     float *cdz2 = nullptr, *xflux = nullptr, *yflux = nullptr;
     int *glayer = nullptr;
+    /* SC_OPTION = 1: the outer grid's band forecast of NEWQ_SC (the fused
+     * step has written the outer grid's real level 2 by then) */
+    float *sm2 = nullptr, *sn2 = nullptr;
     float *h = nullptr; /* own depth (members made from faults), else the class's */
     int fty = 16; /* tile height of the outer grid's fused launch */
     /* the last global step this member needs a launch at: single-grid
@@ -127,6 +135,7 @@ GcLayerDev child_view(const EngClass &C, const EngMember &M, int cur) {
     d.z1w = M.cz[cur]; d.m1w = M.cm[cur]; d.n1w = M.cn[cur];
     d.z2 = M.cz[cur ^ 1]; d.m2 = M.cm[cur ^ 1]; d.n2 = M.cn[cur ^ 1];
     d.h = C.d_ch; d.hp = C.d_chp; d.hq = C.d_chq; d.rows = C.d_crows; d.dz2 = M.cdz2;
+    d.rows2 = C.d_crows2;
     return d;
 }
 
@@ -213,24 +222,40 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
      * column 0 alone, which JNZ never reads, so it may precede JNZ. */
     cudaStream_t cs = e->caux[a];
     const GcLayerDev Cv1 = child_view(C, M, cc);
+    /* SC_OPTION = 1: NEWQ_SC's band forecast goes to the member's scratch
+     * fields in place of the outer grid's level 2 */
+    GcLayerDev Pf = P;
+    if (C.has_sc) { Pf.m2 = M.sm2; Pf.n2 = M.sn2; }
     cudaEventRecord(e->ev_cfork[a], s);
     cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
-    gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
+    if (C.has_sc) gc_launch_sc_edges(Pf, Cv1, C.sc, 1, C.rel_time, Cv1.z1, cs);
+    else gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
     gc_launch_mass(Cv1, cs);
     gc_launch_moment(Cv1, cs);
     gc_launch_update_edges(Cv1, cs);
     cudaEventRecord(e->ev_cjoin[a], cs);
     gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
     cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
-    if (nhalf == 1) { gc_launch_jnz(P, Cv1, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
+    auto jnz = [&](const GcLayerDev &Cv) {
+        if (C.has_sc) gc_launch_sc_jnz(P, Cv, C.sc, s);
+        else gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s);
+        e->launches++;
+    };
+    if (nhalf == 1) jnz(Cv1);
     cc ^= 1;
     e->launches += 4;
     for (int t = 2; t <= C.rel_time; t++) {
         const GcLayerDev Cv = child_view(C, M, cc);
-        gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
+        if (C.has_sc) {
+            gc_launch_sc_forecast(Pf, C.sc, s);
+            gc_launch_sc_edges(Pf, Cv, C.sc, t, C.rel_time, Cv.z1, s);
+            e->launches++;
+        } else {
+            gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
+        }
         gc_launch_mass(Cv, s);
         gc_launch_moment(Cv, s);
-        if (t == nhalf) { gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s); e->launches++; }
+        if (t == nhalf) jnz(Cv);
         gc_launch_update_edges(Cv, s);
         cc ^= 1;
         e->launches += 4;
@@ -494,6 +519,7 @@ int gc_engine_destroy(gc_engine *e) {
         if (M.block) cudaFreeAsync(M.block, e->stream);
     for (auto &C : e->classes) {
         if (C.block) cudaFreeAsync(C.block, e->stream);
+        if (C.sc_block) cudaFree(C.sc_block);
         if (C.d_lon) cudaFreeAsync(C.d_lon, e->stream);
     }
     if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
@@ -551,6 +577,7 @@ static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges, bool 
         size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
         bytes += 7 * cfield + a256((size_t)2 * C.nx * sizeof(float)) + a256((size_t)2 * C.ny * sizeof(float))
                  + a256((size_t)ngauges * sizeof(int));
+        if (C.has_sc) bytes += 2 * field;
     }
     return bytes;
 }
@@ -630,6 +657,11 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
         M.xflux = (float *)p; p += a256((size_t)2 * C.nx * sizeof(float));
         M.yflux = (float *)p; p += a256((size_t)2 * C.ny * sizeof(float));
         M.glayer = (int *)p;
+        p += a256((size_t)ngauges * sizeof(int));
+        if (C.has_sc) {
+            M.sm2 = (float *)p; p += field;
+            M.sn2 = (float *)p; p += field;
+        }
         GC_CUDA_OR_RET(cudaMemsetAsync(c0, 0, (size_t)(p - c0), e->stream));
         if (cz0)
             GC_CUDA_OR_RET(cudaMemcpy2DAsync(M.cz[0], (size_t)C.cpitch * sizeof(float), cz0,
@@ -671,6 +703,14 @@ int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int
 int gc_engine_add_nested_member(gc_engine *e, int cls, const float *z0, const float *child_z0, int nsteps,
                                 int ngauges, const int *glayer, const int *gij, const float *gw,
                                 float arrival_thr) {
+    if (e && cls >= 0 && cls < (int)e->classes.size() && e->classes[cls].has_sc && child_z0) {
+        /* at its first sub-step the reference's SC edges test wetness on the
+         * child's level 2, which is still zero (all_grids.f90:1029); the
+         * engine tests level 1, the same once both levels are equal */
+        const EngClass &C = e->classes[cls];
+        for (size_t c = 0; c < (size_t)C.cnx * C.cny; c++)
+            if (child_z0[c] != 0.0f) return GC_ENOTSUP;
+    }
     return eng_add_member(e, cls, z0, child_z0, nsteps, ngauges, glayer, gij, gw, arrival_thr);
 }
 
@@ -705,11 +745,18 @@ int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc
     const int is = d->corners[0], ie = d->corners[1], js = d->corners[2], je = d->corners[3];
     /* the NEWQ forecast reads outer rows JS-3 and columns IS-3
      * (all_grids.f90:692-700,765-772), and the edge fluxes reach IE+2 / JE+2 */
+    const bool sc = d->sc_pos != nullptr;
+    if (sc && (!d->sc_cxy || d->laycord != 1)) return GC_EINVAL;
+    /* an SC_OPTION = 1 child keeps its window's size; its corners are the extent of POS */
+    const bool sized = sc || (d->nx == (ie - is + 1) * d->rel_size + 1 && d->ny == (je - js + 1) * d->rel_size + 1);
     if (d->rel_size < 1 || d->rel_time < 1 || is < 4 || js < 4 || ie > Pc.nx - 2 || je > Pc.ny - 2 || ie < is
-        || je < js || d->nx != (ie - is + 1) * d->rel_size + 1 || d->ny != (je - js + 1) * d->rel_size + 1)
+        || je < js || !sized || d->nx < 3 || d->ny < 3)
         return GC_EINVAL;
-    if ((d->laycord != 0 && d->laycord != 1) || (d->laygov != 0 && d->laygov != 1)) return GC_EINVAL;
-    if (d->laycord == 0 && (d->laygov != 0 || !d->rows)) return GC_ENOTSUP;
+    if ((d->laycord != 0 && d->laycord != 1) || d->laygov < 0 || d->laygov > 3) return GC_EINVAL;
+    /* spherical children need their row coefficients; LAYGOV 3 on a
+     * spherical layer carries R2 / R4 without the depth factor, which only
+     * the reference-ABI path (full R2 / R4 fields) runs */
+    if (d->laycord == 0 && (!d->rows || d->laygov == 3 || (d->laygov == 1 && !d->rows2))) return GC_ENOTSUP;
     if (d->fric_switch != 0 && d->fric_switch != 1) return GC_EINVAL;
     EngClass C = Pc;
     C.block = nullptr;
@@ -724,7 +771,8 @@ int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc
     const size_t cells = (size_t)d->nx * d->ny;
     const size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
     const size_t rb = a256((size_t)GC_ROWW * C.cny * sizeof(float));
-    C.bytes = 3 * cfield + rb;
+    const size_t rb2 = a256((size_t)2 * C.cny * sizeof(float));
+    C.bytes = 3 * cfield + rb + rb2;
     if (e->in_use + (long long)C.bytes > e->budget) return GC_ENOMEM;
     /* HP/HQ from the caller, else PQ_DEPTH (initialization.f90:2501-2526) */
     std::vector<float> hp(cells, 0.0f), hq(cells, 0.0f);
@@ -752,7 +800,8 @@ int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc
     C.d_ch = (float *)p; p += cfield;
     C.d_chp = (float *)p; p += cfield;
     C.d_chq = (float *)p; p += cfield;
-    C.d_crows = (float *)p;
+    C.d_crows = (float *)p; p += rb;
+    C.d_crows2 = (float *)p;
     GC_CUDA_OR_RET(cudaMemsetAsync(blk, 0, C.bytes, e->stream));
     const size_t sp = (size_t)C.cpitch * sizeof(float), hpitch = (size_t)d->nx * sizeof(float);
     GC_CUDA_OR_RET(cudaMemcpy2DAsync(C.d_ch, sp, d->h, hpitch, hpitch, (size_t)d->ny, cudaMemcpyHostToDevice,
@@ -763,7 +812,27 @@ int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc
                                      cudaMemcpyHostToDevice, e->stream));
     GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_crows, rec.data(), rec.size() * sizeof(float), cudaMemcpyHostToDevice,
                                    e->stream));
+    std::vector<float> rec2((size_t)2 * C.cny, 0.0f);
+    if (d->rows2)
+        for (int j = 0; j < C.cny; j++) {
+            rec2[2 * (size_t)j] = d->rows2[j];
+            rec2[2 * (size_t)j + 1] = d->rows2[(size_t)C.cny + j];
+        }
+    GC_CUDA_OR_RET(cudaMemcpyAsync(C.d_crows2, rec2.data(), rec2.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                   e->stream));
     GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream)); /* the host vectors end here */
+    if (sc) {
+        size_t sb = 0;
+        const char *err = gc_sc_tables(d->nx, d->ny, C.cpitch, d->sc_pos, d->sc_cxy, d->corners, Pc.nx, Pc.ny,
+                                       d->rel_size, d->sc_fix_top != 0, d->parent_modscm, &C.sc, &C.sc_block, &sb);
+        if (err || e->in_use + (long long)(C.bytes + sb) > e->budget) {
+            if (C.sc_block) cudaFree(C.sc_block);
+            cudaFreeAsync(C.block, e->stream);
+            return err ? GC_EINVAL : GC_ENOMEM;
+        }
+        C.has_sc = true;
+        C.bytes += sb;
+    }
     e->in_use += (long long)C.bytes;
     e->classes.push_back(C);
     return (int)e->classes.size() - 1;

@@ -122,6 +122,9 @@ struct GcScView {
     int modscm;          /* the parent's MODSCM (0 adds the modified-scheme term) */
     float half;          /* REL_SIZE**2 / 2 */
 };
+const char *gc_sc_tables(int nx, int ny, int cpitch, const int *pos, const float *cxy, const int corners[4],
+                         int pnx, int pny, int rel_size, int fix_top, int modscm, GcScView *out, void **block,
+                         size_t *bytes);
 void gc_launch_sc_edges(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, int t, int rel_time,
                         const float *zwet, cudaStream_t s);
 void gc_launch_sc_forecast(const GcLayerDev &P, const GcScView &sv, cudaStream_t s);

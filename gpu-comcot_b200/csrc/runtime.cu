@@ -302,34 +302,36 @@ void gcomcot_set_sc_tables_(int *id, int *pos, float *cxy, int *nx, int *ny, int
     }
 }
 
-/* device tables of an SC_OPTION = 1 child (see GcScView) */
-static void sc_build(GcLayer &L, const GcLayer &P, const GcPendingParams &pp) {
-    const int nx = L.nx, ny = L.ny;
-    auto fail = [&](const char *what) {
-        fprintf(stderr, "gcomcot: SC tables of layer %d: %s\n", L.id, what);
-        exit(EXIT_FAILURE);
-    };
-    if (pp.sc_pos.size() != (size_t)2 * nx * ny) fail("sized for another layer");
-    auto ki = [&](int i, int j) { return pp.sc_pos[2 * ((size_t)j * nx + i)]; };
-    auto kj = [&](int i, int j) { return pp.sc_pos[2 * ((size_t)j * nx + i) + 1]; };
+} /* extern "C" */
+
+/* device tables of an SC_OPTION = 1 child (see GcScView) from POS / CXY
+ * in [ny][nx][2] and [ny][nx][4] order; returns nullptr when they are
+ * usable, else what is wrong with them */
+const char *gc_sc_tables(int nx, int ny, int cpitch, const int *pos, const float *cxy, const int corners[4],
+                         int pnx, int pny, int rel_size, int fix_top, int modscm, GcScView *out, void **block,
+                         size_t *bytes) {
+    *block = nullptr;
+    auto ki = [&](int i, int j) { return pos[2 * ((size_t)j * nx + i)]; };
+    auto kj = [&](int i, int j) { return pos[2 * ((size_t)j * nx + i) + 1]; };
     /* every node inside the parent with its whole 2x2 stencil */
     for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++)
-            if (ki(i, j) < 1 || kj(i, j) < 1 || ki(i, j) > P.nx - 1 || kj(i, j) > P.ny - 1)
-                fail("a node lies outside the parent's interior");
+            if (ki(i, j) < 1 || kj(i, j) < 1 || ki(i, j) > pnx - 1 || kj(i, j) > pny - 1)
+                return "a node lies outside the parent's interior";
+    const int c0 = corners[0], c1 = corners[1], c2 = corners[2], c3 = corners[3];
+    if (c0 < 1 || c2 < 1 || c1 > pnx || c3 > pny || c1 < c0 || c3 < c2) return "corners outside the parent";
     const int ne = 2 * ny + 2 * nx;
     std::vector<int2> epos(ne);
     std::vector<float4> ew(ne);
     auto put = [&](int k, int i, int j) {
         const size_t c = (size_t)j * nx + i;
         epos[k] = make_int2(ki(i, j), kj(i, j));
-        ew[k] = make_float4(pp.sc_cxy[4 * c], pp.sc_cxy[4 * c + 1], pp.sc_cxy[4 * c + 2], pp.sc_cxy[4 * c + 3]);
+        ew[k] = make_float4(cxy[4 * c], cxy[4 * c + 1], cxy[4 * c + 2], cxy[4 * c + 3]);
     };
     for (int j = 0; j < ny; j++) { put(j, 0, j); put(ny + j, nx - 1, j); }
     for (int i = 0; i < nx; i++) { put(2 * ny + i, i, 0); put(2 * ny + nx + i, i, ny - 1); }
     /* the parent window and, per parent cell, the child nodes in it, child
      * I outermost as JNZ_SC sums them */
-    const int c0 = L.corners[0], c1 = L.corners[1], c2 = L.corners[2], c3 = L.corners[3];
     const int ww = c1 - c0 + 1, wh = c3 - c2 + 1;
     std::vector<int> start((size_t)ww * wh + 1, 0), cell;
     for (int i = 0; i < nx; i++)
@@ -343,49 +345,72 @@ static void sc_build(GcLayer &L, const GcLayer &P, const GcPendingParams &pp) {
     for (int i = 0; i < nx; i++)
         for (int j = 0; j < ny; j++) {
             const int a = ki(i, j), b = kj(i, j);
-            if (a >= c0 && a <= c1 && b >= c2 && b <= c3) cell[fill[(size_t)(b - c2) * ww + (a - c0)]++] = j * L.pitch + i;
+            if (a >= c0 && a <= c1 && b >= c2 && b <= c3) cell[fill[(size_t)(b - c2) * ww + (a - c0)]++] = j * cpitch + i;
         }
     /* forecast bands (all_grids.f90:1131-1134, 1165-1168, 1199-1202, 1233-1236), 0-based */
     GcScView v{};
     auto band = [&](int b, int i0, int i1, int j0, int j1, bool xflux) {
         /* the M band reads column I+1, the N band row J+1 */
-        if (i0 < 1 || j0 < 1 || (xflux ? i1 + 1 > P.nx || j1 > P.ny : i1 > P.nx || j1 + 1 > P.ny))
-            fail("a forecast band reaches past the parent's edge");
+        if (i0 < 1 || j0 < 1 || (xflux ? i1 + 1 > pnx || j1 > pny : i1 > pnx || j1 + 1 > pny)) return false;
         v.band[b][0] = i0 - 1; v.band[b][1] = i1 - 1; v.band[b][2] = j0 - 1; v.band[b][3] = j1 - 1;
+        return true;
     };
     int a = ki(0, 0), b = ki(0, ny - 1);
-    band(0, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
+    bool ok = band(0, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
     a = ki(nx - 1, 0); b = ki(nx - 1, ny - 1);
-    band(1, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
+    ok = ok && band(1, std::min(a, b) - 2, std::max(a, b) + 2, c2 - 2, c3 + 2, true);
     a = kj(0, ny - 1); b = kj(nx - 1, ny - 1);
-    band(2, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
+    ok = ok && band(2, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
     a = kj(0, 0); b = kj(nx - 1, 0);
-    band(3, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
+    ok = ok && band(3, c0 - 2, c1 + 2, std::min(a, b) - 2, std::max(a, b) + 2, false);
+    if (!ok) return "a forecast band reaches past the parent's edge";
     const size_t b_epos = ((size_t)ne * sizeof(int2) + 255) & ~(size_t)255;
     const size_t b_ew = ((size_t)ne * sizeof(float4) + 255) & ~(size_t)255;
     const size_t b_start = (start.size() * sizeof(int) + 255) & ~(size_t)255;
     const size_t b_cell = ((cell.size() + 1) * sizeof(int) + 255) & ~(size_t)255;
     char *blk = nullptr;
-    GC_CUDA_OR_DIE(cudaMalloc((void **)&blk, b_epos + b_ew + b_start + b_cell));
-    L.sc_block = blk;
-    GC_CUDA_OR_DIE(cudaMemcpy(blk, epos.data(), ne * sizeof(int2), cudaMemcpyHostToDevice));
-    GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos, ew.data(), ne * sizeof(float4), cudaMemcpyHostToDevice));
-    GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos + b_ew, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
-    if (!cell.empty())
-        GC_CUDA_OR_DIE(cudaMemcpy(blk + b_epos + b_ew + b_start, cell.data(), cell.size() * sizeof(int),
-                                  cudaMemcpyHostToDevice));
+    if (cudaMalloc((void **)&blk, b_epos + b_ew + b_start + b_cell) != cudaSuccess) return "device allocation failed";
+    bool copied = cudaMemcpy(blk, epos.data(), ne * sizeof(int2), cudaMemcpyHostToDevice) == cudaSuccess
+                  && cudaMemcpy(blk + b_epos, ew.data(), ne * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess
+                  && cudaMemcpy(blk + b_epos + b_ew, start.data(), start.size() * sizeof(int),
+                                cudaMemcpyHostToDevice) == cudaSuccess
+                  && (cell.empty() || cudaMemcpy(blk + b_epos + b_ew + b_start, cell.data(), cell.size() * sizeof(int),
+                                                 cudaMemcpyHostToDevice) == cudaSuccess);
+    if (!copied) {
+        cudaFree(blk);
+        return "device copy failed";
+    }
     v.epos = (const int2 *)blk;
     v.ew = (const float4 *)(blk + b_epos);
     v.start = (const int *)(blk + b_epos + b_ew);
     v.cell = (const int *)(blk + b_epos + b_ew + b_start);
     v.wi0 = c0 - 1; v.wi1 = c1 - 1; v.wj0 = c2 - 1; v.wj1 = c3 - 1;
-    v.fix_top = pp.sc_fix_top;
-    v.modscm = pp.sc_modscm;
-    v.half = (float)(L.rel_size * L.rel_size) / 2.0f;
-    L.sc = v;
+    v.fix_top = fix_top;
+    v.modscm = modscm;
+    v.half = (float)(rel_size * rel_size) / 2.0f;
+    *out = v;
+    *block = blk;
+    if (bytes) *bytes = b_epos + b_ew + b_start + b_cell;
+    return nullptr;
+}
+
+/* device tables of an SC_OPTION = 1 child */
+static void sc_build(GcLayer &L, const GcLayer &P, const GcPendingParams &pp) {
+    if (pp.sc_pos.size() != (size_t)2 * L.nx * L.ny) {
+        fprintf(stderr, "gcomcot: SC tables of layer %d: sized for another layer\n", L.id);
+        exit(EXIT_FAILURE);
+    }
+    const char *err = gc_sc_tables(L.nx, L.ny, L.pitch, pp.sc_pos.data(), pp.sc_cxy.data(), L.corners, P.nx, P.ny,
+                                   L.rel_size, pp.sc_fix_top, pp.sc_modscm, &L.sc, &L.sc_block, nullptr);
+    if (err) {
+        fprintf(stderr, "gcomcot: SC tables of layer %d: %s\n", L.id, err);
+        exit(EXIT_FAILURE);
+    }
     L.has_sc = true;
     L.sc_stepped = false;
 }
+
+extern "C" {
 
 /* GPUcomcot.cu:214-251 */
 void gcomcot_init_layer_(int *layerid, int *parent, int *level, int *rel_size, int *rel_time,

@@ -163,13 +163,21 @@ int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float
 int gc_engine_release(gc_engine *e, int member);
 
 /* A nested grid class: the outer grid of class `parent_cls` with one child
- * layer (ALL_GRID sub-cycle, all_grids.f90:4-312; SC_OPTION = 0 coupling).
+ * layer (ALL_GRID sub-cycle, all_grids.f90:4-312).
  * corners = IS, IE, JS, JE in the outer grid (1-based, at least 4 cells from
  * its edge); nx = (IE-IS+1)*rel_size+1, ny likewise.  laycord/laygov select
  * the child's solver: (1,1) CONMASS/CONMOME with wet/dry and Manning
- * friction, (1,0) MASS_C/MOMT_C, (0,0) MASS_S/MOMT_S (then `rows` is the
- * child's [7][ny] block).  hp/hq may be NULL (then PQ_DEPTH of h).  Members
- * of a nested class step with the per-phase kernels. */
+ * friction, (1,0) MASS_C/MOMT_C, (1,2|3) MASS_C_D/MOMT_C_D, (0,0)
+ * MASS_S/MOMT_S, (0,1) CONMASS_S/CONMOME_S, (0,2) MASS_S_D/MOMT_S_D; a
+ * spherical child needs `rows`, its [7][ny] block (R1, R11, R6, R3, R5, R2
+ * and R4 per row), and a nonlinear spherical one also `rows2`, [2][ny]
+ * (R0, R22 per row).  hp/hq may be NULL (then PQ_DEPTH of h).
+ * SC_OPTION = 1 (a Cartesian child coupled through the UTM tables,
+ * all_grids.f90:996-1425): sc_pos [ny][nx][2] 1-based (KI, KJ) and sc_cxy
+ * [ny][nx][4] as SUBGRID_MATCHING builds them, corners their extent (nx, ny
+ * then need not follow the corners), sc_fix_top and parent_modscm as in
+ * gcomcot_set_sc_tables_; members of such a class start from a flat child
+ * surface.  Members of a nested class step with the per-phase kernels. */
 typedef struct {
     int nx, ny;
     int corners[4];
@@ -177,6 +185,10 @@ typedef struct {
     int laycord, laygov, linchk, modscm, fric_switch;
     float dt, rx, ry, grx, gry, fric_coef;
     const float *h, *hp, *hq, *rows;
+    const float *rows2;
+    const int *sc_pos;
+    const float *sc_cxy;
+    int sc_fix_top, parent_modscm;
 } gc_child_desc;
 int gc_engine_add_nested_class(gc_engine *e, int parent_cls, const gc_child_desc *child);
 /* a member of a nested class: child_z0 may be NULL (still water); gauge g

@@ -174,3 +174,37 @@ def test_members_joining_mid_run(oracle_mod):
             assert np.array_equal(g[k].view(np.uint32), ref[k].view(np.uint32)), (cs.root.nx, k)
         assert np.array_equal(g["arrival"], ref["arrival"])
         assert np.array_equal(g["ts"].view(np.uint32), ts.view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["sc_option_1", "dispersion_cartesian", "nonlinear_spherical", "dispersion_spherical"])
+def test_engine_nested_child_kinds_match_oracle(oracle_mod, kind):
+    """nested engine members whose child is coupled by SC_OPTION = 1 (UTM
+    tables, band forecast in member scratch), or runs MASS_C_D/MOMT_C_D,
+    CONMASS_S/CONMOME_S or MASS_S_D/MOMT_S_D: bitwise equal to the oracle,
+    with graphs, rel_time 2"""
+    if kind == "sc_option_1":
+        case = synth.nested_sc_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=3, rel_time=2)
+    elif kind == "dispersion_cartesian":
+        case = synth.nested_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=5, rel_time=2, child_laygov=2)
+    elif kind == "nonlinear_spherical":
+        case = synth.nested_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=5, rel_time=2,
+                                 child_laycord=0, child_laygov=1)
+    else:
+        case = synth.nested_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=5, rel_time=2,
+                                 child_laycord=0, child_laygov=2)
+    case.gauges = case.gauges[:3]
+    with Engine(budget=2 << 30) as eng:
+        eng.config(variant=-1, use_graphs=1, chunk=8)
+        mid = eng.add(case)
+        eng.step(45)
+        eng.sync()
+        assert eng.done(mid)
+        got = eng.read(mid)
+    o = oracle_mod.OracleRun(case)
+    o.run(case.nsteps)
+    ref, rc = o.layer(0), o.layer(1)
+    assert np.abs(rc["m"]).max() > 0
+    for k in ("z", "m", "n", "zmax"):
+        assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), k
+    for k in ("z", "m", "n"):
+        assert np.array_equal(got["child_" + k].view(np.uint32), rc[k].view(np.uint32)), "child " + k
