@@ -198,13 +198,15 @@ def run_c4(args, torch, dist, rank, world, local):
     case = Case("C4", [L], run_steps)
     tune_reps = 2
     from comcot_b200 import _lib
-    ncand = 2 * _lib.load().gc_engine_num_variants()  # tile variants x tile-height rules
+    ncand = _lib.load().gc_engine_num_candidates()  # tile variants x tile-height rules
     extra = ncand * (tune_reps + 1) + args.warmup  # the autotuner's steps
     eng = Engine(budget=120 << 30)
     eng.config(variant=args.variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
     ids = [eng.add(case, z0=z, cls=cls, nsteps=run_steps + extra, gauges=[], arrival_thr=0.05) for z in srcs]
-    variant = eng.autotune(tune_reps) if args.variant < 0 else args.variant
+    if args.variant < 0:
+        eng.autotune(tune_reps)
+    variant = eng.variant()  # variant + variants x tile-height rule
     eng.step(args.warmup)
     eng.prepare()  # step-chunk graph built before the timed region
     eng.sync()
@@ -407,10 +409,12 @@ def run_c5(args, torch, dist, rank, world, local):
     variant = args.variant
     if variant < 0:
         big = [r for r in reqs if r.case.root.nx == 1921 and len(r.case.layers) == 1][:4]
+        from comcot_b200 import _lib
         with Engine(budget=16 << 30) as eng:
             for r in big:
-                eng.add(r.case, nsteps=200)
-            variant = eng.autotune(2)
+                eng.add(r.case, nsteps=3 * _lib.load().gc_engine_num_candidates() + 8)
+            eng.autotune(2)
+            variant = eng.variant()  # variant + variants x tile-height rule
     budget = int(args.budget_gb * (1 << 30))
     # warm-up: a few requests through the server (module load, first graphs)
     with serving.ForecastServer(budget, chunk=args.chunk, variant=variant) as srv:
@@ -569,7 +573,7 @@ def run_single(args, torch, dist, rank, world, local):
     from comcot_b200 import _lib
 
     lib = _lib.load()
-    ncand = 2 * lib.gc_engine_num_variants()  # the autotuner's candidates: tile variants x tile-height rules
+    ncand = lib.gc_engine_num_candidates()  # the autotuner's candidates: tile variants x tile-height rules
     total = ncand * (tune_reps + 1) + args.warmup + args.steps + 8
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)
@@ -579,7 +583,9 @@ def run_single(args, torch, dist, rank, world, local):
     eng = Engine(budget=8 << 30)
     eng.config(variant=args.variant, use_graphs=1, chunk=64)
     eng.add(case)
-    variant = eng.autotune(tune_reps) if args.variant < 0 else args.variant
+    if args.variant < 0:
+        eng.autotune(tune_reps)
+    variant = eng.variant()  # variant + variants x tile-height rule
     eng.step(args.warmup)
     eng.prepare()  # step-chunk graph built before the timed region
     eng.sync()

@@ -95,6 +95,7 @@ SIGNATURES = {
     "gc_engine_autotune": (C.c_int, [VP, C.c_int]),
     "gc_engine_variant": (C.c_int, [VP]),
     "gc_engine_num_variants": (C.c_int, []),
+    "gc_engine_num_candidates": (C.c_int, []),
     "gc_engine_prepare": (C.c_int, [C.c_void_p]),
     "gc_engine_launches": (C.c_longlong, [VP]),
     "gc_engine_stream": (VP, [VP]),

@@ -1004,6 +1004,7 @@ int gc_engine_prepare(gc_engine *e) {
 
 int gc_engine_variant(gc_engine *e) { return e ? e->variant + gc_fused_num_variants() * e->ty_rule : GC_EINVAL; }
 int gc_engine_num_variants(void) { return gc_fused_num_variants(); }
+int gc_engine_num_candidates(void) { return gc_fused_num_variants() * GC_TY_RULES; }
 
 void *gc_engine_stream(gc_engine *e) { return e ? (void *)e->stream : nullptr; }
 long long gc_engine_launches(gc_engine *e) { return e ? e->launches : GC_EINVAL; }

@@ -223,6 +223,8 @@ int gc_engine_prepare(gc_engine *e);
 int gc_engine_variant(gc_engine *e);
 /* number of compiled tile variants (all compute identical results) */
 int gc_engine_num_variants(void);
+/* candidates gc_engine_autotune times, one step set each: variants x tile-height rules */
+int gc_engine_num_candidates(void);
 long long gc_engine_launches(gc_engine *e);
 /* the cudaStream_t the engine issues its kernels on */
 void *gc_engine_stream(gc_engine *e);
