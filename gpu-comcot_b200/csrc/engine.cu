@@ -146,7 +146,7 @@ struct gc_engine {
     cudaStream_t stream = nullptr;
     std::vector<EngClass> classes;
     std::vector<EngMember> members;
-    int variant = 15; /* until tuned: the fastest single-grid variant on B200 */
+    int variant = 16; /* until tuned: the fastest single-grid variant on B200 */
     bool tuned = false;
     int use_graphs = 1, chunk = 32;
     int gstep = 0; /* steps issued */

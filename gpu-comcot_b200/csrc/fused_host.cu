@@ -12,9 +12,9 @@ static int g_variant = -1;
 int gc_default_variant() {
     if (g_variant >= 0) return g_variant;
     const char *v = getenv("GCOMCOT_FUSED_VARIANT");
-    /* 15: 4 warps x 4 stages, one copy issuer, Z1/max-eta in registers (the
-     * fastest on the 2401x2001 single grid on B200) */
-    g_variant = v ? atoi(v) : 15;
+    /* 16: 4 warps x 3 stages, N of row r-2 carried in registers, 20 warps
+     * per SM (the fastest on the 2401x2001 single grid on B200) */
+    g_variant = v ? atoi(v) : 16;
     if (g_variant < 0 || g_variant >= gc_fused_num_variants()) g_variant = 0;
     return g_variant;
 }
@@ -39,7 +39,8 @@ bool gc_fused_step(GcLayer &L, bool maxamp, bool arrival, int step, float thr, i
     int v = gc_default_variant();
     static int cached_nx = -1, cached_ny = -1, cached_v = -1, cached_ty = 16;
     if (cached_nx != L.nx || cached_ny != L.ny || cached_v != v) {
-        cached_ty = gc_fused_pick_ty(v, 1, &L.nx, &L.ny);
+        /* the single-grid kernel; rule 1 (fewest rows for the busiest warp) */
+        cached_ty = gc_fused_pick_ty(v, 1, &L.nx, &L.ny, 1, false);
         cached_nx = L.nx; cached_ny = L.ny; cached_v = v;
     }
     g.ty = cached_ty;

@@ -18,7 +18,10 @@
  * r the warp computes the new surface Z2 of row r (plus the east halo
  * column, kept in a two-row shared ring), then the momentum of row r-1,
  * which needs Z2 of rows r-1 and r; the copies for row r+S-2 are issued as
- * soon as row r-2's stage is free.  There is no block barrier: warps of a
+ * soon as row r-2's stage is free (flag FL_NC: the momentum's N of row r-2
+ * rides in registers, so row r-1's stage is refilled, with row r+S-1, right
+ * after row r; three stages then keep a row in flight, and the smaller ring
+ * lets 20 warps share an SM).  There is no block barrier: warps of a
  * CTA work on independent tiles.  The halo row/column of Z2 is recomputed by
  * both neighbouring tiles from the same inputs, bit-identically.
  *
@@ -158,6 +161,11 @@ constexpr int WAIT_LIMIT = 1 << 22;
  * one row ahead into registers (the stage then holds M, N, H and the row
  * record only, 40 % less shared memory, so more warps fit on an SM). */
 constexpr int FL_ONE = 1, FL_ZD = 2;
+/* FL_NC: the momentum's N of row j-1 is carried from the previous row in
+ * five registers per lane instead of read from that row's stage, so a stage
+ * is free (and refilled) one row earlier: a 3-stage ring keeps one row in
+ * flight, and its smaller footprint lets more warps share an SM. */
+constexpr int FL_NC = 4;
 
 /* one pipeline stage holds one grid row of a warp tile (byte offsets) */
 template <int FL>
@@ -199,6 +207,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     using ST = Stage<FL>;
     constexpr bool ZD = (FL & FL_ZD) != 0;
     constexpr bool ONE = (FL & FL_ONE) != 0;
+    constexpr bool NC = (FL & FL_NC) != 0;
     constexpr int SB_ = ST::BYTES;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -363,6 +372,8 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     const int wi0 = Gref.wi0, wi1 = Gref.wi1, wj0 = Gref.wj0, wj1 = Gref.wj1;
     const bool inwin = Gref.has_win && i0 <= wi1 && i0 + TXW - 1 >= wi0 && j0 <= wj1 && j0 + TY - 1 >= wj0;
     const bool edge = inwin || !(i0 >= 1 && i0 + TXW <= nx - 2 && j0 >= 1 && j0 + TY <= ny - 2);
+    /* FL_NC: N of rows r-1 (this row's stage B) and r-2 (carried) at columns c0..c0+4 */
+    float nbk[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, nck[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     for (int k = 1; k <= TY + 1 && ok; k++) {
         const int r = j0 + k - 1;
         const bool rv = k < K;
@@ -381,6 +392,11 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
             if (i0 == 0 && lane == 0) SA[ST::M / 4 + 3] = SA[ST::M / 4 + 4]; /* IM1 = max(I-1,1) */
         }
         __syncwarp();
+        if constexpr (NC) {
+            const float *nBr = SB + ST::N / 4;
+            const float4 t = lds4(nBr + c0);
+            nbk[0] = t.x; nbk[1] = t.y; nbk[2] = t.z; nbk[3] = t.w; nbk[4] = nBr[c0 + 4];
+        }
         float *zA = zr + (k & 1) * ZR_FLOATS, *zB = zr + ((k - 1) & 1) * ZR_FLOATS;
         auto body = [&](auto edge_tag) {
             constexpr bool EDGE = decltype(edge_tag)::value;
@@ -473,7 +489,6 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
             const int j = r - 1;
             if (k >= 2 && j < ny && own) {
                 const float *mB = SB + ST::M / 4 + 4, *mA = SA + ST::M / 4 + 4;
-                const float *nB = SB + ST::N / 4, *nC = SC + ST::N / 4;
                 const float *hB = SB + ST::H / 4, *hA = SA + ST::H / 4;
                 float cx = 0.0f, cy = 0.0f;
                 if constexpr (!XR24) { cx = SB[ST::C / 4 + GC_CX]; cy = SB[ST::C / 4 + GC_CY]; }
@@ -483,8 +498,14 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                 {
                     float4 t;
                     t = lds4(hB + c0); hb[0] = t.x; hb[1] = t.y; hb[2] = t.z; hb[3] = t.w; hb[4] = hB[c0 + 4];
-                    t = lds4(nB + c0); nb[0] = t.x; nb[1] = t.y; nb[2] = t.z; nb[3] = t.w; nb[4] = nB[c0 + 4];
-                    t = lds4(nC + c0); nc[0] = t.x; nc[1] = t.y; nc[2] = t.z; nc[3] = t.w; nc[4] = nC[c0 + 4];
+                    if constexpr (NC) {
+#pragma unroll
+                        for (int q = 0; q < 5; q++) { nb[q] = nbk[q]; nc[q] = nck[q]; }
+                    } else {
+                        const float *nB = SB + ST::N / 4, *nC = SC + ST::N / 4;
+                        t = lds4(nB + c0); nb[0] = t.x; nb[1] = t.y; nb[2] = t.z; nb[3] = t.w; nb[4] = nB[c0 + 4];
+                        t = lds4(nC + c0); nc[0] = t.x; nc[1] = t.y; nc[2] = t.z; nc[3] = t.w; nc[4] = nC[c0 + 4];
+                    }
                     t = lds4(zB + c0); zb[0] = t.x; zb[1] = t.y; zb[2] = t.z; zb[3] = t.w; zb[4] = zB[c0 + 4];
                     t = lds4(mB + c0); mb[0] = mB[c0 - 1]; mb[1] = t.x; mb[2] = t.y; mb[3] = t.z; mb[4] = t.w;
                     t = lds4(mA + c0); ma[0] = mA[c0 - 1]; ma[1] = t.x; ma[2] = t.y; ma[3] = t.z; ma[4] = t.w;
@@ -535,8 +556,15 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
         zxp += P;
         if (k >= 2) { m2p += P; n2p += P; }
         __syncwarp();
-        /* row k-2 is no longer needed: refill its stage S rows ahead */
-        if (k >= 2 && k - 2 + S < K) issue(k - 2 + S, stC);
+        if constexpr (NC) {
+            /* row k-1 is no longer needed (its N rides on in registers) */
+#pragma unroll
+            for (int q = 0; q < 5; q++) nck[q] = nbk[q];
+            if (k - 1 + S < K) issue(k - 1 + S, stB);
+        } else {
+            /* row k-2 is no longer needed: refill its stage S rows ahead */
+            if (k >= 2 && k - 2 + S < K) issue(k - 2 + S, stC);
+        }
         stC = stB; stB = stA; parB = parA;
     }
     seq = seq0 + K;
@@ -601,17 +629,18 @@ const Variant kVariants[] = {
     GC_VARIANT(4, 6, FL_ONE), GC_VARIANT(8, 4, FL_ONE),
     GC_VARIANT(4, 6, FL_ZD), GC_VARIANT(8, 4, FL_ZD), GC_VARIANT(4, 4, FL_ZD),
     GC_VARIANT(4, 6, FL_ONE | FL_ZD), GC_VARIANT(8, 4, FL_ONE | FL_ZD), GC_VARIANT(4, 4, FL_ONE | FL_ZD),
+    GC_VARIANT(4, 3, FL_NC), GC_VARIANT(2, 3, FL_NC), GC_VARIANT(4, 4, FL_NC),
 };
 #undef GC_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 int variant_smem(const Variant &v) {
-    return v.w * ((v.fl & FL_ZD) ? (v.fl & FL_ONE ? warp_smem_bytes<FL_ONE | FL_ZD>(v.s) : warp_smem_bytes<FL_ZD>(v.s))
-                                 : (v.fl & FL_ONE ? warp_smem_bytes<FL_ONE>(v.s) : warp_smem_bytes<0>(v.s)));
+    /* the stage layout depends on FL_ZD alone */
+    return v.w * ((v.fl & FL_ZD) ? warp_smem_bytes<FL_ZD>(v.s) : warp_smem_bytes<0>(v.s));
 }
 
 void prepare(const Variant &v) {
-    static bool done[32] = {false};
+    static bool done[64] = {false};
     int idx = (int)(&v - kVariants);
     if (done[idx]) return;
     cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
