@@ -231,8 +231,16 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     if (C.has_sc) gc_launch_sc_edges(Pf, Cv1, C.sc, 1, C.rel_time, Cv1.z1, cs);
     else gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
     gc_launch_mass(Cv1, cs);
-    gc_launch_moment(Cv1, cs);
-    gc_launch_update_edges(Cv1, cs);
+    /* JNZ_SC sums every child node inside the parent window, row and column
+     * 0 included, so in the sub-step that feeds back UPDATE's edge copy
+     * follows it (all_grids.f90 order: MOMENT, JNZ, UPDATE) */
+    const bool late_update1 = C.has_sc && nhalf == 1;
+    if (late_update1) {
+        gc_launch_moment(Cv1, cs);
+        e->launches += 3;
+    } else {
+        e->launches += 2 + gc_launch_moment_update(Cv1, cs);
+    }
     cudaEventRecord(e->ev_cjoin[a], cs);
     gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
     cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
@@ -242,8 +250,11 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
         e->launches++;
     };
     if (nhalf == 1) jnz(Cv1);
+    if (late_update1) {
+        gc_launch_update_edges(Cv1, s);
+        e->launches++;
+    }
     cc ^= 1;
-    e->launches += 4;
     for (int t = 2; t <= C.rel_time; t++) {
         const GcLayerDev Cv = child_view(C, M, cc);
         if (C.has_sc) {
@@ -254,11 +265,19 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
             gc_launch_edges(P, Cv, C.rel_size, C.rel_time, C.corners, t, s);
         }
         gc_launch_mass(Cv, s);
-        gc_launch_moment(Cv, s);
-        if (t == nhalf) jnz(Cv);
-        gc_launch_update_edges(Cv, s);
+        if (C.has_sc && t == nhalf) {
+            gc_launch_moment(Cv, s);
+            jnz(Cv);
+            gc_launch_update_edges(Cv, s);
+            e->launches += 4;
+        } else {
+            /* UPDATE's edge copy writes the child's row and column 0 alone,
+             * which JNZ never reads (its blocks start at child index 1), so
+             * it may precede JNZ */
+            e->launches += 2 + gc_launch_moment_update(Cv, s);
+            if (t == nhalf) jnz(Cv);
+        }
         cc ^= 1;
-        e->launches += 4;
     }
     /* the window's momentum (which the surface JNZ wrote changes) and its
      * max-eta / arrival / gauges, side by side; both read the final surface,

@@ -103,6 +103,9 @@ void gc_launch_moment(const GcLayerDev &L, cudaStream_t s);
 /* linear spherical momentum over the 0-based cells [i0,i1] x [j0,j1] only */
 void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1, cudaStream_t s);
 void gc_launch_update_edges(const GcLayerDev &L, cudaStream_t s);
+/* a child's momentum followed by UPDATE's edge copy; the copy rides in the
+ * momentum launch where that is safe.  Returns the launches issued. */
+int gc_launch_moment_update(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                      const int *corners, int t, cudaStream_t s);
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,

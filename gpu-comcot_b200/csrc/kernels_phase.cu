@@ -396,38 +396,25 @@ __global__ void k_momt_c(GcLayerDev L) {
 /* WAVE_BREAKING (moment.f90:1272-1384).  DZ(:,:,1) is identically    */
 /* zero in the reference, so DP1 = 0.25*(DZ2(I)+DZ2(I+1)) etc.         */
 /* ---------------------------------------------------------------- */
-struct NlView {
-    const float *dz;
-    int nx, ny, P;
-    __device__ __forceinline__ float d(int i, int j) const { return dz[(size_t)j * P + i]; }
-    __device__ __forceinline__ float dp1(int i, int j) const {
-        int ip1 = i + 1 < nx ? i + 1 : nx - 1;
-        float v = 0.25f * (d(i, j) + 0.0f + d(ip1, j) + 0.0f);
-        return v < CC_GX ? 0.0f : v;
-    }
-    __device__ __forceinline__ float dp2(int i, int j) const {
-        int ip1 = i + 1 < nx ? i + 1 : nx - 1;
-        float v = 0.50f * (d(i, j) + d(ip1, j));
-        return v < CC_GX ? 0.0f : v;
-    }
-    __device__ __forceinline__ float dq1(int i, int j) const {
-        int jp1 = j + 1 < ny ? j + 1 : ny - 1;
-        float v = 0.25f * (d(i, j) + 0.0f + d(i, jp1) + 0.0f);
-        return v < CC_GX ? 0.0f : v;
-    }
-    __device__ __forceinline__ float dq2(int i, int j) const {
-        int jp1 = j + 1 < ny ? j + 1 : ny - 1;
-        float v = 0.50f * (d(i, j) + d(i, jp1));
-        return v < CC_GX ? 0.0f : v;
-    }
-};
+/* face depths from two total depths (moment.f90:345-366): the x form
+ * DP1/DP2 of cells (I,J),(I+1,J), the y form DQ1/DQ2 of (I,J),(I,J+1) */
+__device__ __forceinline__ float face1(float a, float b) {
+    float v = 0.25f * (a + 0.0f + b + 0.0f);
+    return v < CC_GX ? 0.0f : v;
+}
+__device__ __forceinline__ float face2(float a, float b) {
+    float v = 0.50f * (a + b);
+    return v < CC_GX ? 0.0f : v;
+}
 
-__device__ __forceinline__ void wave_breaking(const GcLayerDev &L, size_t c, float &advx,
+/* WAVE_BREAKING (moment.f90:1302-1335) on one cell's total depth, new and
+ * old surface */
+__device__ __forceinline__ void wave_breaking(float dz2c, float z2c, float z1c, float dt, float &advx,
                                               float &advy) {
-    float cc = sqrtf(CC_GRAV * L.dz2[c]);
+    float cc = sqrtf(CC_GRAV * dz2c);
     float dzdt_f = CC_BRK_F * cc;
     float dzdt_i = CC_BRK_I * cc;
-    float dzdt = fabs_(L.z2[c] - L.z1[c]) / L.dt;
+    float dzdt = fabs_(z2c - z1c) / dt;
     if (dzdt > dzdt_f) {
         float ref = (dzdt - dzdt_f) / (dzdt_i - dzdt_f);
         float coef = cc_expf(-(1.0f * ref));
@@ -441,17 +428,37 @@ __device__ __forceinline__ void wave_breaking(const GcLayerDev &L, size_t c, flo
  * HP + (Z + Z(I+1))/2, the pressure coefficient R2 / R4 of its row, Coriolis
  * +4 R3 XQQ / -4 R5 XPP, advection coefficients R21 (= R1) / R0 / R22 per
  * row, and applies the y friction to XQ (the Cartesian routine subtracts it
- * from XP, moment.f90:672). */
+ * from XP, moment.f90:672).
+ *
+ * Every value a face can need (its stencil reaches two cells back along the
+ * face normal's neighbour axis and one cell forward) is loaded first, as
+ * one batch of independent loads at clamped, in-bounds indices; the
+ * branches then run on registers.  Clamped indices coincide with the
+ * reference's wherever a value is used: the two-back neighbours are read
+ * only inside the advection span, whose cells are at least 10 from every
+ * edge. */
 template <bool SPH>
-__global__ void k_conmome(GcLayerDev L) {
+__global__ void k_conmome(GcLayerDev L, int upd) {
     pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
     int j = blockIdx.y * BY + threadIdx.y;
     if (i >= L.nx || j >= L.ny) return;
     const int P = L.pitch, ix = L.nx, jy = L.ny;
     const size_t c = (size_t)j * P + i;
-    const NlView D{L.dz2, ix, jy, P};
-    const float *z = L.z2, *hz = L.h, *p = L.m1, *q = L.n1;
+    /* upd: UPDATE's edge copy of a child (all_grids.f90:323-324), done here
+     * by the threads of row and column 0, which compute no face.  The host
+     * sets it only where no face reads the surface on row or column 0 (a
+     * child without the MODSCM term), and the copy reads rows and columns
+     * >= 1, which nothing in this launch writes. */
+    if (upd && blockIdx.z == 0) {
+        if (j == 0) L.z2[i] = L.z2[(size_t)P + (i == 0 ? 1 : i)];
+        else if (i == 0) L.z2[c] = L.z2[c + 1];
+    }
+    const float *__restrict__ z = L.z2;
+    const float *__restrict__ hz = L.h;
+    const float *__restrict__ p = L.m1;
+    const float *__restrict__ q = L.n1;
+    const float *__restrict__ dz = L.dz2;
     const float konst = (L.fric_switch != 1) ? 0.5f * L.dt * CC_GRAV : 0.0f;
     const float fm = L.fric_coef;
     /* Fortran spans: I > 10 .AND. I < IX-10 with I = i+1 */
@@ -459,26 +466,40 @@ __global__ void k_conmome(GcLayerDev L) {
                       && (j + 1 < jy - CC_SPAN);
     const int im1 = i > 0 ? i - 1 : 0, ip1 = i + 1 < ix ? i + 1 : ix - 1;
     const int jm1 = j > 0 ? j - 1 : 0, jp1 = j + 1 < jy ? j + 1 : jy - 1;
-#define AT(a, ii, jj) (a)[(size_t)(jj) * P + (ii)]
+    const size_t rj = (size_t)j * P, rjm = (size_t)jm1 * P, rjp = (size_t)jp1 * P;
+#define AT(a, ii, jj) __ldg((a) + (size_t)(jj) * P + (ii))
 
     /* ---------------- x direction (blockIdx.z = 0) ---------------- */
     if (blockIdx.z == 0) {
         bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
         float out = 0.0f;
         if (inx) {
-            size_t cp = (size_t)j * P + ip1;
+            const size_t cp = rj + ip1;
+            const int ip2 = i + 2 < ix ? i + 2 : ix - 1;
+            const size_t rjm2 = (size_t)(j >= 2 ? j - 2 : 0) * P;
+            const float h_c = __ldg(hz + c), h_p = __ldg(hz + cp), hp_c = __ldg(L.hp + c);
+            const float d_c = __ldg(dz + c), d_p = __ldg(dz + cp), d_p2 = __ldg(dz + rj + ip2);
+            const float d_m = __ldg(dz + rj + im1);
+            const float d_cn = __ldg(dz + rjp + i), d_pn = __ldg(dz + rjp + ip1);
+            const float d_cs = __ldg(dz + rjm + i), d_ps = __ldg(dz + rjm + ip1);
+            const float z_c = __ldg(z + c), z_p = __ldg(z + cp), z1_c = __ldg(L.z1 + c);
+            const float q_c = __ldg(q + c), q_p = __ldg(q + cp);
+            const float q_cs = __ldg(q + rjm + i), q_ps = __ldg(q + rjm + ip1);
+            const float q_cn = __ldg(q + rjp + i), q_pn = __ldg(q + rjp + ip1);
+            const float q_cs2 = __ldg(q + rjm2 + i), q_ps2 = __ldg(q + rjm2 + ip1);
+            const float p_c = __ldg(p + c), p_p = __ldg(p + cp), p_m = __ldg(p + rj + im1);
+            const float p_n = __ldg(p + rjp + i), p_s = __ldg(p + rjm + i);
             float dd = 0.0f, df = 0.0f, ff;
             bool noflux = false;
-            if (hz[c] <= CC_ELMAX || L.hp[c] <= CC_ELMAX) {
+            if (h_c <= CC_ELMAX || hp_c <= CC_ELMAX) {
                 noflux = true;
             } else {
-                float dzc = D.d(i, j), dzp = D.d(ip1, j);
-                if (dzc > CC_GX && dzp > CC_GX) {
-                    dd = D.dp2(i, j); df = D.dp1(i, j);
-                } else if (dzc > CC_GX && dzp <= CC_GX && hz[cp] + z[c] > CC_GX) {
-                    dd = SPH ? L.hp[c] + 0.5f * (z[c] + z[cp]) : 0.5f * dzc; df = dd;
-                } else if (dzc <= CC_GX && dzp > CC_GX && hz[c] + z[cp] > CC_GX) {
-                    dd = SPH ? L.hp[c] + 0.5f * (z[c] + z[cp]) : 0.5f * dzp; df = dd;
+                if (d_c > CC_GX && d_p > CC_GX) {
+                    dd = face2(d_c, d_p); df = face1(d_c, d_p);
+                } else if (d_c > CC_GX && d_p <= CC_GX && h_p + z_c > CC_GX) {
+                    dd = SPH ? hp_c + 0.5f * (z_c + z_p) : 0.5f * d_c; df = dd;
+                } else if (d_c <= CC_GX && d_p > CC_GX && h_c + z_p > CC_GX) {
+                    dd = SPH ? hp_c + 0.5f * (z_c + z_p) : 0.5f * d_p; df = dd;
                 } else {
                     noflux = true;
                 }
@@ -486,61 +507,59 @@ __global__ void k_conmome(GcLayerDev L) {
             }
             if (!noflux) {
                 if (df < CC_DFMIN) df = CC_DFMIN;
-                float xqq = 0.25f * (q[c] + q[cp] + AT(q, i, jm1) + AT(q, ip1, jm1));
+                float xqq = 0.25f * (q_c + q_p + q_cs + q_ps);
                 if (L.fric_switch != 1)
-                    ff = konst * fm * fm * sqrtf(p[c] * p[c] + xqq * xqq) / cc_powf(df, CC_MANNEXP);
+                    ff = konst * fm * fm * sqrtf(p_c * p_c + xqq * xqq) / cc_powf(df, CC_MANNEXP);
                 else
                     ff = 0.0f;
                 const float cpx = SPH ? GC_ROW(L, GC_CX, j) : L.grx;
-                float xp = p[c] - cpx * dd * (z[cp] - z[c]);
+                float xp = p_c - cpx * dd * (z_p - z_c);
                 if (L.modscm == 0 && j + 1 < jy) {
                     float scm = cpx * dd / 12.0f
-                                * ((AT(z, ip1, jp1) - 2.0f * z[cp] + AT(z, ip1, jm1))
-                                   - (AT(z, i, jp1) - 2.0f * z[c] + AT(z, i, jm1)));
+                                * ((AT(z, ip1, jp1) - 2.0f * z_p + AT(z, ip1, jm1))
+                                   - (AT(z, i, jp1) - 2.0f * z_c + AT(z, i, jm1)));
                     xp = xp - scm;
                 }
-                if (L.fric_switch != 1) xp = xp - ff * p[c];
+                if (L.fric_switch != 1) xp = xp - ff * p_c;
                 if (SPH) xp = xp + 4.0f * GC_ROW(L, GC_R3, j) * xqq;
                 const float ax = SPH ? GC_ROW(L, GC_R1, j) : L.rx;   /* R21 = R1 */
                 const float ay = SPH ? L.rows2[2 * (size_t)j] : L.ry;   /* R0 */
-                float dp1c = D.dp1(i, j);
+                float dp1c = face1(d_c, d_p);
                 if (L.linchk == 1 && dp1c >= CC_GX && span) {
                     float advx, advy;
-                    if (p[c] < 0.0f) {
-                        float dp1p = D.dp1(ip1, j);
-                        if (dp1p < CC_GX || D.d(ip1, j) < CC_GX)
-                            advx = ax * (-(p[c] * p[c] / dp1c));
+                    if (p_c < 0.0f) {
+                        float dp1p = face1(d_p, d_p2);
+                        if (dp1p < CC_GX || d_p < CC_GX)
+                            advx = ax * (-(p_c * p_c / dp1c));
                         else
-                            advx = ax * (p[cp] * p[cp] / dp1p - p[c] * p[c] / dp1c);
+                            advx = ax * (p_p * p_p / dp1p - p_c * p_c / dp1c);
                     } else {
-                        float dp1m = D.dp1(im1, j);
-                        float pm = AT(p, im1, j);
-                        if (dp1m < CC_GX || D.d(i, j) < CC_GX)
-                            advx = ax * (p[c] * p[c] / dp1c);
+                        float dp1m = face1(d_m, d_c);
+                        if (dp1m < CC_GX || d_c < CC_GX)
+                            advx = ax * (p_c * p_c / dp1c);
                         else
-                            advx = ax * (p[c] * p[c] / dp1c - pm * pm / dp1m);
+                            advx = ax * (p_c * p_c / dp1c - p_m * p_m / dp1m);
                     }
                     if (xqq < 0.0f) {
-                        if (D.d(i, jp1) < CC_GX || D.d(ip1, jp1) < CC_GX) {
-                            advy = ay * (-(p[c] * xqq / dp1c));
-                        } else if (D.dp1(i, jp1) < CC_GX) {
-                            advy = ay * (-(p[c] * xqq / dp1c));
+                        if (d_cn < CC_GX || d_pn < CC_GX) {
+                            advy = ay * (-(p_c * xqq / dp1c));
+                        } else if (face1(d_cn, d_pn) < CC_GX) {
+                            advy = ay * (-(p_c * xqq / dp1c));
                         } else {
-                            float xqe = 0.25f * (AT(q, i, jp1) + AT(q, ip1, jp1) + q[c] + q[cp]);
-                            advy = ay * (AT(p, i, jp1) * xqe / D.dp1(i, jp1) - p[c] * xqq / dp1c);
+                            float xqe = 0.25f * (q_cn + q_pn + q_c + q_p);
+                            advy = ay * (p_n * xqe / face1(d_cn, d_pn) - p_c * xqq / dp1c);
                         }
                     } else {
-                        if (D.d(i, jm1) < CC_GX || D.d(ip1, jm1) < CC_GX) {
-                            advy = ay * (p[c] * xqq / dp1c);
-                        } else if (D.dp1(i, jm1) < CC_GX) {
-                            advy = ay * (p[c] * xqq / dp1c);
+                        if (d_cs < CC_GX || d_ps < CC_GX) {
+                            advy = ay * (p_c * xqq / dp1c);
+                        } else if (face1(d_cs, d_ps) < CC_GX) {
+                            advy = ay * (p_c * xqq / dp1c);
                         } else {
-                            float xqe = 0.25f * (AT(q, i, jm1) + AT(q, ip1, jm1) + AT(q, i, j - 2)
-                                                 + AT(q, ip1, j - 2));
-                            advy = ay * (p[c] * xqq / dp1c - AT(p, i, jm1) * xqe / D.dp1(i, jm1));
+                            float xqe = 0.25f * (q_cs + q_ps + q_cs2 + q_ps2);
+                            advy = ay * (p_c * xqq / dp1c - p_s * xqe / face1(d_cs, d_ps));
                         }
                     }
-                    wave_breaking(L, c, advx, advy);
+                    wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
                     xp = xp - advx - advy;
                 }
                 if (L.fric_switch != 1) xp = xp / (1.0f + ff);
@@ -558,19 +577,32 @@ __global__ void k_conmome(GcLayerDev L) {
         bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
         float out = 0.0f;
         if (iny) {
-            size_t cq = (size_t)jp1 * P + i;
+            const size_t cq = rjp + i;
+            const int im2 = i >= 2 ? i - 2 : 0;
+            const size_t rjp2 = (size_t)(j + 2 < jy ? j + 2 : jy - 1) * P;
+            const float h_c = __ldg(hz + c), h_q = __ldg(hz + cq), hq_c = __ldg(L.hq + c);
+            const float d_c = __ldg(dz + c), d_q = __ldg(dz + cq), d_q2 = __ldg(dz + rjp2 + i);
+            const float d_s = __ldg(dz + rjm + i);
+            const float d_e = __ldg(dz + rj + ip1), d_eq = __ldg(dz + rjp + ip1);
+            const float d_w = __ldg(dz + rj + im1), d_wq = __ldg(dz + rjp + im1);
+            const float z_c = __ldg(z + c), z_q = __ldg(z + cq), z1_c = __ldg(L.z1 + c);
+            const float p_c = __ldg(p + c), p_q = __ldg(p + cq);
+            const float p_w = __ldg(p + rj + im1), p_wq = __ldg(p + rjp + im1);
+            const float p_e = __ldg(p + rj + ip1), p_eq = __ldg(p + rjp + ip1);
+            const float p_w2 = __ldg(p + rj + im2), p_w2q = __ldg(p + rjp + im2);
+            const float q_c = __ldg(q + c), q_q = __ldg(q + cq), q_s = __ldg(q + rjm + i);
+            const float q_e = __ldg(q + rj + ip1), q_w = __ldg(q + rj + im1);
             float dd = 0.0f, df = 0.0f, ff;
             bool noflux = false;
-            if (hz[c] <= CC_ELMAX || L.hq[c] <= CC_ELMAX) {
+            if (h_c <= CC_ELMAX || hq_c <= CC_ELMAX) {
                 noflux = true;
             } else {
-                float dzc = D.d(i, j), dzq = D.d(i, jp1);
-                if (dzc > CC_GX && dzq > CC_GX) {
-                    dd = D.dq2(i, j); df = D.dq1(i, j);
-                } else if (dzc > CC_GX && dzq <= CC_GX && hz[cq] + z[c] > CC_GX) {
-                    dd = SPH ? L.hq[c] + 0.5f * (z[c] + z[cq]) : 0.5f * dzc; df = dd;
-                } else if (dzc <= CC_GX && dzq > CC_GX && hz[c] + z[cq] > CC_GX) {
-                    dd = SPH ? L.hq[c] + 0.5f * (z[c] + z[cq]) : 0.5f * dzq; df = dd;
+                if (d_c > CC_GX && d_q > CC_GX) {
+                    dd = face2(d_c, d_q); df = face1(d_c, d_q);
+                } else if (d_c > CC_GX && d_q <= CC_GX && h_q + z_c > CC_GX) {
+                    dd = SPH ? hq_c + 0.5f * (z_c + z_q) : 0.5f * d_c; df = dd;
+                } else if (d_c <= CC_GX && d_q > CC_GX && h_c + z_q > CC_GX) {
+                    dd = SPH ? hq_c + 0.5f * (z_c + z_q) : 0.5f * d_q; df = dd;
                 } else {
                     noflux = true;
                 }
@@ -578,63 +610,61 @@ __global__ void k_conmome(GcLayerDev L) {
             }
             if (!noflux) {
                 if (df < CC_DFMIN) df = CC_DFMIN;
-                float xpp = 0.25f * (p[c] + p[cq] + AT(p, im1, j) + AT(p, im1, jp1));
+                float xpp = 0.25f * (p_c + p_q + p_w + p_wq);
                 if (L.fric_switch != 1)
-                    ff = konst * fm * fm * sqrtf(q[c] * q[c] + xpp * xpp) / cc_powf(df, CC_MANNEXP);
+                    ff = konst * fm * fm * sqrtf(q_c * q_c + xpp * xpp) / cc_powf(df, CC_MANNEXP);
                 else
                     ff = 0.0f;
                 const float cqy = SPH ? GC_ROW(L, GC_CY, j) : L.gry;
-                float xq = q[c] - cqy * dd * (z[cq] - z[c]);
+                float xq = q_c - cqy * dd * (z_q - z_c);
                 if (L.modscm == 0 && i + 1 < ix) {
                     float scm = cqy * dd / 12.0f
-                                * ((AT(z, ip1, jp1) - 2.0f * z[cq] + AT(z, im1, jp1))
-                                   - (AT(z, ip1, j) - 2.0f * z[c] + AT(z, im1, j)));
+                                * ((AT(z, ip1, jp1) - 2.0f * z_q + AT(z, im1, jp1))
+                                   - (AT(z, ip1, j) - 2.0f * z_c + AT(z, im1, j)));
                     xq = xq - scm;
                 }
                 /* CONMOME applies -FF*Q to XP, which is unused (moment.f90:672):
                  * no term on XQ; CONMOME_S applies it to XQ (moment.f90:1150) */
-                if (SPH && L.fric_switch != 1) xq = xq - ff * q[c];
+                if (SPH && L.fric_switch != 1) xq = xq - ff * q_c;
                 if (SPH) xq = xq - 4.0f * GC_ROW(L, GC_R5, j) * xpp;
                 const float by = SPH ? L.rows2[2 * (size_t)j] : L.ry;        /* R0 */
                 const float bx = SPH ? L.rows2[2 * (size_t)j + 1] : L.rx;    /* R22 */
-                float dq1c = D.dq1(i, j);
+                float dq1c = face1(d_c, d_q);
                 if (L.linchk == 1 && dq1c >= CC_GX && span) {
                     float advx, advy;
-                    if (q[c] < 0.0f) {
-                        float dq1q = D.dq1(i, jp1);
-                        if (dq1q < CC_GX || D.d(i, jp1) < CC_GX)
-                            advy = by * (-(q[c] * q[c] / dq1c));
+                    if (q_c < 0.0f) {
+                        float dq1q = face1(d_q, d_q2);
+                        if (dq1q < CC_GX || d_q < CC_GX)
+                            advy = by * (-(q_c * q_c / dq1c));
                         else
-                            advy = by * (q[cq] * q[cq] / dq1q - q[c] * q[c] / dq1c);
+                            advy = by * (q_q * q_q / dq1q - q_c * q_c / dq1c);
                     } else {
-                        float dq1m = D.dq1(i, jm1);
-                        float qm = AT(q, i, jm1);
-                        if (dq1m < CC_GX || D.d(i, j) < CC_GX)
-                            advy = by * (q[c] * q[c] / dq1c);
+                        float dq1m = face1(d_s, d_c);
+                        if (dq1m < CC_GX || d_c < CC_GX)
+                            advy = by * (q_c * q_c / dq1c);
                         else
-                            advy = by * (q[c] * q[c] / dq1c - qm * qm / dq1m);
+                            advy = by * (q_c * q_c / dq1c - q_s * q_s / dq1m);
                     }
                     if (xpp < 0.0f) {
-                        if (D.d(ip1, j) < CC_GX || D.d(ip1, jp1) < CC_GX) {
-                            advx = bx * (-(q[c] * xpp / dq1c));
-                        } else if (D.dq1(ip1, j) < CC_GX) {
-                            advx = bx * (-(q[c] * xpp / dq1c));
+                        if (d_e < CC_GX || d_eq < CC_GX) {
+                            advx = bx * (-(q_c * xpp / dq1c));
+                        } else if (face1(d_e, d_eq) < CC_GX) {
+                            advx = bx * (-(q_c * xpp / dq1c));
                         } else {
-                            float xpe = 0.25f * (AT(p, ip1, j) + AT(p, ip1, jp1) + p[c] + p[cq]);
-                            advx = bx * (AT(q, ip1, j) * xpe / D.dq1(ip1, j) - q[c] * xpp / dq1c);
+                            float xpe = 0.25f * (p_e + p_eq + p_c + p_q);
+                            advx = bx * (q_e * xpe / face1(d_e, d_eq) - q_c * xpp / dq1c);
                         }
                     } else {
-                        if (D.d(im1, j) < CC_GX || D.d(im1, jp1) < CC_GX) {
-                            advx = bx * (q[c] * xpp / dq1c);
-                        } else if (D.dq1(i - 1, j) < CC_GX) {
-                            advx = bx * (q[c] * xpp / dq1c);
+                        if (d_w < CC_GX || d_wq < CC_GX) {
+                            advx = bx * (q_c * xpp / dq1c);
+                        } else if (face1(d_w, d_wq) < CC_GX) {
+                            advx = bx * (q_c * xpp / dq1c);
                         } else {
-                            float xpe = 0.25f * (AT(p, im1, j) + AT(p, im1, jp1) + AT(p, i - 2, j)
-                                                 + AT(p, i - 2, jp1));
-                            advx = bx * (q[c] * xpp / dq1c - AT(q, im1, j) * xpe / D.dq1(im1, j));
+                            float xpe = 0.25f * (p_w + p_wq + p_w2 + p_w2q);
+                            advx = bx * (q_c * xpp / dq1c - q_w * xpe / face1(d_w, d_wq));
                         }
                     }
-                    wave_breaking(L, c, advx, advy);
+                    wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
                     xq = xq - advx - advy;
                 }
                 if (L.fric_switch != 1) xq = xq / (1.0f + ff);
@@ -1116,10 +1146,22 @@ void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
     if (L.laygov == 2 || L.laygov == 3) {
         if (L.laycord == 0) launch(k_momt_d<true>, grid2(L), dim3(BX, BY), 0, s, L);
         else launch(k_momt_d<false>, grid2(L), dim3(BX, BY), 0, s, L);
-    } else if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L);
+    } else if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, 0);
     else if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
-    else if (L.laygov == 1) launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L);
+    else if (L.laygov == 1) launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L, 0);
     else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);
+}
+
+int gc_launch_moment_update(const GcLayerDev &L, cudaStream_t s) {
+    if (L.laygov == 1 && !L.root && L.modscm != 0) {
+        const dim3 g2(grid2(L).x, grid2(L).y, 2);
+        if (L.laycord == 0) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, 1);
+        else launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L, 1);
+        return 1;
+    }
+    gc_launch_moment(L, s);
+    gc_launch_update_edges(L, s);
+    return 2;
 }
 
 void gc_launch_momt_s_window(const GcLayerDev &L, int i0, int i1, int j0, int j1, cudaStream_t s) {

@@ -807,17 +807,29 @@ void gc_subcycle(int parent_id) {
             gc_launch_mass(C.view(), g_rt.stream);
             C.z2_valid = true;
             gc_subcycle(cid);
-            gc_launch_moment(C.view(), g_rt.stream);
+            /* UPDATE's edge copy writes the child's row and column 0 alone,
+             * which JNZ never reads (its blocks start at child index 1), so
+             * it may precede JNZ; JNZ_SC sums every child node in the window,
+             * so at its sub-step the copy follows it */
+            const bool late_update = C.has_sc && k == nhalf;
+            if (late_update) {
+                gc_launch_moment(C.view(), g_rt.stream);
+                g_rt.launches += 3;
+            } else {
+                g_rt.launches += 2 + gc_launch_moment_update(C.view(), g_rt.stream);
+            }
             C.mn2_valid = true;
             if (k == nhalf) {
                 if (C.has_sc) gc_launch_sc_jnz(P.view(), C.view(), C.sc, g_rt.stream);
                 else gc_launch_jnz(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, g_rt.stream);
                 g_rt.launches++;
             }
-            gc_launch_update_edges(C.view(), g_rt.stream);
+            if (late_update) {
+                gc_launch_update_edges(C.view(), g_rt.stream);
+                g_rt.launches++;
+            }
             gc_swap(C);
             C.sc_stepped = true;
-            g_rt.launches += 4;
         }
     }
 }

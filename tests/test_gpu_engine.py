@@ -176,14 +176,18 @@ def test_members_joining_mid_run(oracle_mod):
         assert np.array_equal(g["ts"].view(np.uint32), ts.view(np.uint32))
 
 
-@pytest.mark.parametrize("kind", ["sc_option_1", "dispersion_cartesian", "nonlinear_spherical", "dispersion_spherical"])
+@pytest.mark.parametrize("kind", ["sc_option_1", "sc_option_1_rel1", "dispersion_cartesian", "nonlinear_spherical",
+                                  "dispersion_spherical"])
 def test_engine_nested_child_kinds_match_oracle(oracle_mod, kind):
     """nested engine members whose child is coupled by SC_OPTION = 1 (UTM
     tables, band forecast in member scratch), or runs MASS_C_D/MOMT_C_D,
     CONMASS_S/CONMOME_S or MASS_S_D/MOMT_S_D: bitwise equal to the oracle,
-    with graphs, rel_time 2"""
+    with graphs, rel_time 2 (and 1 for SC_OPTION = 1, where JNZ_SC falls in
+    the first sub-step and reads the child's row and column 0 before UPDATE)"""
     if kind == "sc_option_1":
         case = synth.nested_sc_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=3, rel_time=2)
+    elif kind == "sc_option_1_rel1":
+        case = synth.nested_sc_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=3, rel_time=1)
     elif kind == "dispersion_cartesian":
         case = synth.nested_case("k", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 40, seed=5, rel_time=2, child_laygov=2)
     elif kind == "nonlinear_spherical":

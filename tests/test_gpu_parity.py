@@ -199,3 +199,23 @@ def test_dispersion_scheme_child(oracle_mod, laygov, laycord, modscm):
                        (cn, rc["n"], "child N")):
         _cmp(a, b, what)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
+@pytest.mark.parametrize("modscm,rel_time", [(1, 2), (0, 2), (0, None)])
+def test_nonlinear_child_update_edges(oracle_mod, modscm, rel_time):
+    """UPDATE's edge copy of a nonlinear Cartesian child (all_grids.f90:323-324)
+    rides in the CONMOME launch when the child has no MODSCM term (nothing
+    there reads the surface on row or column 0), and is a launch of its own
+    after the momentum otherwise (MODSCM 0 forced); both bitwise against the
+    oracle, over sub-steps before and after JNZ"""
+    case = synth.nested_case("u", 97, 81, 2.0, 2.0, [60, 79, 30, 49], 3, 0, seed=9, rel_time=rel_time)
+    case.layers[1].modscm = modscm
+    gpu, _, o, _ = _run_both(case, 50, oracle_mod)
+    ref, rc = o.layer(0), o.layer(1)
+    cz, (cm, cn) = gpu["children"][0]
+    assert np.abs(rc["m"]).max() > 0
+    assert np.array_equal(rc["z"][0, 1:], rc["z"][1, 1:]) and np.array_equal(rc["z"][1:, 0], rc["z"][1:, 1])
+    for a, b, what in ((gpu["z"], ref["z"], "parent eta"), (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"),
+                       (cn, rc["n"], "child N")):
+        _cmp(a, b, what)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
