@@ -72,12 +72,18 @@ static int snapshot() {
     return GC_OK;
 }
 
+static int g_last = -1; /* registry slot of the previous lookup */
+
 /* serves gcomcot_get_z_; returns false when the caller must fall back */
 bool gc_gauge_lookup(int lid, int i, int j, float *out4) {
     int n = (int)g_reg.size();
     int found = -1;
-    for (int g = 0; g < n; g++)
-        if (g_reg[g].lid == lid && g_reg[g].i == i && g_reg[g].j == j) { found = g; break; }
+    /* a driver asks for its gauges in the same order every step: try the
+     * slot after the previous one first */
+    const int guess = (g_last + 1 < n) ? g_last + 1 : 0;
+    if (guess < n && g_reg[guess].lid == lid && g_reg[guess].i == i && g_reg[guess].j == j) found = guess;
+    for (int g = 0; found < 0 && g < n; g++)
+        if (g_reg[g].lid == lid && g_reg[g].i == i && g_reg[g].j == j) found = g;
     if (found < 0) {
         /* keep same-layer gauges contiguous */
         size_t pos = g_reg.size();
@@ -93,6 +99,7 @@ bool gc_gauge_lookup(int lid, int i, int j, float *out4) {
         if (snapshot() != GC_OK) return false;
     }
     memcpy(out4, g_h_out + 4 * found, 4 * sizeof(float));
+    g_last = found;
     return true;
 }
 
@@ -101,6 +108,7 @@ void gc_gauge_release() {
     if (g_h_out) cudaFreeHost(g_h_out);
     g_d_ij = nullptr; g_h_out = nullptr; g_d_out = nullptr; g_cap = 0;
     g_reg.clear();
+    g_last = -1;
     g_snap_valid = false;
     g_ij_stale = true;
 }
