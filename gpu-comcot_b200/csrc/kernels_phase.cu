@@ -890,6 +890,44 @@ __global__ void k_jnz(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is,
     Pl.z2[(size_t)(J - 1) * Pl.pitch + (I - 1)] = (count > half) ? sum / count : 0.0f;
 }
 
+/* the same for a compile-time ratio R: the R x R block's surfaces and depths
+ * are loaded as one batch of independent loads, then summed in the order
+ * above (child I outermost) */
+template <int R, bool EVEN>
+__global__ void k_jnz_r(GcLayerDev Pl, GcLayerDev C, int is, int ie, int js, int je) {
+    pdl_enter();
+    int I = is + blockIdx.x * blockDim.x + threadIdx.x;
+    int J = js + blockIdx.y;
+    if (I > ie || J > je) return;
+    const float half = (float)(R * R) / 2.0f;
+    const int i0 = (I - is) * R, j0 = (J - js) * R;
+    const float *__restrict__ z2p = C.z2;
+    const float *__restrict__ z1p = C.z1;
+    const float *__restrict__ hp = C.h;
+    float z2[R][R], hh[R][R], z1[R][R];
+#pragma unroll
+    for (int ki = 0; ki < R; ki++)
+#pragma unroll
+        for (int kj = 0; kj < R; kj++) {
+            const size_t c = (size_t)(j0 + 1 + kj) * C.pitch + (i0 + 1 + ki);
+            z2[ki][kj] = __ldg(z2p + c);
+            hh[ki][kj] = __ldg(hp + c);
+            if (EVEN) z1[ki][kj] = __ldg(z1p + c);
+        }
+    float sum = 0.0f, count = 0.0f;
+#pragma unroll
+    for (int ki = 0; ki < R; ki++)
+#pragma unroll
+        for (int kj = 0; kj < R; kj++) {
+            if (hh[ki][kj] + z2[ki][kj] > CC_GX) {
+                if (EVEN) sum = sum + 0.5f * (z1[ki][kj] + z2[ki][kj]);
+                else sum = sum + z2[ki][kj];
+                count = count + 1.0f;
+            }
+        }
+    Pl.z2[(size_t)(J - 1) * Pl.pitch + (I - 1)] = (count > half) ? sum / count : 0.0f;
+}
+
 /* ---------------------------------------------------------------- */
 /* outputs                                                           */
 /* ---------------------------------------------------------------- */
@@ -1197,6 +1235,20 @@ void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int r
                    const int *corners, cudaStream_t s) {
     int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
     dim3 grid((unsigned)((ie - is + 1 + 127) / 128), (unsigned)(je - js + 1), 1);
+    const bool even = (rel_time % 2) == 0;
+#define GC_JNZ_R(R)                                                                             \
+    case R:                                                                                     \
+        if (even) launch(k_jnz_r<R, true>, grid, 128, 0, s, P, C, is, ie, js, je);             \
+        else launch(k_jnz_r<R, false>, grid, 128, 0, s, P, C, is, ie, js, je);                 \
+        return;
+    switch (rel_size) {
+        GC_JNZ_R(2)
+        GC_JNZ_R(3)
+        GC_JNZ_R(4)
+        GC_JNZ_R(5)
+        default: break;
+    }
+#undef GC_JNZ_R
     launch(k_jnz, grid, 128, 0, s, P, C, rel_size, rel_time, is, ie, js, je);
 }
 
