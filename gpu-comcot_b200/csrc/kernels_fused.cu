@@ -490,7 +490,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
             if (k >= 2 && j < ny && own) {
                 const float *mB = SB + ST::M / 4 + 4, *mA = SA + ST::M / 4 + 4;
                 const float *hB = SB + ST::H / 4, *hA = SA + ST::H / 4;
-                float cx = 0.0f, cy = 0.0f;
+                [[maybe_unused]] float cx = 0.0f, cy = 0.0f; /* explicit R2/R4 fields need neither */
                 if constexpr (!XR24) { cx = SB[ST::C / 4 + GC_CX]; cy = SB[ST::C / 4 + GC_CY]; }
                 const float r3 = SB[ST::C / 4 + GC_R3], r5 = SB[ST::C / 4 + GC_R5];
                 /* columns c0..c0+4 of H, N(j), N(j-1), Z2(j); c0-1..c0+3 of M(j), M(j+1) */
