@@ -396,6 +396,22 @@ __global__ void k_momt_c(GcLayerDev L) {
 /* WAVE_BREAKING (moment.f90:1272-1384).  DZ(:,:,1) is identically    */
 /* zero in the reference, so DP1 = 0.25*(DZ2(I)+DZ2(I+1)) etc.         */
 /* ---------------------------------------------------------------- */
+/* a / b bit for bit, without the division where a is a signed zero and b
+ * positive (IEEE 754 gives a itself there).  Still water makes many zero
+ * numerators, and a correctly rounded division costs far more than the
+ * test.  NaN or non-positive b always takes the division. */
+__device__ __forceinline__ float qdiv(float a, float b) {
+    if (a == 0.0f && b > 0.0f) return a;
+    return a / b;
+}
+/* a / (1 + ff) for the friction divisor: also without the division where
+ * 1 + ff rounded to exactly 1 (friction below 2^-24, as in deep water) and
+ * a is a number */
+__device__ __forceinline__ float fdiv1(float a, float onepff) {
+    if (onepff == 1.0f && a == a) return a;
+    return qdiv(a, onepff);
+}
+
 /* face depths from two total depths (moment.f90:345-366): the x form
  * DP1/DP2 of cells (I,J),(I+1,J), the y form DQ1/DQ2 of (I,J),(I,J+1) */
 __device__ __forceinline__ float face1(float a, float b) {
@@ -414,7 +430,7 @@ __device__ __forceinline__ void wave_breaking(float dz2c, float z2c, float z1c, 
     float cc = sqrtf(CC_GRAV * dz2c);
     float dzdt_f = CC_BRK_F * cc;
     float dzdt_i = CC_BRK_I * cc;
-    float dzdt = fabs_(z2c - z1c) / dt;
+    float dzdt = qdiv(fabs_(z2c - z1c), dt);
     if (dzdt > dzdt_f) {
         float ref = (dzdt - dzdt_f) / (dzdt_i - dzdt_f);
         float coef = cc_expf(-(1.0f * ref));
@@ -509,13 +525,17 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
                 if (df < CC_DFMIN) df = CC_DFMIN;
                 float xqq = 0.25f * (q_c + q_p + q_cs + q_ps);
                 if (L.fric_switch != 1)
-                    ff = konst * fm * fm * sqrtf(p_c * p_c + xqq * xqq) / cc_powf(df, CC_MANNEXP);
+                    {
+                        /* df >= DFMIN here unless it is NaN, so the power is positive */
+                        const float fnum = konst * fm * fm * sqrtf(p_c * p_c + xqq * xqq);
+                        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
+                    }
                 else
                     ff = 0.0f;
                 const float cpx = SPH ? GC_ROW(L, GC_CX, j) : L.grx;
                 float xp = p_c - cpx * dd * (z_p - z_c);
                 if (L.modscm == 0 && j + 1 < jy) {
-                    float scm = cpx * dd / 12.0f
+                    float scm = qdiv(cpx * dd, 12.0f)
                                 * ((AT(z, ip1, jp1) - 2.0f * z_p + AT(z, ip1, jm1))
                                    - (AT(z, i, jp1) - 2.0f * z_c + AT(z, i, jm1)));
                     xp = xp - scm;
@@ -530,39 +550,39 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
                     if (p_c < 0.0f) {
                         float dp1p = face1(d_p, d_p2);
                         if (dp1p < CC_GX || d_p < CC_GX)
-                            advx = ax * (-(p_c * p_c / dp1c));
+                            advx = ax * (-(qdiv(p_c * p_c, dp1c)));
                         else
-                            advx = ax * (p_p * p_p / dp1p - p_c * p_c / dp1c);
+                            advx = ax * (qdiv(p_p * p_p, dp1p) - qdiv(p_c * p_c, dp1c));
                     } else {
                         float dp1m = face1(d_m, d_c);
                         if (dp1m < CC_GX || d_c < CC_GX)
-                            advx = ax * (p_c * p_c / dp1c);
+                            advx = ax * (qdiv(p_c * p_c, dp1c));
                         else
-                            advx = ax * (p_c * p_c / dp1c - p_m * p_m / dp1m);
+                            advx = ax * (qdiv(p_c * p_c, dp1c) - qdiv(p_m * p_m, dp1m));
                     }
                     if (xqq < 0.0f) {
                         if (d_cn < CC_GX || d_pn < CC_GX) {
-                            advy = ay * (-(p_c * xqq / dp1c));
+                            advy = ay * (-(qdiv(p_c * xqq, dp1c)));
                         } else if (face1(d_cn, d_pn) < CC_GX) {
-                            advy = ay * (-(p_c * xqq / dp1c));
+                            advy = ay * (-(qdiv(p_c * xqq, dp1c)));
                         } else {
                             float xqe = 0.25f * (q_cn + q_pn + q_c + q_p);
-                            advy = ay * (p_n * xqe / face1(d_cn, d_pn) - p_c * xqq / dp1c);
+                            advy = ay * (qdiv(p_n * xqe, face1(d_cn, d_pn)) - qdiv(p_c * xqq, dp1c));
                         }
                     } else {
                         if (d_cs < CC_GX || d_ps < CC_GX) {
-                            advy = ay * (p_c * xqq / dp1c);
+                            advy = ay * (qdiv(p_c * xqq, dp1c));
                         } else if (face1(d_cs, d_ps) < CC_GX) {
-                            advy = ay * (p_c * xqq / dp1c);
+                            advy = ay * (qdiv(p_c * xqq, dp1c));
                         } else {
                             float xqe = 0.25f * (q_cs + q_ps + q_cs2 + q_ps2);
-                            advy = ay * (p_c * xqq / dp1c - p_s * xqe / face1(d_cs, d_ps));
+                            advy = ay * (qdiv(p_c * xqq, dp1c) - qdiv(p_s * xqe, face1(d_cs, d_ps)));
                         }
                     }
                     wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
                     xp = xp - advx - advy;
                 }
-                if (L.fric_switch != 1) xp = xp / (1.0f + ff);
+                if (L.fric_switch != 1) xp = fdiv1(xp, 1.0f + ff);
                 if (fabs_(xp) < CC_EPS) xp = 0.0f;
                 float lim = CC_VLIMIT * dd;
                 if (xp > lim) xp = lim;
@@ -612,13 +632,17 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
                 if (df < CC_DFMIN) df = CC_DFMIN;
                 float xpp = 0.25f * (p_c + p_q + p_w + p_wq);
                 if (L.fric_switch != 1)
-                    ff = konst * fm * fm * sqrtf(q_c * q_c + xpp * xpp) / cc_powf(df, CC_MANNEXP);
+                    {
+                        /* df >= DFMIN here unless it is NaN, so the power is positive */
+                        const float fnum = konst * fm * fm * sqrtf(q_c * q_c + xpp * xpp);
+                        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
+                    }
                 else
                     ff = 0.0f;
                 const float cqy = SPH ? GC_ROW(L, GC_CY, j) : L.gry;
                 float xq = q_c - cqy * dd * (z_q - z_c);
                 if (L.modscm == 0 && i + 1 < ix) {
-                    float scm = cqy * dd / 12.0f
+                    float scm = qdiv(cqy * dd, 12.0f)
                                 * ((AT(z, ip1, jp1) - 2.0f * z_q + AT(z, im1, jp1))
                                    - (AT(z, ip1, j) - 2.0f * z_c + AT(z, im1, j)));
                     xq = xq - scm;
@@ -635,39 +659,39 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
                     if (q_c < 0.0f) {
                         float dq1q = face1(d_q, d_q2);
                         if (dq1q < CC_GX || d_q < CC_GX)
-                            advy = by * (-(q_c * q_c / dq1c));
+                            advy = by * (-(qdiv(q_c * q_c, dq1c)));
                         else
-                            advy = by * (q_q * q_q / dq1q - q_c * q_c / dq1c);
+                            advy = by * (qdiv(q_q * q_q, dq1q) - qdiv(q_c * q_c, dq1c));
                     } else {
                         float dq1m = face1(d_s, d_c);
                         if (dq1m < CC_GX || d_c < CC_GX)
-                            advy = by * (q_c * q_c / dq1c);
+                            advy = by * (qdiv(q_c * q_c, dq1c));
                         else
-                            advy = by * (q_c * q_c / dq1c - q_s * q_s / dq1m);
+                            advy = by * (qdiv(q_c * q_c, dq1c) - qdiv(q_s * q_s, dq1m));
                     }
                     if (xpp < 0.0f) {
                         if (d_e < CC_GX || d_eq < CC_GX) {
-                            advx = bx * (-(q_c * xpp / dq1c));
+                            advx = bx * (-(qdiv(q_c * xpp, dq1c)));
                         } else if (face1(d_e, d_eq) < CC_GX) {
-                            advx = bx * (-(q_c * xpp / dq1c));
+                            advx = bx * (-(qdiv(q_c * xpp, dq1c)));
                         } else {
                             float xpe = 0.25f * (p_e + p_eq + p_c + p_q);
-                            advx = bx * (q_e * xpe / face1(d_e, d_eq) - q_c * xpp / dq1c);
+                            advx = bx * (qdiv(q_e * xpe, face1(d_e, d_eq)) - qdiv(q_c * xpp, dq1c));
                         }
                     } else {
                         if (d_w < CC_GX || d_wq < CC_GX) {
-                            advx = bx * (q_c * xpp / dq1c);
+                            advx = bx * (qdiv(q_c * xpp, dq1c));
                         } else if (face1(d_w, d_wq) < CC_GX) {
-                            advx = bx * (q_c * xpp / dq1c);
+                            advx = bx * (qdiv(q_c * xpp, dq1c));
                         } else {
                             float xpe = 0.25f * (p_w + p_wq + p_w2 + p_w2q);
-                            advx = bx * (q_c * xpp / dq1c - q_w * xpe / face1(d_w, d_wq));
+                            advx = bx * (qdiv(q_c * xpp, dq1c) - qdiv(q_w * xpe, face1(d_w, d_wq)));
                         }
                     }
                     wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
                     xq = xq - advx - advy;
                 }
-                if (L.fric_switch != 1) xq = xq / (1.0f + ff);
+                if (L.fric_switch != 1) xq = fdiv1(xq, 1.0f + ff);
                 if (fabs_(xq) < CC_EPS) xq = 0.0f;
                 float lim = CC_VLIMIT * dd;
                 if (xq > lim) xq = lim;
