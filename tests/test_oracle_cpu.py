@@ -93,3 +93,29 @@ def test_nested_oracle_runs_and_conserves_masks(oracle_mod):
     assert np.all(c["z"][dry & (H > -50)] == -H[dry & (H > -50)])
     assert np.all(np.isfinite(c["z"]))
     assert np.all(np.abs(c["m"]) <= 20.0 * np.maximum(c["z"] + H, 0) + 1e-3)
+
+
+def test_division_shortcuts_are_ieee_identities():
+    """The momentum kernels skip a correctly rounded division where IEEE 754
+    fixes its result: a signed zero over a positive divisor is that zero, and
+    a number over exactly 1 is itself.  Checked here on the host's IEEE
+    binary32 division over zeros, subnormals, normals, the largest finite
+    value and infinity; a NaN or non-positive divisor never takes the
+    shortcut."""
+    f32 = np.float32
+    tiny = np.finfo(f32).tiny
+    smallest = f32(np.nextafter(f32(0), f32(1)))
+    divisors = np.array([smallest, tiny, f32(1e-3), f32(1.0), f32(2.0), f32(7.25), np.finfo(f32).max, np.inf],
+                        dtype=f32)
+    with np.errstate(all="ignore"):
+        for a in (f32(0.0), f32(-0.0)):
+            q = (np.full_like(divisors, a) / divisors).astype(f32)
+            assert np.array_equal(q.view(np.uint32), np.full_like(divisors, a).view(np.uint32))
+        nums = np.array([f32(0.0), f32(-0.0), smallest, -smallest, tiny, f32(1e-30), f32(0.1), f32(-3.5), f32(1e30),
+                         np.finfo(f32).max, np.inf, -np.inf], dtype=f32)
+        q = (nums / f32(1.0)).astype(f32)
+        assert np.array_equal(q.view(np.uint32), nums.view(np.uint32))
+        # the cases left to the division: 0/0, 0/-x, 0/NaN are not the zero itself
+        assert np.isnan(f32(0.0) / f32(0.0))
+        assert (f32(0.0) / f32(-2.0)).view(np.uint32) != f32(0.0).view(np.uint32)
+        assert np.isnan(f32(0.0) / f32(np.nan))
