@@ -337,7 +337,8 @@ def run_c3(args, torch, dist, rank, world, local):
         s.close()
         fp, fc = P.nx * P.ny * 4, Cl.nx * Cl.ny * 4
         e2e = {"value": cells * args.steps * world / (e2e_ms * 1e-3), "unit": METRIC,
-               "h2d_bytes_per_step": int((9 * fp + 13 * fc) / args.steps),
+               # the outer grid's H and Z, the child's H, Z, HP and HQ, and the 8-float row records
+               "h2d_bytes_per_step": int((2 * fp + 4 * fc + (P.ny + Cl.ny) * 8 * 4) / args.steps),
                "d2h_bytes_per_step": int((2 * fp + fc) / args.steps), "ms_per_step": e2e_ms / args.steps,
                "path": "gcomcot_set_layer_params_/init_layer x2 + per step mass/openbd/all_grid/momt/maxamp/"
                        "update + getz x2/getzmax"}
@@ -632,7 +633,8 @@ def run_single(args, torch, dist, rank, world, local):
         e2e_ms = replicas.reduce_max(e2e_ms, dist, 'cuda')
         nx, ny = case_e.root.nx, case_e.root.ny
         field = nx * ny * 4
-        h2d = (9 * field + ny * 4) / args.steps        # H, Z, R1..R5, R2, R4, R11 fields + R6
+        # H and Z as fields plus the 8-float row record per row; the R fields are read on the host
+        h2d = (2 * field + ny * 8 * 4) / args.steps
         d2h = len(case_e.gauges) * 16 + 2 * field / args.steps
         e2e = {"value": cells * args.steps * world / (e2e_ms * 1e-3), "unit": METRIC,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

@@ -20,6 +20,22 @@ constexpr int BX = 32, BY = 8;
 
 __device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 
+/* a / b bit for bit, without the division where a is a signed zero and b
+ * positive (IEEE 754 gives a itself there).  Still water makes many zero
+ * numerators, and a correctly rounded division costs far more than the
+ * test.  NaN or non-positive b always takes the division. */
+__device__ __forceinline__ float qdiv(float a, float b) {
+    if (a == 0.0f && b > 0.0f) return a;
+    return a / b;
+}
+/* a / (1 + ff) for the friction divisor: also without the division where
+ * 1 + ff rounded to exactly 1 (friction below 2^-24, as in deep water) and
+ * a is a number */
+__device__ __forceinline__ float fdiv1(float a, float onepff) {
+    if (onepff == 1.0f && a == a) return a;
+    return qdiv(a, onepff);
+}
+
 /* ---------------------------------------------------------------- */
 /* continuity                                                        */
 /* ---------------------------------------------------------------- */
@@ -219,14 +235,18 @@ __global__ void k_momt_d(GcLayerDev L) {
             if (L.fric_switch != 1) {
                 const float xqq = 0.25f * (L.n1[c] + L.n1[cp] + L.n1[cm] + L.n1[cm + 1]);
                 if (hm >= 1.0e-3f)
-                    ff = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq) / cc_powf(hm, CC_MANNEXP);
+                    {
+                    /* the guard above keeps hm >= 1e-3, so the power is positive */
+                    const float fnum = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq);
+                    ff = (fnum == 0.0f) ? fnum : fnum / cc_powf(hm, CC_MANNEXP);
+                }
             }
             float xm = (1.0f - ff) * L.m1[c] - L.grx * hm * (z[cp] - z[c]);
             if (L.modscm == 0) {
                 const float scm = L.grx * CC_TWLVTH * hm * ((z[cu + 1] - 2.0f * z[cp] + z[cm + 1]) - (z[cu] - 2.0f * z[c] + z[cm]));
                 xm = xm - scm;
             }
-            if (L.fric_switch != 1) xm = xm / (1.0f + ff);
+            if (L.fric_switch != 1) xm = fdiv1(xm, 1.0f + ff);
             if (fabs_(xm) < CC_EPS) xm = 0.0f;
             L.m2[c] = xm;
         } else {
@@ -261,14 +281,18 @@ __global__ void k_momt_d(GcLayerDev L) {
             if (L.fric_switch != 1) {
                 const float xpp = 0.25f * (L.m1[c] + L.m1[cq] + L.m1[cw] + L.m1[cw + P]);
                 if (hn >= 1.0e-5f)
-                    ff = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp) / cc_powf(hn, CC_MANNEXP);
+                    {
+                    /* the guard above keeps hn >= 1e-5, so the power is positive */
+                    const float fnum = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp);
+                    ff = (fnum == 0.0f) ? fnum : fnum / cc_powf(hn, CC_MANNEXP);
+                }
             }
             float xn = (1.0f - ff) * L.n1[c] - L.gry * hn * (z[cq] - z[c]);
             if (L.modscm == 0) {
                 const float scm = L.gry * CC_TWLVTH * hn * ((z[ce + P] - 2.0f * z[cq] + z[cw + P]) - (z[ce] - 2.0f * z[c] + z[cw]));
                 xn = xn - scm;
             }
-            if (L.fric_switch != 1) xn = xn / (1.0f + ff);
+            if (L.fric_switch != 1) xn = fdiv1(xn, 1.0f + ff);
             if (fabs_(xn) < CC_EPS) xn = 0.0f;
             L.n2[c] = xn;
         } else {
@@ -341,8 +365,11 @@ __global__ void k_momt_c(GcLayerDev L) {
             if (L.fric_switch != 1) {
                 float xqq = 0.25f * (L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1]);
                 if (hm >= 1.0e-3f)
-                    ff = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq)
-                         / cc_powf(hm, CC_MANNEXP);
+                    {
+                    /* the guard above keeps hm >= 1e-3, so the power is positive */
+                    const float fnum = konst * fm * fm * sqrtf(L.m1[c] * L.m1[c] + xqq * xqq);
+                    ff = (fnum == 0.0f) ? fnum : fnum / cc_powf(hm, CC_MANNEXP);
+                }
                 else
                     ff = 0.0f;
                 xm = xm - ff * L.m1[c];
@@ -353,7 +380,7 @@ __global__ void k_momt_c(GcLayerDev L) {
                                - (z[cpj] - 2.0f * z[c] + z[cm]));
                 xm = xm - scm;
             }
-            if (L.fric_switch != 1) xm = xm / (1.0f + ff);
+            if (L.fric_switch != 1) xm = fdiv1(xm, 1.0f + ff);
             if (fabs_(xm) < CC_EPS) xm = 0.0f;
         }
     }
@@ -371,8 +398,11 @@ __global__ void k_momt_c(GcLayerDev L) {
                 float xpp = 0.25f * (L.m1[c] + L.m1[cq] + L.m1[(size_t)j * P + im1]
                                      + L.m1[(size_t)(j + 1) * P + im1]);
                 if (hn >= 1.0e-5f)
-                    ff = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp)
-                         / cc_powf(hn, CC_MANNEXP);
+                    {
+                    /* the guard above keeps hn >= 1e-5, so the power is positive */
+                    const float fnum = konst * fm * fm * sqrtf(L.n1[c] * L.n1[c] + xpp * xpp);
+                    ff = (fnum == 0.0f) ? fnum : fnum / cc_powf(hn, CC_MANNEXP);
+                }
                 else
                     ff = 0.0f;
                 xn = xn - ff * L.n1[c];
@@ -384,7 +414,7 @@ __global__ void k_momt_c(GcLayerDev L) {
                                - (z[r0 + ip1] - 2.0f * z[r0 + i] + z[r0 + im1]));
                 xn = xn - scm;
             }
-            if (L.fric_switch != 1) xn = xn / (1.0f + ff);
+            if (L.fric_switch != 1) xn = fdiv1(xn, 1.0f + ff);
             if (fabs_(xn) < CC_EPS) xn = 0.0f;
         }
     }
@@ -396,22 +426,6 @@ __global__ void k_momt_c(GcLayerDev L) {
 /* WAVE_BREAKING (moment.f90:1272-1384).  DZ(:,:,1) is identically    */
 /* zero in the reference, so DP1 = 0.25*(DZ2(I)+DZ2(I+1)) etc.         */
 /* ---------------------------------------------------------------- */
-/* a / b bit for bit, without the division where a is a signed zero and b
- * positive (IEEE 754 gives a itself there).  Still water makes many zero
- * numerators, and a correctly rounded division costs far more than the
- * test.  NaN or non-positive b always takes the division. */
-__device__ __forceinline__ float qdiv(float a, float b) {
-    if (a == 0.0f && b > 0.0f) return a;
-    return a / b;
-}
-/* a / (1 + ff) for the friction divisor: also without the division where
- * 1 + ff rounded to exactly 1 (friction below 2^-24, as in deep water) and
- * a is a number */
-__device__ __forceinline__ float fdiv1(float a, float onepff) {
-    if (onepff == 1.0f && a == a) return a;
-    return qdiv(a, onepff);
-}
-
 /* face depths from two total depths (moment.f90:345-366): the x form
  * DP1/DP2 of cells (I,J),(I+1,J), the y form DQ1/DQ2 of (I,J),(I,J+1) */
 __device__ __forceinline__ float face1(float a, float b) {

@@ -19,6 +19,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "runtime.h"
@@ -152,45 +154,60 @@ int gc_layer_download_field(GcLayer &L, const float *src, float *dst) {
  * (initialization.f90:2512-2523).  Returns the per-row factors when the
  * caller's field has exactly that form in every cell, so the kernels can
  * rebuild R2 from H instead of streaming a second field. */
-static bool factor_rows(int nx, int ny, const float *H, const float *R, bool xdir, float *fac) {
-    std::vector<float> hp((size_t)nx);
-    for (int j = 0; j < ny; j++) {
-        float best = 0.0f;
-        int bi = -1;
-        for (int i = 0; i < nx; i++) {
-            size_t c = (size_t)j * nx + i;
-            float v = 0.0f;
-            if (H[c] > CC_GX) {
-                size_t c2;
-                if (xdir) c2 = (size_t)j * nx + std::min(i + 1, nx - 1);
-                else c2 = (size_t)std::min(j + 1, ny - 1) * nx + i;
-                v = 0.5f * (H[c] + H[c2]);
-            }
-            hp[i] = v > 0.0f ? v : 0.0f;
-            if (hp[i] > best) { best = hp[i]; bi = i; }
+static bool factor_row(int nx, int ny, int j, const float *H, const float *R, bool xdir, float *hp, float *fac) {
+    float best = 0.0f;
+    int bi = -1;
+    for (int i = 0; i < nx; i++) {
+        size_t c = (size_t)j * nx + i;
+        float v = 0.0f;
+        if (H[c] > CC_GX) {
+            size_t c2;
+            if (xdir) c2 = (size_t)j * nx + std::min(i + 1, nx - 1);
+            else c2 = (size_t)std::min(j + 1, ny - 1) * nx + i;
+            v = 0.5f * (H[c] + H[c2]);
         }
-        float cands[3];
-        int nc;
-        if (bi < 0) {
-            cands[0] = 0.0f; nc = 1;
-        } else {
-            float c0 = (float)((double)R[(size_t)j * nx + bi] / (double)best);
-            cands[0] = c0; cands[1] = nextafterf(c0, 3.0e38f); cands[2] = nextafterf(c0, -3.0e38f);
-            nc = 3;
-        }
-        bool ok = false;
-        for (int k = 0; k < nc && !ok; k++) {
-            ok = true;
-            for (int i = 0; i < nx && ok; i++) {
-                float want = R[(size_t)j * nx + i];
-                float got = cands[k] * hp[i];
-                if (memcmp(&want, &got, sizeof(float)) != 0 && !(want == 0.0f && got == 0.0f)) ok = false;
-            }
-            if (ok) fac[j] = cands[k];
-        }
-        if (!ok) return false;
+        hp[i] = v > 0.0f ? v : 0.0f;
+        if (hp[i] > best) { best = hp[i]; bi = i; }
     }
-    return true;
+    float cands[3];
+    int nc;
+    if (bi < 0) {
+        cands[0] = 0.0f; nc = 1;
+    } else {
+        float c0 = (float)((double)R[(size_t)j * nx + bi] / (double)best);
+        cands[0] = c0; cands[1] = nextafterf(c0, 3.0e38f); cands[2] = nextafterf(c0, -3.0e38f);
+        nc = 3;
+    }
+    for (int k = 0; k < nc; k++) {
+        bool ok = true;
+        for (int i = 0; i < nx && ok; i++) {
+            float want = R[(size_t)j * nx + i];
+            float got = cands[k] * hp[i];
+            if (memcmp(&want, &got, sizeof(float)) != 0 && !(want == 0.0f && got == 0.0f)) ok = false;
+        }
+        if (ok) {
+            fac[j] = cands[k];
+            return true;
+        }
+    }
+    return false;
+}
+
+/* rows are independent: host threads take every nt-th row */
+static bool factor_rows(int nx, int ny, const float *H, const float *R, bool xdir, float *fac) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = std::max(1, std::min({(int)(hw ? hw : 1), 16, (int)(((size_t)nx * ny) >> 18) + 1}));
+    std::atomic<bool> all_ok{true};
+    auto work = [&](int t) {
+        std::vector<float> hp((size_t)nx);
+        for (int j = t; j < ny && all_ok.load(std::memory_order_relaxed); j += nt)
+            if (!factor_row(nx, ny, j, H, R, xdir, hp.data(), fac)) all_ok.store(false);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    return all_ok.load();
 }
 
 static void init_runtime() {
