@@ -61,13 +61,20 @@ void gc_root_change_hook(GcLayer &L) {
 extern "C" {
 
 /* extension: record, per wet cell of layer `id`, the first outer step after
- * which the surface exceeds `thr` (metres); -1 until then.  The reference has
- * no arrival-time product; this is evaluated at every CHANGE of layer 1. */
+ * which the surface exceeds `thr` (metres); 0 for a wet cell already above it
+ * when the call is made, -1 until then elsewhere.  The reference has no
+ * arrival-time product; this is evaluated at every CHANGE of layer 1. */
 void gcomcot_set_arrival_(int *id, float *thr) {
     (void)id;
     g_arr.on = true;
     g_arr.thr = *thr;
     g_arr.step = 1;
+    GcRuntime &rt = gc_rt();
+    if (rt.inited && rt.root >= 0) {
+        GcLayer &L = rt.layers[rt.root];
+        gc_launch_arrival_start(L.arrival, L.z[L.cur], L.h, L.nx, L.ny, L.pitch, *thr, rt.stream);
+        rt.launches++;
+    }
 }
 
 void gcomcot_get_arrival_(int *arr, int *id) {

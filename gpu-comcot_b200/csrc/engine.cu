@@ -203,7 +203,7 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     /* the fused launch records max-eta and arrival outside the JNZ window
      * (IS..IE x JS..JE, 0-based IS-1..IE-1); the outputs kernel does the window */
     const int win[4] = {C.corners[0] - 1, C.corners[1] - 1, C.corners[2] - 1, C.corners[3] - 1};
-    const int flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
+    const int flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL | GC_F_ARR_BYMAX : 0);
     /* the step number comes from the device counter (arrival steps); the
      * member's level-1 buffer is 0 at its first step, so the kernel's parity
      * equals `cur` */
@@ -390,7 +390,7 @@ static int eng_rebuild(gc_engine *e) {
             g.ty = ty;
             gc_fused_tiles(C.nx, C.ny, ty, &g.tiles_x);
             g.step0 = M.step0; g.cur0 = 0; g.nsteps = M.nsteps;
-            g.flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL : 0);
+            g.flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL | GC_F_ARR_BYMAX : 0);
             g.thr = M.thr;
             for (int q = 0; q < 2; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
             g.h = M.h ? M.h : C.d_h; g.rows = C.d_rows;
@@ -658,6 +658,10 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
                                          e->stream));
     }
     GC_CUDA_OR_RET(cudaMemcpyAsync(M.zmax, M.z[0], field, cudaMemcpyDeviceToDevice, e->stream));
+    if (arrival_thr >= 0.0f) {
+        gc_launch_arrival_start(M.arrival, M.z[0], M.h ? M.h : C.d_h, C.nx, C.ny, C.pitch, arrival_thr, e->stream);
+        GC_CUDA_OR_RET(cudaGetLastError());
+    }
     if (ngauges > 0) {
         GC_CUDA_OR_RET(cudaMemcpyAsync(M.gij, gij, (size_t)2 * ngauges * sizeof(int), cudaMemcpyHostToDevice,
                                        e->stream));

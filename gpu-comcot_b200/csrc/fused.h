@@ -9,6 +9,10 @@
 
 #define GC_F_MAXAMP 1
 #define GC_F_ARRIVAL 2
+/* arrival decided from max-eta (set by the engine, whose members record
+ * max-eta every step and start arrival at 0 where the initial surface is
+ * already above the threshold on a wet cell) */
+#define GC_F_ARR_BYMAX 4
 
 struct GcFusedGrid {
     int nx, ny, pitch, root, explicit_r24;

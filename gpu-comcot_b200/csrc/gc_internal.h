@@ -134,6 +134,9 @@ void gc_launch_sc_forecast(const GcLayerDev &P, const GcScView &sv, cudaStream_t
 void gc_launch_sc_jnz(const GcLayerDev &P, const GcLayerDev &C, const GcScView &sv, cudaStream_t s);
 void gc_launch_maxamp(const GcLayerDev &L, cudaStream_t s);
 void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s);
+/* arrival at the start of tracking: 0 on a wet cell already above `thr`, -1 elsewhere */
+void gc_launch_arrival_start(int *arrival, const float *z, const float *h, int nx, int ny, int pitch, float thr,
+                             cudaStream_t s);
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s);
 void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out, cudaStream_t s);
 /* max-eta (flags & 1), arrival (flags & 2) and gauge samples after one outer

@@ -231,6 +231,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     int *__restrict__ arrival = Gref.arrival;
     const bool do_max = (flags & GC_F_MAXAMP) != 0;
     const bool do_arr = (flags & GC_F_ARRIVAL) != 0;
+    const bool by_max = do_max && (flags & GC_F_ARR_BYMAX) != 0;
     const int txi = lt % tiles_x, tyi = lt / tiles_x;
     const int i0 = txi * TXW, j0 = tyi * TY;
 
@@ -460,13 +461,15 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                         for (int q = 0; q < 4; q++)
                             skip[q] = inwin && r >= wj0 && r <= wj1 && ib + q >= wi0 && ib + q <= wi1;
                     }
+                    float xo[4] = {0.0f, 0.0f, 0.0f, 0.0f}; /* max-eta before this step */
                     if (do_max) {
                         float4 x4;
                         if constexpr (ZD) x4 = xcur;
                         else x4 = lds4(SA + ST::X / 4 + c0);
-                        float zx[4] = {x4.x, x4.y, x4.z, x4.w};
+                        xo[0] = x4.x; xo[1] = x4.y; xo[2] = x4.z; xo[3] = x4.w;
+                        float zx[4];
 #pragma unroll
-                        for (int q = 0; q < 4; q++) zx[q] = (zx[q] >= zn[q] || skip[q]) ? zx[q] : zn[q];
+                        for (int q = 0; q < 4; q++) zx[q] = (xo[q] >= zn[q] || skip[q]) ? xo[q] : zn[q];
                         if constexpr (EDGE) st4p(zxp, ib, nx, zx);
                         else *reinterpret_cast<float4 *>(zxp) = make_float4(zx[0], zx[1], zx[2], zx[3]);
                     }
@@ -477,7 +480,16 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                             for (int q = 0; q < 4; q++) {
                                 if (ib + q < nx && zn[q] > thr && hv[q] > CC_GX && !skip[q]) {
                                     int *a = arrival + (size_t)r * P + ib + q;
-                                    if (*a < 0) *a = local + 1;
+                                    /* GC_F_ARR_BYMAX: max-eta has taken every step
+                                     * since the start, so a wet cell whose max so
+                                     * far is at or below the threshold has not
+                                     * arrived (cells starting above it start at
+                                     * step 0), and the arrival field need not be read */
+                                    if (by_max) {
+                                        if (xo[q] <= thr) *a = local + 1;
+                                    } else if (*a < 0) {
+                                        *a = local + 1;
+                                    }
                                 }
                             }
                         }

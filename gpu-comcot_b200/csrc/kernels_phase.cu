@@ -1115,6 +1115,18 @@ __global__ void k_sponge(GcLayerDev L, const float *__restrict__ spx, const floa
     }
 }
 
+/* arrival at the start of tracking: step 0 on a wet cell whose surface is
+ * already above the threshold, -1 (not yet) elsewhere */
+__global__ void k_arrival_start(int *arrival, const float *z, const float *h, int nx, int ny, int pitch,
+                                float thr) {
+    pdl_enter();
+    int i = blockIdx.x * BX + threadIdx.x;
+    int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    size_t c = (size_t)j * pitch + i;
+    arrival[c] = (h[c] > CC_GX && z[c] > thr) ? 0 : -1;
+}
+
 __global__ void k_arrival(GcLayerDev L, int step, float thr) {
     pdl_enter();
     int i = blockIdx.x * BX + threadIdx.x;
@@ -1319,6 +1331,12 @@ void gc_launch_sc_jnz(const GcLayerDev &P, const GcLayerDev &C, const GcScView &
 
 void gc_launch_sponge(const GcLayerDev &L, const float *spx, const float *spy, float dt, cudaStream_t s) {
     launch(k_sponge, grid2(L), dim3(BX, BY), 0, s, L, spx, spy, dt);
+}
+
+void gc_launch_arrival_start(int *arrival, const float *z, const float *h, int nx, int ny, int pitch, float thr,
+                             cudaStream_t s) {
+    dim3 grid((unsigned)((nx + BX - 1) / BX), (unsigned)((ny + BY - 1) / BY), 1);
+    launch(k_arrival_start, grid, dim3(BX, BY), 0, s, arrival, z, h, nx, ny, pitch, thr);
 }
 
 void gc_launch_arrival(const GcLayerDev &L, int step, float thr, cudaStream_t s) {

@@ -90,7 +90,9 @@ void sponge_launch_(const int *lid);
  * FIX_TOP (1: the top edge blends C2*YN1 instead of the C1*YN1 of
  * all_grids.f90:1357).  Call before gcomcot_init_layer_ of that child. */
 void gcomcot_set_sc_tables_(int *id, int *pos, float *cxy, int *nx, int *ny, int *parent_modscm, int *fix_top);
-/* no counterpart in the reference: arrival-step tracking on the outer layer */
+/* no counterpart in the reference: arrival-step tracking on the outer layer
+ * (the first outer step after which a wet cell's surface exceeds `thr`; 0 for
+ * a wet cell already above it at this call, -1 until then elsewhere) */
 void gcomcot_set_arrival_(int *id, float *thr);
 void gcomcot_get_arrival_(int *arrival, int *id);
 

@@ -1433,9 +1433,18 @@ void ocl_maxamp(ocl_layer *L) {
         if (!(L->zmax[c] >= L->z2[c])) L->zmax[c] = L->z2[c];
 }
 
+void ocl_arrival_start(ocl_layer *L, double thr) {
+    /* arrival at the start of tracking: step 0 for a wet cell (H > GX) whose
+     * surface is already above thr, -1 (not yet) elsewhere */
+    size_t n = (size_t)L->nx * L->ny;
+    REAL t = R(thr);
+    for (size_t c = 0; c < n; c++) L->arrival[c] = (L->h[c] > R(CC_GX) && L->z1[c] > t) ? 0 : -1;
+}
+
 void ocl_arrival(ocl_layer *L, int step, double thr) {
     /* arrival step: the first outer step after which a wet cell (H > GX)
-     * has Z2 > thr; -1 until then.  The reference has no arrival-time
+     * has Z2 > thr; 0 where the surface was above thr when tracking began
+     * (ocl_arrival_start), -1 until then.  The reference has no arrival-time
      * product; this definition is shared with the CUDA kernels. */
     size_t n = (size_t)L->nx * L->ny;
     REAL t = R(thr);

@@ -72,6 +72,7 @@ void ocl_sponge(ocl_layer *L);
  * layer with axes x[nx], y[ny] (degrees, or metres for laycord 1) */
 void ocl_sponge_coef(int nx, int ny, int laycord, const REAL *x, const REAL *y, const REAL *h, REAL *coefx,
                      REAL *coefy);
+void ocl_arrival_start(ocl_layer *L, double thr);
 void ocl_arrival(ocl_layer *L, int step, double thr);
 void ocl_all_grid(ocl_layer *layers, int n);
 void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr);

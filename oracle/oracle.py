@@ -35,6 +35,7 @@ def load(dtype=np.float32):
         build()
     lib = C.CDLL(str(path))
     lib.ocl_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+    lib.ocl_arrival_start.argtypes = [C.c_void_p, C.c_double]
     lib.ocl_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ocl_run.restype = C.c_int
@@ -119,6 +120,8 @@ class OracleRun:
         self.fields = []
         for k, L in enumerate(case.layers):
             self.fields.append(self._fill(self.arr[k], L, k == 0, coefs64[k] if coefs64 else None))
+        # arrival at the start: step 0 where a wet cell is already above the threshold
+        self.lib.ocl_arrival_start(C.addressof(self.arr[0]), float(case.arrival_thr))
 
     def _a(self, x, dt=None):
         a = np.ascontiguousarray(x, dtype=dt or self.dtype)
