@@ -119,3 +119,28 @@ def test_division_shortcuts_are_ieee_identities():
         assert np.isnan(f32(0.0) / f32(0.0))
         assert (f32(0.0) / f32(-2.0)).view(np.uint32) != f32(0.0).view(np.uint32)
         assert np.isnan(f32(0.0) / f32(np.nan))
+
+
+def test_arrival_definition(oracle_mod):
+    """Arrival step (no counterpart in the reference; the CUDA paths share this
+    definition): 0 on a wet cell whose initial surface is already above the
+    threshold, else the first outer step after which its surface is above it,
+    -1 where that never happens and on dry cells.  The expectation is built
+    from the surfaces of a step-by-step run, then compared with one run of
+    all the steps."""
+    case = _case(seed=17)
+    L = case.root
+    thr = np.float32(case.arrival_thr)
+    wet = L.H > np.float32(1e-5)            # CC_GX
+    nsteps = 25
+    step_by_step = oracle_mod.OracleRun(case)
+    expect = np.where(wet & (L.Z0 > thr), 0, -1).astype(np.int32)
+    assert np.array_equal(step_by_step.layer(0)["arrival"], expect)
+    for k in range(1, nsteps + 1):
+        step_by_step.run(1)
+        z = step_by_step.layer(0)["z"]
+        expect = np.where((expect < 0) & wet & (z > thr), k, expect).astype(np.int32)
+    whole = oracle_mod.OracleRun(case)
+    whole.run(nsteps)
+    assert np.array_equal(whole.layer(0)["arrival"], expect)
+    assert (expect == 0).sum() > 0 and (expect > 0).sum() > 0 and (expect < 0).sum() > 0
