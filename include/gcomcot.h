@@ -92,7 +92,8 @@ void sponge_launch_(const int *lid);
 void gcomcot_set_sc_tables_(int *id, int *pos, float *cxy, int *nx, int *ny, int *parent_modscm, int *fix_top);
 /* no counterpart in the reference: arrival-step tracking on the outer layer
  * (the first outer step after which a wet cell's surface exceeds `thr`; 0 for
- * a wet cell already above it at this call, -1 until then elsewhere) */
+ * a wet cell already above it at this call, -1 until then elsewhere).  Call
+ * it after gcomcot_init_layer_ of the outer layer. */
 void gcomcot_set_arrival_(int *id, float *thr);
 void gcomcot_get_arrival_(int *arrival, int *id);
 
