@@ -86,6 +86,7 @@ SIGNATURES = {
     "gc_engine_add_member": (C.c_int, [VP, C.c_int, P_F, C.c_int, C.c_int, P_I, P_F, C.c_float]),
     "gc_engine_step": (C.c_int, [VP, C.c_int]),
     "gc_engine_member_done": (C.c_int, [VP, C.c_int]),
+    "gc_engine_member_steps": (C.c_int, [VP, C.c_int]),
     "gc_engine_sync": (C.c_int, [VP]),
     "gc_engine_read": (C.c_int, [VP, C.c_int, P_F, P_F, P_F, P_F, P_I, P_F]),
     "gc_engine_release": (C.c_int, [VP, C.c_int]),

@@ -28,14 +28,28 @@ def _i(v):
 
 
 class ReferenceSession:
-    def __init__(self, case: Case, fusion: bool = True, arrival: bool = False, init_layers: bool = True):
+    def __init__(self, case: Case, fusion: bool = True, arrival: bool = False, init_layers: bool = True,
+                 host_cache: dict | None = None):
+        """host_cache: a dict shared by sessions over the same layers; the
+        Fortran-order arrays of a layer (all but its surface) are built once
+        and kept there, as a Fortran caller holds them for the whole run"""
         self.lib = _lib.load()
         self.case = case
         self.lib.gcomcot_init_gpu_()
         self.lib.gcomcot_set_fusion(1 if fusion else 0)
         self._keep = []
         # the host arrays a Fortran caller already holds (LO%R1 ... LO%Z), built once
-        self._host = {L.id: self._host_arrays(L) for L in case.layers}
+        self._host = {}
+        for L in case.layers:
+            key = (id(L.H), L.id)
+            if host_cache is not None and key in host_cache:
+                a = dict(host_cache[key])
+                a["Z"] = np.ascontiguousarray(L.Z0, dtype=F32)
+            else:
+                a = self._host_arrays(L)
+                if host_cache is not None:
+                    host_cache[key] = a
+            self._host[L.id] = a
         if init_layers:
             self.init_layers()
         if arrival:

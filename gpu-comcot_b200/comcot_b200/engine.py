@@ -172,6 +172,13 @@ class Engine:
     def done(self, mid: int) -> bool:
         return self.lib.gc_engine_member_done(self.h, mid) == 1
 
+    def steps_done(self, mid: int) -> int:
+        """outer steps the member has been issued (complete after sync())"""
+        rc = self.lib.gc_engine_member_steps(self.h, mid)
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_member_steps failed: {rc}")
+        return rc
+
     def read(self, mid: int, fields=("z", "m", "n", "zmax", "arrival", "ts")) -> dict:
         """results of a member (the named fields only); nested members also
         give child_z/child_m/child_n when "child" is among the fields or the

@@ -176,6 +176,64 @@ class ForecastServer:
         return requests
 
 
+class PlainServer:
+    """The plain path a warning centre runs without batching: one request at
+    a time, in arrival order, through the reference C ABI exactly as the
+    Fortran driver calls it (layer upload, then per step MASS, OPEN,
+    ALL_GRID, MOMENT, MAX_AMP and the gauge stencils, one kernel per phase),
+    products read back when the run ends.  Serves the same traces as
+    ForecastServer so their latencies compare on equal terms."""
+
+    def __init__(self, fusion: bool = False):
+        from .abi import ReferenceSession
+
+        self._session = ReferenceSession
+        self.fusion = fusion
+        self.host_cache = {}   # Fortran-order arrays per layer, as the caller holds them
+
+    def prepare(self, requests):
+        """builds the callers' host arrays of every grid class in the trace"""
+        for r in requests:
+            s = self._session(r.case, fusion=self.fusion, init_layers=False, host_cache=self.host_cache)
+            s.close()
+
+    def run_one(self, r: Request) -> dict:
+        s = self._session(r.case, fusion=self.fusion, arrival=True, host_cache=self.host_cache)
+        try:
+            st = s.drive(r.case.nsteps, maxamp=True)
+            res = {"zmax": s.getzmax(1), "arrival": s.getarrival(1), "ts": gauge_series(st, r.case.gauges)}
+        finally:
+            s.close()
+        return res
+
+    def serve(self, requests, speed: float = 1.0, clock=time.perf_counter):
+        for r in requests:
+            r.t_arrival_wall = r.t_arrival / speed if np.isfinite(speed) else 0.0
+        t0 = clock()
+        for r in sorted(requests, key=lambda q: q.t_arrival_wall):
+            wait = r.t_arrival_wall - (clock() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            r.t_admit = clock() - t0
+            r.result = self.run_one(r)
+            r.status = "done"
+            r.t_done = clock() - t0
+        return requests
+
+
+def gauge_series(stencils, gauges):
+    """GET_TS (output.f90:1078-1090): bilinear interpolation of the 2x2
+    stencils [nsteps, ngauges, 4] in float32, left to right"""
+    st = np.asarray(stencils, dtype=np.float32)
+    out = np.zeros(st.shape[:2], np.float32)
+    one = np.float32(1.0)
+    for g, (_lid, _ki, _kj, cx, cy) in enumerate(gauges):
+        cx, cy = np.float32(cx), np.float32(cy)
+        l1, l2, l3, l4 = (st[:, g, q] for q in range(4))
+        out[:, g] = l1 * (one - cx) * (one - cy) + l2 * cx * (one - cy) + l3 * (one - cx) * cy + l4 * cx * cy
+    return out
+
+
 def percentiles(x, qs=(50, 99)):
     x = np.sort(np.asarray(x, dtype=np.float64))
     return {f"p{q}": float(np.percentile(x, q)) for q in qs}

@@ -880,6 +880,12 @@ int gc_engine_member_done(gc_engine *e, int id) {
     return e->members[id].done ? 1 : 0;
 }
 
+int gc_engine_member_steps(gc_engine *e, int id) {
+    if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used) return GC_EINVAL;
+    const EngMember &M = e->members[id];
+    return std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
+}
+
 int gc_engine_read(gc_engine *e, int id, float *z, float *m, float *n, float *zmax, int *arrival, float *ts) {
     if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used) return GC_EINVAL;
     EngMember &M = e->members[id];

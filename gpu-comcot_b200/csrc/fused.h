@@ -61,6 +61,8 @@ cudaError_t gc_fused_launch_multi(int variant, const GcFusedGrid *d_grids, const
 int gc_fused_max_ctas(int variant, bool multi = true);
 /* 1 if a pipeline wait in the fused kernel gave up since the last call (clears it) */
 int gc_fused_take_error();
+/* clears that flag in stream order on `s` */
+cudaError_t gc_fused_clear_error_async(cudaStream_t s);
 /* single grid, descriptor by value */
 cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cudaStream_t s);
 /* single grid at step step_off + *d_step_base (d_step_base may be NULL) */

@@ -34,6 +34,8 @@
  * Arithmetic is evaluated in the Fortran order with separately rounded
  * float operations (the library is built with -fmad=false).
  */
+#include <atomic>
+#include <mutex>
 #include <type_traits>
 
 #include "fused.h"
@@ -651,13 +653,24 @@ int variant_smem(const Variant &v) {
     return v.w * ((v.fl & FL_ZD) ? warp_smem_bytes<FL_ZD>(v.s) : warp_smem_bytes<0>(v.s));
 }
 
+/* the dynamic shared-memory limit of a variant's kernels, set once per
+ * device (the attribute belongs to the device that is current when it is set) */
+constexpr int kMaxDevices = 64;
+static_assert(kNumVariants <= 64, "one flag per variant");
+std::atomic<uint64_t> g_prepared[kMaxDevices];
+std::mutex g_prepare_mu;
+
 void prepare(const Variant &v) {
-    static bool done[64] = {false};
-    int idx = (int)(&v - kVariants);
-    if (done[idx]) return;
+    const int idx = (int)(&v - kVariants);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+    const uint64_t bit = 1ull << idx;
+    if (g_prepared[dev].load(std::memory_order_acquire) & bit) return;
+    std::lock_guard<std::mutex> lock(g_prepare_mu);
+    if (g_prepared[dev].load(std::memory_order_relaxed) & bit) return;
     cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
     cudaFuncSetAttribute(v.multi, cudaFuncAttributeMaxDynamicSharedMemorySize, variant_smem(v));
-    done[idx] = true;
+    g_prepared[dev].fetch_or(bit, std::memory_order_release);
 }
 
 } // namespace
@@ -688,6 +701,14 @@ int gc_fused_take_error() {
     cudaMemcpyFromSymbol(&v, g_pipe_error, sizeof v);
     if (v) cudaMemcpyToSymbol(g_pipe_error, &z, sizeof z);
     return v;
+}
+
+/* clears the pipeline-error flag in stream order (no host memory involved) */
+cudaError_t gc_fused_clear_error_async(cudaStream_t s) {
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_pipe_error);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(addr, 0, sizeof(int), s);
 }
 
 GcTileCfg gc_fused_variant(int v) {

@@ -159,6 +159,9 @@ int gc_engine_add_member(gc_engine *e, int cls, const float *z0, int nsteps, int
 int gc_engine_step(gc_engine *e, int nsteps);
 /* 1 once the member has run all its steps (after gc_engine_sync) */
 int gc_engine_member_done(gc_engine *e, int member);
+/* outer steps the member has been issued so far (complete after
+ * gc_engine_sync); gc_engine_read returns the state after that many steps */
+int gc_engine_member_steps(gc_engine *e, int member);
 int gc_engine_sync(gc_engine *e);
 /* results of a member: any pointer may be NULL */
 int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
@@ -253,9 +256,13 @@ typedef struct {
  * acceptable): one outer step (MASS_S + OPEN + MOMT_S + max) of every grid in
  * one launch on `stream`, with its work list in a fixed array built into the
  * library (at most 64 grids and 24576 tiles of 128 columns; larger requests
- * return -1).  Calls share that array: calls that overlap on the GPU race.
- * The first call on a device does a one-time set-up and should come before any
- * stream capture.  Returns 0 or a negative status. */
+ * return -1).  The grid list travels in the launch parameters of a small
+ * kernel that fills the array, so nothing is copied from host memory and the
+ * call returns once its work is queued.  Calls share that array: calls that
+ * overlap on the GPU race.  The first call on a device does a one-time set-up
+ * and should come before any stream capture.  A bounded pipeline wait that
+ * gives up is reported by gcomcot_sync() (GC_ETIMEOUT) after the caller has
+ * synchronised `stream`.  Returns 0 or a negative status. */
 int gcomcot_fused_step_noalloc(int ngrids, const gc_grid_step_io *grids, void *stream);
 
 #ifdef __cplusplus

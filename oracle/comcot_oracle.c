@@ -18,7 +18,7 @@
 #include <string.h>
 
 #include "comcot_oracle.h"
-#include "comcot_consts.h"
+#include "oracle_consts.h"
 #include "comcot_math.h"
 
 #define R(x) ((REAL)(x))
@@ -26,13 +26,23 @@
 #define MAX(a, b) ((a) > (b) ? (a) : (b))
 #define MIN(a, b) ((a) < (b) ? (a) : (b))
 
-/* elementary functions: shared deterministic versions in float, libm in the twin */
+/* elementary functions: the deterministic versions the library also uses
+ * (comcot_math.h) in float, libm in the FP64 twin.  Built with -DOCL_LIBM the
+ * float build calls libm's expf/powf instead, an independent check that the
+ * shared functions hide no error (tests/test_oracle_libm_cpu.py). */
+#ifdef OCL_LIBM
+#define O_EXPF(x) expf(x)
+#define O_POWF(x, y) powf((x), (y))
+#else
+#define O_EXPF(x) cc_expf(x)
+#define O_POWF(x, y) cc_powf((x), (y))
+#endif
 static inline REAL o_exp(REAL x) {
-    if (sizeof(REAL) == sizeof(float)) return (REAL)cc_expf((float)x);
+    if (sizeof(REAL) == sizeof(float)) return (REAL)O_EXPF((float)x);
     return (REAL)exp((double)x);
 }
 static inline REAL o_pow(REAL x, REAL y) {
-    if (sizeof(REAL) == sizeof(float)) return (REAL)cc_powf((float)x, (float)y);
+    if (sizeof(REAL) == sizeof(float)) return (REAL)O_POWF((float)x, (float)y);
     return (REAL)pow((double)x, (double)y);
 }
 static inline REAL o_sqrt(REAL x) {

@@ -25,11 +25,16 @@ def build(quiet=True):
                    stdout=subprocess.DEVNULL if quiet else None)
 
 
-def load(dtype=np.float32):
-    key = np.dtype(dtype).name
+def load(dtype=np.float32, libm=False):
+    """the float oracle, its FP64 twin, or (libm=True) the float build whose
+    exp/pow are libm's expf/powf instead of the shared comcot_math.h ones"""
+    key = np.dtype(dtype).name + ("_libm" if libm else "")
     if key in _libs:
         return _libs[key]
-    name = "liboracle_f32.so" if key == "float32" else "liboracle_f64.so"
+    if libm and np.dtype(dtype) != np.float32:
+        raise ValueError("the libm build is a float build")
+    name = {"float32": "liboracle_f32.so", "float64": "liboracle_f64.so",
+            "float32_libm": "liboracle_f32_libm.so"}[key]
     path = BUILD / name
     if not path.exists():
         build()
@@ -110,10 +115,10 @@ class OLayer(C.Structure):
 class OracleRun:
     """Oracle state for every layer of a case."""
 
-    def __init__(self, case, dtype=np.float32, coefs64=None):
+    def __init__(self, case, dtype=np.float32, coefs64=None, libm=False):
         self.case = case
         self.dtype = np.dtype(dtype)
-        self.lib = load(self.dtype)
+        self.lib = load(self.dtype, libm=libm)
         n = len(case.layers)
         self.arr = (OLayer * n)()
         self.keep = []
