@@ -57,7 +57,7 @@ WORKLOADS = {"c1": "C1: 361x301 2' linear spherical, Gaussian hump, OPEN, max-et
              "c2": "C2: 2401x2001 1' linear spherical, OPEN, max-eta, 32 gauges, dt 1 s"}
 FORECAST_STEPS = {"c1": 3600, "c2": 7200}  # one whole forecast of the config
 FALLBACK_HBM_GBS = 6650.0
-BYTES_PER_CELL = 36  # Z1,M1,N1,H in + Z2,M2,N2 out (28 B) + max-eta read/write (8 B)
+BYTES_PER_CELL = 36  # per launch: Z1,M1,N1,H in + Z,M,N out (28 B) + max-eta read/write (8 B)
 TOL = 1e-4           # max|d eta| <= 1e-4 max|eta|, max|d(M,N)| <= 1e-4 max|M,N|
 GX = np.float32(1e-5)
 
@@ -224,6 +224,14 @@ def parity_record(got, ref, steps, H=None, ts=None, ts_ref=None, child=None, chi
     return rec
 
 
+def steps_per_launch(variant):
+    """2 when the engine's chosen candidate is the two-step kernel
+    (candidates past the one-step variants x their tile-height rules)"""
+    from comcot_b200 import _lib
+
+    return 2 if variant >= 2 * _lib.load().gc_engine_num_variants() else 1
+
+
 def merge_parity(records):
     """one summary over several parity records"""
     return {"within_tolerance": all(r["within_tolerance"] for r in records),
@@ -308,7 +316,7 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
     case = Case("C4", [L], steps)
     tune_reps = 2
     ncand = _lib.load().gc_engine_num_candidates()  # tile variants x tile-height rules
-    extra = ncand * (tune_reps + 1) + warmup  # the autotuner's steps
+    extra = ncand * (2 * tune_reps + 2) + warmup  # the autotuner's steps (two-step candidates run pairs)
     eng = Engine(budget=120 << 30)
     eng.config(variant=variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
@@ -384,9 +392,11 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
             recs.append(parity_record(plain_state, st[steps]["layers"][0], steps, H=L.H,
                                       what="plain path scenario 0 (reference ABI, per phase)"))
     peak, peak_kind = peaks()
-    bpc = 24.0 + 4.0 / nscen + 8.0  # per member-cell: Z,M,N in/out, shared H, max-eta r/w
-    achieved = bpc * cells * nscen / (ms * 1e-3 / steps) / 1e9
-    tr = profiled_traffic("fused_ensemble_step_c4.txt", "traffic_bytes_per_member_launch")
+    spl = steps_per_launch(chosen)
+    bpc = 24.0 + 4.0 / nscen + 8.0  # per member-cell and launch: Z,M,N in/out, shared H, max-eta r/w
+    achieved = bpc * cells * nscen / (ms * 1e-3 / steps * spl) / 1e9
+    tr = profiled_traffic("pair_ensemble_step_c4.txt" if spl == 2 else "fused_ensemble_step_c4.txt",
+                          "traffic_bytes_per_member_launch")
     rec = {"metric": "ensemble scenarios/hour", "value": scen_per_hour, "unit": "scenarios/hour",
            "steps": steps, "warmup": warmup, "ms_per_step": ms / steps, "cell_updates_per_s": value_cells,
            "config": {"workload": f"C4: {nscen} dipole scenarios on 1201x1001 2' linear spherical, shared H, "
@@ -396,7 +406,7 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": None if tr is None else nscen * tr,
                         "peak_kind": f"{peak_kind} (copy bandwidth)",
-                        "algorithmic_bytes_per_launch": bpc * cells * nscen},
+                        "algorithmic_bytes_per_launch": bpc * cells * nscen, "steps_per_launch": spl},
            "clocks": ck, "gpu_launches": launches, "parity": merge_parity(recs)}
     if plain:
         rec["plain_path"] = plain
@@ -540,7 +550,7 @@ def run_c3(args, torch, dist, rank, world, local):
 # ---------------------------------------------------------------------------
 # C5: serving
 # ---------------------------------------------------------------------------
-def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, rank=0, world=1):
+def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, rank=0, world=1, dist=None):
     """C5 serving: a seeded Poisson stream of forecast requests (mean `rate`
     req/s; outer grids 481x401, 961x801 or 1921x1601 at 2'; 30 % nested with
     a 301x251 ratio-5 nonlinear child; 30-120 simulated minutes at dt 2 s; a
@@ -568,7 +578,7 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
             big = [serving.Request(0, 0.0, synth.c5_request_case(tpl, (1921, 1601), 64, False, 77))]
         with Engine(budget=16 << 30) as eng:
             for r in big:
-                eng.add(r.case, nsteps=3 * _lib.load().gc_engine_num_candidates() + 8)
+                eng.add(r.case, nsteps=6 * _lib.load().gc_engine_num_candidates() + 8)
             eng.autotune(2)
             variant = eng.variant()  # variant + variants x tile-height rule
     budget = int(budget_gb * (1 << 30))
@@ -591,6 +601,22 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
     lat = np.array([r.latency for r in reqs])
     span = max(r.t_done for r in reqs)
     pl = serving.percentiles(lat)
+    ranks = None
+    if dist is not None and world > 1:
+        # every rank's latencies to rank 0 through the group's store, with a
+        # bounded wait: a rank that died is reported, not waited for
+        store = replicas.default_store(dist)
+        if store is not None:
+            hb = replicas.Heartbeat(store, rank, world)
+            got, missing, stale = replicas.collect(store, rank, world, {"lat": lat.tolist(), "span": span},
+                                                   timeout_s=300.0, hb=hb)
+            if rank == 0:
+                lat = np.concatenate([np.asarray(g["lat"], dtype=np.float64) for g in got.values()])
+                span = max(g["span"] for g in got.values())
+                pl = serving.percentiles(lat)
+                served = len(lat)
+                ranks = {"ranks_reporting": sorted(got), "ranks_missing": missing, "ranks_stale": stale,
+                         "requests_unserved": nreq - served}
     # 2) saturation: every request at t = 0
     reqs_sat = make_requests()
     torch.cuda.synchronize()
@@ -642,11 +668,13 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
                                   "30-120 min at dt 2 s, 16 gauges", "hbm_budget_gb": budget_gb,
                       "graph_chunk": chunk, "tile_variant": variant},
            "p50_s": pl["p50"], "p99_s": pl["p99"], "mean_s": float(lat.mean()), "max_s": float(lat.max()),
-           "scenarios_per_hour_under_load": len(reqs) * 3600.0 / span,
+           "scenarios_per_hour_under_load": len(lat) * 3600.0 / span,
            "scenarios_per_hour_saturated": capacity, "saturated_seconds": sat_s,
            "cell_updates_per_s_saturated": cell_updates / sat_s,
            "max_active": max_active, "max_active_saturated": sat_active, "admission_waits": refused,
            "clocks": ck, "gpu_launches": launches, "parity": merge_parity(recs)}
+    if ranks:
+        rec["replicas"] = ranks
     if plain_rec:
         rec["plain_path"] = plain_rec
         rec["capacity_vs_plain"] = capacity / plain_rec["scenarios_per_hour"]
@@ -656,7 +684,7 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
 
 def run_c5(args, torch, dist, rank, world, local):
     rec = bench_c5(torch, local, args.requests, args.rate, args.budget_gb, args.chunk, args.variant,
-                   plain=not args.no_plain, rank=rank, world=world)
+                   plain=not args.no_plain, rank=rank, world=world, dist=dist)
     line = {"metric": rec["metric"], "value": rec["value"], "unit": "s", "n_gpus": world, "steps": rec["steps"],
             "warmup": 3, "ms_per_step": None, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
@@ -688,7 +716,7 @@ def run_single(args, torch, dist, rank, world, local):
     tune_reps = 3
     lib = _lib.load()
     ncand = lib.gc_engine_num_candidates()  # the autotuner's candidates: tile variants x tile-height rules
-    total = ncand * (tune_reps + 1) + args.warmup + args.steps + 8
+    total = ncand * (2 * tune_reps + 2) + args.warmup + args.steps + 8  # two-step candidates run pairs
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)
     cells = case.root.nx * case.root.ny
@@ -763,9 +791,10 @@ def run_single(args, torch, dist, rank, world, local):
         s.close()
 
     peak, peak_kind = peaks()
-    bytes_launch = BYTES_PER_CELL * cells
-    achieved = bytes_launch / (ms * 1e-3 / args.steps) / 1e9
-    traffic = profiled_traffic()
+    spl = steps_per_launch(variant)
+    bytes_launch = BYTES_PER_CELL * cells  # per launch: one step, or two in the two-step kernel
+    achieved = bytes_launch / (ms * 1e-3 / args.steps * spl) / 1e9
+    traffic = profiled_traffic("pair_linear_step_c2.txt" if spl == 2 else "fused_linear_step_c2.txt")
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -778,7 +807,7 @@ def run_single(args, torch, dist, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": f"{peak_kind} (copy bandwidth)",
-                     "algorithmic_bytes_per_launch": bytes_launch},
+                     "algorithmic_bytes_per_launch": bytes_launch, "steps_per_launch": spl},
         "clocks": ck,
         "gpu_launches": launches,
     }

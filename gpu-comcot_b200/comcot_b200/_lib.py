@@ -79,6 +79,8 @@ SIGNATURES = {
     "gcomcot_set_fusion": (None, [C.c_int]),
     "gcomcot_sync": (C.c_int, []),
     "gcomcot_stream": (VP, []),
+    "gcomcot_set_wait_limit": (None, [C.c_int]),
+    "gcomcot_inject_stall": (None, []),
     "gcomcot_drive": (C.c_int, [C.c_int, C.c_int, C.c_int, P_I, P_I, P_I, P_F]),
     "gc_engine_create": (C.c_int, [C.c_longlong, C.POINTER(VP)]),
     "gc_engine_destroy": (C.c_int, [VP]),
@@ -88,6 +90,7 @@ SIGNATURES = {
     "gc_engine_member_done": (C.c_int, [VP, C.c_int]),
     "gc_engine_member_steps": (C.c_int, [VP, C.c_int]),
     "gc_engine_sync": (C.c_int, [VP]),
+    "gc_engine_query": (C.c_int, [VP]),
     "gc_engine_read": (C.c_int, [VP, C.c_int, P_F, P_F, P_F, P_F, P_I, P_F]),
     "gc_engine_release": (C.c_int, [VP, C.c_int]),
     "gc_engine_bytes_in_use": (C.c_longlong, [VP]),

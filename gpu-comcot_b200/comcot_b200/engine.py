@@ -169,6 +169,13 @@ class Engine:
         if rc != 0:
             raise RuntimeError(f"gc_engine_sync failed: {rc}")
 
+    def idle(self) -> bool:
+        """True when everything issued so far has finished (does not wait)"""
+        rc = self.lib.gc_engine_query(self.h)
+        if rc < 0:
+            raise RuntimeError(f"gc_engine_query failed: {rc}")
+        return rc == 1
+
     def done(self, mid: int) -> bool:
         return self.lib.gc_engine_member_done(self.h, mid) == 1
 

@@ -84,3 +84,29 @@ def gather(store, world: int, timeout_s: float, poll_s: float = 0.02):
             break
         time.sleep(poll_s)
     return got, [r for r in range(world) if r not in got]
+
+
+def default_store(dist):
+    """the key-value store of the default process group (None where the
+    build does not expose it)"""
+    try:
+        from torch.distributed import distributed_c10d as c10d
+
+        return c10d._get_default_store()
+    except Exception:
+        return None
+
+
+def collect(store, rank: int, world: int, summary: dict, timeout_s: float, hb: Heartbeat | None = None):
+    """every rank publishes its summary; rank 0 waits at most timeout_s for
+    the others and returns ({rank: summary}, missing ranks, ranks whose
+    heartbeat is older than timeout_s); other ranks return (None, None, None).
+    A rank that died is reported, not waited for."""
+    if hb is not None:
+        hb.beat()
+    publish(store, rank, summary)
+    if rank != 0:
+        return None, None, None
+    got, missing = gather(store, world, timeout_s)
+    stale = hb.dead(stale_s=timeout_s) if hb is not None else []
+    return got, missing, stale

@@ -126,24 +126,32 @@ class ForecastServer:
         active = []
         idle_refusals = 0
         t0 = clock()
-        while pending or waiting or active:
+
+        def take_arrivals():
+            """queues what has arrived, drops cancelled requests, admits in
+            arrival order while the budget has room; returns the admissions"""
             t = clock() - t0
             while pending and pending[0].t_arrival_wall <= t:
                 waiting.append(pending.popleft())
-            # cancellations of queued requests
             for r in list(waiting):
                 if r.rid in self._cancel or t >= r.t_arrival_wall + r.cancel_at:
                     waiting.remove(r)
                     r.status, r.t_done = "cancelled", t
+            n = 0
             while waiting and self._try_admit(waiting[0]):
                 r = waiting.popleft()
                 r.t_admit = clock() - t0
-                idle_refusals = 0
+                n += 1
                 if r.status == "rejected":
                     r.t_done = r.t_admit
                 else:
                     active.append(r)
             self.max_active = max(self.max_active, len(active))
+            return n
+
+        while pending or waiting or active:
+            if take_arrivals():
+                idle_refusals = 0
             if not active:
                 if waiting:
                     # nothing runs, so nothing will free memory: retry a few times
@@ -160,6 +168,11 @@ class ForecastServer:
                     time.sleep(max(0.0, min(0.002, pending[0].t_arrival_wall - (clock() - t0))))
                 continue
             self.eng.step(self.chunk)
+            # while the chunk runs: arrivals are admitted now (their state is
+            # uploaded behind the chunk) and join at the next one
+            while not self.eng.idle():
+                take_arrivals()
+                time.sleep(0.0002)
             self.eng.sync()
             still = []
             t = clock() - t0

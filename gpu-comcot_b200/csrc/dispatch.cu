@@ -98,9 +98,14 @@ int gcomcot_sync(void) {
     gc_flush();
     GC_CUDA_OR_RET(cudaStreamSynchronize(gc_rt().stream));
     GC_CUDA_OR_RET(cudaGetLastError());
-    if (gc_fused_take_error()) return GC_ETIMEOUT;
+    const int a = gc_fused_take_error(), b = gc_pair_take_error();
+    if (a || b) return GC_ETIMEOUT;
     return GC_OK;
 }
+
+void gcomcot_set_wait_limit(int polls) { gc_pair_set_wait_limit(polls); }
+
+void gcomcot_inject_stall(void) { gc_pair_stall_next(); }
 
 /* the library's stream, for callers that time work with CUDA events */
 void *gcomcot_stream(void) { return (void *)gc_rt().stream; }

@@ -69,7 +69,11 @@ struct EngMember {
     float thr = -1.0f;
     void *block = nullptr;
     size_t bytes = 0;
-    float *z[2] = {nullptr, nullptr}, *m[2] = {nullptr, nullptr}, *n[2] = {nullptr, nullptr};
+    /* time levels: nested members ping-pong two buffers (level L in L & 1);
+     * single-grid members keep three (level L in L % 3), so a two-step
+     * launch writes level L + 2 to a buffer it does not read */
+    int nbuf = 3;
+    float *z[3] = {nullptr, nullptr, nullptr}, *m[3] = {nullptr, nullptr, nullptr}, *n[3] = {nullptr, nullptr, nullptr};
     float *zmax = nullptr, *ts = nullptr, *gw = nullptr;
     int *arrival = nullptr, *gij = nullptr;
     /* nested members: the child's levels, DZ, the outer grid's NEWQ caches */
@@ -85,6 +89,8 @@ struct EngMember {
     /* the last global step this member needs a launch at: single-grid
      * members sample their last gauges in the launch after their last step */
     int last_step() const { return nested ? step0 + nsteps - 1 : step0 + nsteps; }
+    /* the buffer holding the level after `done` steps */
+    int level_buf(int done) const { return nbuf == 3 ? done % 3 : (done & 1); }
 };
 
 size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -166,6 +172,13 @@ struct gc_engine {
     long long chunk_launches = 0; /* kernels in one replay of the chunk graph */
     int pdl = 1;                  /* programmatic dependent launch (GCOMCOT_PDL=0 turns it off) */
     int ty_rule = 1;              /* tile-height rule (gc_fused_pick_ty), tuned with the variant */
+    /* two steps per launch (kernels_pair.cu) for the single-grid members */
+    int pair_on = 1;              /* the chosen candidate uses it */
+    int pair_allowed = 1;         /* GCOMCOT_PAIR=0 turns it off altogether */
+    int pair_variant = 0, pair_rule = 0;
+    bool pair_ok = false;         /* the current members allow it */
+    int2 *d_ptiles = nullptr;
+    int ptiles_cap = 0, nptiles = 0;
     int *d_health = nullptr;      /* one int for gc_engine_member_health */
     std::vector<int> nested_ids; /* active nested members */
     cudaStream_t aux[kMaxAux] = {};
@@ -297,19 +310,21 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
  * and device step step_off0 + *d_base: the fused launch over the single-grid
  * members on the engine stream, each nested member's chain on a forked
  * stream, joined back before return */
-static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count);
+static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count, int pair_room);
 
 /* the engine's kernels go out with programmatic dependent launch: each one
  * is scheduled while its predecessor in the stream runs and waits for it on
  * the device, which hides the launch gap of a chain of short kernels */
-static cudaError_t eng_launch_steps(gc_engine *e, const int *d_base, int step_off0, int count) {
+static cudaError_t eng_launch_steps(gc_engine *e, const int *d_base, int step_off0, int count, int pair_room) {
     gc_set_pdl(e->pdl != 0);
-    cudaError_t err = eng_launch_steps_(e, d_base, step_off0, count);
+    cudaError_t err = eng_launch_steps_(e, d_base, step_off0, count, pair_room);
     gc_set_pdl(false);
     return err;
 }
 
-static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count) {
+/* pair_room: how many of the `count` steps may go two at a time (every
+ * single-grid member computes both steps of a pair) */
+static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_off0, int count, int pair_room) {
     const int nn = (int)e->nested_ids.size();
     const int naux = std::min(nn, kMaxAux);
     if (naux > 0) {
@@ -321,7 +336,20 @@ static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_o
         }
     }
     if (e->ntiles > 0) {
-        for (int k = 0; k < count; k++) {
+        /* two steps per launch while both lie inside every member's window
+         * (the launch after a member's last step only samples its gauges) */
+        int k = 0;
+        if (e->pair_ok)
+            for (; k + 1 < count && k + 2 <= pair_room; k += 2) {
+                cudaError_t err = e->single
+                                      ? gc_pair_launch_one_at(e->pair_variant, e->one_grid, d_base, step_off0 + k,
+                                                              e->stream)
+                                      : gc_pair_launch_multi(e->pair_variant, e->d_grids, e->d_ptiles, e->nptiles,
+                                                             d_base, step_off0 + k, e->stream);
+                if (err != cudaSuccess) return err;
+                e->launches++;
+            }
+        for (; k < count; k++) {
             cudaError_t err = e->single ? gc_fused_launch_one_at(e->variant, e->one_grid, d_base, step_off0 + k, e->stream)
                                         : gc_fused_launch_multi(e->variant, e->d_grids, e->d_tiles, e->ntiles, d_base,
                                                                 step_off0 + k, e->nctas, e->stream);
@@ -376,6 +404,11 @@ static int eng_rebuild(gc_engine *e) {
     const bool single = anx.size() == 1;
     const int ty = anx.empty() ? 16 : gc_fused_pick_ty(e->variant, (int)anx.size(), anx.data(), any.data(),
                                                        e->ty_rule, !single);
+    const int pty = anx.empty() ? 32 : gc_pair_pick_ty(e->pair_variant, (int)anx.size(), anx.data(), any.data(),
+                                                       e->pair_rule, !single);
+    /* two-step launches need at most 64 gauges per member */
+    bool pair_ok = e->pair_on != 0 && e->pair_allowed != 0 && !anx.empty();
+    std::vector<int2> ptiles;
     /* active members grouped by class */
     for (size_t c = 0; c < e->classes.size(); c++) {
         EngClass &C = e->classes[c];
@@ -392,7 +425,10 @@ static int eng_rebuild(gc_engine *e) {
             g.step0 = M.step0; g.cur0 = 0; g.nsteps = M.nsteps;
             g.flags = GC_F_MAXAMP | (M.thr >= 0.0f ? GC_F_ARRIVAL | GC_F_ARR_BYMAX : 0);
             g.thr = M.thr;
-            for (int q = 0; q < 2; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
+            g.nbuf = 3;
+            g.pty = pty;
+            gc_pair_tiles(C.nx, C.ny, pty, &g.ptiles_x);
+            for (int q = 0; q < 3; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
             g.h = M.h ? M.h : C.d_h; g.rows = C.d_rows;
             g.zmax = M.zmax; g.arrival = M.arrival;
             g.ng = M.ng; g.gij = M.gij; g.gw = M.gw; g.ts = M.ts; g.ts_len = M.nsteps;
@@ -402,6 +438,11 @@ static int eng_rebuild(gc_engine *e) {
         int nt = gc_fused_tiles(C.nx, C.ny, ty, nullptr);
         for (int t = 0; t < nt; t++)
             for (int g : idx) tiles.push_back(make_int2(g, t));
+        const int npt = gc_pair_tiles(C.nx, C.ny, pty, nullptr);
+        for (int t = 0; t < npt; t++)
+            for (int g : idx) ptiles.push_back(make_int2(g, t));
+        for (int g : idx)
+            if (grids[g].ng > 64) pair_ok = false;
     }
     if (eng_make_aux(e, (int)e->nested_ids.size()) != GC_OK) return GC_ECUDA;
     /* the outer grid of a nested member is stepped alone on its own stream */
@@ -429,6 +470,16 @@ static int eng_rebuild(gc_engine *e) {
     if (e->ntiles)
         GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_tiles, tiles.data(), tiles.size() * sizeof(int2),
                                        cudaMemcpyHostToDevice, e->stream));
+    e->nptiles = (int)ptiles.size();
+    if (e->nptiles > e->ptiles_cap) {
+        if (e->d_ptiles) cudaFreeAsync(e->d_ptiles, e->stream);
+        e->ptiles_cap = std::max(e->nptiles, 2 * e->ptiles_cap);
+        GC_CUDA_OR_RET(cudaMallocAsync((void **)&e->d_ptiles, (size_t)e->ptiles_cap * sizeof(int2), e->stream));
+    }
+    if (e->nptiles)
+        GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_ptiles, ptiles.data(), ptiles.size() * sizeof(int2),
+                                       cudaMemcpyHostToDevice, e->stream));
+    e->pair_ok = pair_ok;
     /* the host copies above are from pageable memory and complete before return */
     e->nctas = e->ntiles;
     if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
@@ -452,7 +503,7 @@ static cudaError_t eng_build_graph(gc_engine *e) {
     long long before = e->launches;
     cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    cudaError_t lerr = eng_launch_steps(e, e->d_step, 1, e->chunk);
+    cudaError_t lerr = eng_launch_steps(e, e->d_step, 1, e->chunk, e->chunk);
     if (lerr == cudaSuccess) k_advance<<<1, 32, 0, e->stream>>>(e->d_step, e->chunk);
     cudaError_t cerr = cudaStreamEndCapture(e->stream, &graph);
     e->chunk_launches = e->launches - before + 1; /* + k_advance */
@@ -473,14 +524,20 @@ static int eng_issue(gc_engine *e, int nsteps) {
         if (e->ntiles == 0 && e->nested_ids.empty()) break;
         /* steps until the next member finishes: the member set is constant */
         int horizon = nsteps - issued;
+        /* steps that every single-grid member computes (not only samples) */
+        int room = horizon;
         for (auto &M : e->members)
-            if (M.used && !M.done) horizon = std::min(horizon, M.last_step() - e->gstep);
+            if (M.used && !M.done) {
+                horizon = std::min(horizon, M.last_step() - e->gstep);
+                if (!M.nested) room = std::min(room, M.step0 + M.nsteps - 1 - e->gstep);
+            }
         if (horizon <= 0) horizon = 1;
-        if (e->use_graphs && horizon >= e->chunk) {
+        if (room < 0) room = 0;
+        if (e->use_graphs && horizon >= e->chunk && (!e->pair_ok || room >= e->chunk)) {
             /* the device counter must equal the host's step count */
             GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_step, &e->gstep, sizeof(int), cudaMemcpyHostToDevice, e->stream));
             if (!e->gexec) GC_CUDA_OR_RET(eng_build_graph(e));
-            int reps = horizon / e->chunk;
+            int reps = (e->pair_ok ? std::min(horizon, room) : horizon) / e->chunk;
             if (reps * e->chunk > nsteps - issued) reps = (nsteps - issued) / e->chunk;
             if (reps <= 0) reps = 0;
             for (int r = 0; r < reps; r++) {
@@ -492,7 +549,7 @@ static int eng_issue(gc_engine *e, int nsteps) {
             if (reps > 0) continue;
         }
         int n = std::min(horizon, nsteps - issued);
-        if (eng_launch_steps(e, nullptr, e->gstep + 1, n) != cudaSuccess) return GC_ECUDA;
+        if (eng_launch_steps(e, nullptr, e->gstep + 1, n, room) != cudaSuccess) return GC_ECUDA;
         e->gstep += n;
         issued += n;
     }
@@ -526,6 +583,8 @@ int gc_engine_create(long long hbm_budget_bytes, gc_engine **out) {
     if (v) { e->variant = atoi(v); e->tuned = true; }
     const char *pd = getenv("GCOMCOT_PDL");
     if (pd && pd[0] == '0') e->pdl = 0;
+    const char *pr = getenv("GCOMCOT_PAIR");
+    if (pr && pr[0] == '0') e->pair_on = e->pair_allowed = 0;
     *out = e;
     return GC_OK;
 }
@@ -543,6 +602,7 @@ int gc_engine_destroy(gc_engine *e) {
     }
     if (e->d_grids) cudaFreeAsync(e->d_grids, e->stream);
     if (e->d_tiles) cudaFreeAsync(e->d_tiles, e->stream);
+    if (e->d_ptiles) cudaFreeAsync(e->d_ptiles, e->stream);
     if (e->d_step) cudaFreeAsync(e->d_step, e->stream);
     if (e->d_health) cudaFreeAsync(e->d_health, e->stream);
     cudaStreamSynchronize(e->stream);
@@ -591,7 +651,8 @@ static size_t eng_member_bytes(const EngClass &C, int nsteps, int ngauges, bool 
     size_t field = a256((size_t)C.pitch * C.ny * sizeof(float));
     size_t tsb = a256((size_t)nsteps * ngauges * sizeof(float));
     size_t gb = a256((size_t)2 * ngauges * sizeof(int)) + a256((size_t)2 * ngauges * sizeof(float));
-    size_t bytes = (own_h ? 9 : 8) * field + tsb + gb;
+    /* single-grid members: three levels of Z, M, N; nested: two */
+    size_t bytes = ((C.nested ? 8 : 11) + (own_h ? 1 : 0)) * field + tsb + gb;
     if (C.nested) {
         size_t cfield = a256((size_t)C.cpitch * C.cny * sizeof(float));
         bytes += 7 * cfield + a256((size_t)2 * C.nx * sizeof(float)) + a256((size_t)2 * C.ny * sizeof(float))
@@ -629,7 +690,8 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
     M.nested = C.nested;
     GC_CUDA_OR_RET(cudaMallocAsync(&M.block, bytes, e->stream));
     char *p = (char *)M.block;
-    for (int q = 0; q < 2; q++) {
+    M.nbuf = C.nested ? 2 : 3;
+    for (int q = 0; q < M.nbuf; q++) {
         M.z[q] = (float *)p; p += field;
         M.m[q] = (float *)p; p += field;
         M.n[q] = (float *)p; p += field;
@@ -639,7 +701,7 @@ static int eng_add_member(gc_engine *e, int cls, const float *z0, const float *c
     M.ts = (float *)p; p += tsb;
     M.gij = (int *)p; p += a256((size_t)2 * ngauges * sizeof(int));
     M.gw = (float *)p; p += a256((size_t)2 * ngauges * sizeof(float));
-    GC_CUDA_OR_RET(cudaMemsetAsync(M.block, 0, 6 * field, e->stream));
+    GC_CUDA_OR_RET(cudaMemsetAsync(M.block, 0, (size_t)3 * M.nbuf * field, e->stream));
     GC_CUDA_OR_RET(cudaMemsetAsync(M.arrival, 0xff, field, e->stream));
     if (own_h) {
         /* still water, then the faults' deformation on Z and on the member's own H */
@@ -870,8 +932,17 @@ int gc_engine_sync(gc_engine *e) {
     if (!e) return GC_EINVAL;
     GC_CUDA_OR_RET(cudaStreamSynchronize(e->stream));
     GC_CUDA_OR_RET(cudaGetLastError());
-    if (gc_fused_take_error()) return GC_ETIMEOUT;
+    const int a = gc_fused_take_error(), b = gc_pair_take_error();
+    if (a || b) return GC_ETIMEOUT;
     return GC_OK;
+}
+
+int gc_engine_query(gc_engine *e) {
+    if (!e) return GC_EINVAL;
+    const cudaError_t q = cudaStreamQuery(e->stream);
+    if (q == cudaErrorNotReady) return 0;
+    GC_CUDA_OR_RET(q);
+    return 1;
 }
 
 int gc_engine_member_done(gc_engine *e, int id) {
@@ -892,7 +963,7 @@ int gc_engine_read(gc_engine *e, int id, float *z, float *m, float *n, float *zm
     EngClass &C = e->classes[M.cls];
     /* level 1 after the member's completed steps */
     int done_steps = std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
-    int cur = done_steps & 1;
+    int cur = M.level_buf(done_steps);
     size_t sp = (size_t)C.pitch * sizeof(float), dp = (size_t)C.nx * sizeof(float);
     auto dl = [&](void *dst, const void *src) {
         return cudaMemcpy2DAsync(dst, dp, src, sp, dp, (size_t)C.ny, cudaMemcpyDeviceToHost, e->stream);
@@ -928,9 +999,12 @@ int gc_engine_read_child(gc_engine *e, int id, float *z, float *m, float *n) {
 }
 
 /* Scans the member's max-eta and current surfaces (outer grid and child).
- * The running maximum keeps a NaN once one appeared, so a NaN or Inf at any
- * past step shows.  Returns 0 (healthy), a bit set (1: a NaN or Inf,
- * 2: |eta| above `bound` metres) or a negative status. */
+ * The running maximum does not keep a NaN (a NaN maximum is replaced by the
+ * next surface), but a NaN in a wet cell's surface persists: every stencil
+ * operation and clamp of the step passes it on, so the current surface
+ * shows it.  An Inf or |eta| beyond the bound shows in either field.
+ * Returns 0 (healthy), a bit set (1: a NaN or Inf, 2: |eta| above `bound`
+ * metres) or a negative status. */
 int gc_engine_member_health(gc_engine *e, int id, float bound) {
     if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used || !(bound > 0.0f))
         return GC_EINVAL;
@@ -939,7 +1013,7 @@ int gc_engine_member_health(gc_engine *e, int id, float bound) {
     if (!e->d_health) GC_CUDA_OR_RET(cudaMallocAsync((void **)&e->d_health, sizeof(int), e->stream));
     GC_CUDA_OR_RET(cudaMemsetAsync(e->d_health, 0, sizeof(int), e->stream));
     const int done_steps = std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
-    const int cur = done_steps & 1;
+    const int cur = M.level_buf(done_steps);
     k_health<<<256, 256, 0, e->stream>>>(M.zmax, C.nx, C.ny, C.pitch, bound, e->d_health);
     k_health<<<256, 256, 0, e->stream>>>(M.z[cur], C.nx, C.ny, C.pitch, bound, e->d_health);
     e->launches += 2;
@@ -966,14 +1040,36 @@ int gc_engine_release(gc_engine *e, int id) {
 
 long long gc_engine_bytes_in_use(gc_engine *e) { return e ? e->in_use : GC_EINVAL; }
 
+/* candidates: c < nv * R1 is the one-step kernel, variant c % nv with
+ * tile-height rule c / nv; above that the two-step kernel, variant p % np
+ * with rule p / np (p = c - nv * R1) */
+constexpr int GC_PAIR_RULES = 2;
+
+static int eng_num_candidates() {
+    return gc_fused_num_variants() * GC_TY_RULES + gc_pair_num_variants() * GC_PAIR_RULES;
+}
+
+static bool eng_set_candidate(gc_engine *e, int c) {
+    const int nv = gc_fused_num_variants(), n1 = nv * GC_TY_RULES, np = gc_pair_num_variants();
+    if (c < 0 || c >= eng_num_candidates()) return false;
+    if (c < n1) {
+        e->variant = c % nv;
+        e->ty_rule = c / nv;
+        e->pair_on = 0;
+    } else {
+        const int q = c - n1;
+        e->pair_variant = q % np;
+        e->pair_rule = q / np;
+        e->pair_on = 1;
+    }
+    e->dirty = true;
+    return true;
+}
+
 int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk) {
     if (!e) return GC_EINVAL;
     if (variant >= 0) {
-        /* variant + num_variants * rule selects a tile-height rule as well */
-        const int nv = gc_fused_num_variants();
-        if (variant >= nv * GC_TY_RULES) return GC_EINVAL;
-        e->variant = variant % nv;
-        e->ty_rule = variant / nv;
+        if (!eng_set_candidate(e, variant)) return GC_EINVAL;
         e->tuned = true;
     }
     e->use_graphs = use_graphs ? 1 : 0;
@@ -983,36 +1079,36 @@ int gc_engine_config(gc_engine *e, int variant, int use_graphs, int graph_chunk)
     return GC_OK;
 }
 
-/* Times `reps` real steps of every tile variant on the current members and
- * keeps the fastest.  Every variant computes bit-identical results, so the
+/* Times real steps of every candidate on the current members and keeps the
+ * fastest per step.  Every candidate computes bit-identical results, so the
  * tuning steps are ordinary steps of the run. */
 int gc_engine_autotune(gc_engine *e, int reps) {
     if (!e || reps < 1) return GC_EINVAL;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    int best = e->variant, best_rule = e->ty_rule;
+    const int nv = gc_fused_num_variants(), n1 = nv * GC_TY_RULES;
+    int best = -1;
     float best_ms = 3.0e38f;
     int saved_graphs = e->use_graphs;
     e->use_graphs = 0;
-    for (int v = 0; v < gc_fused_num_variants(); v++) {
-        for (int rule = 0; rule < GC_TY_RULES; rule++) {
-            e->variant = v;
-            e->ty_rule = rule;
-            e->dirty = true;
-            if (eng_issue(e, 1) < 0) return GC_ECUDA; /* warm */
-            cudaEventRecord(a, e->stream);
-            int got = eng_issue(e, reps);
-            cudaEventRecord(b, e->stream);
-            cudaEventSynchronize(b);
-            if (got < reps) break;
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, a, b);
-            if (ms < best_ms) { best_ms = ms; best = v; best_rule = rule; }
-        }
+    for (int c = 0; c < eng_num_candidates(); c++) {
+        if (c >= n1 && !e->pair_allowed) break;
+        eng_set_candidate(e, c);
+        const int n = c >= n1 ? 2 * reps : reps; /* whole pairs */
+        if (eng_issue(e, c >= n1 ? 2 : 1) < 0) return GC_ECUDA; /* warm */
+        cudaEventRecord(a, e->stream);
+        int got = eng_issue(e, n);
+        cudaEventRecord(b, e->stream);
+        cudaEventSynchronize(b);
+        if (got < n) break;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        ms /= (float)got;
+        if (ms < best_ms) { best_ms = ms; best = c; }
     }
-    e->variant = best;
-    e->ty_rule = best_rule;
+    if (best < 0) best = e->pair_allowed ? n1 : 16;
+    eng_set_candidate(e, best);
     e->tuned = true;
     e->use_graphs = saved_graphs;
     e->dirty = true;
@@ -1031,9 +1127,14 @@ int gc_engine_prepare(gc_engine *e) {
     return GC_OK;
 }
 
-int gc_engine_variant(gc_engine *e) { return e ? e->variant + gc_fused_num_variants() * e->ty_rule : GC_EINVAL; }
+int gc_engine_variant(gc_engine *e) {
+    if (!e) return GC_EINVAL;
+    if (e->pair_on && e->pair_allowed)
+        return gc_fused_num_variants() * GC_TY_RULES + e->pair_variant + gc_pair_num_variants() * e->pair_rule;
+    return e->variant + gc_fused_num_variants() * e->ty_rule;
+}
 int gc_engine_num_variants(void) { return gc_fused_num_variants(); }
-int gc_engine_num_candidates(void) { return gc_fused_num_variants() * GC_TY_RULES; }
+int gc_engine_num_candidates(void) { return eng_num_candidates(); }
 
 void *gc_engine_stream(gc_engine *e) { return e ? (void *)e->stream : nullptr; }
 long long gc_engine_launches(gc_engine *e) { return e ? e->launches : GC_EINVAL; }

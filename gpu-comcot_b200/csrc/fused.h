@@ -22,7 +22,12 @@ struct GcFusedGrid {
     int nsteps;       /* steps this grid runs; the step after the last only samples gauges */
     int flags;        /* GC_F_MAXAMP | GC_F_ARRIVAL */
     float thr;        /* arrival threshold */
-    float *z[2], *m[2], *n[2];
+    /* time levels: nbuf 2 (or 0): level L of the window in buffer cur0 ^ (L & 1);
+     * nbuf 3: level L in buffer L % 3 (the engine's single-grid members, which
+     * the two-step kernel also steps) */
+    int nbuf;
+    int ptiles_x, pty; /* two-step kernel: tiles along I and rows per tile */
+    float *z[3], *m[3], *n[3];
     const float *h, *rows, *r2, *r4;
     float *zmax;
     int *arrival;
@@ -69,5 +74,28 @@ cudaError_t gc_fused_launch_one(int variant, const GcFusedGrid &g, int step, cud
 cudaError_t gc_fused_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
                                    cudaStream_t s);
 int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x);
+
+/* ---- two steps per launch (kernels_pair.cu): grids with nbuf 3, the
+ * outermost layer only, factored R2/R4, max-eta on, arrival by max-eta,
+ * at most 64 gauges; both steps inside every grid's window ---- */
+int gc_pair_num_variants();
+GcTileCfg gc_pair_variant(int v);
+/* tiles of one grid: tile t stores columns [120t+4, 120t+123] (the first
+ * [0, 123], the last to the grid's edge) x ty rows */
+int gc_pair_tiles(int nx, int ny, int ty, int *tiles_x);
+int gc_pair_max_ctas(int variant, bool multi = true);
+int gc_pair_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule, bool multi = true);
+/* steps (*d_step_base + step_off) and the next one */
+cudaError_t gc_pair_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
+                                  cudaStream_t s);
+cudaError_t gc_pair_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles, int ntiles,
+                                 const int *d_step_base, int step_off, cudaStream_t s);
+/* 1 if a pipeline wait of the two-step kernel gave up since the last call (clears it) */
+int gc_pair_take_error();
+/* polls before a pipeline wait of the two-step kernel gives up (default 2^22) */
+void gc_pair_set_wait_limit(int polls);
+/* the next two-step launch makes its first warp wait for a row nothing
+ * delivers (no copy is issued for it): the bounded wait then gives up */
+void gc_pair_stall_next();
 
 #endif

@@ -222,13 +222,21 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
     const bool root = Gref.root != 0;
     const int local = step - step0; /* 0-based index of the step being computed */
     if (local < 0 || local > nsteps) return true;
-    const int cur = Gref.cur0 ^ (local & 1);
+    /* buffers of levels local and local + 1: ping-pong, or level L in L % 3 */
+    int cur, nxt;
+    if (Gref.nbuf == 3) {
+        cur = local % 3;
+        nxt = cur == 2 ? 0 : cur + 1;
+    } else {
+        cur = Gref.cur0 ^ (local & 1);
+        nxt = cur ^ 1;
+    }
     const float *__restrict__ z1 = Gref.z[cur];
     const float *__restrict__ m1 = Gref.m[cur];
     const float *__restrict__ n1 = Gref.n[cur];
-    float *__restrict__ z2 = Gref.z[cur ^ 1];
-    float *__restrict__ m2 = Gref.m[cur ^ 1];
-    float *__restrict__ n2 = Gref.n[cur ^ 1];
+    float *__restrict__ z2 = Gref.z[nxt];
+    float *__restrict__ m2 = Gref.m[nxt];
+    float *__restrict__ n2 = Gref.n[nxt];
     float *__restrict__ zmax = Gref.zmax;
     int *__restrict__ arrival = Gref.arrival;
     const bool do_max = (flags & GC_F_MAXAMP) != 0;

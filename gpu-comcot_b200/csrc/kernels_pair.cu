@@ -1,0 +1,684 @@
+/*
+ * Two linear-spherical time steps per pass over HBM, for sm_100a.
+ *
+ * One launch advances every grid of a work list by two outer steps: MASS_S
+ * (mass.f90:61-100), the OPEN radiation boundary of the outermost layer
+ * (boundaries.f90:22-202) and MOMT_S (moment.f90:65-149) at step A, then the
+ * same again at step B on step A's results, with the maximum-amplitude
+ * recorder (GPUOutput.cu:46-53) and the arrival record after each of them and
+ * the gauge samples (GET_TS, output.f90:1078-1090) of both surfaces.  Step A's
+ * surface and fluxes never leave the chip, so a step moves half the bytes of
+ * the one-step kernel (kernels_fused.cu): per cell and launch Z1, M1, N1, H
+ * and max-eta are read and Z3, M3, N3 and max-eta written, 36 bytes for two
+ * steps.
+ *
+ * Work decomposition: a warp computes a strip of 128 columns (lane l owns
+ * the four columns s+4l .. s+4l+3, as a float4) and marches down its rows.
+ * Every stencil neighbour along I is a warp shuffle of the adjacent lane's
+ * float4, so each lane reads only its own 16 bytes of a row: no halo loads,
+ * no shared-memory bank conflicts.  A step's results are exact only where all
+ * their inputs were, which loses at most two columns at each side of the
+ * strip per step; tiles therefore overlap, and a tile stores only its middle
+ * 120 columns (lanes 1..30).  At the grid's west and east edges no halo is
+ * needed (the perimeter cells use OPEN and the IM1 clamp, which read nothing
+ * beyond the edge), so the first tile stores 124 columns from column 0 and
+ * the last one runs to the grid's last column.  Along J, step B at output row
+ * j needs step A at rows j-1 .. j+2, and step A at row j needs the inputs of
+ * rows j-1 .. j+1: a tile of TY output rows reads rows j0-2 .. j0+TY+1.
+ *
+ * Each row's Z1, M1, N1, H, max-eta and 32-byte coefficient record arrive by
+ * 1-D bulk copies (cp.async.bulk, completing on an mbarrier) into an S-stage
+ * shared-memory ring private to the warp; a stage is read into registers as
+ * soon as it lands and refilled with the row S ahead.  What later rows need
+ * of earlier ones (step A's surface and fluxes of the two previous rows, step
+ * B's of the previous one) is carried in registers.
+ *
+ * Ping-pong: the engine keeps three time levels per member, level L in
+ * buffer L % 3, so a launch reading level L writes level L + 2 to a buffer no
+ * tile reads (the one-step kernel writes L + 1 the same way).  Level L + 1 is
+ * never stored.
+ *
+ * Every pipeline wait is bounded by the `wait_limit` launch parameter; a wait
+ * that gives up sets g_pair_error and the warp leaves once its copies in
+ * flight have landed (or a second bounded wait expired).  `stall` != 0 makes
+ * the first warp of the launch expect 16 bytes that no copy delivers on its
+ * first row (nothing is issued for that row), so a test can watch the bound
+ * work without any copy left in flight.
+ *
+ * Arithmetic follows the Fortran order with separately rounded float
+ * operations (the library is built with -fmad=false); both steps give the
+ * bits of two launches of the one-step kernel.
+ */
+#include "bulk_pipe.cuh"
+#include "fused.h"
+
+namespace {
+
+using namespace gcpipe;
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kPairOut = 120; /* columns an interior tile stores */
+
+__device__ int g_pair_error; /* set when a pipeline wait gave up */
+
+/* one stage holds one row of a warp strip (byte offsets) */
+struct PStage {
+    static constexpr int Z = 0, M = 512, N = 1024, H = 1536, X = 2048, C = 2560;
+    static constexpr int BYTES = 2688; /* 2592 rounded up to 128 */
+};
+
+template <int S>
+__host__ __device__ constexpr int pair_warp_bytes() {
+    return (S * PStage::BYTES + S * 8 + 127) / 128 * 128;
+}
+
+__device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
+__device__ __forceinline__ float shw(float v) { return __shfl_up_sync(FULL, v, 1); }   /* lane - 1 */
+__device__ __forceinline__ float she(float v) { return __shfl_down_sync(FULL, v, 1); } /* lane + 1 */
+__device__ __forceinline__ float comp(const float4 &v, int q) {
+    return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ float4 lds4(const char *p) { return *reinterpret_cast<const float4 *>(p); }
+
+/* OPEN on a perimeter cell of the outermost layer (boundaries.f90:42-200).
+ * h, m, n at (i,j); hs, ns at (i,j-1); mw at (i-1,j). */
+__device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h, float hs, float m, float mw,
+                                           float n, float ns) {
+    if (!(h > CC_GX)) return 0.0f;
+    float cc = sqrtf(CC_GRAV * h);
+    float zz;
+    bool corner = (i == 0 || i == nx - 1) && (j == 0 || j == ny - 1);
+    if (!corner) {
+        if (j == 0) {
+            float uh = 0.5f * (m + mw);
+            float uu = sqrtf(uh * uh + n * n);
+            zz = uu / cc;
+            if (n > 0.0f) zz = -zz;
+        } else if (j == ny - 1) {
+            float uh = 0.5f * (m + mw);
+            float uu = sqrtf(uh * uh + ns * ns);
+            zz = uu / cc;
+            if (ns < 0.0f) zz = -zz;
+        } else if (i == 0) {
+            float uh = (hs > CC_GX) ? 0.5f * (n + ns) : n;
+            float uu = sqrtf(uh * uh + m * m);
+            zz = uu / cc;
+            if (m > 0.0f) zz = -zz;
+        } else {
+            float uh = 0.5f * (n + ns);
+            float uu = sqrtf(uh * uh + mw * mw);
+            zz = uu / cc;
+            if (mw < 0.0f) zz = -zz;
+        }
+    } else {
+        float qx = (i == 0) ? m : mw;
+        float qy = (j == 0) ? n : ns;
+        float uh = sqrtf(qx * qx + qy * qy);
+        zz = uh / cc;
+        bool neg;
+        if (i == 0 && j == 0) neg = (qx > 0.0f || qy > 0.0f);
+        else if (j == 0) neg = (qx < 0.0f || qy > 0.0f);
+        else if (i == 0) neg = (qx > 0.0f || qy < 0.0f);
+        else neg = (qx < 0.0f || qy < 0.0f);
+        if (neg) zz = -zz;
+    }
+    if (fabs_(zz) > CC_UB) zz = 0.0f;
+    return zz;
+}
+
+/* MASS_S at one cell (mass.f90:82-95) */
+__device__ __forceinline__ float mass1(float z1, float m, float mw, float n, float ns, float h, float r1, float r11,
+                                       float r6, float r6m) {
+    float zz = z1 - r1 * (m - mw) - r11 * (n * r6 - ns * r6m);
+    zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+    zz = ((zz + h) <= CC_EPS) ? -h : zz;
+    return (h > CC_GX) ? zz : 0.0f;
+}
+
+/* the new surface of a lane's four cells at row r: OPEN on the perimeter
+ * (EDGE), MASS_S elsewhere.  mw: M at the column left of the first cell;
+ * ns, hs: N and H of row r-1 */
+template <bool EDGE>
+__device__ __forceinline__ float4 surface4(const float4 &z1, const float4 &m, float mw, const float4 &n,
+                                           const float4 &ns, const float4 &h, const float4 &hs, float r1, float r11,
+                                           float r6, float r6m, int ib, int r, int nx, int ny) {
+    const float mv[4] = {m.x, m.y, m.z, m.w}, nv[4] = {n.x, n.y, n.z, n.w}, nsv[4] = {ns.x, ns.y, ns.z, ns.w};
+    const float hv[4] = {h.x, h.y, h.z, h.w}, hsv[4] = {hs.x, hs.y, hs.z, hs.w}, zv[4] = {z1.x, z1.y, z1.z, z1.w};
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float w = q == 0 ? mw : mv[q - 1];
+        if constexpr (EDGE) {
+            const int i = ib + q;
+            if (i == 0 || i == nx - 1 || r == 0 || r == ny - 1)
+                o[q] = open_cell(i, r, nx, ny, hv[q], hsv[q], mv[q], w, nv[q], nsv[q]);
+            else
+                o[q] = mass1(zv[q], mv[q], w, nv[q], nsv[q], hv[q], r1, r11, r6, r6m);
+        } else {
+            o[q] = mass1(zv[q], mv[q], w, nv[q], nsv[q], hv[q], r1, r11, r6, r6m);
+        }
+    }
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
+/* MOMT_S, x direction, at row j (moment.f90:86-115): M' from M, the surface
+ * of row j and its east neighbour ze, N of rows j (nb) and j-1 (nc) with
+ * their east neighbours, H of row j with its east neighbour.  mdom: the
+ * domain test of the outer layer (I <= NX-1). */
+template <bool EDGE>
+__device__ __forceinline__ float4 flux_m4(const float4 &m, const float4 &z, float ze, const float4 &nb, float nbe,
+                                          const float4 &nc, float nce, const float4 &h, float he, float cx, float r3,
+                                          int ib, int nx) {
+    const float mv[4] = {m.x, m.y, m.z, m.w};
+    const float zv[5] = {z.x, z.y, z.z, z.w, ze}, nbv[5] = {nb.x, nb.y, nb.z, nb.w, nbe};
+    const float ncv[5] = {nc.x, nc.y, nc.z, nc.w, nce}, hv[5] = {h.x, h.y, h.z, h.w, he};
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float h0 = hv[q], hp1 = hv[q + 1];
+        const float tot_n = nbv[q] + nbv[q + 1] + ncv[q] + ncv[q + 1];
+        const float r2 = cx * (0.5f * (h0 + hp1));
+        float vm = mv[q] - r2 * (zv[q + 1] - zv[q]) + r3 * tot_n;
+        vm = (fabs_(vm) < CC_EPS) ? 0.0f : vm;
+        bool dom = true;
+        if constexpr (EDGE) dom = ib + q <= nx - 2;
+        o[q] = (dom && h0 > CC_GX && hp1 > CC_GX) ? vm : 0.0f;
+    }
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
+/* MOMT_S, y direction, at row j (moment.f90:117-145): N' from N of row j, the
+ * surfaces of rows j+1 (za) and j (zb), M of rows j (mb) and j+1 (ma) with
+ * their west neighbours, H of rows j and j+1.  ndom: J <= NY-1 and I <= NX. */
+template <bool EDGE>
+__device__ __forceinline__ float4 flux_n4(const float4 &n, const float4 &za, const float4 &zb, const float4 &mb,
+                                          float mbw, const float4 &ma, float maw, const float4 &h, const float4 &ha,
+                                          float cy, float r5, int ib, int j, int nx, int ny) {
+    const float nv[4] = {n.x, n.y, n.z, n.w}, zav[4] = {za.x, za.y, za.z, za.w}, zbv[4] = {zb.x, zb.y, zb.z, zb.w};
+    const float mbv[5] = {mbw, mb.x, mb.y, mb.z, mb.w}, mav[5] = {maw, ma.x, ma.y, ma.z, ma.w};
+    const float hv[4] = {h.x, h.y, h.z, h.w}, hav[4] = {ha.x, ha.y, ha.z, ha.w};
+    float o[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float tot_m = mbv[q] + mav[q] + mbv[q + 1] + mav[q + 1];
+        const float r4 = cy * (0.5f * (hv[q] + hav[q]));
+        float vn = nv[q] - r4 * (zav[q] - zbv[q]) - r5 * tot_m;
+        vn = (fabs_(vn) < CC_EPS) ? 0.0f : vn;
+        bool dom = true;
+        if constexpr (EDGE) dom = j <= ny - 2 && ib + q < nx;
+        o[q] = (dom && hv[q] > CC_GX && hav[q] > CC_GX) ? vn : 0.0f;
+    }
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
+/* max-eta: keeps the old value unless the new surface is above it */
+__device__ __forceinline__ float4 max4(const float4 &x, const float4 &z) {
+    return make_float4(x.x >= z.x ? x.x : z.x, x.y >= z.y ? x.y : z.y, x.z >= z.z ? x.z : z.z,
+                       x.w >= z.w ? x.w : z.w);
+}
+
+/* arrival by max-eta: a wet cell above the threshold whose maximum before
+ * this step was not arrives at `step` */
+__device__ __forceinline__ void arrive4(int *row, int ib, int lo, int hi, const float4 &z, const float4 &xo,
+                                        const float4 &h, float thr, int step) {
+    const float zv[4] = {z.x, z.y, z.z, z.w}, xv[4] = {xo.x, xo.y, xo.z, xo.w}, hv[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (ib + q >= lo && ib + q <= hi && zv[q] > thr && hv[q] > CC_GX && xv[q] <= thr) row[ib + q] = step;
+}
+
+/* store of a lane's four cells, masked to columns [lo, hi] */
+__device__ __forceinline__ void st4m(float *row, int ib, int lo, int hi, const float4 &v) {
+    if (ib >= lo && ib + 3 <= hi) {
+        *reinterpret_cast<float4 *>(row + ib) = v;
+    } else if (ib + 3 >= lo && ib <= hi) {
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (ib + q >= lo && ib + q <= hi) row[ib + q] = vv[q];
+    }
+}
+
+/* one gauge stencil from two rows held as float4 per lane (GET_TS weights) */
+__device__ __forceinline__ float gauge_sample(const float4 &lo_row, const float4 &hi_row, int ki, int s, float cx,
+                                              float cy) {
+    const int c0 = ki - s, c1 = ki + 1 - s;
+    const float l1 = __shfl_sync(FULL, comp(lo_row, c0 & 3), c0 >> 2);
+    const float l2 = __shfl_sync(FULL, comp(lo_row, c1 & 3), c1 >> 2);
+    const float l3 = __shfl_sync(FULL, comp(hi_row, c0 & 3), c0 >> 2);
+    const float l4 = __shfl_sync(FULL, comp(hi_row, c1 & 3), c1 >> 2);
+    const float a = l1 * (1.0f - cx) * (1.0f - cy);
+    const float b = l2 * (cx) * (1.0f - cy);
+    const float d = l3 * (1.0f - cx) * (cy);
+    const float e = l4 * (cx) * (cy);
+    return a + b + d + e;
+}
+
+/* tile geometry along I: tile t computes columns [s, s+127] and stores
+ * [lo, hi] (0-based, clipped to the grid) */
+__host__ __device__ __forceinline__ void pair_cols(int t, int nx, int &s, int &lo, int &hi) {
+    s = t == 0 ? 0 : kPairOut * t;
+    lo = t == 0 ? 0 : s + 4;
+    hi = s + 123;
+    if (hi + 4 >= nx - 1) hi = nx - 1; /* the last tile runs to the grid's edge */
+    if (hi > nx - 1) hi = nx - 1;
+}
+
+template <int S, bool EDGE>
+__device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, int hi, int j0, int ty, int local,
+                                          char *wsm, int &seq, int wait_limit, bool stall) {
+    static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
+    const int lane = threadIdx.x & 31;
+    const int nx = G.nx, ny = G.ny;
+    const size_t P = (size_t)G.pitch;
+    const int l0 = local % 3, l2 = (l0 + 2) % 3; /* buffers of levels L and L + 2 */
+    const bool do_arr = (G.flags & GC_F_ARRIVAL) != 0;
+    const float thr = G.thr;
+
+    /* rows: inputs rs .. rr (real rows), iterations rs .. re (rows past the
+     * grid's last carry nothing new; they finish the last rows' step B) */
+    const int jl = min(j0 + ty - 1, ny - 1); /* last output row */
+    const int rs = max(j0 - 2, 0), rr = min(j0 + ty + 1, ny - 1), re = min(j0 + ty + 1, ny + 1);
+    const int K = rr - rs + 1;
+    const uint32_t wbase = smem_u32(wsm);
+    const uint32_t bars = wbase + S * PStage::BYTES;
+    const int seq0 = seq;
+    /* copies of one row: columns [s, c1) of the strip */
+    const int c1 = min(s + 128, G.pitch);
+    const uint32_t cb = 4u * (uint32_t)(c1 - s);
+    /* row k of the tile (k = r - rs) lives in stage (seq0 + k) % S */
+    auto stage_of = [&](int k) { return (seq0 + k) % S; };
+    auto issue = [&](int k, bool fake) {
+        if (lane == 0) {
+            const int r = rs + k;
+            const int st = stage_of(k);
+            const uint32_t bar = bars + 8 * st, sb = wbase + st * PStage::BYTES;
+            const bool out = r >= j0 && r <= jl;
+            fence_proxy_async(); /* the warp's reads of this stage come first */
+            if (fake) {
+                mbar_expect_tx(bar, 16u); /* nothing will deliver these bytes */
+                return;
+            }
+            mbar_expect_tx(bar, (out ? 5u : 4u) * cb + 32u);
+            const size_t ro = (size_t)r * P + s;
+            bulk_g2s(sb + PStage::Z, G.z[l0] + ro, cb, bar);
+            bulk_g2s(sb + PStage::M, G.m[l0] + ro, cb, bar);
+            bulk_g2s(sb + PStage::N, G.n[l0] + ro, cb, bar);
+            bulk_g2s(sb + PStage::H, G.h + ro, cb, bar);
+            if (out) bulk_g2s(sb + PStage::X, G.zmax + ro, cb, bar);
+            bulk_g2s(sb + PStage::C, G.rows + (size_t)r * GC_ROWW, 32u, bar);
+        }
+    };
+    __syncwarp();
+    const int kk = min(S, K);
+    for (int k = 0; k < kk; k++) issue(k, stall && k == 0);
+    int issued = kk;
+
+    /* gauges whose base cell this tile owns (at most 64 per grid) */
+    const int ng = G.ng;
+    unsigned gm0 = 0, gm1 = 0;
+    if (ng > 0) {
+        const float *z1g = G.z[l0];
+        bool in0 = false, in1 = false;
+        for (int h = 0; h < 2; h++) {
+            const int g = lane + 32 * h;
+            bool in = false;
+            if (g < ng) {
+                const int ki = G.gij[2 * g] - 1, kj = G.gij[2 * g + 1] - 1;
+                in = ki >= lo && ki <= hi && kj >= j0 && kj <= jl;
+                /* the surface the previous launch left (level L) */
+                if (in && local > 0) {
+                    const size_t c = (size_t)kj * P + ki;
+                    const float l1 = z1g[c], l2v = z1g[c + 1], l3 = z1g[c + P], l4 = z1g[c + P + 1];
+                    const float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
+                    const float a = l1 * (1.0f - cx) * (1.0f - cy);
+                    const float b = l2v * (cx) * (1.0f - cy);
+                    const float d = l3 * (1.0f - cx) * (cy);
+                    const float e = l4 * (cx) * (cy);
+                    G.ts[(size_t)(local - 1) * ng + g] = a + b + d + e;
+                }
+            }
+            if (h == 0) in0 = in;
+            else in1 = in;
+        }
+        gm0 = __ballot_sync(FULL, in0);
+        gm1 = __ballot_sync(FULL, in1);
+    }
+
+    const int ib = s + 4 * lane;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    /* step A's results of earlier rows, carried in registers (p: row r-1,
+     * pp: row r-2) */
+    float4 z2p = zero4, m2p = zero4, m2pp = zero4, n2p = zero4, z3p = zero4;
+    float m2ppw = 0.f, n2pe = 0.f;
+    bool ok = true;
+    int k = 0; /* real rows consumed */
+    for (int r = rs; r <= re; r++) {
+        const bool real = r <= ny - 1;
+        /* this row's inputs */
+        float4 z1 = zero4, m1 = zero4, n1 = zero4, h = zero4;
+        float r1 = 0.f, r11 = 0.f, r6 = 0.f, r3 = 0.f, cx = 0.f;
+        if (real) {
+            const int st = stage_of(k);
+            const uint32_t par = (uint32_t)(((seq0 + k) / S) & 1);
+            const bool got = mbar_wait(bars + 8 * st, par, wait_limit);
+            ok = __all_sync(FULL, got) != 0;
+            if (!ok) break;
+            const char *sp = wsm + st * PStage::BYTES;
+            z1 = lds4(sp + PStage::Z + 16 * lane);
+            m1 = lds4(sp + PStage::M + 16 * lane);
+            n1 = lds4(sp + PStage::N + 16 * lane);
+            h = lds4(sp + PStage::H + 16 * lane);
+            const float4 ca = lds4(sp + PStage::C), cc = lds4(sp + PStage::C + 16);
+            r1 = ca.x; r11 = ca.y; r6 = ca.z; r3 = ca.w; cx = cc.y;
+            k++;
+        }
+        /* rows r-1 and r-2, still staged (JM1 = max(J-1,1): row "-1" is row 0) */
+        const int kp = r - 1 - rs, kpp = r - 2 - rs;
+        const char *spp_ = wsm + stage_of(kp >= 0 ? kp : 0) * PStage::BYTES;
+        const char *sppp = wsm + stage_of(kpp >= 0 ? kpp : (kp >= 0 ? kp : 0)) * PStage::BYTES;
+        float4 n1p, m1p, hp, hpp, xp;
+        float r1p, r11p, r6p, r3p, r5p, cxp, cyp, r6pp, r5pp, cypp;
+        if (kp >= 0) {
+            n1p = lds4(spp_ + PStage::N + 16 * lane);
+            m1p = lds4(spp_ + PStage::M + 16 * lane);
+            hp = lds4(spp_ + PStage::H + 16 * lane);
+            const float4 ca = lds4(spp_ + PStage::C), cc = lds4(spp_ + PStage::C + 16);
+            r1p = ca.x; r11p = ca.y; r6p = ca.z; r3p = ca.w; r5p = cc.x; cxp = cc.y; cyp = cc.z;
+        } else {
+            n1p = n1; m1p = m1; hp = h;
+            r1p = r1; r11p = r11; r6p = r6; r3p = r3; r5p = 0.f; cxp = cx; cyp = 0.f;
+        }
+        if (kpp >= 0) {
+            hpp = lds4(sppp + PStage::H + 16 * lane);
+            const float4 ca = lds4(sppp + PStage::C), cc = lds4(sppp + PStage::C + 16);
+            r6pp = ca.z; r5pp = cc.x; cypp = cc.z;
+        } else {
+            hpp = hp; r6pp = r6p; r5pp = r5p; cypp = cyp;
+        }
+        /* neighbours along I */
+        float m1w = shw(m1.w), m1pw = shw(m1p.w);
+        if (EDGE && ib == 0) { m1w = m1.x; m1pw = m1p.x; } /* IM1 = max(I-1,1) */
+        const float n1e = she(n1.x), he = she(h.x), n1pe = she(n1p.x), hpe = she(hp.x);
+
+        /* ---------------- step A ---------------- */
+        float4 z2 = zero4, m2 = zero4, n2 = zero4;
+        if (real && r >= j0 - 1)
+            z2 = surface4<EDGE>(z1, m1, m1w, n1, n1p, h, hp, r1, r11, r6, r > 0 ? r6p : 0.0f, ib, r, nx, ny);
+        if (real && r >= j0 && r <= j0 + ty) {
+            const float z2e = she(z2.x);
+            m2 = flux_m4<EDGE>(m1, z2, z2e, n1, n1e, n1p, n1pe, h, he, cx, r3, ib, nx);
+        }
+        /* N of row r-1 needs the surface of row r */
+        if (r - 1 >= max(j0 - 1, 0) && r - 1 <= j0 + ty && r - 1 <= ny - 2)
+            n2 = flux_n4<EDGE>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, cyp, r5p, ib, r - 1, nx, ny);
+        /* (N at the grid's last row stays 0: J <= NY-1 fails) */
+        /* gauges of step A: base row r-1, upper row r */
+        if ((gm0 | gm1) && r - 1 >= j0 && r - 1 <= jl) {
+            for (int h2 = 0; h2 < 2; h2++) {
+                unsigned bits = h2 == 0 ? gm0 : gm1;
+                while (bits) {
+                    const int g = __ffs(bits) - 1 + 32 * h2;
+                    bits &= bits - 1;
+                    if (G.gij[2 * g + 1] - 1 != r - 1) continue;
+                    const float v = gauge_sample(z2p, z2, G.gij[2 * g] - 1, s, G.gw[2 * g], G.gw[2 * g + 1]);
+                    if (lane == 0) G.ts[(size_t)local * ng + g] = v;
+                }
+            }
+        }
+
+        /* ---------------- step B ---------------- */
+        const int rb = r - 1; /* step B's surface row */
+        const float n2e = she(n2.x);
+        float4 z3 = zero4;
+        float m2w = shw(m2p.w);
+        if (EDGE && ib == 0) m2w = m2p.x;
+        if (rb >= j0 && rb <= min(j0 + ty, ny - 1)) {
+            const float4 nsb = (rb == 0) ? n2 : n2p; /* N of row rb-1, JM1 clamp at row 0 */
+            z3 = surface4<EDGE>(z2p, m2p, m2w, n2, nsb, hp, hpp, r1p, r11p, r6p, rb > 0 ? r6pp : 0.0f, ib, rb, nx,
+                                ny);
+            if (rb <= jl) {
+                /* max-eta and arrival after step A, then after step B */
+                xp = lds4(spp_ + PStage::X + 16 * lane);
+                const float4 xa = max4(xp, z2p), xb = max4(xa, z3);
+                const size_t ro = (size_t)rb * P;
+                float *zrow = G.z[l2] + ro;
+                st4m(zrow, ib, lo, hi, z3);
+                st4m(G.zmax + ro, ib, lo, hi, xb);
+                if (do_arr) {
+                    if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
+                        arrive4(G.arrival + ro, ib, lo, hi, z2p, xp, hp, thr, local + 1);
+                    if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
+                        arrive4(G.arrival + ro, ib, lo, hi, z3, xa, hp, thr, local + 2);
+                }
+                /* M of row rb */
+                const float z3e = she(z3.x);
+                const float4 ncb = (rb == 0) ? n2 : n2p;
+                const float nce = (rb == 0) ? n2e : n2pe;
+                const float4 m3 = flux_m4<EDGE>(m2p, z3, z3e, n2, n2e, ncb, nce, hp, hpe, cxp, r3p, ib, nx);
+                st4m(G.m[l2] + ro, ib, lo, hi, m3);
+            }
+        }
+        /* N of row rb-1 needs the surface of row rb */
+        if (rb - 1 >= j0 && rb - 1 <= jl) {
+            float4 n3 = zero4;
+            if (rb - 1 <= ny - 2)
+                n3 = flux_n4<EDGE>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, cypp, r5pp, ib, rb - 1, nx, ny);
+            st4m(G.n[l2] + (size_t)(rb - 1) * P, ib, lo, hi, n3);
+        }
+
+        /* ---------------- carry ---------------- */
+        z2p = z2;
+        m2pp = m2p; m2ppw = m2w; m2p = m2;
+        n2p = n2; n2pe = n2e;
+        z3p = z3;
+        /* row r-2 is no longer needed: refill its stage S rows ahead */
+        __syncwarp();
+        if (kpp >= 0 && kpp + S < K) {
+            issue(kpp + S, false);
+            issued = kpp + S + 1;
+        }
+    }
+    seq = seq0 + K;
+    if (!ok) {
+        /* record the failure, then give the copies still in flight a bounded
+         * chance to land before the warp leaves */
+        if (lane == 0) atomicExch(&g_pair_error, 1);
+        for (int q = k; q < issued; q++) {
+            const int n = seq0 + q;
+            mbar_wait(bars + 8 * (n % S), (uint32_t)((n / S) & 1), 1 << 12);
+        }
+        return false;
+    }
+    __syncwarp();
+    return true;
+}
+
+template <int S>
+__device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step, char *wsm, int &seq,
+                                          int wait_limit, bool stall) {
+    const int local = step - G.step0; /* step A's 0-based index */
+    /* both steps must lie in the window, and three time levels exist */
+    if (local < 0 || local + 1 >= G.nsteps || G.nbuf != 3) return true;
+    const int tx = lt % G.ptiles_x, tyi = lt / G.ptiles_x;
+    const int ty = G.pty, j0 = tyi * ty;
+    int s, lo, hi;
+    pair_cols(tx, G.nx, s, lo, hi);
+    /* a tile none of whose computed cells (halo rows and columns included)
+     * lies on the grid's perimeter or beyond it runs the body compiled
+     * without boundary logic */
+    const bool edge = !(s >= 1 && s + 127 <= G.nx - 2 && j0 - 2 >= 1 && j0 + ty + 1 <= G.ny - 2);
+    return edge ? pair_rows<S, true>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall)
+                : pair_rows<S, false>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall);
+}
+
+template <int W, int S, bool MULTI>
+__global__ void __launch_bounds__(32 * W) k_pair(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                  const int2 *__restrict__ tiles, int ntiles,
+                                                  const int *__restrict__ step_base, int step_off, int wait_limit,
+                                                  int stall) {
+    extern __shared__ __align__(128) char smem[];
+    /* programmatic dependent launch: the previous kernel in the stream has
+     * finished and its writes are visible past this point */
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int step = step_off + (step_base ? *step_base : 0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char *wsm = smem + warp * pair_warp_bytes<S>();
+    const uint32_t bars = smem_u32(wsm) + S * PStage::BYTES;
+    if (lane == 0) {
+        for (int q = 0; q < S; q++) mbar_init(bars + 8 * q, 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    int seq = 0;
+    bool first = stall != 0 && blockIdx.x == 0 && warp == 0;
+    for (int tile = blockIdx.x * W + warp; tile < ntiles; tile += gridDim.x * W) {
+        bool ok;
+        if (MULTI) {
+            const int2 w = tiles[tile];
+            ok = pair_tile<S>(grids[w.x], w.y, step, wsm, seq, wait_limit, first);
+        } else {
+            ok = pair_tile<S>(one, tile, step, wsm, seq, wait_limit, first);
+        }
+        first = false;
+        if (!ok) return;
+    }
+}
+
+struct PairVariant {
+    int w, s;
+    void (*one)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
+    void (*multi)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
+};
+
+#define GC_PVARIANT(W, S) {W, S, k_pair<W, S, false>, k_pair<W, S, true>}
+const PairVariant kPairVariants[] = {
+    GC_PVARIANT(4, 5), GC_PVARIANT(4, 4), GC_PVARIANT(2, 5), GC_PVARIANT(4, 6),
+};
+#undef GC_PVARIANT
+constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
+
+int pair_smem(const PairVariant &v) {
+    switch (v.s) {
+    case 4: return v.w * pair_warp_bytes<4>();
+    case 5: return v.w * pair_warp_bytes<5>();
+    default: return v.w * pair_warp_bytes<6>();
+    }
+}
+
+int g_wait_limit = 1 << 22; /* polls before a pipeline wait gives up */
+int g_stall_next = 0;       /* the next launch injects one stalled row */
+
+void prepare_pair(const PairVariant &v) {
+    static bool done[64][8];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    const int idx = (int)(&v - kPairVariants);
+    if (done[dev][idx]) return;
+    cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem(v));
+    cudaFuncSetAttribute(v.multi, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem(v));
+    done[dev][idx] = true;
+}
+
+cudaError_t launch_pair(void (*kern)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int),
+                        int ctas, int threads, int smem, cudaStream_t s, const GcFusedGrid &g,
+                        const GcFusedGrid *grids, const int2 *tiles, int ntiles, const int *step_base,
+                        int step_off) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = gc_pdl_on() ? 1 : 0;
+    const int stall = g_stall_next;
+    g_stall_next = 0;
+    return cudaLaunchKernelEx(&cfg, kern, g, grids, tiles, ntiles, step_base, step_off, g_wait_limit, stall);
+}
+
+} // namespace
+
+int gc_pair_num_variants() { return kNumPairVariants; }
+
+GcTileCfg gc_pair_variant(int v) {
+    if (v < 0 || v >= kNumPairVariants) v = 0;
+    return GcTileCfg{kPairVariants[v].w, kPairVariants[v].s};
+}
+
+int gc_pair_tiles(int nx, int ny, int ty, int *tiles_x) {
+    const int tx = nx <= 128 ? 1 : 1 + (nx - 128 + kPairOut - 1) / kPairOut;
+    if (tiles_x) *tiles_x = tx;
+    return tx * ((ny + ty - 1) / ty);
+}
+
+int gc_pair_max_ctas(int variant, bool multi) {
+    if (variant < 0 || variant >= kNumPairVariants) variant = 0;
+    const PairVariant &v = kPairVariants[variant];
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    prepare_pair(v);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, multi ? v.multi : v.one, 32 * v.w, pair_smem(v));
+    return sms * (per > 0 ? per : 1);
+}
+
+int gc_pair_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule, bool multi) {
+    const int slots = gc_pair_max_ctas(variant, multi) * gc_pair_variant(variant).warps;
+    auto tiles = [&](int ty) {
+        long long t = 0;
+        for (int g = 0; g < ngrids; g++) t += gc_pair_tiles(nx[g], ny[g], ty, nullptr);
+        return t;
+    };
+    /* a warp's time is about (rows + 4 halo rows) per tile; a launch lasts
+     * waves x that.  Rule 0: the height minimising it; rule 1: the same
+     * among heights of at least 24 rows (less halo per row when many waves) */
+    const int tmin = rule == 0 ? 8 : 24;
+    int best = 32;
+    long long best_cost = -1, best_waves = 0;
+    for (int ty = tmin; ty <= 256; ty++) {
+        const long long waves = (tiles(ty) + slots - 1) / slots;
+        const long long cost = waves * (ty + 4);
+        if (best_cost < 0 || cost < best_cost || (cost == best_cost && waves < best_waves)) {
+            best = ty;
+            best_cost = cost;
+            best_waves = waves;
+        }
+    }
+    return best;
+}
+
+cudaError_t gc_pair_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
+                                  cudaStream_t s) {
+    if (variant < 0 || variant >= kNumPairVariants) variant = 0;
+    const PairVariant &v = kPairVariants[variant];
+    const int ntiles = gc_pair_tiles(g.nx, g.ny, g.pty, nullptr);
+    prepare_pair(v);
+    return launch_pair(v.one, (ntiles + v.w - 1) / v.w, 32 * v.w, pair_smem(v), s, g, nullptr, nullptr, ntiles,
+                       d_step_base, step_off);
+}
+
+cudaError_t gc_pair_launch_multi(int variant, const GcFusedGrid *d_grids, const int2 *d_tiles, int ntiles,
+                                 const int *d_step_base, int step_off, cudaStream_t s) {
+    if (variant < 0 || variant >= kNumPairVariants) variant = 0;
+    const PairVariant &v = kPairVariants[variant];
+    if (ntiles <= 0) return cudaSuccess;
+    GcFusedGrid dummy;
+    memset(&dummy, 0, sizeof dummy);
+    prepare_pair(v);
+    return launch_pair(v.multi, (ntiles + v.w - 1) / v.w, 32 * v.w, pair_smem(v), s, dummy, d_grids, d_tiles,
+                       ntiles, d_step_base, step_off);
+}
+
+int gc_pair_take_error() {
+    int v = 0, z = 0;
+    cudaMemcpyFromSymbol(&v, g_pair_error, sizeof v);
+    if (v) cudaMemcpyToSymbol(g_pair_error, &z, sizeof z);
+    return v;
+}
+
+void gc_pair_set_wait_limit(int polls) { g_wait_limit = polls > 0 ? polls : (1 << 22); }
+void gc_pair_stall_next() { g_stall_next = 1; }

@@ -467,6 +467,237 @@ __device__ __forceinline__ void wave_breaking(float dz2c, float z2c, float z1c, 
  * reference's wherever a value is used: the two-back neighbours are read
  * only inside the advection span, whose cells are at least 10 from every
  * edge. */
+/* the stencil of one x face (I,J)-(I+1,J): names give the cell relative to
+ * (I,J): p = I+1, m = I-1, p2 = I+2, n = J+1, s = J-1, s2 = J-2; zpn etc.
+ * are the surface's corners for the modified-scheme term */
+struct XFace {
+    float h_c, h_p, hp_c, d_c, d_p, d_p2, d_m, d_cn, d_pn, d_cs, d_ps;
+    float z_c, z_p, z1_c, q_c, q_p, q_cs, q_ps, q_cn, q_pn, q_cs2, q_ps2;
+    float p_c, p_p, p_m, p_n, p_s;
+    float z_pn, z_ps, z_cn, z_cs;
+};
+/* the stencil of one y face (I,J)-(I,J+1): q = J+1, q2 = J+2, s = J-1,
+ * e = I+1, w = I-1, w2 = I-2 */
+struct YFace {
+    float h_c, h_q, hq_c, d_c, d_q, d_q2, d_s, d_e, d_eq, d_w, d_wq;
+    float z_c, z_q, z1_c, p_c, p_q, p_w, p_wq, p_e, p_eq, p_w2, p_w2q;
+    float q_c, q_q, q_s, q_e, q_w;
+    float z_eq, z_wq, z_e, z_w;
+};
+
+/* CONMOME / CONMOME_S x direction at one face (moment.f90:409-568,
+ * 1272-1384); `span`: inside the advection span */
+template <bool SPH>
+__device__ __forceinline__ float conmome_x(const GcLayerDev &L, const XFace &f, int j, int jy, bool span) {
+    const float konst = (L.fric_switch != 1) ? 0.5f * L.dt * CC_GRAV : 0.0f;
+    const float fm = L.fric_coef;
+    float dd = 0.0f, df = 0.0f, ff;
+    bool noflux = false;
+    if (f.h_c <= CC_ELMAX || f.hp_c <= CC_ELMAX) {
+        noflux = true;
+    } else {
+        if (f.d_c > CC_GX && f.d_p > CC_GX) {
+            dd = face2(f.d_c, f.d_p); df = face1(f.d_c, f.d_p);
+        } else if (f.d_c > CC_GX && f.d_p <= CC_GX && f.h_p + f.z_c > CC_GX) {
+            dd = SPH ? f.hp_c + 0.5f * (f.z_c + f.z_p) : 0.5f * f.d_c; df = dd;
+        } else if (f.d_c <= CC_GX && f.d_p > CC_GX && f.h_c + f.z_p > CC_GX) {
+            dd = SPH ? f.hp_c + 0.5f * (f.z_c + f.z_p) : 0.5f * f.d_p; df = dd;
+        } else {
+            noflux = true;
+        }
+        if (!noflux && dd < CC_GX) noflux = true;
+    }
+    if (noflux) return 0.0f;
+    if (df < CC_DFMIN) df = CC_DFMIN;
+    float xqq = 0.25f * (f.q_c + f.q_p + f.q_cs + f.q_ps);
+    if (L.fric_switch != 1) {
+        /* df >= DFMIN here unless it is NaN, so the power is positive */
+        const float fnum = konst * fm * fm * sqrtf(f.p_c * f.p_c + xqq * xqq);
+        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
+    } else {
+        ff = 0.0f;
+    }
+    const float cpx = SPH ? GC_ROW(L, GC_CX, j) : L.grx;
+    float xp = f.p_c - cpx * dd * (f.z_p - f.z_c);
+    if (L.modscm == 0 && j + 1 < jy) {
+        float scm = qdiv(cpx * dd, 12.0f) * ((f.z_pn - 2.0f * f.z_p + f.z_ps) - (f.z_cn - 2.0f * f.z_c + f.z_cs));
+        xp = xp - scm;
+    }
+    if (L.fric_switch != 1) xp = xp - ff * f.p_c;
+    if (SPH) xp = xp + 4.0f * GC_ROW(L, GC_R3, j) * xqq;
+    const float ax = SPH ? GC_ROW(L, GC_R1, j) : L.rx;   /* R21 = R1 */
+    const float ay = SPH ? L.rows2[2 * (size_t)j] : L.ry; /* R0 */
+    float dp1c = face1(f.d_c, f.d_p);
+    if (L.linchk == 1 && dp1c >= CC_GX && span) {
+        float advx, advy;
+        if (f.p_c < 0.0f) {
+            float dp1p = face1(f.d_p, f.d_p2);
+            if (dp1p < CC_GX || f.d_p < CC_GX)
+                advx = ax * (-(qdiv(f.p_c * f.p_c, dp1c)));
+            else
+                advx = ax * (qdiv(f.p_p * f.p_p, dp1p) - qdiv(f.p_c * f.p_c, dp1c));
+        } else {
+            float dp1m = face1(f.d_m, f.d_c);
+            if (dp1m < CC_GX || f.d_c < CC_GX)
+                advx = ax * (qdiv(f.p_c * f.p_c, dp1c));
+            else
+                advx = ax * (qdiv(f.p_c * f.p_c, dp1c) - qdiv(f.p_m * f.p_m, dp1m));
+        }
+        if (xqq < 0.0f) {
+            if (f.d_cn < CC_GX || f.d_pn < CC_GX) {
+                advy = ay * (-(qdiv(f.p_c * xqq, dp1c)));
+            } else if (face1(f.d_cn, f.d_pn) < CC_GX) {
+                advy = ay * (-(qdiv(f.p_c * xqq, dp1c)));
+            } else {
+                float xqe = 0.25f * (f.q_cn + f.q_pn + f.q_c + f.q_p);
+                advy = ay * (qdiv(f.p_n * xqe, face1(f.d_cn, f.d_pn)) - qdiv(f.p_c * xqq, dp1c));
+            }
+        } else {
+            if (f.d_cs < CC_GX || f.d_ps < CC_GX) {
+                advy = ay * (qdiv(f.p_c * xqq, dp1c));
+            } else if (face1(f.d_cs, f.d_ps) < CC_GX) {
+                advy = ay * (qdiv(f.p_c * xqq, dp1c));
+            } else {
+                float xqe = 0.25f * (f.q_cs + f.q_ps + f.q_cs2 + f.q_ps2);
+                advy = ay * (qdiv(f.p_c * xqq, dp1c) - qdiv(f.p_s * xqe, face1(f.d_cs, f.d_ps)));
+            }
+        }
+        wave_breaking(f.d_c, f.z_c, f.z1_c, L.dt, advx, advy);
+        xp = xp - advx - advy;
+    }
+    if (L.fric_switch != 1) xp = fdiv1(xp, 1.0f + ff);
+    if (fabs_(xp) < CC_EPS) xp = 0.0f;
+    float lim = CC_VLIMIT * dd;
+    if (xp > lim) xp = lim;
+    if (xp < -lim) xp = -lim;
+    return xp;
+}
+
+/* CONMOME / CONMOME_S y direction at one face (moment.f90:570-780) */
+template <bool SPH>
+__device__ __forceinline__ float conmome_y(const GcLayerDev &L, const YFace &f, int i, int j, int ix, bool span) {
+    const float konst = (L.fric_switch != 1) ? 0.5f * L.dt * CC_GRAV : 0.0f;
+    const float fm = L.fric_coef;
+    float dd = 0.0f, df = 0.0f, ff;
+    bool noflux = false;
+    if (f.h_c <= CC_ELMAX || f.hq_c <= CC_ELMAX) {
+        noflux = true;
+    } else {
+        if (f.d_c > CC_GX && f.d_q > CC_GX) {
+            dd = face2(f.d_c, f.d_q); df = face1(f.d_c, f.d_q);
+        } else if (f.d_c > CC_GX && f.d_q <= CC_GX && f.h_q + f.z_c > CC_GX) {
+            dd = SPH ? f.hq_c + 0.5f * (f.z_c + f.z_q) : 0.5f * f.d_c; df = dd;
+        } else if (f.d_c <= CC_GX && f.d_q > CC_GX && f.h_c + f.z_q > CC_GX) {
+            dd = SPH ? f.hq_c + 0.5f * (f.z_c + f.z_q) : 0.5f * f.d_q; df = dd;
+        } else {
+            noflux = true;
+        }
+        if (!noflux && dd < CC_GX) noflux = true;
+    }
+    if (noflux) return 0.0f;
+    if (df < CC_DFMIN) df = CC_DFMIN;
+    float xpp = 0.25f * (f.p_c + f.p_q + f.p_w + f.p_wq);
+    if (L.fric_switch != 1) {
+        /* df >= DFMIN here unless it is NaN, so the power is positive */
+        const float fnum = konst * fm * fm * sqrtf(f.q_c * f.q_c + xpp * xpp);
+        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
+    } else {
+        ff = 0.0f;
+    }
+    const float cqy = SPH ? GC_ROW(L, GC_CY, j) : L.gry;
+    float xq = f.q_c - cqy * dd * (f.z_q - f.z_c);
+    if (L.modscm == 0 && i + 1 < ix) {
+        float scm = qdiv(cqy * dd, 12.0f) * ((f.z_eq - 2.0f * f.z_q + f.z_wq) - (f.z_e - 2.0f * f.z_c + f.z_w));
+        xq = xq - scm;
+    }
+    /* CONMOME applies -FF*Q to XP, which is unused (moment.f90:672):
+     * no term on XQ; CONMOME_S applies it to XQ (moment.f90:1150) */
+    if (SPH && L.fric_switch != 1) xq = xq - ff * f.q_c;
+    if (SPH) xq = xq - 4.0f * GC_ROW(L, GC_R5, j) * xpp;
+    const float by = SPH ? L.rows2[2 * (size_t)j] : L.ry;     /* R0 */
+    const float bx = SPH ? L.rows2[2 * (size_t)j + 1] : L.rx; /* R22 */
+    float dq1c = face1(f.d_c, f.d_q);
+    if (L.linchk == 1 && dq1c >= CC_GX && span) {
+        float advx, advy;
+        if (f.q_c < 0.0f) {
+            float dq1q = face1(f.d_q, f.d_q2);
+            if (dq1q < CC_GX || f.d_q < CC_GX)
+                advy = by * (-(qdiv(f.q_c * f.q_c, dq1c)));
+            else
+                advy = by * (qdiv(f.q_q * f.q_q, dq1q) - qdiv(f.q_c * f.q_c, dq1c));
+        } else {
+            float dq1m = face1(f.d_s, f.d_c);
+            if (dq1m < CC_GX || f.d_c < CC_GX)
+                advy = by * (qdiv(f.q_c * f.q_c, dq1c));
+            else
+                advy = by * (qdiv(f.q_c * f.q_c, dq1c) - qdiv(f.q_s * f.q_s, dq1m));
+        }
+        if (xpp < 0.0f) {
+            if (f.d_e < CC_GX || f.d_eq < CC_GX) {
+                advx = bx * (-(qdiv(f.q_c * xpp, dq1c)));
+            } else if (face1(f.d_e, f.d_eq) < CC_GX) {
+                advx = bx * (-(qdiv(f.q_c * xpp, dq1c)));
+            } else {
+                float xpe = 0.25f * (f.p_e + f.p_eq + f.p_c + f.p_q);
+                advx = bx * (qdiv(f.q_e * xpe, face1(f.d_e, f.d_eq)) - qdiv(f.q_c * xpp, dq1c));
+            }
+        } else {
+            if (f.d_w < CC_GX || f.d_wq < CC_GX) {
+                advx = bx * (qdiv(f.q_c * xpp, dq1c));
+            } else if (face1(f.d_w, f.d_wq) < CC_GX) {
+                advx = bx * (qdiv(f.q_c * xpp, dq1c));
+            } else {
+                float xpe = 0.25f * (f.p_w + f.p_wq + f.p_w2 + f.p_w2q);
+                advx = bx * (qdiv(f.q_c * xpp, dq1c) - qdiv(f.q_w * xpe, face1(f.d_w, f.d_wq)));
+            }
+        }
+        wave_breaking(f.d_c, f.z_c, f.z1_c, L.dt, advx, advy);
+        xq = xq - advx - advy;
+    }
+    if (L.fric_switch != 1) xq = fdiv1(xq, 1.0f + ff);
+    if (fabs_(xq) < CC_EPS) xq = 0.0f;
+    float lim = CC_VLIMIT * dd;
+    if (xq > lim) xq = lim;
+    if (xq < -lim) xq = -lim;
+    return xq;
+}
+
+/* a face's stencil from a field accessor get(field, di, dj), di/dj relative
+ * to the face's cell; the accessor clamps to the grid */
+template <typename Get>
+__device__ __forceinline__ void load_x(XFace &f, const Get &get) {
+    f.d_c = get(0, 0, 0); f.d_p = get(0, 1, 0); f.d_p2 = get(0, 2, 0); f.d_m = get(0, -1, 0);
+    f.d_cn = get(0, 0, 1); f.d_pn = get(0, 1, 1); f.d_cs = get(0, 0, -1); f.d_ps = get(0, 1, -1);
+    f.z_c = get(1, 0, 0); f.z_p = get(1, 1, 0);
+    f.z_pn = get(1, 1, 1); f.z_ps = get(1, 1, -1); f.z_cn = get(1, 0, 1); f.z_cs = get(1, 0, -1);
+    f.q_c = get(3, 0, 0); f.q_p = get(3, 1, 0); f.q_cs = get(3, 0, -1); f.q_ps = get(3, 1, -1);
+    f.q_cn = get(3, 0, 1); f.q_pn = get(3, 1, 1); f.q_cs2 = get(3, 0, -2); f.q_ps2 = get(3, 1, -2);
+    f.p_c = get(2, 0, 0); f.p_p = get(2, 1, 0); f.p_m = get(2, -1, 0); f.p_n = get(2, 0, 1); f.p_s = get(2, 0, -1);
+}
+template <typename Get>
+__device__ __forceinline__ void load_y(YFace &f, const Get &get) {
+    f.d_c = get(0, 0, 0); f.d_q = get(0, 0, 1); f.d_q2 = get(0, 0, 2); f.d_s = get(0, 0, -1);
+    f.d_e = get(0, 1, 0); f.d_eq = get(0, 1, 1); f.d_w = get(0, -1, 0); f.d_wq = get(0, -1, 1);
+    f.z_c = get(1, 0, 0); f.z_q = get(1, 0, 1);
+    f.z_eq = get(1, 1, 1); f.z_wq = get(1, -1, 1); f.z_e = get(1, 1, 0); f.z_w = get(1, -1, 0);
+    f.p_c = get(2, 0, 0); f.p_q = get(2, 0, 1); f.p_w = get(2, -1, 0); f.p_wq = get(2, -1, 1);
+    f.p_e = get(2, 1, 0); f.p_eq = get(2, 1, 1); f.p_w2 = get(2, -2, 0); f.p_w2q = get(2, -2, 1);
+    f.q_c = get(3, 0, 0); f.q_q = get(3, 0, 1); f.q_s = get(3, 0, -1); f.q_e = get(3, 1, 0); f.q_w = get(3, -1, 0);
+}
+
+/* Fortran spans: I > 10 .AND. I < IX-10 with I = i+1 */
+__device__ __forceinline__ bool adv_span(int i, int j, int ix, int jy) {
+    return (i + 1 > CC_SPAN) && (i + 1 < ix - CC_SPAN) && (j + 1 > CC_SPAN) && (j + 1 < jy - CC_SPAN);
+}
+
+/* CONMOME, one face per thread, the x and y directions as two grid layers.
+ * Every value a face can need (its stencil reaches two cells back along the
+ * face normal's neighbour axis and one cell forward) is loaded first, as
+ * one batch of independent loads at clamped, in-bounds indices; the
+ * branches then run on registers.  Clamped indices coincide with the
+ * reference's wherever a value is used: the two-back neighbours are read
+ * only inside the advection span, whose cells are at least 10 from every
+ * edge. */
 template <bool SPH>
 __global__ void k_conmome(GcLayerDev L, int upd) {
     pdl_enter();
@@ -484,238 +715,94 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
         if (j == 0) L.z2[i] = L.z2[(size_t)P + (i == 0 ? 1 : i)];
         else if (i == 0) L.z2[c] = L.z2[c + 1];
     }
-    const float *__restrict__ z = L.z2;
-    const float *__restrict__ hz = L.h;
-    const float *__restrict__ p = L.m1;
-    const float *__restrict__ q = L.n1;
-    const float *__restrict__ dz = L.dz2;
-    const float konst = (L.fric_switch != 1) ? 0.5f * L.dt * CC_GRAV : 0.0f;
-    const float fm = L.fric_coef;
-    /* Fortran spans: I > 10 .AND. I < IX-10 with I = i+1 */
-    const bool span = (i + 1 > CC_SPAN) && (i + 1 < ix - CC_SPAN) && (j + 1 > CC_SPAN)
-                      && (j + 1 < jy - CC_SPAN);
-    const int im1 = i > 0 ? i - 1 : 0, ip1 = i + 1 < ix ? i + 1 : ix - 1;
-    const int jm1 = j > 0 ? j - 1 : 0, jp1 = j + 1 < jy ? j + 1 : jy - 1;
-    const size_t rj = (size_t)j * P, rjm = (size_t)jm1 * P, rjp = (size_t)jp1 * P;
-#define AT(a, ii, jj) __ldg((a) + (size_t)(jj) * P + (ii))
-
-    /* ---------------- x direction (blockIdx.z = 0) ---------------- */
+    const float *fields[4] = {L.dz2, L.z2, L.m1, L.n1};
+    auto get = [&](int f, int di, int dj) {
+        const int ii = min(max(i + di, 0), ix - 1), jj = min(max(j + dj, 0), jy - 1);
+        return __ldg(fields[f] + (size_t)jj * P + ii);
+    };
+    const bool span = adv_span(i, j, ix, jy);
     if (blockIdx.z == 0) {
-        bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
+        const bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
         float out = 0.0f;
         if (inx) {
-            const size_t cp = rj + ip1;
-            const int ip2 = i + 2 < ix ? i + 2 : ix - 1;
-            const size_t rjm2 = (size_t)(j >= 2 ? j - 2 : 0) * P;
-            const float h_c = __ldg(hz + c), h_p = __ldg(hz + cp), hp_c = __ldg(L.hp + c);
-            const float d_c = __ldg(dz + c), d_p = __ldg(dz + cp), d_p2 = __ldg(dz + rj + ip2);
-            const float d_m = __ldg(dz + rj + im1);
-            const float d_cn = __ldg(dz + rjp + i), d_pn = __ldg(dz + rjp + ip1);
-            const float d_cs = __ldg(dz + rjm + i), d_ps = __ldg(dz + rjm + ip1);
-            const float z_c = __ldg(z + c), z_p = __ldg(z + cp), z1_c = __ldg(L.z1 + c);
-            const float q_c = __ldg(q + c), q_p = __ldg(q + cp);
-            const float q_cs = __ldg(q + rjm + i), q_ps = __ldg(q + rjm + ip1);
-            const float q_cn = __ldg(q + rjp + i), q_pn = __ldg(q + rjp + ip1);
-            const float q_cs2 = __ldg(q + rjm2 + i), q_ps2 = __ldg(q + rjm2 + ip1);
-            const float p_c = __ldg(p + c), p_p = __ldg(p + cp), p_m = __ldg(p + rj + im1);
-            const float p_n = __ldg(p + rjp + i), p_s = __ldg(p + rjm + i);
-            float dd = 0.0f, df = 0.0f, ff;
-            bool noflux = false;
-            if (h_c <= CC_ELMAX || hp_c <= CC_ELMAX) {
-                noflux = true;
-            } else {
-                if (d_c > CC_GX && d_p > CC_GX) {
-                    dd = face2(d_c, d_p); df = face1(d_c, d_p);
-                } else if (d_c > CC_GX && d_p <= CC_GX && h_p + z_c > CC_GX) {
-                    dd = SPH ? hp_c + 0.5f * (z_c + z_p) : 0.5f * d_c; df = dd;
-                } else if (d_c <= CC_GX && d_p > CC_GX && h_c + z_p > CC_GX) {
-                    dd = SPH ? hp_c + 0.5f * (z_c + z_p) : 0.5f * d_p; df = dd;
-                } else {
-                    noflux = true;
-                }
-                if (!noflux && dd < CC_GX) noflux = true;
-            }
-            if (!noflux) {
-                if (df < CC_DFMIN) df = CC_DFMIN;
-                float xqq = 0.25f * (q_c + q_p + q_cs + q_ps);
-                if (L.fric_switch != 1)
-                    {
-                        /* df >= DFMIN here unless it is NaN, so the power is positive */
-                        const float fnum = konst * fm * fm * sqrtf(p_c * p_c + xqq * xqq);
-                        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
-                    }
-                else
-                    ff = 0.0f;
-                const float cpx = SPH ? GC_ROW(L, GC_CX, j) : L.grx;
-                float xp = p_c - cpx * dd * (z_p - z_c);
-                if (L.modscm == 0 && j + 1 < jy) {
-                    float scm = qdiv(cpx * dd, 12.0f)
-                                * ((AT(z, ip1, jp1) - 2.0f * z_p + AT(z, ip1, jm1))
-                                   - (AT(z, i, jp1) - 2.0f * z_c + AT(z, i, jm1)));
-                    xp = xp - scm;
-                }
-                if (L.fric_switch != 1) xp = xp - ff * p_c;
-                if (SPH) xp = xp + 4.0f * GC_ROW(L, GC_R3, j) * xqq;
-                const float ax = SPH ? GC_ROW(L, GC_R1, j) : L.rx;   /* R21 = R1 */
-                const float ay = SPH ? L.rows2[2 * (size_t)j] : L.ry;   /* R0 */
-                float dp1c = face1(d_c, d_p);
-                if (L.linchk == 1 && dp1c >= CC_GX && span) {
-                    float advx, advy;
-                    if (p_c < 0.0f) {
-                        float dp1p = face1(d_p, d_p2);
-                        if (dp1p < CC_GX || d_p < CC_GX)
-                            advx = ax * (-(qdiv(p_c * p_c, dp1c)));
-                        else
-                            advx = ax * (qdiv(p_p * p_p, dp1p) - qdiv(p_c * p_c, dp1c));
-                    } else {
-                        float dp1m = face1(d_m, d_c);
-                        if (dp1m < CC_GX || d_c < CC_GX)
-                            advx = ax * (qdiv(p_c * p_c, dp1c));
-                        else
-                            advx = ax * (qdiv(p_c * p_c, dp1c) - qdiv(p_m * p_m, dp1m));
-                    }
-                    if (xqq < 0.0f) {
-                        if (d_cn < CC_GX || d_pn < CC_GX) {
-                            advy = ay * (-(qdiv(p_c * xqq, dp1c)));
-                        } else if (face1(d_cn, d_pn) < CC_GX) {
-                            advy = ay * (-(qdiv(p_c * xqq, dp1c)));
-                        } else {
-                            float xqe = 0.25f * (q_cn + q_pn + q_c + q_p);
-                            advy = ay * (qdiv(p_n * xqe, face1(d_cn, d_pn)) - qdiv(p_c * xqq, dp1c));
-                        }
-                    } else {
-                        if (d_cs < CC_GX || d_ps < CC_GX) {
-                            advy = ay * (qdiv(p_c * xqq, dp1c));
-                        } else if (face1(d_cs, d_ps) < CC_GX) {
-                            advy = ay * (qdiv(p_c * xqq, dp1c));
-                        } else {
-                            float xqe = 0.25f * (q_cs + q_ps + q_cs2 + q_ps2);
-                            advy = ay * (qdiv(p_c * xqq, dp1c) - qdiv(p_s * xqe, face1(d_cs, d_ps)));
-                        }
-                    }
-                    wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
-                    xp = xp - advx - advy;
-                }
-                if (L.fric_switch != 1) xp = fdiv1(xp, 1.0f + ff);
-                if (fabs_(xp) < CC_EPS) xp = 0.0f;
-                float lim = CC_VLIMIT * dd;
-                if (xp > lim) xp = lim;
-                if (xp < -lim) xp = -lim;
-                out = xp;
-            }
+            XFace f;
+            load_x(f, get);
+            f.h_c = __ldg(L.h + c); f.h_p = __ldg(L.h + c + 1); f.hp_c = __ldg(L.hp + c);
+            f.z1_c = __ldg(L.z1 + c);
+            out = conmome_x<SPH>(L, f, j, jy, span);
         }
         L.m2[c] = out;
-    }
-    /* ---------------- y direction (blockIdx.z = 1) ---------------- */
-    else {
-        bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
+    } else {
+        const bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
         float out = 0.0f;
         if (iny) {
-            const size_t cq = rjp + i;
-            const int im2 = i >= 2 ? i - 2 : 0;
-            const size_t rjp2 = (size_t)(j + 2 < jy ? j + 2 : jy - 1) * P;
-            const float h_c = __ldg(hz + c), h_q = __ldg(hz + cq), hq_c = __ldg(L.hq + c);
-            const float d_c = __ldg(dz + c), d_q = __ldg(dz + cq), d_q2 = __ldg(dz + rjp2 + i);
-            const float d_s = __ldg(dz + rjm + i);
-            const float d_e = __ldg(dz + rj + ip1), d_eq = __ldg(dz + rjp + ip1);
-            const float d_w = __ldg(dz + rj + im1), d_wq = __ldg(dz + rjp + im1);
-            const float z_c = __ldg(z + c), z_q = __ldg(z + cq), z1_c = __ldg(L.z1 + c);
-            const float p_c = __ldg(p + c), p_q = __ldg(p + cq);
-            const float p_w = __ldg(p + rj + im1), p_wq = __ldg(p + rjp + im1);
-            const float p_e = __ldg(p + rj + ip1), p_eq = __ldg(p + rjp + ip1);
-            const float p_w2 = __ldg(p + rj + im2), p_w2q = __ldg(p + rjp + im2);
-            const float q_c = __ldg(q + c), q_q = __ldg(q + cq), q_s = __ldg(q + rjm + i);
-            const float q_e = __ldg(q + rj + ip1), q_w = __ldg(q + rj + im1);
-            float dd = 0.0f, df = 0.0f, ff;
-            bool noflux = false;
-            if (h_c <= CC_ELMAX || hq_c <= CC_ELMAX) {
-                noflux = true;
-            } else {
-                if (d_c > CC_GX && d_q > CC_GX) {
-                    dd = face2(d_c, d_q); df = face1(d_c, d_q);
-                } else if (d_c > CC_GX && d_q <= CC_GX && h_q + z_c > CC_GX) {
-                    dd = SPH ? hq_c + 0.5f * (z_c + z_q) : 0.5f * d_c; df = dd;
-                } else if (d_c <= CC_GX && d_q > CC_GX && h_c + z_q > CC_GX) {
-                    dd = SPH ? hq_c + 0.5f * (z_c + z_q) : 0.5f * d_q; df = dd;
-                } else {
-                    noflux = true;
-                }
-                if (!noflux && dd < CC_GX) noflux = true;
-            }
-            if (!noflux) {
-                if (df < CC_DFMIN) df = CC_DFMIN;
-                float xpp = 0.25f * (p_c + p_q + p_w + p_wq);
-                if (L.fric_switch != 1)
-                    {
-                        /* df >= DFMIN here unless it is NaN, so the power is positive */
-                        const float fnum = konst * fm * fm * sqrtf(q_c * q_c + xpp * xpp);
-                        ff = (fnum == 0.0f && df >= CC_DFMIN) ? fnum : fnum / cc_powf(df, CC_MANNEXP);
-                    }
-                else
-                    ff = 0.0f;
-                const float cqy = SPH ? GC_ROW(L, GC_CY, j) : L.gry;
-                float xq = q_c - cqy * dd * (z_q - z_c);
-                if (L.modscm == 0 && i + 1 < ix) {
-                    float scm = qdiv(cqy * dd, 12.0f)
-                                * ((AT(z, ip1, jp1) - 2.0f * z_q + AT(z, im1, jp1))
-                                   - (AT(z, ip1, j) - 2.0f * z_c + AT(z, im1, j)));
-                    xq = xq - scm;
-                }
-                /* CONMOME applies -FF*Q to XP, which is unused (moment.f90:672):
-                 * no term on XQ; CONMOME_S applies it to XQ (moment.f90:1150) */
-                if (SPH && L.fric_switch != 1) xq = xq - ff * q_c;
-                if (SPH) xq = xq - 4.0f * GC_ROW(L, GC_R5, j) * xpp;
-                const float by = SPH ? L.rows2[2 * (size_t)j] : L.ry;        /* R0 */
-                const float bx = SPH ? L.rows2[2 * (size_t)j + 1] : L.rx;    /* R22 */
-                float dq1c = face1(d_c, d_q);
-                if (L.linchk == 1 && dq1c >= CC_GX && span) {
-                    float advx, advy;
-                    if (q_c < 0.0f) {
-                        float dq1q = face1(d_q, d_q2);
-                        if (dq1q < CC_GX || d_q < CC_GX)
-                            advy = by * (-(qdiv(q_c * q_c, dq1c)));
-                        else
-                            advy = by * (qdiv(q_q * q_q, dq1q) - qdiv(q_c * q_c, dq1c));
-                    } else {
-                        float dq1m = face1(d_s, d_c);
-                        if (dq1m < CC_GX || d_c < CC_GX)
-                            advy = by * (qdiv(q_c * q_c, dq1c));
-                        else
-                            advy = by * (qdiv(q_c * q_c, dq1c) - qdiv(q_s * q_s, dq1m));
-                    }
-                    if (xpp < 0.0f) {
-                        if (d_e < CC_GX || d_eq < CC_GX) {
-                            advx = bx * (-(qdiv(q_c * xpp, dq1c)));
-                        } else if (face1(d_e, d_eq) < CC_GX) {
-                            advx = bx * (-(qdiv(q_c * xpp, dq1c)));
-                        } else {
-                            float xpe = 0.25f * (p_e + p_eq + p_c + p_q);
-                            advx = bx * (qdiv(q_e * xpe, face1(d_e, d_eq)) - qdiv(q_c * xpp, dq1c));
-                        }
-                    } else {
-                        if (d_w < CC_GX || d_wq < CC_GX) {
-                            advx = bx * (qdiv(q_c * xpp, dq1c));
-                        } else if (face1(d_w, d_wq) < CC_GX) {
-                            advx = bx * (qdiv(q_c * xpp, dq1c));
-                        } else {
-                            float xpe = 0.25f * (p_w + p_wq + p_w2 + p_w2q);
-                            advx = bx * (qdiv(q_c * xpp, dq1c) - qdiv(q_w * xpe, face1(d_w, d_wq)));
-                        }
-                    }
-                    wave_breaking(d_c, z_c, z1_c, L.dt, advx, advy);
-                    xq = xq - advx - advy;
-                }
-                if (L.fric_switch != 1) xq = fdiv1(xq, 1.0f + ff);
-                if (fabs_(xq) < CC_EPS) xq = 0.0f;
-                float lim = CC_VLIMIT * dd;
-                if (xq > lim) xq = lim;
-                if (xq < -lim) xq = -lim;
-                out = xq;
-            }
+            YFace f;
+            load_y(f, get);
+            f.h_c = __ldg(L.h + c); f.h_q = __ldg(L.h + c + P); f.hq_c = __ldg(L.hq + c);
+            f.z1_c = __ldg(L.z1 + c);
+            out = conmome_y<SPH>(L, f, i, j, ix, span);
         }
         L.n2[c] = out;
     }
-#undef AT
+}
+
+/* CONMOME with both directions per thread, the stencil staged through
+ * shared memory: a block stages its (BX+4) x (BY+4) window of DZ, Z, M and
+ * N (two cells of halo, at the same clamped indices the one-face kernel
+ * reads) with one batch of independent loads, then each thread computes
+ * its cell's x and y faces from shared memory.  Same values, same
+ * arithmetic (conmome_x / conmome_y): the same bits. */
+template <bool SPH>
+__global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd) {
+    pdl_enter();
+    constexpr int TW = BX + 4, TH = BY + 4;
+    __shared__ float tile[4][TH][TW];
+    const int P = L.pitch, ix = L.nx, jy = L.ny;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const float *fields[4] = {L.dz2, L.z2, L.m1, L.n1};
+    for (int t = threadIdx.y * BX + threadIdx.x; t < TW * TH; t += BX * BY) {
+        const int tj = t / TW, ti = t - tj * TW;
+        const int ii = min(max(i0 + ti - 2, 0), ix - 1), jj = min(max(j0 + tj - 2, 0), jy - 1);
+        const size_t g = (size_t)jj * P + ii;
+#pragma unroll
+        for (int f = 0; f < 4; f++) tile[f][tj][ti] = __ldg(fields[f] + g);
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    if (i >= ix || j >= jy) return;
+    const size_t c = (size_t)j * P + i;
+    /* UPDATE's edge copy as in k_conmome: row and column 0 feed no face here */
+    if (upd) {
+        if (j == 0) L.z2[i] = L.z2[(size_t)P + (i == 0 ? 1 : i)];
+        else if (i == 0) L.z2[c] = L.z2[c + 1];
+    }
+    /* the tile holds the clamped neighbour of every in-grid cell it covers;
+     * for a cell near the grid edge the clamp is repeated on the offset */
+    auto get = [&](int f, int di, int dj) {
+        const int ii = min(max(i + di, 0), ix - 1) - i0 + 2, jj = min(max(j + dj, 0), jy - 1) - j0 + 2;
+        return tile[f][jj][ii];
+    };
+    const bool span = adv_span(i, j, ix, jy);
+    const bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
+    const bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
+    const float h_c = __ldg(L.h + c), z1_c = __ldg(L.z1 + c);
+    float outx = 0.0f, outy = 0.0f;
+    if (inx) {
+        XFace f;
+        load_x(f, get);
+        f.h_c = h_c; f.h_p = __ldg(L.h + c + 1); f.hp_c = __ldg(L.hp + c);
+        f.z1_c = z1_c;
+        outx = conmome_x<SPH>(L, f, j, jy, span);
+    }
+    if (iny) {
+        YFace f;
+        load_y(f, get);
+        f.h_c = h_c; f.h_q = __ldg(L.h + c + P); f.hq_c = __ldg(L.hq + c);
+        f.z1_c = z1_c;
+        outy = conmome_y<SPH>(L, f, i, j, ix, span);
+    }
+    L.m2[c] = outx;
+    L.n2[c] = outy;
 }
 
 /* ---------------------------------------------------------------- */
@@ -1228,23 +1315,41 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
+/* CONMOME: the shared-memory tile form (both faces per thread), or with
+ * GCOMCOT_CONMOME_TILE=0 the one-face form (x and y as two grid layers);
+ * both compute the same bits */
+static bool conmome_tiled() {
+    static const int on = [] {
+        const char *v = getenv("GCOMCOT_CONMOME_TILE");
+        return (v && v[0] == '0') ? 0 : 1;
+    }();
+    return on != 0;
+}
+
+static void launch_conmome(const GcLayerDev &L, int upd, cudaStream_t s) {
+    const bool sph = L.laycord == 0;
+    if (conmome_tiled()) {
+        if (sph) launch(k_conmome_tile<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
+        else launch(k_conmome_tile<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
+    } else {
+        const dim3 g2(grid2(L).x, grid2(L).y, 2);
+        if (sph) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, upd);
+        else launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L, upd);
+    }
+}
+
 void gc_launch_moment(const GcLayerDev &L, cudaStream_t s) {
-    /* CONMOME's two directions are independent: one grid layer each */
-    const dim3 g2(grid2(L).x, grid2(L).y, 2);
     if (L.laygov == 2 || L.laygov == 3) {
         if (L.laycord == 0) launch(k_momt_d<true>, grid2(L), dim3(BX, BY), 0, s, L);
         else launch(k_momt_d<false>, grid2(L), dim3(BX, BY), 0, s, L);
-    } else if (L.laycord == 0 && L.laygov == 1) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, 0);
+    } else if (L.laygov == 1) launch_conmome(L, 0, s);
     else if (L.laycord == 0) launch(k_momt_s, grid2(L), dim3(BX, BY), 0, s, L, 0, 0, L.nx, L.ny);
-    else if (L.laygov == 1) launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L, 0);
     else launch(k_momt_c, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
 int gc_launch_moment_update(const GcLayerDev &L, cudaStream_t s) {
     if (L.laygov == 1 && !L.root && L.modscm != 0) {
-        const dim3 g2(grid2(L).x, grid2(L).y, 2);
-        if (L.laycord == 0) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, 1);
-        else launch(k_conmome<false>, g2, dim3(BX, BY), 0, s, L, 1);
+        launch_conmome(L, 1, s);
         return 1;
     }
     gc_launch_moment(L, s);

@@ -107,6 +107,17 @@ void gcomcot_set_fusion(int on);
 int gcomcot_sync(void);
 /* the cudaStream_t the library issues work on */
 void *gcomcot_stream(void);
+/* no counterpart in the reference (whose kernels never wait on one another):
+ * the polls after which a pipeline wait of the two-step kernel gives up,
+ * sets the library's error flag and lets its warp leave (default 2^22;
+ * <= 0 restores it).  gcomcot_sync / gc_engine_sync then return
+ * GC_ETIMEOUT. */
+void gcomcot_set_wait_limit(int polls);
+/* diagnostics, no counterpart in the reference: the next two-step launch
+ * makes its first warp wait for a row that no copy delivers (nothing is
+ * issued for it), so the bounded wait above gives up; for tests of the
+ * failure path without faulting a GPU */
+void gcomcot_inject_stall(void);
 
 /* Runs `nsteps` outer steps through the Part-1 entry points in the order of
  * comcot.f90:359-439 (MASS, OPEN, ALL_GRID, MOMENT, MAX_AMP, GET_TS per
@@ -163,6 +174,9 @@ int gc_engine_member_done(gc_engine *e, int member);
  * gc_engine_sync); gc_engine_read returns the state after that many steps */
 int gc_engine_member_steps(gc_engine *e, int member);
 int gc_engine_sync(gc_engine *e);
+/* 1 when all work issued so far has finished, 0 while it runs (does not
+ * wait; gc_engine_sync still reports errors) */
+int gc_engine_query(gc_engine *e);
 /* results of a member: any pointer may be NULL */
 int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
                    int *arrival, float *ts);

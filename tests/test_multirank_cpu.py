@@ -87,3 +87,61 @@ def test_shard_rejects_bad_rank():
     with pytest.raises(ValueError):
         replicas.shard([1, 2], 2, 2)
     assert replicas.shard(range(5), 1, 2) == [1, 3]
+
+
+def _serve_worker(rank, world, port, dies, out):
+    """each rank serves its round-robin share of a trace (forecast server
+    over the fake engine of the serving tests); rank 0 gathers the ranks'
+    latencies through the store with a bounded wait"""
+    sys.path.insert(0, os.path.join(HERE, "..", "gpu-comcot_b200"))
+    sys.path.insert(0, HERE)
+    import datetime
+
+    from torch.distributed import TCPStore
+
+    from comcot_b200 import replicas
+    from comcot_b200.serving import ForecastServer, Request, percentiles
+    from test_serving_cpu import FakeCase, FakeEngine
+
+    store = TCPStore("127.0.0.1", port + 1, world, rank == 0, timeout=datetime.timedelta(seconds=20))
+    hb = replicas.Heartbeat(store, rank, world)
+    hb.beat()
+    trace = [(0.001 * k, 10 + 3 * k, 10) for k in range(12)]
+    mine = replicas.shard(trace, rank, world)
+    reqs = [Request(k, t, FakeCase(nsteps=n, nbytes=b)) for k, (t, n, b) in enumerate(mine)]
+    srv = ForecastServer(100, chunk=4, engine=FakeEngine(budget=100))
+    srv.serve(reqs, speed=float("inf"))
+    if dies and rank == 1:
+        os._exit(0)                       # leaves after its work, before reporting it
+    lat = [r.latency for r in reqs]
+    got, missing, stale = replicas.collect(store, rank, world, {"lat": lat, "done": [r.status for r in reqs]},
+                                           timeout_s=2.0, hb=hb)
+    if rank == 0:
+        merged = sum((g["lat"] for g in got.values()), [])
+        out.put({"n": len(merged), "missing": missing, "p99": percentiles(merged)["p99"],
+                 "done": sum((g["done"] for g in got.values()), [])})
+
+
+def _run_serve(dies):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    ps = [ctx.Process(target=_serve_worker, args=(r, 2, port, dies, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = q.get(timeout=60)
+    for p in ps:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in ps)
+    return res
+
+
+def test_served_shares_are_gathered_over_two_ranks():
+    r = _run_serve(dies=False)
+    assert r["n"] == 12 and r["missing"] == [] and set(r["done"]) == {"done"}
+    assert r["p99"] >= 0.0
+
+
+def test_serving_rank_that_dies_is_reported_not_waited_for():
+    r = _run_serve(dies=True)
+    assert r["missing"] == [1] and r["n"] == 6

@@ -53,6 +53,9 @@ class FakeEngine:
     def sync(self):
         pass
 
+    def idle(self):
+        return True     # step() above runs to completion before it returns
+
     def done(self, mid):
         c, k = self.members[mid]
         return k >= c.nsteps
