@@ -1585,11 +1585,14 @@ static ocl_layer *find_layer(ocl_layer *layers, int n, int id) {
     return NULL;
 }
 
-int ocl_run(ocl_layer *layers, int n, int nsteps, double arrival_thr, int ngauges,
-            const int *g_layer, const int *g_ki, const int *g_kj, const double *g_cx,
-            const double *g_cy, REAL *ts) {
+/* outer steps first .. first + nsteps - 1 (1-based: the arrival step a
+ * cell records is the outer step's number, so a run may continue where an
+ * earlier one stopped); gauge samples go to ts[0 .. nsteps-1] */
+int ocl_run_from(ocl_layer *layers, int n, int first, int nsteps, double arrival_thr, int ngauges,
+                 const int *g_layer, const int *g_ki, const int *g_kj, const double *g_cx,
+                 const double *g_cy, REAL *ts) {
     for (int k = 1; k <= nsteps; k++) {
-        ocl_step(layers, n, k, arrival_thr);
+        ocl_step(layers, n, first + k - 1, arrival_thr);
         for (int g = 0; g < ngauges; g++) {
             ocl_layer *G = find_layer(layers, n, g_layer[g]);
             if (!G) return -1;
@@ -1598,6 +1601,12 @@ int ocl_run(ocl_layer *layers, int n, int nsteps, double arrival_thr, int ngauge
         ocl_change(&layers[0]);
     }
     return 0;
+}
+
+int ocl_run(ocl_layer *layers, int n, int nsteps, double arrival_thr, int ngauges,
+            const int *g_layer, const int *g_ki, const int *g_kj, const double *g_cx,
+            const double *g_cy, REAL *ts) {
+    return ocl_run_from(layers, n, 1, nsteps, arrival_thr, ngauges, g_layer, g_ki, g_kj, g_cx, g_cy, ts);
 }
 
 /* ------------------------------------------------------------------ */

@@ -77,6 +77,10 @@ void ocl_arrival(ocl_layer *L, int step, double thr);
 void ocl_all_grid(ocl_layer *layers, int n);
 void ocl_step(ocl_layer *layers, int n, int step, double arrival_thr);
 double ocl_gauge(ocl_layer *L, int ki, int kj, double cx, double cy);
+/* outer steps first .. first + nsteps - 1 (continues an earlier run) */
+int  ocl_run_from(ocl_layer *layers, int n, int first, int nsteps, double arrival_thr, int ngauges,
+                  const int *g_layer, const int *g_ki, const int *g_kj, const double *g_cx,
+                  const double *g_cy, REAL *ts);
 int  ocl_run(ocl_layer *layers, int n, int nsteps, double arrival_thr,
              int ngauges, const int *g_layer, const int *g_ki, const int *g_kj,
              const double *g_cx, const double *g_cy, REAL *ts);

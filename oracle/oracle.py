@@ -44,6 +44,9 @@ def load(dtype=np.float32, libm=False):
     lib.ocl_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ocl_run.restype = C.c_int
+    lib.ocl_run_from.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ocl_run_from.restype = C.c_int
     lib.ocl_set_threads.argtypes = [C.c_int]
     for fn in ("ocl_mass", "ocl_moment", "ocl_open", "ocl_change", "ocl_update", "ocl_maxamp"):
         getattr(lib, fn).argtypes = [C.c_void_p]
@@ -127,6 +130,7 @@ class OracleRun:
             self.fields.append(self._fill(self.arr[k], L, k == 0, coefs64[k] if coefs64 else None))
         # arrival at the start: step 0 where a wet cell is already above the threshold
         self.lib.ocl_arrival_start(C.addressof(self.arr[0]), float(case.arrival_thr))
+        self.steps_done = 0  # outer steps run so far (a later run() continues the count)
 
     def _a(self, x, dt=None):
         a = np.ascontiguousarray(x, dtype=dt or self.dtype)
@@ -178,7 +182,9 @@ class OracleRun:
         return f
 
     def run(self, nsteps, threads=1, arrival=True, maxamp=True):
-        """Runs nsteps outer steps; returns the gauge series [nsteps, ng]."""
+        """Runs the next nsteps outer steps (numbered on from earlier runs, so
+        arrival steps are the forecast's); returns their gauge series
+        [nsteps, ng]."""
         self.lib.ocl_set_threads(int(threads))
         root = self.arr[0]
         saved_z, saved_a = root.zmax, root.arrival
@@ -194,12 +200,13 @@ class OracleRun:
         gx = np.array([x[3] for x in g] or [0], np.float64)
         gy = np.array([x[4] for x in g] or [0], np.float64)
         ts = np.zeros((max(nsteps, 1), max(ng, 1)), self.dtype)
-        rc = self.lib.ocl_run(C.addressof(self.arr), len(self.case.layers), int(nsteps),
-                              float(self.case.arrival_thr), ng, gl.ctypes.data, gi.ctypes.data,
-                              gj.ctypes.data, gx.ctypes.data, gy.ctypes.data, ts.ctypes.data)
+        rc = self.lib.ocl_run_from(C.addressof(self.arr), len(self.case.layers), self.steps_done + 1, int(nsteps),
+                                   float(self.case.arrival_thr), ng, gl.ctypes.data, gi.ctypes.data,
+                                   gj.ctypes.data, gx.ctypes.data, gy.ctypes.data, ts.ctypes.data)
         root.zmax, root.arrival = saved_z, saved_a
         if rc != 0:
             raise RuntimeError("oracle run failed")
+        self.steps_done += int(nsteps)
         return ts[:nsteps, :ng]
 
     def layer(self, k=0):

@@ -144,3 +144,22 @@ def test_arrival_definition(oracle_mod):
     whole.run(nsteps)
     assert np.array_equal(whole.layer(0)["arrival"], expect)
     assert (expect == 0).sum() > 0 and (expect > 0).sum() > 0 and (expect < 0).sum() > 0
+
+
+def test_split_runs_number_steps_like_one_run(oracle_mod):
+    """arrival steps are the forecast's step numbers: a run continued in a
+    second call gives the same state as one call (the parity checks of the
+    benchmark snapshot the oracle midway)"""
+    import numpy as np
+
+    from comcot_b200 import synth
+
+    case = synth.config_c1(nsteps=240)
+    a = oracle_mod.OracleRun(case)
+    a.run(240, threads=4)
+    b = oracle_mod.OracleRun(case)
+    b.run(100, threads=4)
+    b.run(140, threads=4)
+    for k in ("z", "m", "n", "zmax", "arrival"):
+        assert np.array_equal(a.layer(0)[k], b.layer(0)[k]), k
+    assert (a.layer(0)["arrival"] > 100).sum() > 0   # arrivals in the second call
