@@ -93,6 +93,12 @@ SIGNATURES = {
     "gc_engine_query": (C.c_int, [VP]),
     "gc_engine_read": (C.c_int, [VP, C.c_int, P_F, P_F, P_F, P_F, P_I, P_F]),
     "gc_engine_release": (C.c_int, [VP, C.c_int]),
+    "gc_engine_read_async": (C.c_int, [VP, C.c_int, P_F, P_F, P_F, P_F, P_I, P_F, C.POINTER(VP)]),
+    "gc_event_query": (C.c_int, [VP]),
+    "gc_event_wait": (C.c_int, [VP]),
+    "gc_event_release": (C.c_int, [VP]),
+    "gc_host_alloc": (VP, [C.c_longlong]),
+    "gc_host_free": (C.c_int, [VP]),
     "gc_engine_bytes_in_use": (C.c_longlong, [VP]),
     "gc_engine_member_bytes": (C.c_longlong, [VP, C.c_int]),
     "gc_engine_config": (C.c_int, [VP, C.c_int, C.c_int, C.c_int]),

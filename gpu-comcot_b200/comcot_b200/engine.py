@@ -14,6 +14,58 @@ from .synth import Case
 F32 = np.float32
 
 
+class PinnedPool:
+    """page-locked host blocks (gc_host_alloc) reused by size, so results
+    can be copied from the device while the host goes on"""
+
+    def __init__(self, lib):
+        self.lib = lib
+        self.free = {}
+
+    def take(self, nbytes: int) -> int:
+        blocks = self.free.get(nbytes)
+        if blocks:
+            return blocks.pop()
+        ptr = self.lib.gc_host_alloc(int(nbytes))
+        if not ptr:
+            raise MemoryError("page-locked host memory refused")
+        return ptr
+
+    def give(self, nbytes: int, ptr: int):
+        self.free.setdefault(nbytes, []).append(ptr)
+
+    def close(self):
+        for blocks in self.free.values():
+            for ptr in blocks:
+                self.lib.gc_host_free(ptr)
+        self.free.clear()
+
+
+class PendingRead:
+    """results on their way from the device (Engine.read_async)"""
+
+    def __init__(self, lib, pool, event, ptr, nbytes, views):
+        self.lib, self.pool, self.event, self.ptr, self.nbytes, self.views = lib, pool, event, ptr, nbytes, views
+
+    def done(self) -> bool:
+        rc = self.lib.gc_event_query(self.event)
+        if rc < 0:
+            raise RuntimeError(f"gc_event_query failed: {rc}")
+        return rc == 1
+
+    def take(self) -> dict:
+        """waits for the copies, returns the results as ordinary arrays and
+        gives the page-locked block back to the pool"""
+        rc = self.lib.gc_event_wait(self.event)
+        if rc != 0:
+            raise RuntimeError(f"gc_event_wait failed: {rc}")
+        out = {k: np.array(v, copy=True) for k, v in self.views.items()}
+        self.lib.gc_event_release(self.event)
+        self.pool.give(self.nbytes, self.ptr)
+        self.event = None
+        return out
+
+
 class Engine:
     def __init__(self, budget: int):
         self.lib = _lib.load()
@@ -25,6 +77,7 @@ class Engine:
         self.classes = {}
         self.members = {}
         self._axes = set()
+        self.pinned = PinnedPool(self.lib)
 
     def __enter__(self):
         return self
@@ -36,6 +89,7 @@ class Engine:
         if self.h:
             self.lib.gc_engine_destroy(self.h)
             self.h = None
+            self.pinned.close()
 
     def config(self, variant=-1, use_graphs=1, chunk=32):
         rc = self.lib.gc_engine_config(self.h, int(variant), int(use_graphs), int(chunk))
@@ -217,6 +271,37 @@ class Engine:
             if rc != 0:
                 raise RuntimeError(f"gc_engine_read_child failed: {rc}")
         return out
+
+    def read_async(self, mid: int, fields=("zmax", "arrival", "ts")) -> PendingRead:
+        """the named results (z, m, n, zmax, arrival, ts) copied into
+        page-locked host memory behind the member's issued steps; the host
+        goes on at once.  The member may be released right after."""
+        nx, ny, n, ng, _child = self.members[mid]
+        shapes = {"z": ((ny, nx), F32), "m": ((ny, nx), F32), "n": ((ny, nx), F32), "zmax": ((ny, nx), F32),
+                  "arrival": ((ny, nx), np.int32), "ts": ((n, ng), F32)}
+        want = [k for k in ("z", "m", "n", "zmax", "arrival", "ts") if k in fields and not (k == "ts" and ng == 0)]
+        offs, total = {}, 0
+        for k in want:
+            shape, dt = shapes[k]
+            offs[k] = total
+            total += (int(np.prod(shape)) * np.dtype(dt).itemsize + 255) // 256 * 256
+        total = max(total, 256)
+        ptr = self.pinned.take(total)
+        views = {}
+        for k in want:
+            shape, dt = shapes[k]
+            cnt = int(np.prod(shape))
+            buf = (C.c_byte * (cnt * np.dtype(dt).itemsize)).from_address(ptr + offs[k])
+            views[k] = np.frombuffer(buf, dtype=dt, count=cnt).reshape(shape)
+        ptrs = {k: (views[k].ctypes.data_as(_lib.P_I if k == "arrival" else _lib.P_F) if k in views else None)
+                for k in shapes}
+        ev = C.c_void_p()
+        rc = self.lib.gc_engine_read_async(self.h, mid, ptrs["z"], ptrs["m"], ptrs["n"], ptrs["zmax"],
+                                           ptrs["arrival"], ptrs["ts"], C.byref(ev))
+        if rc != 0:
+            self.pinned.give(total, ptr)
+            raise RuntimeError(f"gc_engine_read_async failed: {rc}")
+        return PendingRead(self.lib, self.pinned, ev, ptr, total, views)
 
     def release(self, mid: int):
         rc = self.lib.gc_engine_release(self.h, mid)

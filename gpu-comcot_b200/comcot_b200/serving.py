@@ -11,7 +11,11 @@ does not depend on what else was in the batch: every member's kernels read
 and write only that member's state.
 
 Time-to-forecast is measured per request from its arrival to the moment its
-products are in host memory.
+products are in host memory.  Finished requests' products are copied from
+the device behind the running steps into page-locked host memory
+(Engine.read_async); the loop takes them when the copy's event completes and
+hands them to the file writer's thread, so neither the copies nor the files
+hold up the next chunk.
 
 Failure handling (all on the host; nothing faults a GPU): a request the
 engine refuses as malformed, or one larger than the whole budget, is marked
@@ -102,18 +106,31 @@ class ForecastServer:
         r.status = "running"
         return True
 
-    def _harvest(self, r: Request):
+    def _harvest(self, r: Request) -> bool:
+        """True when the request is finished here; False when its results
+        are still on their way to host memory (r._pending)"""
         h = self.eng.health(r._mid, self.blowup_m)
         if h:
             r.status = "diverged"
             r.error = ("non-finite surface" if h & 1 else "") + (" |eta| above %g m" % self.blowup_m if h & 2 else "")
-        else:
-            r.result = self.eng.read(r._mid, fields=self.keep)
-            r.status = "done"
-            if self.writer:
-                L = r.case.root
-                self.writer.submit(outputs.write_forecast, f"{self.out_dir}/req_{r.rid:05d}", r.result, L.H, L.dt)
+            self.eng.release(r._mid)
+            return True
+        if hasattr(self.eng, "read_async"):
+            # copied behind the steps into page-locked memory; the loop goes on
+            r._pending = self.eng.read_async(r._mid, fields=self.keep)
+            self.eng.release(r._mid)
+            r.status = "draining"
+            return False
+        r.result = self.eng.read(r._mid, fields=self.keep)
         self.eng.release(r._mid)
+        self._finish(r)
+        return True
+
+    def _finish(self, r: Request):
+        r.status = "done"
+        if self.writer:
+            L = r.case.root
+            self.writer.submit(outputs.write_forecast, f"{self.out_dir}/req_{r.rid:05d}", r.result, L.H, L.dt)
 
     def serve(self, requests, speed: float = 1.0, clock=time.perf_counter):
         """Runs the trace.  Request k arrives t_arrival / speed wall seconds
@@ -149,7 +166,23 @@ class ForecastServer:
             self.max_active = max(self.max_active, len(active))
             return n
 
-        while pending or waiting or active:
+        draining = []
+
+        def drain(wait=False):
+            """finishes requests whose results have reached host memory"""
+            nonlocal draining
+            still = []
+            for r in draining:
+                if wait or r._pending.done():
+                    r.result = r._pending.take()
+                    r.t_done = clock() - t0
+                    self._finish(r)
+                else:
+                    still.append(r)
+            draining = still
+
+        while pending or waiting or active or draining:
+            drain()
             if take_arrivals():
                 idle_refusals = 0
             if not active:
@@ -166,12 +199,15 @@ class ForecastServer:
                     continue
                 if pending:
                     time.sleep(max(0.0, min(0.002, pending[0].t_arrival_wall - (clock() - t0))))
+                elif draining:
+                    drain(wait=True)
                 continue
             self.eng.step(self.chunk)
             # while the chunk runs: arrivals are admitted now (their state is
             # uploaded behind the chunk) and join at the next one
             while not self.eng.idle():
                 take_arrivals()
+                drain()
                 time.sleep(0.0002)
             self.eng.sync()
             still = []
@@ -181,11 +217,14 @@ class ForecastServer:
                     self.eng.release(r._mid)
                     r.status, r.t_done = "cancelled", clock() - t0
                 elif self.eng.done(r._mid):
-                    self._harvest(r)
-                    r.t_done = clock() - t0
+                    if self._harvest(r):
+                        r.t_done = clock() - t0
+                    else:
+                        draining.append(r)
                 else:
                     still.append(r)
             active = still
+        drain(wait=True)
         return requests
 
 

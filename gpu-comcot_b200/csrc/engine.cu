@@ -980,6 +980,64 @@ int gc_engine_read(gc_engine *e, int id, float *z, float *m, float *n, float *zm
     return GC_OK;
 }
 
+int gc_engine_read_async(gc_engine *e, int id, float *z, float *m, float *n, float *zmax, int *arrival, float *ts,
+                         void **done) {
+    if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used || !done) return GC_EINVAL;
+    EngMember &M = e->members[id];
+    EngClass &C = e->classes[M.cls];
+    const int done_steps = std::min(std::max(e->gstep - M.step0 + 1, 0), M.nsteps);
+    const int cur = M.level_buf(done_steps);
+    size_t sp = (size_t)C.pitch * sizeof(float), dp = (size_t)C.nx * sizeof(float);
+    auto dl = [&](void *dst, const void *src) {
+        return cudaMemcpy2DAsync(dst, dp, src, sp, dp, (size_t)C.ny, cudaMemcpyDeviceToHost, e->stream);
+    };
+    if (z) GC_CUDA_OR_RET(dl(z, M.z[cur]));
+    if (m) GC_CUDA_OR_RET(dl(m, M.m[cur]));
+    if (n) GC_CUDA_OR_RET(dl(n, M.n[cur]));
+    if (zmax) GC_CUDA_OR_RET(dl(zmax, M.zmax));
+    if (arrival) GC_CUDA_OR_RET(dl(arrival, M.arrival));
+    if (ts && M.ng > 0)
+        GC_CUDA_OR_RET(cudaMemcpyAsync(ts, M.ts, (size_t)M.nsteps * M.ng * sizeof(float), cudaMemcpyDeviceToHost,
+                                       e->stream));
+    cudaEvent_t ev;
+    GC_CUDA_OR_RET(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    GC_CUDA_OR_RET(cudaEventRecord(ev, e->stream));
+    *done = (void *)ev;
+    return GC_OK;
+}
+
+int gc_event_query(void *ev) {
+    if (!ev) return GC_EINVAL;
+    const cudaError_t q = cudaEventQuery((cudaEvent_t)ev);
+    if (q == cudaErrorNotReady) return 0;
+    GC_CUDA_OR_RET(q);
+    return 1;
+}
+
+int gc_event_wait(void *ev) {
+    if (!ev) return GC_EINVAL;
+    GC_CUDA_OR_RET(cudaEventSynchronize((cudaEvent_t)ev));
+    return GC_OK;
+}
+
+int gc_event_release(void *ev) {
+    if (!ev) return GC_EINVAL;
+    GC_CUDA_OR_RET(cudaEventDestroy((cudaEvent_t)ev));
+    return GC_OK;
+}
+
+void *gc_host_alloc(long long bytes) {
+    void *p = nullptr;
+    if (bytes <= 0 || cudaHostAlloc(&p, (size_t)bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    return p;
+}
+
+int gc_host_free(void *p) {
+    if (!p) return GC_EINVAL;
+    GC_CUDA_OR_RET(cudaFreeHost(p));
+    return GC_OK;
+}
+
 int gc_engine_read_child(gc_engine *e, int id, float *z, float *m, float *n) {
     if (!e || id < 0 || id >= (int)e->members.size() || !e->members[id].used || !e->members[id].nested)
         return GC_EINVAL;

@@ -513,10 +513,10 @@ __device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step
 }
 
 template <int W, int S, bool MULTI>
-__global__ void __launch_bounds__(32 * W) k_pair(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
-                                                  const int2 *__restrict__ tiles, int ntiles,
-                                                  const int *__restrict__ step_base, int step_off, int wait_limit,
-                                                  int stall) {
+__device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFusedGrid *__restrict__ grids,
+                                            const int2 *__restrict__ tiles, int ntiles,
+                                            const int *__restrict__ step_base, int step_off, int wait_limit,
+                                            int stall) {
     extern __shared__ __align__(128) char smem[];
     /* programmatic dependent launch: the previous kernel in the stream has
      * finished and its writes are visible past this point */
@@ -546,6 +546,24 @@ __global__ void __launch_bounds__(32 * W) k_pair(GcFusedGrid one, const GcFusedG
     }
 }
 
+template <int W, int S, bool MULTI>
+__global__ void __launch_bounds__(32 * W) k_pair(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                  const int2 *__restrict__ tiles, int ntiles,
+                                                  const int *__restrict__ step_base, int step_off, int wait_limit,
+                                                  int stall) {
+    pair_kernel<W, S, MULTI>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
+}
+
+/* the work-list form with its registers capped so that 16 warps fit an SM
+ * (the autotuner weighs that occupancy against the spills it costs) */
+template <int W, int S>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_pair_capped(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                                const int2 *__restrict__ tiles, int ntiles,
+                                                                const int *__restrict__ step_base, int step_off,
+                                                                int wait_limit, int stall) {
+    pair_kernel<W, S, true>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
+}
+
 struct PairVariant {
     int w, s;
     void (*one)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
@@ -553,10 +571,13 @@ struct PairVariant {
 };
 
 #define GC_PVARIANT(W, S) {W, S, k_pair<W, S, false>, k_pair<W, S, true>}
+#define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair<W, S, false>, k_pair_capped<W, S>}
 const PairVariant kPairVariants[] = {
     GC_PVARIANT(4, 5), GC_PVARIANT(4, 4), GC_PVARIANT(2, 5), GC_PVARIANT(4, 6),
+    GC_PVARIANT_CAPPED(4, 5), GC_PVARIANT_CAPPED(4, 4),
 };
 #undef GC_PVARIANT
+#undef GC_PVARIANT_CAPPED
 constexpr int kNumPairVariants = sizeof(kPairVariants) / sizeof(kPairVariants[0]);
 
 int pair_smem(const PairVariant &v) {

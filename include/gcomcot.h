@@ -181,6 +181,21 @@ int gc_engine_query(gc_engine *e);
 int gc_engine_read(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
                    int *arrival, float *ts);
 int gc_engine_release(gc_engine *e, int member);
+/* the same results copied asynchronously, queued on the engine's stream
+ * behind the member's issued steps, into host memory the caller owns (from
+ * gc_host_alloc, so the copies do not stall the host); *done receives an event
+ * that completes with the copies (gc_event_query / gc_event_wait, then
+ * gc_event_release).  The member may be released right after: its storage is
+ * freed in stream order, behind the copies. */
+int gc_engine_read_async(gc_engine *e, int member, float *z, float *m, float *n, float *zmax,
+                         int *arrival, float *ts, void **done);
+/* 1 when the event completed, 0 while pending, < 0 on error */
+int gc_event_query(void *event);
+int gc_event_wait(void *event);
+int gc_event_release(void *event);
+/* page-locked host memory for asynchronous reads (NULL when refused) */
+void *gc_host_alloc(long long bytes);
+int gc_host_free(void *p);
 
 /* A nested grid class: the outer grid of class `parent_cls` with one child
  * layer (ALL_GRID sub-cycle, all_grids.f90:4-312).

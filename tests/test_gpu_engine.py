@@ -212,3 +212,21 @@ def test_engine_nested_child_kinds_match_oracle(oracle_mod, kind):
         assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), k
     for k in ("z", "m", "n"):
         assert np.array_equal(got["child_" + k].view(np.uint32), rc[k].view(np.uint32)), "child " + k
+
+
+def test_read_async_matches_read_and_outlives_release():
+    """results copied behind the steps into page-locked memory equal the
+    blocking read; the member is released before the copy is waited for"""
+    cases = [_case(97, 81, 71, 40), _case(130, 70, 72, 33)]
+    with Engine(budget=1 << 30) as eng:
+        ids = [eng.add(c) for c in cases]
+        eng.step(45)
+        eng.sync()
+        want = [eng.read(i, fields=("z", "zmax", "arrival", "ts")) for i in ids]
+        pend = [eng.read_async(i, fields=("z", "zmax", "arrival", "ts")) for i in ids]
+        for i in ids:
+            eng.release(i)
+        got = [p.take() for p in pend]
+    for g, w in zip(got, want):
+        for k in ("z", "zmax", "arrival", "ts"):
+            assert np.array_equal(g[k], w[k]), k
