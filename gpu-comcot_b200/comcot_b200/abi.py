@@ -50,15 +50,18 @@ class ReferenceSession:
                 if host_cache is not None:
                     host_cache[key] = a
             self._host[L.id] = a
+        # arrival tracking starts once the outer layer is on the device
+        self._arrival = arrival
         if init_layers:
             self.init_layers()
-        if arrival:
-            self.lib.gcomcot_set_arrival_(_i(case.root.id), _f(case.arrival_thr))
 
     def init_layers(self):
-        """GCOMCOT_INIT_LAYER for layer 1 then every sub-layer (comcot.f90:281-296)"""
+        """GCOMCOT_INIT_LAYER for layer 1 then every sub-layer
+        (comcot.f90:281-296), then arrival tracking if asked for"""
         for L in self.case.layers:
             self._init_layer(L)
+        if self._arrival:
+            self.lib.gcomcot_set_arrival_(_i(self.case.root.id), _f(self.case.arrival_thr))
 
     def stream(self) -> int:
         return int(self.lib.gcomcot_stream() or 0)

@@ -241,18 +241,27 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     if (C.has_sc) { Pf.m2 = M.sm2; Pf.n2 = M.sn2; }
     cudaEventRecord(e->ev_cfork[a], s);
     cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
-    if (C.has_sc) gc_launch_sc_edges(Pf, Cv1, C.sc, 1, C.rel_time, Cv1.z1, cs);
-    else gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
-    gc_launch_mass(Cv1, cs);
+    /* edge fluxes and mass: one launch for a Cartesian child (JNQ's values
+     * computed where the mass reads them), two otherwise */
+    int pre = 2;
+    if (C.has_sc) {
+        gc_launch_sc_edges(Pf, Cv1, C.sc, 1, C.rel_time, Cv1.z1, cs);
+        gc_launch_mass(Cv1, cs);
+    } else if (gc_launch_edges_mass(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs)) {
+        pre = 1;
+    } else {
+        gc_launch_edges(P, Cv1, C.rel_size, C.rel_time, C.corners, 1, cs);
+        gc_launch_mass(Cv1, cs);
+    }
     /* JNZ_SC sums every child node inside the parent window, row and column
      * 0 included, so in the sub-step that feeds back UPDATE's edge copy
      * follows it (all_grids.f90 order: MOMENT, JNZ, UPDATE) */
     const bool late_update1 = C.has_sc && nhalf == 1;
     if (late_update1) {
         gc_launch_moment(Cv1, cs);
-        e->launches += 3;
+        e->launches += pre + 1;
     } else {
-        e->launches += 2 + gc_launch_moment_update(Cv1, cs);
+        e->launches += pre + gc_launch_moment_update(Cv1, cs);
     }
     cudaEventRecord(e->ev_cjoin[a], cs);
     gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);

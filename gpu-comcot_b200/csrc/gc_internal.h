@@ -110,6 +110,11 @@ void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int
                      const int *corners, int t, cudaStream_t s);
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
                    const int *corners, cudaStream_t s);
+/* JNQ at sub-step t together with a Cartesian child's MASS_C / CONMASS, in
+ * one launch; false (nothing launched) where that form does not apply (t > 1,
+ * other child kinds): then call gc_launch_edges and gc_launch_mass */
+bool gc_launch_edges_mass(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                          const int *corners, int t, cudaStream_t s);
 /* SC_OPTION = 1 coupling of a Cartesian child to a spherical parent: the
  * parent cell (KI, KJ) and bilinear weights of every child edge node, and
  * for JNZ_SC, per parent cell of the child's window, the child nodes that

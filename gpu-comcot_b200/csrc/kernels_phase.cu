@@ -988,6 +988,89 @@ __global__ void k_edges(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int i
     }
 }
 
+/* one value of JNQ's edge interpolation at its first sub-step
+ * (EDGEINTERP_VERT / _HORI, all_grids.f90:502-604, on the parent's level-1
+ * flux as JNQ passes it, all_grids.f90:484-487): the child edge node `run`
+ * (1-based along the edge) of side `side` (0 left M, 1 right M, 2 bottom N,
+ * 3 top N), zero where the child is dry.  The arithmetic of k_edges, node
+ * by node. */
+__device__ __forceinline__ float jnq_node(const GcLayerDev &Pl, const GcLayerDev &C, int side, int run, int ir,
+                                          int is, int ie, int js, int je) {
+    const bool vert = side < 2;
+    const int sd = side & 1;
+    const int line = vert ? (sd == 0 ? is - 1 : ie) : (sd == 0 ? js - 1 : je);
+    const int a0 = vert ? js : is;
+    const int a = a0 + (run - 1) / ir, kk = (run - 1) % ir + 1;
+    const int Pp = Pl.pitch;
+    auto prof = [&](int b) {
+        const int I = vert ? line : b, J = vert ? b : line;
+        const size_t c = (size_t)(J - 1) * Pp + (I - 1);
+        return vert ? Pl.m1[c] : Pl.n1[c];
+    };
+    const float pm = prof(a - 1), p0 = prof(a), pp = prof(a + 1);
+    const float fs = 0.5f * (pm + p0);
+    const float fe = 0.5f * (pp + p0);
+    const float cc1 = (float)((double)(fe - fs) / (double)(2 * ir));
+    const float cc2 = -cc1 + fs;
+    const int fixed = vert ? (sd == 0 ? 0 : C.nx - 1) : (sd == 0 ? 0 : C.ny - 1);
+    const size_t cc = vert ? (size_t)run * C.pitch + fixed : (size_t)fixed * C.pitch + run;
+    float val = 2.0f * (float)kk * cc1 + cc2;
+    if (C.h[cc] + C.z1[cc] <= CC_GX) val = 0.0f;
+    return val;
+}
+
+/* A child's first sub-step of JNQ and its mass (MASS_C / CONMASS) in one
+ * launch.  The threads on the child's edges store JNQ's fluxes there (for
+ * the momentum that follows); a cell next to an edge computes the edge
+ * value it reads itself, by the same arithmetic, instead of waiting for the
+ * store.  Same values as k_edges then k_mass_c. */
+template <bool NONLIN>
+__global__ void k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie, int js, int je) {
+    pdl_enter();
+    const int i = blockIdx.x * BX + threadIdx.x;
+    const int j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const size_t c = (size_t)j * L.pitch + i;
+    const int nx = L.nx, ny = L.ny;
+    /* JNQ's stores: M on columns 0 and nx-1 (rows 1..ny-1), N on rows 0 and
+     * ny-1 (columns 1..nx-1) */
+    if ((i == 0 || i == nx - 1) && j >= 1) L.m1w[c] = jnq_node(Pl, L, i == 0 ? 0 : 1, j, ir, is, ie, js, je);
+    if ((j == 0 || j == ny - 1) && i >= 1) L.n1w[c] = jnq_node(Pl, L, j == 0 ? 2 : 3, i, ir, is, ie, js, je);
+    /* the mass of a child cell (k_mass_c) */
+    if (i == 0 || j == 0) {
+        L.z2[c] = L.z1[c];
+        return;
+    }
+    const float m_c = (i == nx - 1) ? jnq_node(Pl, L, 1, j, ir, is, ie, js, je) : L.m1[c];
+    const float m_w = (i == 1) ? jnq_node(Pl, L, 0, j, ir, is, ie, js, je) : L.m1[c - 1];
+    const float n_c = (j == ny - 1) ? jnq_node(Pl, L, 3, i, ir, is, ie, js, je) : L.n1[c];
+    const float n_s = (j == 1) ? jnq_node(Pl, L, 2, i, ir, is, ie, js, je) : L.n1[c - L.pitch];
+    float h = L.h[c];
+    float zz = L.z1[c] - L.rx * (m_c - m_w) - L.ry * (n_c - n_s);
+    if (fabs_(zz) < CC_EPS) zz = 0.0f;
+    if (!NONLIN) {
+        float out;
+        if (h > CC_GX) {
+            if ((zz + h) <= CC_EPS) zz = -h;
+            out = zz;
+        } else {
+            out = 0.0f;
+        }
+        L.z2[c] = out;
+    } else {
+        float dz, z;
+        if (h > CC_ELMAX) {
+            float dd = zz + h;
+            if (dd >= CC_GX) { dz = dd; z = zz; }
+            else { dz = 0.0f; z = -h; }
+        } else {
+            dz = 0.0f; z = -h;
+        }
+        L.dz2[c] = dz;
+        L.z2[c] = z;
+    }
+}
+
 /* JNZ (all_grids.f90:342-421): mean of wet child surface over each r x r
  * block, summed in the Fortran order (KI outer, KJ inner). */
 __global__ void k_jnz(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int is, int ie, int js,
@@ -1384,6 +1467,16 @@ void gc_launch_edges(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int
     int len = (ie - is + 5) > (je - js + 5) ? (ie - is + 5) : (je - js + 5);
     size_t smem = (size_t)len * sizeof(float);
     launch(k_edges, 4, EDGE_THREADS, smem, s, P, C, rel_size, rel_time, is, ie, js, je, t, len);
+}
+
+bool gc_launch_edges_mass(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
+                          const int *corners, int t, cudaStream_t s) {
+    if (t != 1 || C.root || C.laycord != 1 || (C.laygov != 0 && C.laygov != 1)) return false;
+    const int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
+    (void)rel_time;
+    if (C.laygov == 1) launch(k_mass_c_jnq<true>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
+    else launch(k_mass_c_jnq<false>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
+    return true;
 }
 
 void gc_launch_jnz(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,

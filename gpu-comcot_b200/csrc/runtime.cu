@@ -813,15 +813,21 @@ void gc_subcycle(int parent_id) {
         GcLayer &C = g_rt.layers[cid];
         int nhalf = C.rel_time / 2 + 1;
         for (int k = 1; k <= C.rel_time; k++) {
+            /* edge fluxes and mass: one launch at a Cartesian child's first
+             * sub-step (gc_launch_edges_mass), two otherwise */
+            int pre = 2;
             if (C.has_sc) {
                 /* EDGE_INTERP_SC / NEWQ_SC (all_grids.f90:996-1364) */
                 const GcLayerDev cv = C.view();
                 if (k > 1) { gc_launch_sc_forecast(P.view(), C.sc, g_rt.stream); g_rt.launches++; }
                 gc_launch_sc_edges(P.view(), cv, C.sc, k, C.rel_time, C.sc_stepped ? cv.z1 : cv.z2, g_rt.stream);
+                gc_launch_mass(C.view(), g_rt.stream);
+            } else if (gc_launch_edges_mass(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, k, g_rt.stream)) {
+                pre = 1;
             } else {
                 gc_launch_edges(P.view(), C.view(), C.rel_size, C.rel_time, C.corners, k, g_rt.stream);
+                gc_launch_mass(C.view(), g_rt.stream);
             }
-            gc_launch_mass(C.view(), g_rt.stream);
             C.z2_valid = true;
             gc_subcycle(cid);
             /* UPDATE's edge copy writes the child's row and column 0 alone,
@@ -831,9 +837,9 @@ void gc_subcycle(int parent_id) {
             const bool late_update = C.has_sc && k == nhalf;
             if (late_update) {
                 gc_launch_moment(C.view(), g_rt.stream);
-                g_rt.launches += 3;
+                g_rt.launches += pre + 1;
             } else {
-                g_rt.launches += 2 + gc_launch_moment_update(C.view(), g_rt.stream);
+                g_rt.launches += pre + gc_launch_moment_update(C.view(), g_rt.stream);
             }
             C.mn2_valid = true;
             if (k == nhalf) {
