@@ -44,7 +44,6 @@ namespace {
 
 constexpr int TXW = 128; /* columns per warp tile: 32 lanes x 4 cells */
 
-__device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 
 /* OPEN on a perimeter cell of the outermost layer (boundaries.f90:42-200).
  * h, m, n at (i,j); hs, ns at (i,j-1); mw at (i-1,j). */
@@ -88,7 +87,7 @@ __device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h
         else neg = (qx < 0.0f || qy < 0.0f);
         if (neg) zz = -zz;
     }
-    if (fabs_(zz) > CC_UB) zz = 0.0f;
+    if (fabsf(zz) > CC_UB) zz = 0.0f;
     return zz;
 }
 
@@ -102,7 +101,7 @@ __device__ __forceinline__ float z2_cell(bool root, int i, int r, int nx, int ny
     if (!root && (i == 0 || r == 0)) return z1;
     if (h > CC_GX) {
         float zz = z1 - r1 * (m - mw) - r11 * (n * r6 - ns * r6m);
-        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if (fabsf(zz) < CC_EPS) zz = 0.0f;
         if ((zz + h) <= CC_EPS) zz = -h;
         return zz;
     }
@@ -443,7 +442,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                         /* MASS_S (mass.f90:82-95) */
                         const float h = hv[q];
                         float zz = zv[q] - r1 * (mv[q] - mw) - r11 * (nv[q] * r6 - nbv[q] * r6m);
-                        zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+                        zz = (fabsf(zz) < CC_EPS) ? 0.0f : zz;
                         zz = ((zz + h) <= CC_EPS) ? -h : zz;
                         zn[q] = (h > CC_GX) ? zz : 0.0f;
                     }
@@ -456,7 +455,7 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                     } else {
                         const float h = hA[TXW];
                         float zz = z1h - r1 * (mA[TXW] - mA[TXW - 1]) - r11 * (nA[TXW] * r6 - nB[TXW] * r6m);
-                        zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+                        zz = (fabsf(zz) < CC_EPS) ? 0.0f : zz;
                         zz = ((zz + h) <= CC_EPS) ? -h : zz;
                         zA[TXW] = (h > CC_GX) ? zz : 0.0f;
                     }
@@ -556,11 +555,11 @@ __device__ __forceinline__ bool warp_tile(const GcFusedGrid &Gref, int lt, int s
                         r4 = cy * (0.5f * (h0 + ha[q]));
                     }
                     float vm = mb[q + 1] - r2 * (zb[q + 1] - zb[q]) + r3 * tot_n;
-                    vm = (fabs_(vm) < CC_EPS) ? 0.0f : vm;
+                    vm = (fabsf(vm) < CC_EPS) ? 0.0f : vm;
                     xm[q] = (mdom && h0 > CC_GX && hp1 > CC_GX) ? vm : 0.0f;
                     const float tot_m = mb[q] + ma[q] + mb[q + 1] + ma[q + 1];
                     float vn = nb[q] - r4 * (za[q] - zb[q]) - r5 * tot_m;
-                    vn = (fabs_(vn) < CC_EPS) ? 0.0f : vn;
+                    vn = (fabsf(vn) < CC_EPS) ? 0.0f : vn;
                     xn[q] = (ndom && h0 > CC_GX && ha[q] > CC_GX) ? vn : 0.0f;
                 }
                 if constexpr (EDGE) {

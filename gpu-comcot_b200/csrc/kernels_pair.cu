@@ -72,7 +72,6 @@ __host__ __device__ constexpr int pair_warp_bytes() {
     return (S * PStage::BYTES + S * 8 + 127) / 128 * 128;
 }
 
-__device__ __forceinline__ float fabs_(float x) { return x < 0.0f ? -x : x; }
 __device__ __forceinline__ float shw(float v) { return __shfl_up_sync(FULL, v, 1); }   /* lane - 1 */
 __device__ __forceinline__ float she(float v) { return __shfl_down_sync(FULL, v, 1); } /* lane + 1 */
 __device__ __forceinline__ float comp(const float4 &v, int q) {
@@ -122,7 +121,7 @@ __device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h
         else neg = (qx < 0.0f || qy < 0.0f);
         if (neg) zz = -zz;
     }
-    if (fabs_(zz) > CC_UB) zz = 0.0f;
+    if (fabsf(zz) > CC_UB) zz = 0.0f;
     return zz;
 }
 
@@ -130,7 +129,7 @@ __device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h
 __device__ __forceinline__ float mass1(float z1, float m, float mw, float n, float ns, float h, float r1, float r11,
                                        float r6, float r6m) {
     float zz = z1 - r1 * (m - mw) - r11 * (n * r6 - ns * r6m);
-    zz = (fabs_(zz) < CC_EPS) ? 0.0f : zz;
+    zz = (fabsf(zz) < CC_EPS) ? 0.0f : zz;
     zz = ((zz + h) <= CC_EPS) ? -h : zz;
     return (h > CC_GX) ? zz : 0.0f;
 }
@@ -179,7 +178,7 @@ __device__ __forceinline__ float4 flux_m4(const float4 &m, const float4 &z, floa
         const float tot_n = nbv[q] + nbv[q + 1] + ncv[q] + ncv[q + 1];
         const float r2 = cx * (0.5f * (h0 + hp1));
         float vm = mv[q] - r2 * (zv[q + 1] - zv[q]) + r3 * tot_n;
-        vm = (fabs_(vm) < CC_EPS) ? 0.0f : vm;
+        vm = (fabsf(vm) < CC_EPS) ? 0.0f : vm;
         bool dom = true;
         if constexpr (EDGE) dom = ib + q <= nx - 2;
         o[q] = (dom && h0 > CC_GX && hp1 > CC_GX) ? vm : 0.0f;
@@ -203,7 +202,7 @@ __device__ __forceinline__ float4 flux_n4(const float4 &n, const float4 &za, con
         const float tot_m = mbv[q] + mav[q] + mbv[q + 1] + mav[q + 1];
         const float r4 = cy * (0.5f * (hv[q] + hav[q]));
         float vn = nv[q] - r4 * (zav[q] - zbv[q]) - r5 * tot_m;
-        vn = (fabs_(vn) < CC_EPS) ? 0.0f : vn;
+        vn = (fabsf(vn) < CC_EPS) ? 0.0f : vn;
         bool dom = true;
         if constexpr (EDGE) dom = j <= ny - 2 && ib + q < nx;
         o[q] = (dom && hv[q] > CC_GX && hav[q] > CC_GX) ? vn : 0.0f;
@@ -264,9 +263,140 @@ __host__ __device__ __forceinline__ void pair_cols(int t, int nx, int &s, int &l
     if (hi > nx - 1) hi = nx - 1;
 }
 
-template <int S, bool EDGE>
-__device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, int hi, int j0, int ty, int local,
-                                          char *wsm, int &seq, int wait_limit, bool stall) {
+/* what one warp needs to run its ring of S stages over a tile's rows */
+struct PairRing {
+    char *wsm;      /* the warp's stages (generic address) */
+    uint32_t wbase; /* the same in the shared window */
+    uint32_t bars;  /* the stages' mbarriers */
+    int seq0;       /* ring position of the tile's first row */
+};
+
+/* copies of input row r of a strip (columns s .. s + cb/4 - 1) into the stage
+ * at sb: Z, M, N of the level read, H, max-eta on output rows (out), and the
+ * row's coefficient record.  `fake`: announce 16 bytes no copy delivers. */
+__device__ __forceinline__ void pair_issue(const GcFusedGrid &G, int l0, int r, int s, uint32_t cb, bool out,
+                                           uint32_t sb, uint32_t bar, bool fake) {
+    fence_proxy_async(); /* the warp's reads of this stage come first */
+    if (fake) {
+        mbar_expect_tx(bar, 16u);
+        return;
+    }
+    mbar_expect_tx(bar, (out ? 5u : 4u) * cb + 32u);
+    const size_t ro = (size_t)r * (size_t)G.pitch + s;
+    bulk_g2s(sb + PStage::Z, G.z[l0] + ro, cb, bar);
+    bulk_g2s(sb + PStage::M, G.m[l0] + ro, cb, bar);
+    bulk_g2s(sb + PStage::N, G.n[l0] + ro, cb, bar);
+    bulk_g2s(sb + PStage::H, G.h + ro, cb, bar);
+    if (out) bulk_g2s(sb + PStage::X, G.zmax + ro, cb, bar);
+    bulk_g2s(sb + PStage::C, G.rows + (size_t)r * GC_ROWW, 32u, bar);
+}
+
+/* the first min(S, K) rows of a tile (rows rs ..), issued by lane 0 */
+template <int S>
+__device__ __forceinline__ void pair_prologue(const GcFusedGrid &G, const PairRing &R, int l0, int rs, int K,
+                                              int j0, int jl, int s, uint32_t cb, bool stall) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        const int kk = min(S, K);
+        for (int k = 0; k < kk; k++) {
+            const int st = (R.seq0 + k) % S, r = rs + k;
+            pair_issue(G, l0, r, s, cb, r >= j0 && r <= jl, R.wbase + st * PStage::BYTES, R.bars + 8 * st,
+                       stall && k == 0);
+        }
+    }
+}
+
+/* gauges whose base cell (KI, KJ) lies in the tile's stored block: bit g of
+ * (gm1:gm0).  Also writes the sample of the surface the previous launch left
+ * (level L, step local - 1), which no tile of that launch could take. */
+__device__ __forceinline__ void pair_gauge_setup(const GcFusedGrid &G, int l0, int local, int lo, int hi, int j0,
+                                                 int jl, unsigned &gm0, unsigned &gm1) {
+    const int lane = threadIdx.x & 31;
+    const int ng = G.ng;
+    gm0 = gm1 = 0;
+    if (ng <= 0) return;
+    const size_t P = (size_t)G.pitch;
+    const float *z1g = G.z[l0];
+    bool in0 = false, in1 = false;
+    for (int h = 0; h < 2; h++) {
+        const int g = lane + 32 * h;
+        bool in = false;
+        if (g < ng) {
+            const int ki = G.gij[2 * g] - 1, kj = G.gij[2 * g + 1] - 1;
+            in = ki >= lo && ki <= hi && kj >= j0 && kj <= jl;
+            if (in && local > 0) {
+                const size_t c = (size_t)kj * P + ki;
+                const float l1 = z1g[c], l2v = z1g[c + 1], l3 = z1g[c + P], l4 = z1g[c + P + 1];
+                const float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
+                const float a = l1 * (1.0f - cx) * (1.0f - cy);
+                const float b = l2v * (cx) * (1.0f - cy);
+                const float d = l3 * (1.0f - cx) * (cy);
+                const float e = l4 * (cx) * (cy);
+                G.ts[(size_t)(local - 1) * ng + g] = a + b + d + e;
+            }
+        }
+        if (h == 0) in0 = in;
+        else in1 = in;
+    }
+    gm0 = __ballot_sync(FULL, in0);
+    gm1 = __ballot_sync(FULL, in1);
+}
+
+/* step A's gauge samples whose base row is `row`: surface rows row (lo_row)
+ * and row + 1 (hi_row) */
+__device__ __forceinline__ void pair_gauge_row(const GcFusedGrid &G, unsigned gm0, unsigned gm1, int row,
+                                               const float4 &lo_row, const float4 &hi_row, int s, int local) {
+    for (int h2 = 0; h2 < 2; h2++) {
+        unsigned bits = h2 == 0 ? gm0 : gm1;
+        while (bits) {
+            const int g = __ffs(bits) - 1 + 32 * h2;
+            bits &= bits - 1;
+            if (G.gij[2 * g + 1] - 1 != row) continue;
+            const float v = gauge_sample(lo_row, hi_row, G.gij[2 * g] - 1, s, G.gw[2 * g], G.gw[2 * g + 1]);
+            if ((threadIdx.x & 31) == 0) G.ts[(size_t)local * G.ng + g] = v;
+        }
+    }
+}
+
+/* after a wait gave up: record it, then give the copies still in flight
+ * (ring positions k .. issued-1 of the tile) a bounded chance to land */
+template <int S>
+__device__ __forceinline__ void pair_drain(const PairRing &R, int k, int issued) {
+    if ((threadIdx.x & 31) == 0) atomicExch(&g_pair_error, 1);
+    for (int q = k; q < issued; q++) {
+        const int n = R.seq0 + q;
+        mbar_wait(R.bars + 8 * (n % S), (uint32_t)((n / S) & 1), 1 << 12);
+    }
+}
+
+/* ring stages of rows r (sc), r-1 (sp) and r-2 (spp), and the phase of sc.
+ * Before the tile's second and third rows exist, sp and spp name the first
+ * row's stage (JM1 = max(J-1, 1) at the grid's first row; elsewhere what is
+ * read there feeds only values no output uses). */
+template <int S>
+struct PairStages {
+    int sc, sp, spp;
+    uint32_t ph;
+    __device__ __forceinline__ explicit PairStages(int seq0) {
+        sc = seq0 % S;
+        sp = spp = sc;
+        ph = (uint32_t)((seq0 / S) & 1);
+    }
+    __device__ __forceinline__ void advance() {
+        spp = sp;
+        sp = sc;
+        if (++sc == S) {
+            sc = 0;
+            ph ^= 1u;
+        }
+    }
+};
+
+/* The general body: tiles touching the grid's perimeter (OPEN, the IM1 and
+ * JM1 clamps, the last row's zero N) or running past its last row. */
+template <int S>
+__device__ __forceinline__ bool pair_rows_edge(const GcFusedGrid &G, int s, int lo, int hi, int j0, int ty, int local,
+                                            char *wsm, int &seq, int wait_limit, bool stall) {
     static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
     const int lane = threadIdx.x & 31;
     const int nx = G.nx, ny = G.ny;
@@ -280,70 +410,18 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
     const int jl = min(j0 + ty - 1, ny - 1); /* last output row */
     const int rs = max(j0 - 2, 0), rr = min(j0 + ty + 1, ny - 1), re = min(j0 + ty + 1, ny + 1);
     const int K = rr - rs + 1;
-    const uint32_t wbase = smem_u32(wsm);
-    const uint32_t bars = wbase + S * PStage::BYTES;
-    const int seq0 = seq;
+    PairRing R;
+    R.wsm = wsm;
+    R.wbase = smem_u32(wsm);
+    R.bars = R.wbase + S * PStage::BYTES;
+    R.seq0 = seq;
     /* copies of one row: columns [s, c1) of the strip */
     const int c1 = min(s + 128, G.pitch);
     const uint32_t cb = 4u * (uint32_t)(c1 - s);
-    /* row k of the tile (k = r - rs) lives in stage (seq0 + k) % S */
-    auto stage_of = [&](int k) { return (seq0 + k) % S; };
-    auto issue = [&](int k, bool fake) {
-        if (lane == 0) {
-            const int r = rs + k;
-            const int st = stage_of(k);
-            const uint32_t bar = bars + 8 * st, sb = wbase + st * PStage::BYTES;
-            const bool out = r >= j0 && r <= jl;
-            fence_proxy_async(); /* the warp's reads of this stage come first */
-            if (fake) {
-                mbar_expect_tx(bar, 16u); /* nothing will deliver these bytes */
-                return;
-            }
-            mbar_expect_tx(bar, (out ? 5u : 4u) * cb + 32u);
-            const size_t ro = (size_t)r * P + s;
-            bulk_g2s(sb + PStage::Z, G.z[l0] + ro, cb, bar);
-            bulk_g2s(sb + PStage::M, G.m[l0] + ro, cb, bar);
-            bulk_g2s(sb + PStage::N, G.n[l0] + ro, cb, bar);
-            bulk_g2s(sb + PStage::H, G.h + ro, cb, bar);
-            if (out) bulk_g2s(sb + PStage::X, G.zmax + ro, cb, bar);
-            bulk_g2s(sb + PStage::C, G.rows + (size_t)r * GC_ROWW, 32u, bar);
-        }
-    };
-    __syncwarp();
-    const int kk = min(S, K);
-    for (int k = 0; k < kk; k++) issue(k, stall && k == 0);
-    int issued = kk;
-
-    /* gauges whose base cell this tile owns (at most 64 per grid) */
-    const int ng = G.ng;
-    unsigned gm0 = 0, gm1 = 0;
-    if (ng > 0) {
-        const float *z1g = G.z[l0];
-        bool in0 = false, in1 = false;
-        for (int h = 0; h < 2; h++) {
-            const int g = lane + 32 * h;
-            bool in = false;
-            if (g < ng) {
-                const int ki = G.gij[2 * g] - 1, kj = G.gij[2 * g + 1] - 1;
-                in = ki >= lo && ki <= hi && kj >= j0 && kj <= jl;
-                /* the surface the previous launch left (level L) */
-                if (in && local > 0) {
-                    const size_t c = (size_t)kj * P + ki;
-                    const float l1 = z1g[c], l2v = z1g[c + 1], l3 = z1g[c + P], l4 = z1g[c + P + 1];
-                    const float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
-                    const float a = l1 * (1.0f - cx) * (1.0f - cy);
-                    const float b = l2v * (cx) * (1.0f - cy);
-                    const float d = l3 * (1.0f - cx) * (cy);
-                    const float e = l4 * (cx) * (cy);
-                    G.ts[(size_t)(local - 1) * ng + g] = a + b + d + e;
-                }
-            }
-            if (h == 0) in0 = in;
-            else in1 = in;
-        }
-        gm0 = __ballot_sync(FULL, in0);
-        gm1 = __ballot_sync(FULL, in1);
-    }
+    pair_prologue<S>(G, R, l0, rs, K, j0, jl, s, cb, stall);
+    int issued = min(S, K);
+    unsigned gm0, gm1;
+    pair_gauge_setup(G, l0, local, lo, hi, j0, jl, gm0, gm1);
 
     const int ib = s + 4 * lane;
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -353,18 +431,17 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
     float m2ppw = 0.f, n2pe = 0.f;
     bool ok = true;
     int k = 0; /* real rows consumed */
+    PairStages<S> st(R.seq0);
     for (int r = rs; r <= re; r++) {
         const bool real = r <= ny - 1;
         /* this row's inputs */
         float4 z1 = zero4, m1 = zero4, n1 = zero4, h = zero4;
         float r1 = 0.f, r11 = 0.f, r6 = 0.f, r3 = 0.f, cx = 0.f;
         if (real) {
-            const int st = stage_of(k);
-            const uint32_t par = (uint32_t)(((seq0 + k) / S) & 1);
-            const bool got = mbar_wait(bars + 8 * st, par, wait_limit);
+            const bool got = mbar_wait(R.bars + 8 * st.sc, st.ph, wait_limit);
             ok = __all_sync(FULL, got) != 0;
             if (!ok) break;
-            const char *sp = wsm + st * PStage::BYTES;
+            const char *sp = wsm + st.sc * PStage::BYTES;
             z1 = lds4(sp + PStage::Z + 16 * lane);
             m1 = lds4(sp + PStage::M + 16 * lane);
             n1 = lds4(sp + PStage::N + 16 * lane);
@@ -374,76 +451,52 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
             k++;
         }
         /* rows r-1 and r-2, still staged (JM1 = max(J-1,1): row "-1" is row 0) */
-        const int kp = r - 1 - rs, kpp = r - 2 - rs;
-        const char *spp_ = wsm + stage_of(kp >= 0 ? kp : 0) * PStage::BYTES;
-        const char *sppp = wsm + stage_of(kpp >= 0 ? kpp : (kp >= 0 ? kp : 0)) * PStage::BYTES;
-        float4 n1p, m1p, hp, hpp, xp;
-        float r1p, r11p, r6p, r3p, r5p, cxp, cyp, r6pp, r5pp, cypp;
-        if (kp >= 0) {
-            n1p = lds4(spp_ + PStage::N + 16 * lane);
-            m1p = lds4(spp_ + PStage::M + 16 * lane);
-            hp = lds4(spp_ + PStage::H + 16 * lane);
-            const float4 ca = lds4(spp_ + PStage::C), cc = lds4(spp_ + PStage::C + 16);
-            r1p = ca.x; r11p = ca.y; r6p = ca.z; r3p = ca.w; r5p = cc.x; cxp = cc.y; cyp = cc.z;
-        } else {
-            n1p = n1; m1p = m1; hp = h;
-            r1p = r1; r11p = r11; r6p = r6; r3p = r3; r5p = 0.f; cxp = cx; cyp = 0.f;
-        }
-        if (kpp >= 0) {
-            hpp = lds4(sppp + PStage::H + 16 * lane);
-            const float4 ca = lds4(sppp + PStage::C), cc = lds4(sppp + PStage::C + 16);
-            r6pp = ca.z; r5pp = cc.x; cypp = cc.z;
-        } else {
-            hpp = hp; r6pp = r6p; r5pp = r5p; cypp = cyp;
-        }
+        const char *spp_ = wsm + st.sp * PStage::BYTES;
+        const char *sppp = wsm + st.spp * PStage::BYTES;
+        const float4 n1p = lds4(spp_ + PStage::N + 16 * lane);
+        const float4 m1p = lds4(spp_ + PStage::M + 16 * lane);
+        const float4 hp = lds4(spp_ + PStage::H + 16 * lane);
+        const float4 cap = lds4(spp_ + PStage::C), ccp = lds4(spp_ + PStage::C + 16);
+        const float r1p = cap.x, r11p = cap.y, r6p = cap.z, r3p = cap.w, r5p = ccp.x, cxp = ccp.y, cyp = ccp.z;
+        const float4 hpp = lds4(sppp + PStage::H + 16 * lane);
+        const float4 capp = lds4(sppp + PStage::C), ccpp = lds4(sppp + PStage::C + 16);
+        const float r6pp = capp.z, r5pp = ccpp.x, cypp = ccpp.z;
         /* neighbours along I */
         float m1w = shw(m1.w), m1pw = shw(m1p.w);
-        if (EDGE && ib == 0) { m1w = m1.x; m1pw = m1p.x; } /* IM1 = max(I-1,1) */
+        if (ib == 0) { m1w = m1.x; m1pw = m1p.x; } /* IM1 = max(I-1,1) */
         const float n1e = she(n1.x), he = she(h.x), n1pe = she(n1p.x), hpe = she(hp.x);
 
         /* ---------------- step A ---------------- */
         float4 z2 = zero4, m2 = zero4, n2 = zero4;
         if (real && r >= j0 - 1)
-            z2 = surface4<EDGE>(z1, m1, m1w, n1, n1p, h, hp, r1, r11, r6, r > 0 ? r6p : 0.0f, ib, r, nx, ny);
+            z2 = surface4<true>(z1, m1, m1w, n1, n1p, h, hp, r1, r11, r6, r > 0 ? r6p : 0.0f, ib, r, nx, ny);
         if (real && r >= j0 && r <= j0 + ty) {
             const float z2e = she(z2.x);
-            m2 = flux_m4<EDGE>(m1, z2, z2e, n1, n1e, n1p, n1pe, h, he, cx, r3, ib, nx);
+            m2 = flux_m4<true>(m1, z2, z2e, n1, n1e, n1p, n1pe, h, he, cx, r3, ib, nx);
         }
         /* N of row r-1 needs the surface of row r */
         if (r - 1 >= max(j0 - 1, 0) && r - 1 <= j0 + ty && r - 1 <= ny - 2)
-            n2 = flux_n4<EDGE>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, cyp, r5p, ib, r - 1, nx, ny);
+            n2 = flux_n4<true>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, cyp, r5p, ib, r - 1, nx, ny);
         /* (N at the grid's last row stays 0: J <= NY-1 fails) */
         /* gauges of step A: base row r-1, upper row r */
-        if ((gm0 | gm1) && r - 1 >= j0 && r - 1 <= jl) {
-            for (int h2 = 0; h2 < 2; h2++) {
-                unsigned bits = h2 == 0 ? gm0 : gm1;
-                while (bits) {
-                    const int g = __ffs(bits) - 1 + 32 * h2;
-                    bits &= bits - 1;
-                    if (G.gij[2 * g + 1] - 1 != r - 1) continue;
-                    const float v = gauge_sample(z2p, z2, G.gij[2 * g] - 1, s, G.gw[2 * g], G.gw[2 * g + 1]);
-                    if (lane == 0) G.ts[(size_t)local * ng + g] = v;
-                }
-            }
-        }
+        if ((gm0 | gm1) && r - 1 >= j0 && r - 1 <= jl) pair_gauge_row(G, gm0, gm1, r - 1, z2p, z2, s, local);
 
         /* ---------------- step B ---------------- */
         const int rb = r - 1; /* step B's surface row */
         const float n2e = she(n2.x);
         float4 z3 = zero4;
         float m2w = shw(m2p.w);
-        if (EDGE && ib == 0) m2w = m2p.x;
+        if (ib == 0) m2w = m2p.x;
         if (rb >= j0 && rb <= min(j0 + ty, ny - 1)) {
             const float4 nsb = (rb == 0) ? n2 : n2p; /* N of row rb-1, JM1 clamp at row 0 */
-            z3 = surface4<EDGE>(z2p, m2p, m2w, n2, nsb, hp, hpp, r1p, r11p, r6p, rb > 0 ? r6pp : 0.0f, ib, rb, nx,
+            z3 = surface4<true>(z2p, m2p, m2w, n2, nsb, hp, hpp, r1p, r11p, r6p, rb > 0 ? r6pp : 0.0f, ib, rb, nx,
                                 ny);
             if (rb <= jl) {
                 /* max-eta and arrival after step A, then after step B */
-                xp = lds4(spp_ + PStage::X + 16 * lane);
+                const float4 xp = lds4(spp_ + PStage::X + 16 * lane);
                 const float4 xa = max4(xp, z2p), xb = max4(xa, z3);
                 const size_t ro = (size_t)rb * P;
-                float *zrow = G.z[l2] + ro;
-                st4m(zrow, ib, lo, hi, z3);
+                st4m(G.z[l2] + ro, ib, lo, hi, z3);
                 st4m(G.zmax + ro, ib, lo, hi, xb);
                 if (do_arr) {
                     if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
@@ -455,7 +508,7 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
                 const float z3e = she(z3.x);
                 const float4 ncb = (rb == 0) ? n2 : n2p;
                 const float nce = (rb == 0) ? n2e : n2pe;
-                const float4 m3 = flux_m4<EDGE>(m2p, z3, z3e, n2, n2e, ncb, nce, hp, hpe, cxp, r3p, ib, nx);
+                const float4 m3 = flux_m4<true>(m2p, z3, z3e, n2, n2e, ncb, nce, hp, hpe, cxp, r3p, ib, nx);
                 st4m(G.m[l2] + ro, ib, lo, hi, m3);
             }
         }
@@ -463,7 +516,7 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
         if (rb - 1 >= j0 && rb - 1 <= jl) {
             float4 n3 = zero4;
             if (rb - 1 <= ny - 2)
-                n3 = flux_n4<EDGE>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, cypp, r5pp, ib, rb - 1, nx, ny);
+                n3 = flux_n4<true>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, cypp, r5pp, ib, rb - 1, nx, ny);
             st4m(G.n[l2] + (size_t)(rb - 1) * P, ib, lo, hi, n3);
         }
 
@@ -474,20 +527,147 @@ __device__ __forceinline__ bool pair_rows(const GcFusedGrid &G, int s, int lo, i
         z3p = z3;
         /* row r-2 is no longer needed: refill its stage S rows ahead */
         __syncwarp();
+        const int kpp = r - 2 - rs;
         if (kpp >= 0 && kpp + S < K) {
-            issue(kpp + S, false);
+            if (lane == 0) {
+                const int rn = rs + kpp + S;
+                pair_issue(G, l0, rn, s, cb, rn >= j0 && rn <= jl, R.wbase + st.spp * PStage::BYTES,
+                           R.bars + 8 * st.spp, false);
+            }
             issued = kpp + S + 1;
         }
+        st.advance();
     }
-    seq = seq0 + K;
+    seq = R.seq0 + K;
     if (!ok) {
-        /* record the failure, then give the copies still in flight a bounded
-         * chance to land before the warp leaves */
-        if (lane == 0) atomicExch(&g_pair_error, 1);
-        for (int q = k; q < issued; q++) {
-            const int n = seq0 + q;
-            mbar_wait(bars + 8 * (n % S), (uint32_t)((n / S) & 1), 1 << 12);
+        pair_drain<S>(R, k, issued);
+        return false;
+    }
+    __syncwarp();
+    return true;
+}
+
+/* The body for a tile none of whose computed cells (halo rows and columns
+ * included) lies on the grid's perimeter: every row is real, there is no
+ * boundary logic, and each iteration computes every quantity.  On the first
+ * four iterations some of them come from rows the tile does not hold exactly
+ * (a step-A surface is exact from row j0-1, step-A fluxes from row j0, step
+ * B from row j0 + 1 on the iteration index), and nothing stored or carried
+ * into an exact value reads them: stores are the only guarded operations.
+ * Such a tile stores columns s+4 .. s+123, lanes 1 .. 30 in full.  Its
+ * first row, j0-2, only feeds the N flux of row j0-2 and the surface and
+ * fluxes of row j0-1 through the next iterations' reads of the stage it
+ * stays in, so it gets no iteration of its own. */
+template <int S>
+__device__ __forceinline__ bool pair_rows_int(const GcFusedGrid &G, int s, int j0, int ty, int local, char *wsm,
+                                           int &seq, int wait_limit, bool stall) {
+    static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
+    const int lane = threadIdx.x & 31;
+    const size_t P = (size_t)G.pitch;
+    const int l0 = local % 3, l2 = l0 == 0 ? 2 : l0 - 1; /* buffers of levels L and L + 2 */
+    const bool do_arr = (G.flags & GC_F_ARRIVAL) != 0;
+    const float thr = G.thr;
+    const int jl = j0 + ty - 1, rs = j0 - 2, K = ty + 4;
+    PairRing R;
+    R.wsm = wsm;
+    R.wbase = smem_u32(wsm);
+    R.bars = R.wbase + S * PStage::BYTES;
+    R.seq0 = seq;
+    pair_prologue<S>(G, R, l0, rs, K, j0, jl, s, 512u, stall);
+    int issued = min(S, K);
+    unsigned gm0, gm1;
+    pair_gauge_setup(G, l0, local, s + 4, s + kPairOut + 3, j0, jl, gm0, gm1);
+
+    const int ib = s + 4 * lane;
+    const bool own = lane >= 1 && lane <= 30;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 z2p = zero4, m2p = zero4, m2pp = zero4, n2p = zero4, z3p = zero4;
+    float m2ppw = 0.f, n2pe = 0.f;
+    bool ok = true;
+    int k = 0;
+    PairStages<S> st(R.seq0);
+    /* the tile's first row (j0-2) is read only as row r-1 and r-2 of later
+     * iterations (nothing of its own step-A results is used): wait for it,
+     * and iterate from the row after it */
+    ok = __all_sync(FULL, mbar_wait(R.bars + 8 * st.sc, st.ph, wait_limit)) != 0;
+    if (ok) {
+        k = 1;
+        st.advance();
+    }
+    for (int r = ok ? rs + 1 : rs + K; r < rs + K; r++) {
+        const bool got = mbar_wait(R.bars + 8 * st.sc, st.ph, wait_limit);
+        if (!__all_sync(FULL, got)) {
+            ok = false;
+            break;
         }
+        k++;
+        const char *pc = wsm + st.sc * PStage::BYTES;
+        const char *pp = wsm + st.sp * PStage::BYTES;
+        const char *ppp = wsm + st.spp * PStage::BYTES;
+        const float4 z1 = lds4(pc + PStage::Z + 16 * lane), m1 = lds4(pc + PStage::M + 16 * lane);
+        const float4 n1 = lds4(pc + PStage::N + 16 * lane), h = lds4(pc + PStage::H + 16 * lane);
+        const float4 ca = lds4(pc + PStage::C), cc = lds4(pc + PStage::C + 16);
+        const float4 n1p = lds4(pp + PStage::N + 16 * lane), m1p = lds4(pp + PStage::M + 16 * lane);
+        const float4 hp = lds4(pp + PStage::H + 16 * lane);
+        const float4 cap = lds4(pp + PStage::C), ccp = lds4(pp + PStage::C + 16);
+        const float4 hpp = lds4(ppp + PStage::H + 16 * lane);
+        const float4 capp = lds4(ppp + PStage::C), ccpp = lds4(ppp + PStage::C + 16);
+        /* record: r1 r11 r6 r3 | r5 cx cy - */
+        const float m1w = shw(m1.w), m1pw = shw(m1p.w);
+        const float n1e = she(n1.x), he = she(h.x), n1pe = she(n1p.x), hpe = she(hp.x);
+
+        /* step A: surface of row r, M of row r, N of row r-1 */
+        const float4 z2 = surface4<false>(z1, m1, m1w, n1, n1p, h, hp, ca.x, ca.y, ca.z, cap.z, ib, r, 0, 0);
+        const float4 m2 = flux_m4<false>(m1, z2, she(z2.x), n1, n1e, n1p, n1pe, h, he, cc.y, ca.w, ib, 0);
+        const float4 n2 = flux_n4<false>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, ccp.z, ccp.x, ib, r - 1, 0, 0);
+        if ((gm0 | gm1) && r - 1 >= j0 && r - 1 <= jl) pair_gauge_row(G, gm0, gm1, r - 1, z2p, z2, s, local);
+
+        /* step B: surface and M of row r-1, N of row r-2 */
+        const int rb = r - 1;
+        const float n2e = she(n2.x), m2w = shw(m2p.w);
+        const float4 z3 = surface4<false>(z2p, m2p, m2w, n2, n2p, hp, hpp, cap.x, cap.y, cap.z, capp.z, ib, rb, 0, 0);
+        if (rb >= j0 && rb <= jl) {
+            const float4 m3 = flux_m4<false>(m2p, z3, she(z3.x), n2, n2e, n2p, n2pe, hp, hpe, ccp.y, cap.w, ib, 0);
+            const float4 xp = lds4(pp + PStage::X + 16 * lane);
+            const float4 xa = max4(xp, z2p), xb = max4(xa, z3);
+            const size_t ro = (size_t)rb * P + ib;
+            if (own) {
+                *reinterpret_cast<float4 *>(G.z[l2] + ro) = z3;
+                *reinterpret_cast<float4 *>(G.zmax + ro) = xb;
+                *reinterpret_cast<float4 *>(G.m[l2] + ro) = m3;
+                if (do_arr) {
+                    if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
+                        arrive4(G.arrival + ro - ib, ib, ib, ib + 3, z2p, xp, hp, thr, local + 1);
+                    if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
+                        arrive4(G.arrival + ro - ib, ib, ib, ib + 3, z3, xa, hp, thr, local + 2);
+                }
+            }
+        }
+        if (rb - 1 >= j0 && rb - 1 <= jl) {
+            const float4 n3 =
+                flux_n4<false>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, ccpp.z, ccpp.x, ib, rb - 1, 0, 0);
+            if (own) *reinterpret_cast<float4 *>(G.n[l2] + (size_t)(rb - 1) * P + ib) = n3;
+        }
+
+        z2p = z2;
+        m2pp = m2p; m2ppw = m2w; m2p = m2;
+        n2p = n2; n2pe = n2e;
+        z3p = z3;
+        __syncwarp();
+        const int kpp = r - 2 - rs;
+        if (kpp >= 0 && kpp + S < K) {
+            if (lane == 0) {
+                const int rn = rs + kpp + S;
+                pair_issue(G, l0, rn, s, 512u, rn >= j0 && rn <= jl, R.wbase + st.spp * PStage::BYTES,
+                           R.bars + 8 * st.spp, false);
+            }
+            issued = kpp + S + 1;
+        }
+        st.advance();
+    }
+    seq = R.seq0 + K;
+    if (!ok) {
+        pair_drain<S>(R, k, issued);
         return false;
     }
     __syncwarp();
@@ -508,10 +688,9 @@ __device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step
      * lies on the grid's perimeter or beyond it runs the body compiled
      * without boundary logic */
     const bool edge = !(s >= 1 && s + 127 <= G.nx - 2 && j0 - 2 >= 1 && j0 + ty + 1 <= G.ny - 2);
-    return edge ? pair_rows<S, true>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall)
-                : pair_rows<S, false>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall);
+    return edge ? pair_rows_edge<S>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall)
+                : pair_rows_int<S>(G, s, j0, ty, local, wsm, seq, wait_limit, stall);
 }
-
 template <int W, int S, bool MULTI>
 __device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFusedGrid *__restrict__ grids,
                                             const int2 *__restrict__ tiles, int ntiles,

@@ -74,7 +74,7 @@ __global__ void k_mass_s(GcLayerDev L) {
             float r6 = GC_ROW(L, GC_R6, j), r6m = GC_ROW(L, GC_R6, j - 1);
             float zz = L.z1[c] - r1 * (L.m1[c] - L.m1[c - 1])
                        - r11 * (L.n1[c] * r6 - L.n1[c - L.pitch] * r6m);
-            if (fabs_(zz) < CC_EPS) zz = 0.0f;
+            if (fabsf(zz) < CC_EPS) zz = 0.0f;
             float dd = zz + h;
             if (dd >= CC_GX) { dz = dd; z = zz; }
             else { dz = 0.0f; z = -h; }
@@ -91,7 +91,7 @@ __global__ void k_mass_s(GcLayerDev L) {
         float r6 = GC_ROW(L, GC_R6, j), r6m = GC_ROW(L, GC_R6, j - 1);
         float zz = L.z1[c] - r1 * (L.m1[c] - L.m1[c - 1])
                    - r11 * (L.n1[c] * r6 - L.n1[c - L.pitch] * r6m);
-        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if (fabsf(zz) < CC_EPS) zz = 0.0f;
         if ((zz + h) <= CC_EPS) zz = -h;
         out = zz;
     } else {
@@ -116,7 +116,7 @@ __global__ void k_mass_c(GcLayerDev L) {
     }
     float h = L.h[c];
     float zz = L.z1[c] - L.rx * (L.m1[c] - L.m1[c - 1]) - L.ry * (L.n1[c] - L.n1[c - L.pitch]);
-    if (fabs_(zz) < CC_EPS) zz = 0.0f;
+    if (fabsf(zz) < CC_EPS) zz = 0.0f;
     if (!NONLIN) {
         float out;
         if (h > CC_GX) {
@@ -182,7 +182,7 @@ __global__ void k_mass_d(GcLayerDev L) {
                  - GC_ROW(L, GC_R11, j) * (L.n1[c] * GC_ROW(L, GC_R6, j) - L.n1[c - L.pitch] * GC_ROW(L, GC_R6, j - 1));
         else
             zz = L.z1[c] - L.rx * (L.m1[c] - L.m1[c - 1]) - L.ry * (L.n1[c] - L.n1[c - L.pitch]);
-        if (fabs_(zz) < CC_EPS) zz = 0.0f;
+        if (fabsf(zz) < CC_EPS) zz = 0.0f;
         if ((zz + h) <= 0.0f) zz = -h;
         out = zz;
     }
@@ -226,7 +226,7 @@ __global__ void k_momt_d(GcLayerDev L) {
                     const float scm = r2 * CC_TWLVTH * ((z[cu + 1] - 2.0f * z[cp] + z[cm + 1]) - (z[cu] - 2.0f * z[c] + z[cm]));
                     xm = xm - scm;
                 }
-                if (fabs_(xm) < CC_EPS) xm = 0.0f;
+                if (fabsf(xm) < CC_EPS) xm = 0.0f;
             }
             L.m2[c] = xm;
         } else if (h > CC_GX && hp1 > CC_GX) {
@@ -247,7 +247,7 @@ __global__ void k_momt_d(GcLayerDev L) {
                 xm = xm - scm;
             }
             if (L.fric_switch != 1) xm = fdiv1(xm, 1.0f + ff);
-            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            if (fabsf(xm) < CC_EPS) xm = 0.0f;
             L.m2[c] = xm;
         } else {
             L.m2[c] = L.m1[c];
@@ -272,7 +272,7 @@ __global__ void k_momt_d(GcLayerDev L) {
                     const float scm = r4 * CC_TWLVTH * ((z[ce + P] - 2.0f * z[cq] + z[cw + P]) - (z[ce] - 2.0f * z[c] + z[cw]));
                     xn = xn - scm;
                 }
-                if (fabs_(xn) < CC_EPS) xn = 0.0f;
+                if (fabsf(xn) < CC_EPS) xn = 0.0f;
             }
             L.n2[c] = xn;
         } else if (h > CC_GX && hq1 > CC_GX) {
@@ -293,7 +293,7 @@ __global__ void k_momt_d(GcLayerDev L) {
                 xn = xn - scm;
             }
             if (L.fric_switch != 1) xn = fdiv1(xn, 1.0f + ff);
-            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            if (fabsf(xn) < CC_EPS) xn = 0.0f;
             L.n2[c] = xn;
         } else {
             L.n2[c] = L.n1[c];
@@ -320,7 +320,7 @@ __global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
             float tot_n = L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1];
             xm = L.m1[c] - r2_at(L, i, j, c, h, hp1) * (L.z2[c + 1] - L.z2[c])
                  + GC_ROW(L, GC_R3, j) * tot_n;
-            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            if (fabsf(xm) < CC_EPS) xm = 0.0f;
         }
     }
     L.m2[c] = xm;
@@ -333,7 +333,7 @@ __global__ void k_momt_s(GcLayerDev L, int i0, int j0, int ni, int nj) {
             float tot_m = L.m1[cw] + L.m1[cw + P] + L.m1[c] + L.m1[c + P];
             xn = L.n1[c] - r4_at(L, i, j, c, h, hq1) * (L.z2[c + P] - L.z2[c])
                  - GC_ROW(L, GC_R5, j) * tot_m;
-            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            if (fabsf(xn) < CC_EPS) xn = 0.0f;
         }
     }
     L.n2[c] = xn;
@@ -381,7 +381,7 @@ __global__ void k_momt_c(GcLayerDev L) {
                 xm = xm - scm;
             }
             if (L.fric_switch != 1) xm = fdiv1(xm, 1.0f + ff);
-            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            if (fabsf(xm) < CC_EPS) xm = 0.0f;
         }
     }
     L.m2[c] = xm;
@@ -415,7 +415,7 @@ __global__ void k_momt_c(GcLayerDev L) {
                 xn = xn - scm;
             }
             if (L.fric_switch != 1) xn = fdiv1(xn, 1.0f + ff);
-            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            if (fabsf(xn) < CC_EPS) xn = 0.0f;
         }
     }
     L.n2[c] = xn;
@@ -566,7 +566,7 @@ __device__ __forceinline__ float conmome_x(const GcLayerDev &L, const XFace &f, 
         xp = xp - advx - advy;
     }
     if (L.fric_switch != 1) xp = fdiv1(xp, 1.0f + ff);
-    if (fabs_(xp) < CC_EPS) xp = 0.0f;
+    if (fabsf(xp) < CC_EPS) xp = 0.0f;
     float lim = CC_VLIMIT * dd;
     if (xp > lim) xp = lim;
     if (xp < -lim) xp = -lim;
@@ -655,7 +655,7 @@ __device__ __forceinline__ float conmome_y(const GcLayerDev &L, const YFace &f, 
         xq = xq - advx - advy;
     }
     if (L.fric_switch != 1) xq = fdiv1(xq, 1.0f + ff);
-    if (fabs_(xq) < CC_EPS) xq = 0.0f;
+    if (fabsf(xq) < CC_EPS) xq = 0.0f;
     float lim = CC_VLIMIT * dd;
     if (xq > lim) xq = lim;
     if (xq < -lim) xq = -lim;
@@ -753,7 +753,7 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
  * its cell's x and y faces from shared memory.  Same values, same
  * arithmetic (conmome_x / conmome_y): the same bits. */
 template <bool SPH>
-__global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd) {
+__device__ __forceinline__ void conmome_tile_body(const GcLayerDev &L, int upd) {
     pdl_enter();
     constexpr int TW = BX + 4, TH = BY + 4;
     __shared__ float tile[4][TH][TW];
@@ -777,11 +777,16 @@ __global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd)
         else if (i == 0) L.z2[c] = L.z2[c + 1];
     }
     /* the tile holds the clamped neighbour of every in-grid cell it covers;
-     * for a cell near the grid edge the clamp is repeated on the offset */
+     * for a cell near the grid edge the clamp is repeated on the offset.  A
+     * block whose window lies inside the grid clamps nothing: its cells read
+     * the tile at fixed offsets from their own slot. */
     auto get = [&](int f, int di, int dj) {
         const int ii = min(max(i + di, 0), ix - 1) - i0 + 2, jj = min(max(j + dj, 0), jy - 1) - j0 + 2;
         return tile[f][jj][ii];
     };
+    const float *own = &tile[0][threadIdx.y + 2][threadIdx.x + 2];
+    auto get_in = [&](int f, int di, int dj) { return own[(f * TH + dj) * TW + di]; };
+    const bool inside = i0 >= 2 && i0 + TW - 3 <= ix - 1 && j0 >= 2 && j0 + TH - 3 <= jy - 1;
     const bool span = adv_span(i, j, ix, jy);
     const bool inx = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && i <= ix - 2 && j >= 1);
     const bool iny = L.root ? (i <= ix - 2 && j <= jy - 2) : (i >= 1 && j >= 1 && j <= jy - 2);
@@ -789,20 +794,33 @@ __global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd)
     float outx = 0.0f, outy = 0.0f;
     if (inx) {
         XFace f;
-        load_x(f, get);
+        if (inside) load_x(f, get_in);
+        else load_x(f, get);
         f.h_c = h_c; f.h_p = __ldg(L.h + c + 1); f.hp_c = __ldg(L.hp + c);
         f.z1_c = z1_c;
         outx = conmome_x<SPH>(L, f, j, jy, span);
     }
     if (iny) {
         YFace f;
-        load_y(f, get);
+        if (inside) load_y(f, get_in);
+        else load_y(f, get);
         f.h_c = h_c; f.h_q = __ldg(L.h + c + P); f.hq_c = __ldg(L.hq + c);
         f.z1_c = z1_c;
         outy = conmome_y<SPH>(L, f, i, j, ix, span);
     }
     L.m2[c] = outx;
     L.n2[c] = outy;
+}
+template <bool SPH>
+__global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd) {
+    conmome_tile_body<SPH>(L, upd);
+}
+/* the same with registers capped so that five blocks fit an SM (48
+ * registers, a few spills): a child grid of about 2 blocks per resident
+ * slot then needs two waves of blocks instead of two and a sliver */
+template <bool SPH>
+__global__ void __launch_bounds__(BX * BY, 5) k_conmome_tile5(GcLayerDev L, int upd) {
+    conmome_tile_body<SPH>(L, upd);
 }
 
 /* ---------------------------------------------------------------- */
@@ -861,7 +879,7 @@ __device__ float open_cell(const GcLayerDev &L, int i, int j) {
         else neg = (qx < 0.0f || qy < 0.0f);
         if (neg) zz = -zz;
     }
-    if (fabs_(zz) > CC_UB) zz = 0.0f;
+    if (fabsf(zz) > CC_UB) zz = 0.0f;
     return zz;
 }
 
@@ -956,7 +974,7 @@ __global__ void k_edges(GcLayerDev Pl, GcLayerDev C, int ir, int rel_time, int i
                             x = Pl.n1[c] - Pl.gry * hn * (Pl.z2[c + Pp] - Pl.z2[c]);
                         }
                     }
-                    if (fabs_(x) < CC_EPS) x = 0.0f;
+                    if (fabsf(x) < CC_EPS) x = 0.0f;
                     *cache = x;
                 }
                 v = c1 * (*cache) + c2 * (vert ? Pl.m1[c] : Pl.n1[c]);
@@ -1019,35 +1037,12 @@ __device__ __forceinline__ float jnq_node(const GcLayerDev &Pl, const GcLayerDev
     return val;
 }
 
-/* A child's first sub-step of JNQ and its mass (MASS_C / CONMASS) in one
- * launch.  The threads on the child's edges store JNQ's fluxes there (for
- * the momentum that follows); a cell next to an edge computes the edge
- * value it reads itself, by the same arithmetic, instead of waiting for the
- * store.  Same values as k_edges then k_mass_c. */
+/* CONMASS / MASS_C of one child cell from its fluxes (mass.f90:103-160) */
 template <bool NONLIN>
-__global__ void k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie, int js, int je) {
-    pdl_enter();
-    const int i = blockIdx.x * BX + threadIdx.x;
-    const int j = blockIdx.y * BY + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
-    const size_t c = (size_t)j * L.pitch + i;
-    const int nx = L.nx, ny = L.ny;
-    /* JNQ's stores: M on columns 0 and nx-1 (rows 1..ny-1), N on rows 0 and
-     * ny-1 (columns 1..nx-1) */
-    if ((i == 0 || i == nx - 1) && j >= 1) L.m1w[c] = jnq_node(Pl, L, i == 0 ? 0 : 1, j, ir, is, ie, js, je);
-    if ((j == 0 || j == ny - 1) && i >= 1) L.n1w[c] = jnq_node(Pl, L, j == 0 ? 2 : 3, i, ir, is, ie, js, je);
-    /* the mass of a child cell (k_mass_c) */
-    if (i == 0 || j == 0) {
-        L.z2[c] = L.z1[c];
-        return;
-    }
-    const float m_c = (i == nx - 1) ? jnq_node(Pl, L, 1, j, ir, is, ie, js, je) : L.m1[c];
-    const float m_w = (i == 1) ? jnq_node(Pl, L, 0, j, ir, is, ie, js, je) : L.m1[c - 1];
-    const float n_c = (j == ny - 1) ? jnq_node(Pl, L, 3, i, ir, is, ie, js, je) : L.n1[c];
-    const float n_s = (j == 1) ? jnq_node(Pl, L, 2, i, ir, is, ie, js, je) : L.n1[c - L.pitch];
-    float h = L.h[c];
-    float zz = L.z1[c] - L.rx * (m_c - m_w) - L.ry * (n_c - n_s);
-    if (fabs_(zz) < CC_EPS) zz = 0.0f;
+__device__ __forceinline__ void mass_c_store(const GcLayerDev &L, size_t c, float z1, float m_c, float m_w,
+                                             float n_c, float n_s, float h) {
+    float zz = z1 - L.rx * (m_c - m_w) - L.ry * (n_c - n_s);
+    if (fabsf(zz) < CC_EPS) zz = 0.0f;
     if (!NONLIN) {
         float out;
         if (h > CC_GX) {
@@ -1068,6 +1063,77 @@ __global__ void k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie
         }
         L.dz2[c] = dz;
         L.z2[c] = z;
+    }
+}
+
+/* a child cell on or next to the child's edge: JNQ's stores (M on columns 0
+ * and nx-1, rows 1..ny-1; N on rows 0 and ny-1, columns 1..nx-1), then its
+ * mass with the edge fluxes it reads computed in place */
+template <bool NONLIN>
+__device__ __forceinline__ void mass_c_jnq_edge(const GcLayerDev &Pl, const GcLayerDev &L, int i, int j, int ir, int is,
+                                             int ie, int js, int je) {
+    const int nx = L.nx, ny = L.ny;
+    const size_t c = (size_t)j * L.pitch + i;
+    if ((i == 0 || i == nx - 1) && j >= 1) L.m1w[c] = jnq_node(Pl, L, i == 0 ? 0 : 1, j, ir, is, ie, js, je);
+    if ((j == 0 || j == ny - 1) && i >= 1) L.n1w[c] = jnq_node(Pl, L, j == 0 ? 2 : 3, i, ir, is, ie, js, je);
+    if (i == 0 || j == 0) {
+        L.z2[c] = L.z1[c];
+        return;
+    }
+    const float m_c = (i == nx - 1) ? jnq_node(Pl, L, 1, j, ir, is, ie, js, je) : L.m1[c];
+    const float m_w = (i == 1) ? jnq_node(Pl, L, 0, j, ir, is, ie, js, je) : L.m1[c - 1];
+    const float n_c = (j == ny - 1) ? jnq_node(Pl, L, 3, i, ir, is, ie, js, je) : L.n1[c];
+    const float n_s = (j == 1) ? jnq_node(Pl, L, 2, i, ir, is, ie, js, je) : L.n1[c - L.pitch];
+    mass_c_store<NONLIN>(L, c, L.z1[c], m_c, m_w, n_c, n_s, L.h[c]);
+}
+
+/* A child's first sub-step of JNQ and its mass (MASS_C / CONMASS) in one
+ * launch.  The threads on the child's edges store JNQ's fluxes there (for
+ * the momentum that follows); a cell next to an edge computes the edge
+ * value it reads itself, by the same arithmetic, instead of waiting for the
+ * store.  Same values as k_edges then k_mass_c.  A thread takes two cells
+ * BX columns apart and issues both cells' loads before either's arithmetic,
+ * and blocks of 128 threads with registers capped for ten blocks per SM,
+ * so that a child grid of up to about 370,000 cells runs in one wave of
+ * blocks with two cells' loads in flight per thread. */
+constexpr int MJ_BY = 4; /* rows per block of k_mass_c_jnq (blocks of 2*BX x MJ_BY cells) */
+template <bool NONLIN>
+__global__ void __launch_bounds__(BX *MJ_BY, 10) k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie,
+                                                               int js, int je) {
+    pdl_enter();
+    const int j = blockIdx.y * MJ_BY + threadIdx.y;
+    const int ia = blockIdx.x * (2 * BX) + threadIdx.x;
+    const int nx = L.nx, ny = L.ny;
+    if (j >= ny || ia >= nx) return;
+    const size_t P = (size_t)L.pitch;
+    const float *__restrict__ m1 = L.m1;
+    const float *__restrict__ n1 = L.n1;
+    const float *__restrict__ z1 = L.z1;
+    const float *__restrict__ hf = L.h;
+    const bool row_in = j >= 2 && j <= ny - 2;
+    float mc[2], mw[2], nc[2], ns[2], hh[2], zo[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        /* a cell past the edge or on the edge band loads a safe interior
+         * cell and stores nothing here */
+        const int i = min(max(ia + q * BX, 1), nx - 1);
+        const int jj = max(j, 1);
+        const size_t c = (size_t)jj * P + i;
+        mc[q] = m1[c];
+        mw[q] = m1[c - 1];
+        nc[q] = n1[c];
+        ns[q] = n1[c - P];
+        hh[q] = hf[c];
+        zo[q] = z1[c];
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int i = ia + q * BX;
+        if (i >= nx) break;
+        if (row_in && i >= 2 && i <= nx - 2)
+            mass_c_store<NONLIN>(L, (size_t)j * P + i, zo[q], mc[q], mw[q], nc[q], ns[q], hh[q]);
+        else
+            mass_c_jnq_edge<NONLIN>(Pl, L, i, j, ir, is, ie, js, je);
     }
 }
 
@@ -1223,7 +1289,7 @@ __global__ void k_sc_forecast(GcLayerDev P, GcScView sv) {
                                                  (P.z2[cq] - 2.0f * P.z2[c] + P.z2[cm]));
                 xm = xm - scm;
             }
-            if (fabs_(xm) < CC_EPS) xm = 0.0f;
+            if (fabsf(xm) < CC_EPS) xm = 0.0f;
             out = xm;
         }
         P.m2[c] = out;
@@ -1241,7 +1307,7 @@ __global__ void k_sc_forecast(GcLayerDev P, GcScView sv) {
                                                  (P.z2[ce] - 2.0f * P.z2[c] + P.z2[cw]));
                 xn = xn - scm;
             }
-            if (fabs_(xn) < CC_EPS) xn = 0.0f;
+            if (fabsf(xn) < CC_EPS) xn = 0.0f;
             out = xn;
         }
         P.n2[c] = out;
@@ -1398,20 +1464,27 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
-/* CONMOME: the shared-memory tile form (both faces per thread), or with
+/* CONMOME: the shared-memory tile form (both faces per thread), with
+ * GCOMCOT_CONMOME_TILE=5 its register-capped form, or with
  * GCOMCOT_CONMOME_TILE=0 the one-face form (x and y as two grid layers);
- * both compute the same bits */
-static bool conmome_tiled() {
-    static const int on = [] {
+ * all compute the same bits */
+static int conmome_form() {
+    static const int form = [] {
         const char *v = getenv("GCOMCOT_CONMOME_TILE");
-        return (v && v[0] == '0') ? 0 : 1;
+        if (v && v[0] == '0') return 0;
+        if (v && v[0] == '5') return 5;
+        return 1;
     }();
-    return on != 0;
+    return form;
 }
 
 static void launch_conmome(const GcLayerDev &L, int upd, cudaStream_t s) {
     const bool sph = L.laycord == 0;
-    if (conmome_tiled()) {
+    const int form = conmome_form();
+    if (form == 5) {
+        if (sph) launch(k_conmome_tile5<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
+        else launch(k_conmome_tile5<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
+    } else if (form == 1) {
         if (sph) launch(k_conmome_tile<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
         else launch(k_conmome_tile<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
     } else {
@@ -1474,8 +1547,9 @@ bool gc_launch_edges_mass(const GcLayerDev &P, const GcLayerDev &C, int rel_size
     if (t != 1 || C.root || C.laycord != 1 || (C.laygov != 0 && C.laygov != 1)) return false;
     const int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
     (void)rel_time;
-    if (C.laygov == 1) launch(k_mass_c_jnq<true>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
-    else launch(k_mass_c_jnq<false>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
+    const dim3 g((unsigned)((C.nx + 2 * BX - 1) / (2 * BX)), (unsigned)((C.ny + MJ_BY - 1) / MJ_BY));
+    if (C.laygov == 1) launch(k_mass_c_jnq<true>, g, dim3(BX, MJ_BY), 0, s, P, C, rel_size, is, ie, js, je);
+    else launch(k_mass_c_jnq<false>, g, dim3(BX, MJ_BY), 0, s, P, C, rel_size, is, ie, js, je);
     return true;
 }
 

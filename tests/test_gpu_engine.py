@@ -110,6 +110,24 @@ def test_engine_nested_member_matches_oracle(oracle_mod, rel_time, graphs):
         _check_nested(eng.read(mid), case, oracle_mod)
 
 
+@pytest.mark.parametrize("laygov,rel_time", [(1, 1), (0, 2)])
+def test_engine_wide_child_matches_oracle(oracle_mod, laygov, rel_time):
+    """a 151 x 151 child (interior CONMOME blocks, two-cell JNQ + mass threads)"""
+    case = synth.nested_case("w", 241, 161, 2.0, 2.0, [150, 199, 50, 99], 3, 30, seed=23, rel_time=rel_time,
+                             child_laygov=laygov, ngauges=2)
+    C = case.layers[1]
+    jj, ii = np.mgrid[0:C.ny, 0:C.nx]
+    bump = 0.8 * np.exp(-((ii - 0.45 * C.nx) ** 2 + (jj - 0.55 * C.ny) ** 2) / (2.0 * 18.0 ** 2))
+    C.Z0 = np.where(C.H > 0.0, bump, 0.0).astype(np.float32)
+    with Engine(budget=2 << 30) as eng:
+        eng.config(variant=-1, use_graphs=1, chunk=8)
+        mid = eng.add(case)
+        eng.step(32)
+        eng.sync()
+        assert eng.done(mid)
+        _check_nested(eng.read(mid), case, oracle_mod)
+
+
 def test_engine_nested_and_single_members_in_one_mix(oracle_mod):
     nest = [_nested(61, 2, 34), _nested(62, None, 50)]
     single = [_case(97, 81, 63, 41), _case(70, 60, 64, 66)]

@@ -89,6 +89,32 @@ def test_nested_nonlinear_child(oracle_mod, rel_time):
     assert np.array_equal(cz.view(np.uint32), rc["z"].view(np.uint32))
 
 
+def _wide_nested(laygov, rel_time, seed):
+    """a child 151 x 151 wide with a surface bump of its own: CONMOME blocks
+    whose stencil window lies inside the child (fixed tile offsets) and the
+    first sub-step's JNQ + mass launch with two cells per thread both run"""
+    case = synth.nested_case("w", 241, 161, 2.0, 2.0, [150, 199, 50, 99], 3, 0, seed=seed, rel_time=rel_time,
+                             child_laygov=laygov)
+    C = case.layers[1]
+    jj, ii = np.mgrid[0:C.ny, 0:C.nx]
+    bump = 0.8 * np.exp(-((ii - 0.45 * C.nx) ** 2 + (jj - 0.55 * C.ny) ** 2) / (2.0 * 18.0 ** 2))
+    C.Z0 = np.where(C.H > 0.0, bump, 0.0).astype(np.float32)
+    return case
+
+
+@pytest.mark.parametrize("laygov", [0, 1])
+@pytest.mark.parametrize("rel_time", [1, 2])
+def test_nested_wide_child(oracle_mod, laygov, rel_time):
+    case = _wide_nested(laygov, rel_time, 21 + laygov)
+    gpu, _, o, _ = _run_both(case, 30, oracle_mod)
+    ref, rc = o.layer(0), o.layer(1)
+    cz, (cm, cn) = gpu["children"][0]
+    assert np.abs(rc["m"]).max() > 0 and np.abs(rc["n"]).max() > 0
+    for a, b, what in ((gpu["z"], ref["z"], "parent eta"), (gpu["mn"][0], ref["m"], "parent M"),
+                       (cz, rc["z"], "child eta"), (cm, rc["m"], "child M"), (cn, rc["n"], "child N")):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), what
+
+
 @pytest.mark.parametrize("kind", ["linear_cartesian", "linear_spherical", "nonlinear_spherical"])
 def test_nested_linear_child(oracle_mod, kind):
     """MASS_C/MOMT_C (LAYCORD 1, LAYGOV 0), MASS_S/MOMT_S and
