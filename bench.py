@@ -92,6 +92,19 @@ def profiled_traffic(name="fused_linear_step_c2.txt", key="traffic_bytes_per_lau
     return None
 
 
+def pair_note(rl, one_step_gbs, profile):
+    """a two-step launch reads and writes each cell once for two steps, so its
+    HBM fraction is of half the one-step bytes; it is bounded by instruction
+    issue instead.  Adds the HBM fraction a one-step kernel would need for
+    the same steps/s, and the limiter."""
+    if rl.get("steps_per_launch") == 2:
+        rl["one_step_equivalent_gbs"] = one_step_gbs
+        rl["one_step_equivalent_frac"] = one_step_gbs / rl["peak"]
+        rl["limiter"] = (f"instruction issue (two steps per HBM pass: same bytes per launch as one step); "
+                         f"issue-slot and stall figures in profiles/{profile}")
+    return rl
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -403,10 +416,11 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
                                   f"dt 2 s, max-eta + arrival; scenarios/hour of 3600-step forecasts",
                       "tile_variant": chosen,
                       "l2": f"working set {nscen} x 7 fields x 4.9 MB >> 126 MB L2"},
-           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "traffic": None if tr is None else nscen * tr,
-                        "peak_kind": f"{peak_kind} (copy bandwidth)",
-                        "algorithmic_bytes_per_launch": bpc * cells * nscen, "steps_per_launch": spl},
+           "roofline": pair_note({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                  "frac": achieved / peak, "traffic": None if tr is None else nscen * tr,
+                                  "peak_kind": f"{peak_kind} (copy bandwidth)",
+                                  "algorithmic_bytes_per_launch": bpc * cells * nscen, "steps_per_launch": spl},
+                                 achieved * spl, "pair_ensemble_step_c4.txt"),
            "clocks": ck, "gpu_launches": launches, "parity": merge_parity(recs)}
     if plain:
         rec["plain_path"] = plain
@@ -804,10 +818,11 @@ def run_single(args, torch, dist, rank, world, local):
                    "l2": ("working set 156 MB per step (8 fields x 19.5 MB) > 126 MB L2; no flush"
                           if args.workload == "c2" else "working set 3.5 MB: L2 resident (no flush)"),
                    "tile_variant": variant, "graph_chunk": 64},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_kind": f"{peak_kind} (copy bandwidth)",
-                     "algorithmic_bytes_per_launch": bytes_launch, "steps_per_launch": spl},
+        "roofline": pair_note({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak, "traffic": traffic,
+                               "peak_kind": f"{peak_kind} (copy bandwidth)",
+                               "algorithmic_bytes_per_launch": bytes_launch, "steps_per_launch": spl},
+                              achieved * spl, "pair_linear_step_c2.txt"),
         "clocks": ck,
         "gpu_launches": launches,
     }

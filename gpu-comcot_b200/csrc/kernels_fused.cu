@@ -39,57 +39,15 @@
 #include <type_traits>
 
 #include "fused.h"
+#include "open_bd.cuh"
 
 namespace {
 
 constexpr int TXW = 128; /* columns per warp tile: 32 lanes x 4 cells */
 
 
-/* OPEN on a perimeter cell of the outermost layer (boundaries.f90:42-200).
- * h, m, n at (i,j); hs, ns at (i,j-1); mw at (i-1,j). */
-__device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h, float hs, float m,
-                                           float mw, float n, float ns) {
-    if (!(h > CC_GX)) return 0.0f;
-    float cc = sqrtf(CC_GRAV * h);
-    float zz;
-    bool corner = (i == 0 || i == nx - 1) && (j == 0 || j == ny - 1);
-    if (!corner) {
-        if (j == 0) {
-            float uh = 0.5f * (m + mw);
-            float uu = sqrtf(uh * uh + n * n);
-            zz = uu / cc;
-            if (n > 0.0f) zz = -zz;
-        } else if (j == ny - 1) {
-            float uh = 0.5f * (m + mw);
-            float uu = sqrtf(uh * uh + ns * ns);
-            zz = uu / cc;
-            if (ns < 0.0f) zz = -zz;
-        } else if (i == 0) {
-            float uh = (hs > CC_GX) ? 0.5f * (n + ns) : n;
-            float uu = sqrtf(uh * uh + m * m);
-            zz = uu / cc;
-            if (m > 0.0f) zz = -zz;
-        } else {
-            float uh = 0.5f * (n + ns);
-            float uu = sqrtf(uh * uh + mw * mw);
-            zz = uu / cc;
-            if (mw < 0.0f) zz = -zz;
-        }
-    } else {
-        float qx = (i == 0) ? m : mw;
-        float qy = (j == 0) ? n : ns;
-        float uh = sqrtf(qx * qx + qy * qy);
-        zz = uh / cc;
-        bool neg;
-        if (i == 0 && j == 0) neg = (qx > 0.0f || qy > 0.0f);
-        else if (j == 0) neg = (qx < 0.0f || qy > 0.0f);
-        else if (i == 0) neg = (qx > 0.0f || qy < 0.0f);
-        else neg = (qx < 0.0f || qy < 0.0f);
-        if (neg) zz = -zz;
-    }
-    if (fabsf(zz) > CC_UB) zz = 0.0f;
-    return zz;
-}
+/* OPEN on a perimeter cell of the outermost layer (open_bd.cuh) */
+using gcopen::open_cell;
 
 /* new surface of one cell: OPEN on the outer layer's perimeter, carried
  * level-1 value on a child's I=1 / J=1 edges, MASS_S elsewhere */

@@ -51,6 +51,7 @@
  */
 #include "bulk_pipe.cuh"
 #include "fused.h"
+#include "open_bd.cuh"
 
 namespace {
 
@@ -79,51 +80,8 @@ __device__ __forceinline__ float comp(const float4 &v, int q) {
 }
 __device__ __forceinline__ float4 lds4(const char *p) { return *reinterpret_cast<const float4 *>(p); }
 
-/* OPEN on a perimeter cell of the outermost layer (boundaries.f90:42-200).
- * h, m, n at (i,j); hs, ns at (i,j-1); mw at (i-1,j). */
-__device__ __forceinline__ float open_cell(int i, int j, int nx, int ny, float h, float hs, float m, float mw,
-                                           float n, float ns) {
-    if (!(h > CC_GX)) return 0.0f;
-    float cc = sqrtf(CC_GRAV * h);
-    float zz;
-    bool corner = (i == 0 || i == nx - 1) && (j == 0 || j == ny - 1);
-    if (!corner) {
-        if (j == 0) {
-            float uh = 0.5f * (m + mw);
-            float uu = sqrtf(uh * uh + n * n);
-            zz = uu / cc;
-            if (n > 0.0f) zz = -zz;
-        } else if (j == ny - 1) {
-            float uh = 0.5f * (m + mw);
-            float uu = sqrtf(uh * uh + ns * ns);
-            zz = uu / cc;
-            if (ns < 0.0f) zz = -zz;
-        } else if (i == 0) {
-            float uh = (hs > CC_GX) ? 0.5f * (n + ns) : n;
-            float uu = sqrtf(uh * uh + m * m);
-            zz = uu / cc;
-            if (m > 0.0f) zz = -zz;
-        } else {
-            float uh = 0.5f * (n + ns);
-            float uu = sqrtf(uh * uh + mw * mw);
-            zz = uu / cc;
-            if (mw < 0.0f) zz = -zz;
-        }
-    } else {
-        float qx = (i == 0) ? m : mw;
-        float qy = (j == 0) ? n : ns;
-        float uh = sqrtf(qx * qx + qy * qy);
-        zz = uh / cc;
-        bool neg;
-        if (i == 0 && j == 0) neg = (qx > 0.0f || qy > 0.0f);
-        else if (j == 0) neg = (qx < 0.0f || qy > 0.0f);
-        else if (i == 0) neg = (qx > 0.0f || qy < 0.0f);
-        else neg = (qx < 0.0f || qy < 0.0f);
-        if (neg) zz = -zz;
-    }
-    if (fabsf(zz) > CC_UB) zz = 0.0f;
-    return zz;
-}
+/* OPEN on a perimeter cell of the outermost layer (open_bd.cuh) */
+using gcopen::open_cell;
 
 /* MASS_S at one cell (mass.f90:82-95) */
 __device__ __forceinline__ float mass1(float z1, float m, float mw, float n, float ns, float h, float r1, float r11,
@@ -392,21 +350,58 @@ struct PairStages {
     }
 };
 
-/* The general body: tiles touching the grid's perimeter (OPEN, the IM1 and
- * JM1 clamps, the last row's zero N) or running past its last row. */
+/* the new surface of a lane's four cells on a tile that touches the grid's
+ * perimeter: MASS_S everywhere, then OPEN over it on the perimeter.  On a
+ * perimeter row (warp-uniform) every cell takes OPEN.  Elsewhere OPEN takes
+ * the west column (lane 0's first cell, when the strip starts at column 0)
+ * and the east column (cell qe of lane le): every lane evaluates OPEN on its
+ * own cell at that position, so the warp does not diverge, and the lane that
+ * holds the column keeps it.  mw: M west of the lane's first cell (the IM1
+ * clamp already applied); ns, hs: N and H of row r-1. */
+__device__ __forceinline__ float4 surface4_edge(const float4 &z1, const float4 &m, float mw, const float4 &n,
+                                                const float4 &ns, const float4 &h, const float4 &hs, float r1,
+                                                float r11, float r6, float r6m, int ib, int r, int nx, int ny,
+                                                bool west, bool east, bool hold_e, int qe) {
+    if (r == 0 || r == ny - 1) return surface4<true>(z1, m, mw, n, ns, h, hs, r1, r11, r6, r6m, ib, r, nx, ny);
+    float4 o = surface4<false>(z1, m, mw, n, ns, h, hs, r1, r11, r6, r6m, ib, r, nx, ny);
+    if (west) {
+        const float ow = open_cell(0, r, nx, ny, h.x, hs.x, m.x, mw, n.x, ns.x);
+        if ((threadIdx.x & 31) == 0) o.x = ow;
+    }
+    if (east) {
+        const float mwq = qe == 0 ? mw : comp(m, qe - 1);
+        const float oe = open_cell(nx - 1, r, nx, ny, comp(h, qe), comp(hs, qe), comp(m, qe), mwq, comp(n, qe),
+                                   comp(ns, qe));
+        if (hold_e) {
+            o.x = qe == 0 ? oe : o.x;
+            o.y = qe == 1 ? oe : o.y;
+            o.z = qe == 2 ? oe : o.z;
+            o.w = qe == 3 ? oe : o.w;
+        }
+    }
+    return o;
+}
+
+/* The body for tiles touching the grid's perimeter or running past its last
+ * row.  Same shape as the interior body (every quantity computed on every
+ * iteration, stores guarded), with the boundary applied over it: OPEN on the
+ * perimeter (surface4_edge), the IM1 clamp on the west column, the flux
+ * domains (M to column nx-2, N to row ny-2 and column nx-1: the last row's N
+ * stays 0), the JM1 clamp of M on row 0, and zero inputs on rows past the
+ * grid (the bottom tile iterates two rows beyond it to finish step B).  Rows
+ * above j0-1 and rows past the grid compute values that nothing stored reads. */
 template <int S>
 __device__ __forceinline__ bool pair_rows_edge(const GcFusedGrid &G, int s, int lo, int hi, int j0, int ty, int local,
-                                            char *wsm, int &seq, int wait_limit, bool stall) {
+                                               char *wsm, int &seq, int wait_limit, bool stall) {
     static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
     const int lane = threadIdx.x & 31;
     const int nx = G.nx, ny = G.ny;
     const size_t P = (size_t)G.pitch;
-    const int l0 = local % 3, l2 = (l0 + 2) % 3; /* buffers of levels L and L + 2 */
+    const int l0 = local % 3, l2 = l0 == 0 ? 2 : l0 - 1; /* buffers of levels L and L + 2 */
     const bool do_arr = (G.flags & GC_F_ARRIVAL) != 0;
     const float thr = G.thr;
 
-    /* rows: inputs rs .. rr (real rows), iterations rs .. re (rows past the
-     * grid's last carry nothing new; they finish the last rows' step B) */
+    /* rows: inputs rs .. rr (real rows), iterations rs .. re */
     const int jl = min(j0 + ty - 1, ny - 1); /* last output row */
     const int rs = max(j0 - 2, 0), rr = min(j0 + ty + 1, ny - 1), re = min(j0 + ty + 1, ny + 1);
     const int K = rr - rs + 1;
@@ -424,103 +419,99 @@ __device__ __forceinline__ bool pair_rows_edge(const GcFusedGrid &G, int s, int 
     pair_gauge_setup(G, l0, local, lo, hi, j0, jl, gm0, gm1);
 
     const int ib = s + 4 * lane;
+    const bool west = s == 0, east = s + 127 >= nx - 1;
+    const int le = (nx - 1 - s) >> 2, qe = (nx - 1 - s) & 3; /* lane and cell of column nx-1 */
+    const bool hold_e = east && lane == le;
+    const bool w0 = west && lane == 0; /* IM1 = max(I-1,1) on column 0 */
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    /* step A's results of earlier rows, carried in registers (p: row r-1,
-     * pp: row r-2) */
     float4 z2p = zero4, m2p = zero4, m2pp = zero4, n2p = zero4, z3p = zero4;
     float m2ppw = 0.f, n2pe = 0.f;
     bool ok = true;
     int k = 0; /* real rows consumed */
     PairStages<S> st(R.seq0);
-    for (int r = rs; r <= re; r++) {
+    int r = rs;
+    if (j0 >= 2) {
+        /* the first row (j0-2) is read only as row r-1 and r-2 of later
+         * iterations: wait for it and iterate from the row after it */
+        ok = __all_sync(FULL, mbar_wait(R.bars + 8 * st.sc, st.ph, wait_limit)) != 0;
+        if (ok) {
+            k = 1;
+            st.advance();
+        }
+        r = ok ? rs + 1 : re + 1;
+    }
+    for (; r <= re; r++) {
         const bool real = r <= ny - 1;
-        /* this row's inputs */
-        float4 z1 = zero4, m1 = zero4, n1 = zero4, h = zero4;
-        float r1 = 0.f, r11 = 0.f, r6 = 0.f, r3 = 0.f, cx = 0.f;
+        float4 z1 = zero4, m1 = zero4, n1 = zero4, h = zero4, ca = zero4, cc = zero4;
         if (real) {
             const bool got = mbar_wait(R.bars + 8 * st.sc, st.ph, wait_limit);
             ok = __all_sync(FULL, got) != 0;
             if (!ok) break;
-            const char *sp = wsm + st.sc * PStage::BYTES;
-            z1 = lds4(sp + PStage::Z + 16 * lane);
-            m1 = lds4(sp + PStage::M + 16 * lane);
-            n1 = lds4(sp + PStage::N + 16 * lane);
-            h = lds4(sp + PStage::H + 16 * lane);
-            const float4 ca = lds4(sp + PStage::C), cc = lds4(sp + PStage::C + 16);
-            r1 = ca.x; r11 = ca.y; r6 = ca.z; r3 = ca.w; cx = cc.y;
+            const char *pc = wsm + st.sc * PStage::BYTES;
+            z1 = lds4(pc + PStage::Z + 16 * lane);
+            m1 = lds4(pc + PStage::M + 16 * lane);
+            n1 = lds4(pc + PStage::N + 16 * lane);
+            h = lds4(pc + PStage::H + 16 * lane);
+            ca = lds4(pc + PStage::C);
+            cc = lds4(pc + PStage::C + 16);
             k++;
         }
         /* rows r-1 and r-2, still staged (JM1 = max(J-1,1): row "-1" is row 0) */
-        const char *spp_ = wsm + st.sp * PStage::BYTES;
-        const char *sppp = wsm + st.spp * PStage::BYTES;
-        const float4 n1p = lds4(spp_ + PStage::N + 16 * lane);
-        const float4 m1p = lds4(spp_ + PStage::M + 16 * lane);
-        const float4 hp = lds4(spp_ + PStage::H + 16 * lane);
-        const float4 cap = lds4(spp_ + PStage::C), ccp = lds4(spp_ + PStage::C + 16);
-        const float r1p = cap.x, r11p = cap.y, r6p = cap.z, r3p = cap.w, r5p = ccp.x, cxp = ccp.y, cyp = ccp.z;
-        const float4 hpp = lds4(sppp + PStage::H + 16 * lane);
-        const float4 capp = lds4(sppp + PStage::C), ccpp = lds4(sppp + PStage::C + 16);
-        const float r6pp = capp.z, r5pp = ccpp.x, cypp = ccpp.z;
-        /* neighbours along I */
-        float m1w = shw(m1.w), m1pw = shw(m1p.w);
-        if (ib == 0) { m1w = m1.x; m1pw = m1p.x; } /* IM1 = max(I-1,1) */
+        const char *pp = wsm + st.sp * PStage::BYTES;
+        const char *ppp = wsm + st.spp * PStage::BYTES;
+        const float4 n1p = lds4(pp + PStage::N + 16 * lane), m1p = lds4(pp + PStage::M + 16 * lane);
+        const float4 hp = lds4(pp + PStage::H + 16 * lane);
+        const float4 cap = lds4(pp + PStage::C), ccp = lds4(pp + PStage::C + 16);
+        const float4 hpp = lds4(ppp + PStage::H + 16 * lane);
+        const float4 capp = lds4(ppp + PStage::C), ccpp = lds4(ppp + PStage::C + 16);
+        /* record: r1 r11 r6 r3 | r5 cx cy - */
+        /* every lane takes part in every shuffle (full mask); the IM1 clamp
+         * selects after it */
+        const float m1w_s = shw(m1.w), m1pw_s = shw(m1p.w);
+        const float m1w = w0 ? m1.x : m1w_s, m1pw = w0 ? m1p.x : m1pw_s;
         const float n1e = she(n1.x), he = she(h.x), n1pe = she(n1p.x), hpe = she(hp.x);
 
-        /* ---------------- step A ---------------- */
-        float4 z2 = zero4, m2 = zero4, n2 = zero4;
-        if (real && r >= j0 - 1)
-            z2 = surface4<true>(z1, m1, m1w, n1, n1p, h, hp, r1, r11, r6, r > 0 ? r6p : 0.0f, ib, r, nx, ny);
-        if (real && r >= j0 && r <= j0 + ty) {
-            const float z2e = she(z2.x);
-            m2 = flux_m4<true>(m1, z2, z2e, n1, n1e, n1p, n1pe, h, he, cx, r3, ib, nx);
-        }
-        /* N of row r-1 needs the surface of row r */
-        if (r - 1 >= max(j0 - 1, 0) && r - 1 <= j0 + ty && r - 1 <= ny - 2)
-            n2 = flux_n4<true>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, cyp, r5p, ib, r - 1, nx, ny);
-        /* (N at the grid's last row stays 0: J <= NY-1 fails) */
-        /* gauges of step A: base row r-1, upper row r */
+        /* step A: surface of row r, M of row r, N of row r-1 (0 on the last
+         * row and past it: J <= NY-1 fails) */
+        float4 z2 = surface4_edge(z1, m1, m1w, n1, n1p, h, hp, ca.x, ca.y, ca.z, cap.z, ib, r, nx, ny, west, east,
+                                  hold_e, qe);
+        if (!real) z2 = zero4;
+        const float4 m2 = flux_m4<true>(m1, z2, she(z2.x), n1, n1e, n1p, n1pe, h, he, cc.y, ca.w, ib, nx);
+        const float4 n2 = flux_n4<true>(n1p, z2, z2p, m1p, m1pw, m1, m1w, hp, h, ccp.z, ccp.x, ib, r - 1, nx, ny);
         if ((gm0 | gm1) && r - 1 >= j0 && r - 1 <= jl) pair_gauge_row(G, gm0, gm1, r - 1, z2p, z2, s, local);
 
-        /* ---------------- step B ---------------- */
-        const int rb = r - 1; /* step B's surface row */
+        /* step B: surface and M of row r-1, N of row r-2 */
+        const int rb = r - 1;
         const float n2e = she(n2.x);
-        float4 z3 = zero4;
-        float m2w = shw(m2p.w);
-        if (ib == 0) m2w = m2p.x;
-        if (rb >= j0 && rb <= min(j0 + ty, ny - 1)) {
-            const float4 nsb = (rb == 0) ? n2 : n2p; /* N of row rb-1, JM1 clamp at row 0 */
-            z3 = surface4<true>(z2p, m2p, m2w, n2, nsb, hp, hpp, r1p, r11p, r6p, rb > 0 ? r6pp : 0.0f, ib, rb, nx,
-                                ny);
-            if (rb <= jl) {
-                /* max-eta and arrival after step A, then after step B */
-                const float4 xp = lds4(spp_ + PStage::X + 16 * lane);
-                const float4 xa = max4(xp, z2p), xb = max4(xa, z3);
-                const size_t ro = (size_t)rb * P;
-                st4m(G.z[l2] + ro, ib, lo, hi, z3);
-                st4m(G.zmax + ro, ib, lo, hi, xb);
-                if (do_arr) {
-                    if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
-                        arrive4(G.arrival + ro, ib, lo, hi, z2p, xp, hp, thr, local + 1);
-                    if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
-                        arrive4(G.arrival + ro, ib, lo, hi, z3, xa, hp, thr, local + 2);
-                }
-                /* M of row rb */
-                const float z3e = she(z3.x);
-                const float4 ncb = (rb == 0) ? n2 : n2p;
-                const float nce = (rb == 0) ? n2e : n2pe;
-                const float4 m3 = flux_m4<true>(m2p, z3, z3e, n2, n2e, ncb, nce, hp, hpe, cxp, r3p, ib, nx);
-                st4m(G.m[l2] + ro, ib, lo, hi, m3);
+        const float m2w_s = shw(m2p.w);
+        const float m2w = w0 ? m2p.x : m2w_s;
+        const float4 z3 = surface4_edge(z2p, m2p, m2w, n2, n2p, hp, hpp, cap.x, cap.y, cap.z, capp.z, ib, rb, nx, ny,
+                                        west, east, hold_e, qe);
+        if (rb >= j0 && rb <= jl) {
+            /* M of row rb: N of rows rb and JM1(rb) */
+            const float4 ncb = rb == 0 ? n2 : n2p;
+            const float nce = rb == 0 ? n2e : n2pe;
+            const float4 m3 = flux_m4<true>(m2p, z3, she(z3.x), n2, n2e, ncb, nce, hp, hpe, ccp.y, cap.w, ib, nx);
+            /* max-eta and arrival after step A, then after step B */
+            const float4 xp = lds4(pp + PStage::X + 16 * lane);
+            const float4 xa = max4(xp, z2p), xb = max4(xa, z3);
+            const size_t ro = (size_t)rb * P;
+            st4m(G.z[l2] + ro, ib, lo, hi, z3);
+            st4m(G.zmax + ro, ib, lo, hi, xb);
+            st4m(G.m[l2] + ro, ib, lo, hi, m3);
+            if (do_arr) {
+                if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
+                    arrive4(G.arrival + ro, ib, lo, hi, z2p, xp, hp, thr, local + 1);
+                if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
+                    arrive4(G.arrival + ro, ib, lo, hi, z3, xa, hp, thr, local + 2);
             }
         }
-        /* N of row rb-1 needs the surface of row rb */
         if (rb - 1 >= j0 && rb - 1 <= jl) {
-            float4 n3 = zero4;
-            if (rb - 1 <= ny - 2)
-                n3 = flux_n4<true>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, cypp, r5pp, ib, rb - 1, nx, ny);
+            const float4 n3 =
+                flux_n4<true>(n2p, z3, z3p, m2pp, m2ppw, m2p, m2w, hpp, hp, ccpp.z, ccpp.x, ib, rb - 1, nx, ny);
             st4m(G.n[l2] + (size_t)(rb - 1) * P, ib, lo, hi, n3);
         }
 
-        /* ---------------- carry ---------------- */
         z2p = z2;
         m2pp = m2p; m2ppw = m2w; m2p = m2;
         n2p = n2; n2pe = n2e;
@@ -725,12 +716,23 @@ __device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFuse
     }
 }
 
-template <int W, int S, bool MULTI>
-__global__ void __launch_bounds__(32 * W) k_pair(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
-                                                  const int2 *__restrict__ tiles, int ntiles,
-                                                  const int *__restrict__ step_base, int step_off, int wait_limit,
-                                                  int stall) {
-    pair_kernel<W, S, MULTI>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
+/* the single-grid form, held to 128 registers so that 16 warps fit an SM
+ * (it needs no spill for that) */
+template <int W, int S>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_pair_one(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                              const int2 *__restrict__ tiles, int ntiles,
+                                                              const int *__restrict__ step_base, int step_off,
+                                                              int wait_limit, int stall) {
+    pair_kernel<W, S, false>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
+}
+
+/* the work-list form: each tile's descriptor is loaded from the list */
+template <int W, int S>
+__global__ void __launch_bounds__(32 * W) k_pair_list(GcFusedGrid one, const GcFusedGrid *__restrict__ grids,
+                                                       const int2 *__restrict__ tiles, int ntiles,
+                                                       const int *__restrict__ step_base, int step_off,
+                                                       int wait_limit, int stall) {
+    pair_kernel<W, S, true>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
 }
 
 /* the work-list form with its registers capped so that 16 warps fit an SM
@@ -749,8 +751,8 @@ struct PairVariant {
     void (*multi)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
 };
 
-#define GC_PVARIANT(W, S) {W, S, k_pair<W, S, false>, k_pair<W, S, true>}
-#define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair<W, S, false>, k_pair_capped<W, S>}
+#define GC_PVARIANT(W, S) {W, S, k_pair_one<W, S>, k_pair_list<W, S>}
+#define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair_one<W, S>, k_pair_capped<W, S>}
 const PairVariant kPairVariants[] = {
     GC_PVARIANT(4, 5), GC_PVARIANT(4, 4), GC_PVARIANT(2, 5), GC_PVARIANT(4, 6),
     GC_PVARIANT_CAPPED(4, 5), GC_PVARIANT_CAPPED(4, 4),

@@ -815,13 +815,6 @@ template <bool SPH>
 __global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd) {
     conmome_tile_body<SPH>(L, upd);
 }
-/* the same with registers capped so that five blocks fit an SM (48
- * registers, a few spills): a child grid of about 2 blocks per resident
- * slot then needs two waves of blocks instead of two and a sliver */
-template <bool SPH>
-__global__ void __launch_bounds__(BX * BY, 5) k_conmome_tile5(GcLayerDev L, int upd) {
-    conmome_tile_body<SPH>(L, upd);
-}
 
 /* ---------------------------------------------------------------- */
 /* OPEN radiation boundary (boundaries.f90:22-202), outermost layer  */
@@ -1088,52 +1081,20 @@ __device__ __forceinline__ void mass_c_jnq_edge(const GcLayerDev &Pl, const GcLa
 }
 
 /* A child's first sub-step of JNQ and its mass (MASS_C / CONMASS) in one
- * launch.  The threads on the child's edges store JNQ's fluxes there (for
- * the momentum that follows); a cell next to an edge computes the edge
- * value it reads itself, by the same arithmetic, instead of waiting for the
- * store.  Same values as k_edges then k_mass_c.  A thread takes two cells
- * BX columns apart and issues both cells' loads before either's arithmetic,
- * and blocks of 128 threads with registers capped for ten blocks per SM,
- * so that a child grid of up to about 370,000 cells runs in one wave of
- * blocks with two cells' loads in flight per thread. */
-constexpr int MJ_BY = 4; /* rows per block of k_mass_c_jnq (blocks of 2*BX x MJ_BY cells) */
+ * launch, one cell per thread.  The threads on the child's edges store
+ * JNQ's fluxes there (for the momentum that follows); a cell next to an
+ * edge computes the edge value it reads itself, by the same arithmetic,
+ * instead of waiting for the store.  Same values as k_edges then k_mass_c. */
 template <bool NONLIN>
-__global__ void __launch_bounds__(BX *MJ_BY, 10) k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie,
-                                                               int js, int je) {
+__global__ void k_mass_c_jnq(GcLayerDev Pl, GcLayerDev L, int ir, int is, int ie, int js, int je) {
     pdl_enter();
-    const int j = blockIdx.y * MJ_BY + threadIdx.y;
-    const int ia = blockIdx.x * (2 * BX) + threadIdx.x;
-    const int nx = L.nx, ny = L.ny;
-    if (j >= ny || ia >= nx) return;
-    const size_t P = (size_t)L.pitch;
-    const float *__restrict__ m1 = L.m1;
-    const float *__restrict__ n1 = L.n1;
-    const float *__restrict__ z1 = L.z1;
-    const float *__restrict__ hf = L.h;
-    const bool row_in = j >= 2 && j <= ny - 2;
-    float mc[2], mw[2], nc[2], ns[2], hh[2], zo[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        /* a cell past the edge or on the edge band loads a safe interior
-         * cell and stores nothing here */
-        const int i = min(max(ia + q * BX, 1), nx - 1);
-        const int jj = max(j, 1);
-        const size_t c = (size_t)jj * P + i;
-        mc[q] = m1[c];
-        mw[q] = m1[c - 1];
-        nc[q] = n1[c];
-        ns[q] = n1[c - P];
-        hh[q] = hf[c];
-        zo[q] = z1[c];
-    }
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const int i = ia + q * BX;
-        if (i >= nx) break;
-        if (row_in && i >= 2 && i <= nx - 2)
-            mass_c_store<NONLIN>(L, (size_t)j * P + i, zo[q], mc[q], mw[q], nc[q], ns[q], hh[q]);
-        else
-            mass_c_jnq_edge<NONLIN>(Pl, L, i, j, ir, is, ie, js, je);
+    const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    if (j >= 2 && j <= L.ny - 2 && i >= 2 && i <= L.nx - 2) {
+        const size_t c = (size_t)j * L.pitch + i;
+        mass_c_store<NONLIN>(L, c, L.z1[c], L.m1[c], L.m1[c - 1], L.n1[c], L.n1[c - L.pitch], L.h[c]);
+    } else {
+        mass_c_jnq_edge<NONLIN>(Pl, L, i, j, ir, is, ie, js, je);
     }
 }
 
@@ -1464,27 +1425,20 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
-/* CONMOME: the shared-memory tile form (both faces per thread), with
- * GCOMCOT_CONMOME_TILE=5 its register-capped form, or with
+/* CONMOME: the shared-memory tile form (both faces per thread), or with
  * GCOMCOT_CONMOME_TILE=0 the one-face form (x and y as two grid layers);
- * all compute the same bits */
-static int conmome_form() {
-    static const int form = [] {
+ * both compute the same bits */
+static bool conmome_tiled() {
+    static const int on = [] {
         const char *v = getenv("GCOMCOT_CONMOME_TILE");
-        if (v && v[0] == '0') return 0;
-        if (v && v[0] == '5') return 5;
-        return 1;
+        return (v && v[0] == '0') ? 0 : 1;
     }();
-    return form;
+    return on != 0;
 }
 
 static void launch_conmome(const GcLayerDev &L, int upd, cudaStream_t s) {
     const bool sph = L.laycord == 0;
-    const int form = conmome_form();
-    if (form == 5) {
-        if (sph) launch(k_conmome_tile5<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
-        else launch(k_conmome_tile5<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
-    } else if (form == 1) {
+    if (conmome_tiled()) {
         if (sph) launch(k_conmome_tile<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
         else launch(k_conmome_tile<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
     } else {
@@ -1547,9 +1501,8 @@ bool gc_launch_edges_mass(const GcLayerDev &P, const GcLayerDev &C, int rel_size
     if (t != 1 || C.root || C.laycord != 1 || (C.laygov != 0 && C.laygov != 1)) return false;
     const int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
     (void)rel_time;
-    const dim3 g((unsigned)((C.nx + 2 * BX - 1) / (2 * BX)), (unsigned)((C.ny + MJ_BY - 1) / MJ_BY));
-    if (C.laygov == 1) launch(k_mass_c_jnq<true>, g, dim3(BX, MJ_BY), 0, s, P, C, rel_size, is, ie, js, je);
-    else launch(k_mass_c_jnq<false>, g, dim3(BX, MJ_BY), 0, s, P, C, rel_size, is, ie, js, je);
+    if (C.laygov == 1) launch(k_mass_c_jnq<true>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
+    else launch(k_mass_c_jnq<false>, grid2(C), dim3(BX, BY), 0, s, P, C, rel_size, is, ie, js, je);
     return true;
 }
 
