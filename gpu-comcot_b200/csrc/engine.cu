@@ -415,6 +415,7 @@ static int eng_rebuild(gc_engine *e) {
                                                        e->ty_rule, !single);
     const int pty = anx.empty() ? 32 : gc_pair_pick_ty(e->pair_variant, (int)anx.size(), anx.data(), any.data(),
                                                        e->pair_rule, !single);
+    const int pte = gc_pair_short_ty(e->pair_rule, pty);
     /* two-step launches need at most 64 gauges per member */
     bool pair_ok = e->pair_on != 0 && e->pair_allowed != 0 && !anx.empty();
     std::vector<int2> ptiles;
@@ -436,7 +437,8 @@ static int eng_rebuild(gc_engine *e) {
             g.thr = M.thr;
             g.nbuf = 3;
             g.pty = pty;
-            gc_pair_tiles(C.nx, C.ny, pty, &g.ptiles_x);
+            g.pte = pte;
+            gc_pair_tiles(C.nx, C.ny, pty, pte, &g.ptiles_x);
             for (int q = 0; q < 3; q++) { g.z[q] = M.z[q]; g.m[q] = M.m[q]; g.n[q] = M.n[q]; }
             g.h = M.h ? M.h : C.d_h; g.rows = C.d_rows;
             g.zmax = M.zmax; g.arrival = M.arrival;
@@ -447,7 +449,7 @@ static int eng_rebuild(gc_engine *e) {
         int nt = gc_fused_tiles(C.nx, C.ny, ty, nullptr);
         for (int t = 0; t < nt; t++)
             for (int g : idx) tiles.push_back(make_int2(g, t));
-        const int npt = gc_pair_tiles(C.nx, C.ny, pty, nullptr);
+        const int npt = gc_pair_tiles(C.nx, C.ny, pty, pte, nullptr);
         for (int t = 0; t < npt; t++)
             for (int g : idx) ptiles.push_back(make_int2(g, t));
         for (int g : idx)
@@ -1110,7 +1112,6 @@ long long gc_engine_bytes_in_use(gc_engine *e) { return e ? e->in_use : GC_EINVA
 /* candidates: c < nv * R1 is the one-step kernel, variant c % nv with
  * tile-height rule c / nv; above that the two-step kernel, variant p % np
  * with rule p / np (p = c - nv * R1) */
-constexpr int GC_PAIR_RULES = 2;
 
 static int eng_num_candidates() {
     return gc_fused_num_variants() * GC_TY_RULES + gc_pair_num_variants() * GC_PAIR_RULES;

@@ -26,7 +26,10 @@ struct GcFusedGrid {
      * nbuf 3: level L in buffer L % 3 (the engine's single-grid members, which
      * the two-step kernel also steps) */
     int nbuf;
-    int ptiles_x, pty; /* two-step kernel: tiles along I and rows per tile */
+    /* two-step kernel: tiles along I, rows per tile, and rows per tile of
+     * the edge strips and of the other strips' first and last tile rows (0:
+     * every tile pty rows) */
+    int ptiles_x, pty, pte;
     float *z[3], *m[3], *n[3];
     const float *h, *rows, *r2, *r4;
     float *zmax;
@@ -80,9 +83,15 @@ int gc_fused_tiles(int nx, int ny, int ty, int *tiles_x);
  * at most 64 gauges; both steps inside every grid's window ---- */
 int gc_pair_num_variants();
 GcTileCfg gc_pair_variant(int v);
-/* tiles of one grid: tile t stores columns [120t+4, 120t+123] (the first
- * [0, 123], the last to the grid's edge) x ty rows */
-int gc_pair_tiles(int nx, int ny, int ty, int *tiles_x);
+/* tiles of one grid: strip t stores columns [120t+4, 120t+123] (the first
+ * [0, 123], the last to the grid's edge); tiles are ty rows, except that
+ * with te > 0 the two edge strips take te-row tiles, and so do the other
+ * strips' first and last tile rows (te == 0: every tile ty rows) */
+int gc_pair_tiles(int nx, int ny, int ty, int te, int *tiles_x);
+/* pair tile-height rules: 0 and 1 uniform (1: at least 24 rows), 2 the
+ * balanced layout (shorter tiles where the boundary makes rows dearer) */
+constexpr int GC_PAIR_RULES = 3;
+int gc_pair_short_ty(int rule, int ty);
 int gc_pair_max_ctas(int variant, bool multi = true);
 int gc_pair_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule, bool multi = true);
 /* steps (*d_step_base + step_off) and the next one */

@@ -221,6 +221,65 @@ __host__ __device__ __forceinline__ void pair_cols(int t, int nx, int &s, int &l
     if (hi > nx - 1) hi = nx - 1;
 }
 
+/* Tile layout of one grid.  Strips are 128 columns (pair_cols).  With
+ * te == 0 every tile is ty rows, in row-major order.  With te > 0 the two
+ * edge strips, whose tiles carry OPEN and the IM1/JM1 clamps and cost more
+ * per row, take te-row tiles, and so do the other strips' first and last
+ * tile rows (the perimeter rows); the edge strips' tiles come first in the
+ * order.  Grids of at most two strips, or too few rows, use te == 0. */
+struct PairLayout {
+    int tiles_x, ty, te;
+    int n_ed;  /* tiles of an edge strip */
+    int n_mid; /* ty-row tiles of another strip */
+    int count;
+};
+__host__ __device__ __forceinline__ PairLayout pair_layout(int nx, int ny, int ty, int te) {
+    PairLayout L;
+    L.tiles_x = nx <= 128 ? 1 : 1 + (nx - 128 + kPairOut - 1) / kPairOut;
+    L.ty = ty;
+    L.te = (te > 0 && te < ty && L.tiles_x > 2 && ny >= 2 * te + ty) ? te : 0;
+    if (L.te == 0) {
+        L.n_ed = 0;
+        L.n_mid = (ny + ty - 1) / ty;
+        L.count = L.tiles_x * L.n_mid;
+    } else {
+        L.n_ed = (ny + L.te - 1) / L.te;
+        L.n_mid = (ny - 2 * L.te + ty - 1) / ty;
+        L.count = 2 * L.n_ed + (L.tiles_x - 2) * (L.n_mid + 2);
+    }
+    return L;
+}
+/* tile lt of a layout: strip tx, first output row j0, rows h (the body
+ * clips the last tile of a strip to the grid) */
+__host__ __device__ __forceinline__ void pair_tile_at(const PairLayout &L, int ny, int lt, int &tx, int &j0, int &h) {
+    if (L.te == 0) {
+        tx = lt % L.tiles_x;
+        j0 = (lt / L.tiles_x) * L.ty;
+        h = L.ty;
+        return;
+    }
+    if (lt < 2 * L.n_ed) {
+        const bool east = lt >= L.n_ed;
+        tx = east ? L.tiles_x - 1 : 0;
+        j0 = (lt - (east ? L.n_ed : 0)) * L.te;
+        h = L.te;
+        return;
+    }
+    const int k = lt - 2 * L.n_ed;
+    tx = 1 + k % (L.tiles_x - 2);
+    const int b = k / (L.tiles_x - 2);
+    if (b == 0) {
+        j0 = 0;
+        h = L.te;
+    } else if (b <= L.n_mid) {
+        j0 = L.te + (b - 1) * L.ty;
+        h = min(L.ty, ny - L.te - j0);
+    } else {
+        j0 = ny - L.te;
+        h = L.te;
+    }
+}
+
 /* what one warp needs to run its ring of S stages over a tile's rows */
 struct PairRing {
     char *wsm;      /* the warp's stages (generic address) */
@@ -671,8 +730,8 @@ __device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step
     const int local = step - G.step0; /* step A's 0-based index */
     /* both steps must lie in the window, and three time levels exist */
     if (local < 0 || local + 1 >= G.nsteps || G.nbuf != 3) return true;
-    const int tx = lt % G.ptiles_x, tyi = lt / G.ptiles_x;
-    const int ty = G.pty, j0 = tyi * ty;
+    int tx, j0, ty;
+    pair_tile_at(pair_layout(G.nx, G.ny, G.pty, G.pte), G.ny, lt, tx, j0, ty);
     int s, lo, hi;
     pair_cols(tx, G.nx, s, lo, hi);
     /* a tile none of whose computed cells (halo rows and columns included)
@@ -811,11 +870,15 @@ GcTileCfg gc_pair_variant(int v) {
     return GcTileCfg{kPairVariants[v].w, kPairVariants[v].s};
 }
 
-int gc_pair_tiles(int nx, int ny, int ty, int *tiles_x) {
-    const int tx = nx <= 128 ? 1 : 1 + (nx - 128 + kPairOut - 1) / kPairOut;
-    if (tiles_x) *tiles_x = tx;
-    return tx * ((ny + ty - 1) / ty);
+int gc_pair_tiles(int nx, int ny, int ty, int te, int *tiles_x) {
+    const PairLayout L = pair_layout(nx, ny, ty, te);
+    if (tiles_x) *tiles_x = L.tiles_x;
+    return L.count;
 }
+
+/* rule 2's short tiles: about 60% of ty (a perimeter tile's row costs about
+ * 1.5 interior rows) */
+int gc_pair_short_ty(int rule, int ty) { return (rule == 2 && ty > 6) ? (3 * ty + 2) / 5 : 0; }
 
 int gc_pair_max_ctas(int variant, bool multi) {
     if (variant < 0 || variant >= kNumPairVariants) variant = 0;
@@ -832,13 +895,14 @@ int gc_pair_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int r
     const int slots = gc_pair_max_ctas(variant, multi) * gc_pair_variant(variant).warps;
     auto tiles = [&](int ty) {
         long long t = 0;
-        for (int g = 0; g < ngrids; g++) t += gc_pair_tiles(nx[g], ny[g], ty, nullptr);
+        for (int g = 0; g < ngrids; g++) t += gc_pair_tiles(nx[g], ny[g], ty, gc_pair_short_ty(rule, ty), nullptr);
         return t;
     };
     /* a warp's time is about (rows + 4 halo rows) per tile; a launch lasts
-     * waves x that.  Rule 0: the height minimising it; rule 1: the same
-     * among heights of at least 24 rows (less halo per row when many waves) */
-    const int tmin = rule == 0 ? 8 : 24;
+     * waves x that.  Rules 0 and 2: the height minimising it; rule 1: the
+     * same among heights of at least 24 rows (less halo per row when many
+     * waves) */
+    const int tmin = rule == 1 ? 24 : 8;
     int best = 32;
     long long best_cost = -1, best_waves = 0;
     for (int ty = tmin; ty <= 256; ty++) {
@@ -857,7 +921,7 @@ cudaError_t gc_pair_launch_one_at(int variant, const GcFusedGrid &g, const int *
                                   cudaStream_t s) {
     if (variant < 0 || variant >= kNumPairVariants) variant = 0;
     const PairVariant &v = kPairVariants[variant];
-    const int ntiles = gc_pair_tiles(g.nx, g.ny, g.pty, nullptr);
+    const int ntiles = gc_pair_tiles(g.nx, g.ny, g.pty, g.pte, nullptr);
     prepare_pair(v);
     return launch_pair(v.one, (ntiles + v.w - 1) / v.w, 32 * v.w, pair_smem(v), s, g, nullptr, nullptr, ntiles,
                        d_step_base, step_off);
