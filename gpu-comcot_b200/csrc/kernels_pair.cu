@@ -222,15 +222,17 @@ __host__ __device__ __forceinline__ void pair_cols(int t, int nx, int &s, int &l
 }
 
 /* Tile layout of one grid.  Strips are 128 columns (pair_cols).  With
- * te == 0 every tile is ty rows, in row-major order.  With te > 0 the two
- * edge strips, whose tiles carry OPEN and the IM1/JM1 clamps and cost more
- * per row, take te-row tiles, and so do the other strips' first and last
- * tile rows (the perimeter rows); the edge strips' tiles come first in the
- * order.  Grids of at most two strips, or too few rows, use te == 0. */
+ * te == 0 every tile is ty rows, in row-major order.  With te > 0 the tiles
+ * that carry the boundary (OPEN, the IM1/JM1 clamps) and so cost more per
+ * row are shorter: the west strip's tiles and the other strips' first and
+ * last tile rows take te rows, the east strip's tee = 5/6 te rows (its OPEN
+ * column sits at a cell chosen at run time, a few selects dearer).  The edge
+ * strips' tiles come first in the order.  Grids of at most two strips, or
+ * too few rows, use te == 0. */
 struct PairLayout {
-    int tiles_x, ty, te;
-    int n_ed;  /* tiles of an edge strip */
-    int n_mid; /* ty-row tiles of another strip */
+    int tiles_x, ty, te, tee;
+    int n_w, n_e; /* tiles of the west and east strips */
+    int n_mid;    /* ty-row tiles of another strip */
     int count;
 };
 __host__ __device__ __forceinline__ PairLayout pair_layout(int nx, int ny, int ty, int te) {
@@ -238,14 +240,16 @@ __host__ __device__ __forceinline__ PairLayout pair_layout(int nx, int ny, int t
     L.tiles_x = nx <= 128 ? 1 : 1 + (nx - 128 + kPairOut - 1) / kPairOut;
     L.ty = ty;
     L.te = (te > 0 && te < ty && L.tiles_x > 2 && ny >= 2 * te + ty) ? te : 0;
+    L.tee = L.te > 0 ? max(1, (5 * L.te + 3) / 6) : 0;
     if (L.te == 0) {
-        L.n_ed = 0;
+        L.n_w = L.n_e = 0;
         L.n_mid = (ny + ty - 1) / ty;
         L.count = L.tiles_x * L.n_mid;
     } else {
-        L.n_ed = (ny + L.te - 1) / L.te;
+        L.n_w = (ny + L.te - 1) / L.te;
+        L.n_e = (ny + L.tee - 1) / L.tee;
         L.n_mid = (ny - 2 * L.te + ty - 1) / ty;
-        L.count = 2 * L.n_ed + (L.tiles_x - 2) * (L.n_mid + 2);
+        L.count = L.n_w + L.n_e + (L.tiles_x - 2) * (L.n_mid + 2);
     }
     return L;
 }
@@ -258,14 +262,19 @@ __host__ __device__ __forceinline__ void pair_tile_at(const PairLayout &L, int n
         h = L.ty;
         return;
     }
-    if (lt < 2 * L.n_ed) {
-        const bool east = lt >= L.n_ed;
-        tx = east ? L.tiles_x - 1 : 0;
-        j0 = (lt - (east ? L.n_ed : 0)) * L.te;
+    if (lt < L.n_w) {
+        tx = 0;
+        j0 = lt * L.te;
         h = L.te;
         return;
     }
-    const int k = lt - 2 * L.n_ed;
+    if (lt < L.n_w + L.n_e) {
+        tx = L.tiles_x - 1;
+        j0 = (lt - L.n_w) * L.tee;
+        h = L.tee;
+        return;
+    }
+    const int k = lt - L.n_w - L.n_e;
     tx = 1 + k % (L.tiles_x - 2);
     const int b = k / (L.tiles_x - 2);
     if (b == 0) {
