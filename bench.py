@@ -654,8 +654,9 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
         plain_rec = {"p50_s": pp["p50"], "p99_s": pp["p99"], "mean_s": float(plat.mean()),
                      "scenarios_per_hour": 3600.0 / float(service.mean()),
                      "method": "measured: the same trace served one request at a time in arrival order "
-                               "through the reference C ABI (layer upload, per-phase kernels, per-step gauge "
-                               "reads, products read back)"}
+                               "through the reference C ABI (layer upload, per-phase kernels, the gauge "
+                               "stencils of every step gathered on the device by gcomcot_drive, products read "
+                               "back)"}
     # parity: the smallest un-nested and nested requests of the trace, served in
     # the mix (and on the plain path) against the oracle
     recs = []
@@ -801,7 +802,9 @@ def run_single(args, torch, dist, rank, world, local):
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e2e_ms / E,
                "note": f"one whole forecast ({E} steps) end to end, whatever --steps is",
-               "path": "gcomcot_init_layer_ + per step mass/openbd/momt/maxamp/get_z x32/update + getz/getzmax"}
+               "path": ("gcomcot_init_layer_ + gcomcot_drive (per step mass/openbd/momt/maxamp, the 32 gauge "
+                        "stencils gathered on the device, update; stencils read back once per 1024 steps) "
+                        "+ getz/getzmax")}
         s.close()
 
     peak, peak_kind = peaks()

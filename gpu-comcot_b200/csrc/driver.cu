@@ -1,7 +1,8 @@
 /*
- * The reference driver's per-step call sequence as a library entry point, the
- * gauge snapshot that serves gcomcot_get_z_ after the first step with one
- * device round trip per step, and the DEBUG_CORE comparators.
+ * The reference driver's per-step call sequence as a library entry point
+ * (gauge stencils gathered on the device, read back once per chunk of
+ * steps), the gauge snapshot that serves gcomcot_get_z_ after the first step
+ * with one device round trip per step, and the DEBUG_CORE comparators.
  */
 #include <math.h>
 #include <string.h>
@@ -119,22 +120,68 @@ int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const
                   const int *g_j, float *out4) {
     GcRuntime &rt = gc_rt();
     if (!rt.inited || rt.root < 0) return GC_ESTATE;
+    if (nsteps < 0 || ngauges < 0 || (ngauges > 0 && (!g_layer || !g_i || !g_j || !out4))) return GC_EINVAL;
     int root = rt.root;
     bool nested = !rt.layers[root].children.empty();
-    for (int k = 0; k < nsteps; k++) {
+    for (int g = 0; g < ngauges; g++) {
+        GcLayer *L = gc_layer(g_layer[g]);
+        if (!L || !L->used || g_i[g] < 1 || g_i[g] >= L->nx || g_j[g] < 1 || g_j[g] >= L->ny) return GC_EINVAL;
+    }
+    /* The caller of this entry point receives every step's stencils at the
+     * end, so no step waits for the host: each step's stencils are gathered
+     * on the device (the kernel gcomcot_get_z_'s snapshot launches, at the
+     * same point of the step) into a history of up to kChunk steps, which
+     * goes to out4 with one copy per chunk.  Same values as the per-step
+     * calls. */
+    constexpr int kChunk = 1024;
+    int *d_ij = nullptr;
+    float *d_hist = nullptr;
+    const int chunk = nsteps < kChunk ? (nsteps > 0 ? nsteps : 1) : kChunk;
+    if (ngauges > 0) {
+        std::vector<int> ij((size_t)2 * ngauges);
+        for (int g = 0; g < ngauges; g++) { ij[2 * g] = g_i[g]; ij[2 * g + 1] = g_j[g]; }
+        gc_flush();
+        GC_CUDA_OR_RET(cudaMallocAsync((void **)&d_ij, ij.size() * sizeof(int), rt.stream));
+        GC_CUDA_OR_RET(cudaMallocAsync((void **)&d_hist, (size_t)chunk * ngauges * 4 * sizeof(float), rt.stream));
+        GC_CUDA_OR_RET(cudaMemcpyAsync(d_ij, ij.data(), ij.size() * sizeof(int), cudaMemcpyHostToDevice, rt.stream));
+        GC_CUDA_OR_RET(cudaStreamSynchronize(rt.stream)); /* ij is a local vector */
+    }
+    int rc = GC_OK;
+    for (int k = 0; k < nsteps && rc == GC_OK; k++) {
         mass_launch_(nullptr, nullptr, nullptr, &root);
         openbd_launch_(nullptr);
         if (nested) all_grid_launch_();
         momt_launch_(nullptr, nullptr, nullptr, &root);
         if (maxamp) maxamp_launch_(&root);
-        for (int g = 0; g < ngauges; g++) {
-            float *o = out4 + ((size_t)k * ngauges + g) * 4;
-            int lid = g_layer[g], i = g_i[g], j = g_j[g];
-            gcomcot_get_z_(&lid, o, o + 1, o + 2, o + 3, &i, &j);
+        if (ngauges > 0) {
+            gc_flush();
+            GcPdlScope pdl(true);
+            float *slot = d_hist + (size_t)(k % chunk) * ngauges * 4;
+            int g0 = 0;
+            while (g0 < ngauges) {
+                int g1 = g0;
+                while (g1 < ngauges && g_layer[g1] == g_layer[g0]) g1++;
+                GcLayer *L = gc_layer(g_layer[g0]);
+                GcLayerDev d = L->view();
+                if (!L->z2_valid) d.z2 = L->z[L->cur];
+                gc_launch_gauges(d, g1 - g0, d_ij + 2 * g0, slot + 4 * g0, rt.stream);
+                rt.launches++;
+                g0 = g1;
+            }
+            if ((k + 1) % chunk == 0 || k + 1 == nsteps) {
+                const int first = k - k % chunk, cnt = k - first + 1;
+                if (cudaMemcpyAsync(out4 + (size_t)first * ngauges * 4, d_hist, (size_t)cnt * ngauges * 4 * sizeof(float),
+                                    cudaMemcpyDeviceToHost, rt.stream) != cudaSuccess ||
+                    cudaStreamSynchronize(rt.stream) != cudaSuccess)
+                    rc = GC_ECUDA;
+            }
         }
         cuda_update_layer_(&root);
     }
-    return gcomcot_sync();
+    if (d_ij) cudaFreeAsync(d_ij, rt.stream);
+    if (d_hist) cudaFreeAsync(d_hist, rt.stream);
+    const int rs = gcomcot_sync();
+    return rc != GC_OK ? rc : rs;
 }
 
 /* GPUall_grids.cu:299-394: device JNQ/NEWQ for (idO, idA) at sub-step t,
