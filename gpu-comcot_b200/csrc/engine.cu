@@ -177,9 +177,6 @@ struct gc_engine {
     int pair_allowed = 1;         /* GCOMCOT_PAIR=0 turns it off altogether */
     int pair_variant = 0, pair_rule = 0;
     bool pair_ok = false;         /* the current members allow it */
-    /* a nested member's JNZ, window momentum and outputs in one launch where
-     * the feedback follows the last sub-step (GCOMCOT_TAIL=0: three) */
-    bool tail_fused = true;
     int2 *d_ptiles = nullptr;
     int ptiles_cap = 0, nptiles = 0;
     int *d_health = nullptr;      /* one int for gc_engine_member_health */
@@ -269,17 +266,7 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
     cudaEventRecord(e->ev_cjoin[a], cs);
     gc_fused_launch_one_at(e->variant, g, d_base, step_off, s);
     cudaStreamWaitEvent(s, e->ev_cjoin[a], 0);
-    /* a feedback that follows the child's last sub-step (rel_time 1 or 2,
-     * ratio 2..5, no SC coupling) goes out as one launch with the window's
-     * momentum and outputs (gc_launch_window_tail) */
-    const bool fuse_tail = !C.has_sc && nhalf == C.rel_time && C.rel_size >= 2 && C.rel_size <= 5 &&
-                           C.rel_time <= 2 && e->tail_fused;
-    GcLayerDev Cjnz = Cv1;
     auto jnz = [&](const GcLayerDev &Cv) {
-        if (fuse_tail) {
-            Cjnz = Cv;
-            return;
-        }
         if (C.has_sc) gc_launch_sc_jnz(P, Cv, C.sc, s);
         else gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s);
         e->launches++;
@@ -318,13 +305,6 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
      * max-eta / arrival / gauges, side by side; both read the final surface,
      * neither writes what the other reads.  Fortran (IS-1 .. IE, JS-1 .. JE)
      * -> 0-based (IS-2 .. IE-1, JS-2 .. JE-1) */
-    if (fuse_tail && gc_launch_window_tail(P, Cjnz, C.rel_size, C.rel_time, C.corners, d_base, step_off, M.step0,
-                                           flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc], C.cpitch, M.ts,
-                                           M.nsteps, s)) {
-        e->launches += 2; /* the fused step, the window's tail */
-        return;
-    }
-    if (fuse_tail) gc_launch_jnz(P, Cjnz, C.rel_size, C.rel_time, C.corners, s);
     cudaEventRecord(e->ev_cfork[a], s);
     cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
     gc_launch_step_outputs(P, d_base, step_off, M.step0, flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc],
@@ -616,8 +596,6 @@ int gc_engine_create(long long hbm_budget_bytes, gc_engine **out) {
     if (pd && pd[0] == '0') e->pdl = 0;
     const char *pr = getenv("GCOMCOT_PAIR");
     if (pr && pr[0] == '0') e->pair_on = e->pair_allowed = 0;
-    const char *tf = getenv("GCOMCOT_TAIL");
-    if (tf && tf[0] == '0') e->tail_fused = false;
     *out = e;
     return GC_OK;
 }

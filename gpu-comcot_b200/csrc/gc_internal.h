@@ -147,13 +147,6 @@ void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out
 /* max-eta (flags & 1), arrival (flags & 2) and gauge samples after one outer
  * step of a batched nested member; step = step_off + *step_base; max/arrival
  * over the 0-based window win = {i0, i1, j0, j1} (NULL: the whole layer) */
-/* JNZ, the window's outer momentum and the step's window outputs in one
- * launch, for a child whose feedback follows its last sub-step (rel_time 1
- * or 2) and ratio 2..5; false (nothing launched) otherwise */
-bool gc_launch_window_tail(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
-                           const int *corners, const int *step_base, int step_off, int step0, int flags, float thr,
-                           int ng, const int *gij, const float *gw, const int *glayer, const float *cz, int cpitch,
-                           float *ts, int ts_len, cudaStream_t s);
 void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
                             float thr, int ng, const int *gij, const float *gw, const int *glayer,
                             const float *cz, int cpitch, float *ts, int ts_len, const int *win, cudaStream_t s);

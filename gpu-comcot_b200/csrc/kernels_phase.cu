@@ -1172,89 +1172,6 @@ __global__ void k_jnz_r(GcLayerDev Pl, GcLayerDev C, int is, int ie, int js, int
     Pl.z2[(size_t)(J - 1) * Pl.pitch + (I - 1)] = jnz_value<R, EVEN>(C, is, js, I, J);
 }
 
-/* The tail of a nested outer step in one launch, for a child whose feedback
- * follows its last sub-step: JNZ over the window IS..IE x JS..JE, the outer
- * momentum (MOMT_S) on the rectangle whose stencil JNZ changes, 0-based
- * [i0, i0+ni) x [j0, j0+nj), and the window's max-eta and arrival with the
- * step's gauge samples (as k_step_outputs).  A thread computes the JNZ
- * surface of its own cell and, where its momentum reads them, of its east
- * and north neighbours, by the same arithmetic as the stored value (the same
- * bits); it stores only its own cell's.  Surfaces outside the window come
- * from memory, which the launch does not write, so no thread reads what
- * another stores.  Gauge samples inside the window use the computed values. */
-template <int R, bool EVEN>
-__global__ void k_window_tail(GcLayerDev L, GcLayerDev C, int is, int ie, int js, int je, int i0, int j0, int ni,
-                              int nj, const int *step_base, int step_off, int step0, int flags, float thr, int ng,
-                              const int *gij, const float *gw, const int *glayer, const float *cz, int cpitch,
-                              float *ts, int ts_len) {
-    pdl_enter();
-    const int local = step_off + (step_base ? *step_base : 0) - step0;
-    const bool out_ok = local >= 0 && local < ts_len;
-    const size_t P = (size_t)L.pitch;
-    auto in_win = [&](int ii, int jj) { return ii >= is - 1 && ii <= ie - 1 && jj >= js - 1 && jj <= je - 1; };
-    auto z_at = [&](int ii, int jj) {
-        return in_win(ii, jj) ? jnz_value<R, EVEN>(C, is, js, ii + 1, jj + 1) : L.z2[(size_t)jj * P + ii];
-    };
-    if (blockIdx.x == 0 && blockIdx.y == 0 && ng > 0 && out_ok) {
-        for (int g = threadIdx.y * BX + threadIdx.x; g < ng; g += BX * BY) {
-            const int ki = gij[2 * g] - 1, kj = gij[2 * g + 1] - 1;
-            float l1, l2, l3, l4;
-            if (glayer && glayer[g] != 0) {
-                const size_t cp = (size_t)cpitch, c = (size_t)kj * cp + (size_t)ki;
-                l1 = cz[c]; l2 = cz[c + 1]; l3 = cz[c + cp]; l4 = cz[c + cp + 1];
-            } else {
-                l1 = z_at(ki, kj); l2 = z_at(ki + 1, kj); l3 = z_at(ki, kj + 1); l4 = z_at(ki + 1, kj + 1);
-            }
-            const float cx = gw[2 * g], cy = gw[2 * g + 1];
-            const float a = l1 * (1.0f - cx) * (1.0f - cy);
-            const float b = l2 * (cx) * (1.0f - cy);
-            const float d = l3 * (1.0f - cx) * (cy);
-            const float e = l4 * (cx) * (cy);
-            ts[(size_t)local * ng + g] = a + b + d + e;
-        }
-    }
-    const int i = i0 + blockIdx.x * BX + threadIdx.x;
-    const int j = j0 + blockIdx.y * BY + threadIdx.y;
-    if (i >= i0 + ni || j >= j0 + nj || i >= L.nx || j >= L.ny) return;
-    const size_t c = (size_t)j * P + i;
-    const float zc = z_at(i, j);
-    const int lo = L.root ? 0 : 1;
-    /* x-momentum: i in [lo, nx-2], j in [lo, ny-1]; 0 elsewhere */
-    float xm = 0.0f;
-    if (i >= lo && i <= L.nx - 2 && j >= lo) {
-        float h = L.h[c], hp1 = L.h[c + 1];
-        if (h > CC_GX && hp1 > CC_GX) {
-            size_t cm = (j > 0) ? c - P : c; /* JM1 = max(J-1,1) */
-            float tot_n = L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1];
-            xm = L.m1[c] - r2_at(L, i, j, c, h, hp1) * (z_at(i + 1, j) - zc) + GC_ROW(L, GC_R3, j) * tot_n;
-            if (fabsf(xm) < CC_EPS) xm = 0.0f;
-        }
-    }
-    L.m2[c] = xm;
-    /* y-momentum: j in [lo, ny-2], i in [lo, nx-1]; 0 elsewhere */
-    float xn = 0.0f;
-    if (j >= lo && j <= L.ny - 2 && i >= lo) {
-        float h = L.h[c], hq1 = L.h[c + P];
-        if (h > CC_GX && hq1 > CC_GX) {
-            size_t cw = (i > 0) ? c - 1 : c; /* IM1 = max(I-1,1) */
-            float tot_m = L.m1[cw] + L.m1[cw + P] + L.m1[c] + L.m1[c + P];
-            xn = L.n1[c] - r4_at(L, i, j, c, h, hq1) * (z_at(i, j + 1) - zc) - GC_ROW(L, GC_R5, j) * tot_m;
-            if (fabsf(xn) < CC_EPS) xn = 0.0f;
-        }
-    }
-    L.n2[c] = xn;
-    if (in_win(i, j)) {
-        L.z2[c] = zc;
-        if (out_ok) {
-            if (flags & 1) {
-                float m = L.zmax[c];
-                if (!(m >= zc)) L.zmax[c] = zc;
-            }
-            if ((flags & 2) && L.arrival[c] < 0 && L.h[c] > CC_GX && zc > thr) L.arrival[c] = local + 1;
-        }
-    }
-}
-
 /* ---------------------------------------------------------------- */
 /* outputs                                                           */
 /* ---------------------------------------------------------------- */
@@ -1673,37 +1590,6 @@ void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_
     dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
     launch(k_step_outputs, grid, dim3(BX, BY), 0, s, L, step_base, step_off, step0, flags, thr, ng, gij, gw, glayer,
                                                  cz, cpitch, ts, ts_len, i0, j0, ni, nj);
-}
-
-bool gc_launch_window_tail(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time,
-                           const int *corners, const int *step_base, int step_off, int step0, int flags, float thr,
-                           int ng, const int *gij, const float *gw, const int *glayer, const float *cz, int cpitch,
-                           float *ts, int ts_len, cudaStream_t s) {
-    if (rel_size < 2 || rel_size > 5 || rel_time > 2) return false;
-    const int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
-    const int i0 = is - 2 < 0 ? 0 : is - 2, j0 = js - 2 < 0 ? 0 : js - 2;
-    const int i1 = ie - 1 > P.nx - 1 ? P.nx - 1 : ie - 1, j1 = je - 1 > P.ny - 1 ? P.ny - 1 : je - 1;
-    if (i1 < i0 || j1 < j0) return false;
-    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
-    const dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
-    const bool even = (rel_time % 2) == 0;
-#define GC_TAIL_R(R)                                                                                                \
-    case R:                                                                                                         \
-        if (even)                                                                                                   \
-            launch(k_window_tail<R, true>, grid, dim3(BX, BY), 0, s, P, C, is, ie, js, je, i0, j0, ni, nj, step_base, \
-                   step_off, step0, flags, thr, ng, gij, gw, glayer, cz, cpitch, ts, ts_len);                        \
-        else                                                                                                        \
-            launch(k_window_tail<R, false>, grid, dim3(BX, BY), 0, s, P, C, is, ie, js, je, i0, j0, ni, nj,          \
-                   step_base, step_off, step0, flags, thr, ng, gij, gw, glayer, cz, cpitch, ts, ts_len);            \
-        return true;
-    switch (rel_size) {
-        GC_TAIL_R(2)
-        GC_TAIL_R(3)
-        GC_TAIL_R(4)
-        GC_TAIL_R(5)
-    }
-#undef GC_TAIL_R
-    return false;
 }
 
 void gc_set_pdl(bool on) { t_pdl = on; }
