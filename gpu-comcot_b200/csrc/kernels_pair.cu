@@ -761,7 +761,9 @@ __device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFuse
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int step = step_off + (step_base ? *step_base : 0);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    /* with one warp per CTA the tile index, and with it every address of the
+     * ring and the copies, is uniform across the warp */
+    const int warp = W == 1 ? 0 : (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
     char *wsm = smem + warp * pair_warp_bytes<S>();
     const uint32_t bars = smem_u32(wsm) + S * PStage::BYTES;
     if (lane == 0) {
@@ -823,7 +825,7 @@ struct PairVariant {
 #define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair_one<W, S>, k_pair_capped<W, S>}
 const PairVariant kPairVariants[] = {
     GC_PVARIANT(4, 5), GC_PVARIANT(4, 4), GC_PVARIANT(2, 5), GC_PVARIANT(4, 6),
-    GC_PVARIANT_CAPPED(4, 5), GC_PVARIANT_CAPPED(4, 4),
+    GC_PVARIANT_CAPPED(4, 5), GC_PVARIANT_CAPPED(4, 4), GC_PVARIANT(1, 4), GC_PVARIANT(1, 5),
 };
 #undef GC_PVARIANT
 #undef GC_PVARIANT_CAPPED
@@ -841,7 +843,8 @@ int g_wait_limit = 1 << 22; /* polls before a pipeline wait gives up */
 int g_stall_next = 0;       /* the next launch injects one stalled row */
 
 void prepare_pair(const PairVariant &v) {
-    static bool done[64][8];
+    static bool done[64][16];
+    static_assert(kNumPairVariants <= 16, "one flag per variant");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
     const int idx = (int)(&v - kPairVariants);
