@@ -179,6 +179,12 @@ struct gc_engine {
     bool pair_ok = false;         /* the current members allow it */
     int2 *d_ptiles = nullptr;
     int ptiles_cap = 0, nptiles = 0;
+    /* the single-grid members form one grid class of at most
+     * GC_PAIR_CLASS_MAX members: pairs go out as a class launch (member
+     * table in the parameter bank) instead of over the work list */
+    bool pair_class = false;
+    bool pair_class_on = true; /* GCOMCOT_PAIR_CLASS=0: always the work list */
+    GcPairClass pcls;
     int *d_health = nullptr;      /* one int for gc_engine_member_health */
     std::vector<int> nested_ids; /* active nested members */
     cudaStream_t aux[kMaxAux] = {};
@@ -353,6 +359,8 @@ static cudaError_t eng_launch_steps_(gc_engine *e, const int *d_base, int step_o
                 cudaError_t err = e->single
                                       ? gc_pair_launch_one_at(e->pair_variant, e->one_grid, d_base, step_off0 + k,
                                                               e->stream)
+                                  : e->pair_class
+                                      ? gc_pair_launch_class(e->pair_variant, e->pcls, d_base, step_off0 + k, e->stream)
                                       : gc_pair_launch_multi(e->pair_variant, e->d_grids, e->d_ptiles, e->nptiles,
                                                              d_base, step_off0 + k, e->stream);
                 if (err != cudaSuccess) return err;
@@ -491,6 +499,30 @@ static int eng_rebuild(gc_engine *e) {
         GC_CUDA_OR_RET(cudaMemcpyAsync(e->d_ptiles, ptiles.data(), ptiles.size() * sizeof(int2),
                                        cudaMemcpyHostToDevice, e->stream));
     e->pair_ok = pair_ok;
+    /* one class of single-grid members: the class launch */
+    e->pair_class = false;
+    if (pair_ok && !e->single && e->ngrids >= 2 && e->ngrids <= GC_PAIR_CLASS_MAX && e->pair_class_on) {
+        bool same = true;
+        for (int g = 1; g < e->ngrids && same; g++)
+            same = grids[g].nx == grids[0].nx && grids[g].ny == grids[0].ny && grids[g].pitch == grids[0].pitch &&
+                   grids[g].rows == grids[0].rows;
+        if (same) {
+            memset(&e->pcls, 0, sizeof e->pcls);
+            e->pcls.proto = grids[0];
+            e->pcls.nm = e->ngrids;
+            e->pcls.ntiles = gc_pair_tiles(grids[0].nx, grids[0].ny, pty, pte, nullptr);
+            for (int g = 0; g < e->ngrids; g++) {
+                const GcFusedGrid &G = grids[g];
+                GcPairMember &q = e->pcls.m[g];
+                for (int l = 0; l < 3; l++) { q.z[l] = G.z[l]; q.m[l] = G.m[l]; q.n[l] = G.n[l]; }
+                q.zmax = G.zmax; q.arrival = G.arrival; q.h = G.h;
+                q.gij = G.gij; q.gw = G.gw; q.ts = G.ts;
+                q.step0 = G.step0; q.nsteps = G.nsteps; q.flags = G.flags; q.ng = G.ng; q.ts_len = G.ts_len;
+                q.thr = G.thr;
+            }
+            e->pair_class = true;
+        }
+    }
     /* the host copies above are from pageable memory and complete before return */
     e->nctas = e->ntiles;
     if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
@@ -596,6 +628,8 @@ int gc_engine_create(long long hbm_budget_bytes, gc_engine **out) {
     if (pd && pd[0] == '0') e->pdl = 0;
     const char *pr = getenv("GCOMCOT_PAIR");
     if (pr && pr[0] == '0') e->pair_on = e->pair_allowed = 0;
+    const char *pc = getenv("GCOMCOT_PAIR_CLASS");
+    if (pc && pc[0] == '0') e->pair_class_on = false;
     *out = e;
     return GC_OK;
 }

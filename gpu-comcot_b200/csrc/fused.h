@@ -94,6 +94,31 @@ constexpr int GC_PAIR_RULES = 3;
 int gc_pair_short_ty(int rule, int ty);
 int gc_pair_max_ctas(int variant, bool multi = true);
 int gc_pair_pick_ty(int variant, int ngrids, const int *nx, const int *ny, int rule, bool multi = true);
+/* A class launch of the two-step kernel: members of one grid class (same
+ * geometry, row records and tile layout) stepped by one launch whose member
+ * table is a kernel parameter, so a tile's member and its buffers derive from
+ * the block index and the parameter bank alone (warp-uniform values) instead
+ * of a descriptor loaded from memory.  Tiles are member-minor: tile t is
+ * member t % nm, class tile t / nm. */
+constexpr int GC_PAIR_CLASS_MAX = 64;
+struct GcPairMember {
+    float *z[3], *m[3], *n[3];
+    float *zmax;
+    int *arrival;
+    const float *h;
+    const int *gij;
+    const float *gw;
+    float *ts;
+    int step0, nsteps, flags, ng, ts_len;
+    float thr;
+};
+struct GcPairClass {
+    GcFusedGrid proto; /* the geometry; its member fields are not read */
+    int nm, ntiles;    /* members, tiles per member */
+    GcPairMember m[GC_PAIR_CLASS_MAX];
+};
+cudaError_t gc_pair_launch_class(int variant, const GcPairClass &c, const int *d_step_base, int step_off,
+                                 cudaStream_t s);
 /* steps (*d_step_base + step_off) and the next one */
 cudaError_t gc_pair_launch_one_at(int variant, const GcFusedGrid &g, const int *d_step_base, int step_off,
                                   cudaStream_t s);

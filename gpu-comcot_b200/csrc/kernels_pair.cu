@@ -300,7 +300,8 @@ struct PairRing {
 /* copies of input row r of a strip (columns s .. s + cb/4 - 1) into the stage
  * at sb: Z, M, N of the level read, H, max-eta on output rows (out), and the
  * row's coefficient record.  `fake`: announce 16 bytes no copy delivers. */
-__device__ __forceinline__ void pair_issue(const GcFusedGrid &G, int l0, int r, int s, uint32_t cb, bool out,
+template <class Desc>
+__device__ __forceinline__ void pair_issue(const Desc &G, int l0, int r, int s, uint32_t cb, bool out,
                                            uint32_t sb, uint32_t bar, bool fake) {
     fence_proxy_async(); /* the warp's reads of this stage come first */
     if (fake) {
@@ -318,8 +319,8 @@ __device__ __forceinline__ void pair_issue(const GcFusedGrid &G, int l0, int r, 
 }
 
 /* the first min(S, K) rows of a tile (rows rs ..), issued by lane 0 */
-template <int S>
-__device__ __forceinline__ void pair_prologue(const GcFusedGrid &G, const PairRing &R, int l0, int rs, int K,
+template <int S, class Desc>
+__device__ __forceinline__ void pair_prologue(const Desc &G, const PairRing &R, int l0, int rs, int K,
                                               int j0, int jl, int s, uint32_t cb, bool stall) {
     __syncwarp();
     if ((threadIdx.x & 31) == 0) {
@@ -335,7 +336,8 @@ __device__ __forceinline__ void pair_prologue(const GcFusedGrid &G, const PairRi
 /* gauges whose base cell (KI, KJ) lies in the tile's stored block: bit g of
  * (gm1:gm0).  Also writes the sample of the surface the previous launch left
  * (level L, step local - 1), which no tile of that launch could take. */
-__device__ __forceinline__ void pair_gauge_setup(const GcFusedGrid &G, int l0, int local, int lo, int hi, int j0,
+template <class Desc>
+__device__ __forceinline__ void pair_gauge_setup(const Desc &G, int l0, int local, int lo, int hi, int j0,
                                                  int jl, unsigned &gm0, unsigned &gm1) {
     const int lane = threadIdx.x & 31;
     const int ng = G.ng;
@@ -370,7 +372,8 @@ __device__ __forceinline__ void pair_gauge_setup(const GcFusedGrid &G, int l0, i
 
 /* step A's gauge samples whose base row is `row`: surface rows row (lo_row)
  * and row + 1 (hi_row) */
-__device__ __forceinline__ void pair_gauge_row(const GcFusedGrid &G, unsigned gm0, unsigned gm1, int row,
+template <class Desc>
+__device__ __forceinline__ void pair_gauge_row(const Desc &G, unsigned gm0, unsigned gm1, int row,
                                                const float4 &lo_row, const float4 &hi_row, int s, int local) {
     for (int h2 = 0; h2 < 2; h2++) {
         unsigned bits = h2 == 0 ? gm0 : gm1;
@@ -458,8 +461,8 @@ __device__ __forceinline__ float4 surface4_edge(const float4 &z1, const float4 &
  * stays 0), the JM1 clamp of M on row 0, and zero inputs on rows past the
  * grid (the bottom tile iterates two rows beyond it to finish step B).  Rows
  * above j0-1 and rows past the grid compute values that nothing stored reads. */
-template <int S>
-__device__ __forceinline__ bool pair_rows_edge(const GcFusedGrid &G, int s, int lo, int hi, int j0, int ty, int local,
+template <int S, class Desc>
+__device__ __forceinline__ bool pair_rows_edge(const Desc &G, int s, int lo, int hi, int j0, int ty, int local,
                                                char *wsm, int &seq, int wait_limit, bool stall) {
     static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
     const int lane = threadIdx.x & 31;
@@ -617,8 +620,8 @@ __device__ __forceinline__ bool pair_rows_edge(const GcFusedGrid &G, int s, int 
  * first row, j0-2, only feeds the N flux of row j0-2 and the surface and
  * fluxes of row j0-1 through the next iterations' reads of the stage it
  * stays in, so it gets no iteration of its own. */
-template <int S>
-__device__ __forceinline__ bool pair_rows_int(const GcFusedGrid &G, int s, int j0, int ty, int local, char *wsm,
+template <int S, class Desc>
+__device__ __forceinline__ bool pair_rows_int(const Desc &G, int s, int j0, int ty, int local, char *wsm,
                                            int &seq, int wait_limit, bool stall) {
     static_assert(S >= 4, "rows r-2 .. r stay staged, at least one more in flight");
     const int lane = threadIdx.x & 31;
@@ -733,8 +736,8 @@ __device__ __forceinline__ bool pair_rows_int(const GcFusedGrid &G, int s, int j
     return true;
 }
 
-template <int S>
-__device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step, char *wsm, int &seq,
+template <int S, class Desc>
+__device__ __forceinline__ bool pair_tile(const Desc &G, int lt, int step, char *wsm, int &seq,
                                           int wait_limit, bool stall) {
     const int local = step - G.step0; /* step A's 0-based index */
     /* both steps must lie in the window, and three time levels exist */
@@ -750,11 +753,40 @@ __device__ __forceinline__ bool pair_tile(const GcFusedGrid &G, int lt, int step
     return edge ? pair_rows_edge<S>(G, s, lo, hi, j0, ty, local, wsm, seq, wait_limit, stall)
                 : pair_rows_int<S>(G, s, j0, ty, local, wsm, seq, wait_limit, stall);
 }
-template <int W, int S, bool MULTI>
-__device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFusedGrid *__restrict__ grids,
-                                            const int2 *__restrict__ tiles, int ntiles,
-                                            const int *__restrict__ step_base, int step_off, int wait_limit,
-                                            int stall) {
+/* A class launch's view of one member: the fields the two-step bodies read,
+ * as references into the parameter bank (the class geometry and the
+ * member's record), so each is read where it is used, as the single-grid
+ * form reads its descriptor, instead of being copied into registers. */
+struct PairClassDesc {
+    const int &nx, &ny, &pitch, &pty, &pte, &nbuf;
+    const float *const &rows;
+    float *const (&z)[3];
+    float *const (&m)[3];
+    float *const (&n)[3];
+    float *const &zmax;
+    int *const &arrival;
+    const float *const &h;
+    const int *const &gij;
+    const float *const &gw;
+    float *const &ts;
+    const int &step0, &nsteps, &flags, &ng;
+    const float &thr;
+    __device__ __forceinline__ PairClassDesc(const GcFusedGrid &p, const GcPairMember &q)
+        : nx(p.nx), ny(p.ny), pitch(p.pitch), pty(p.pty), pte(p.pte), nbuf(p.nbuf), rows(p.rows), z(q.z), m(q.m),
+          n(q.n), zmax(q.zmax), arrival(q.arrival), h(q.h), gij(q.gij), gw(q.gw), ts(q.ts), step0(q.step0),
+          nsteps(q.nsteps), flags(q.flags), ng(q.ng), thr(q.thr) {}
+};
+
+/* where a launch's tiles come from: one grid by value, a work list of
+ * {grid, tile} over descriptors in memory, or a class launch's member table
+ * in the parameter bank */
+enum class PairSrc { One, List, Class };
+
+template <int W, int S, PairSrc SRC>
+__device__ __forceinline__ void pair_kernel_src(const GcFusedGrid &one, const GcFusedGrid *__restrict__ grids,
+                                                const int2 *__restrict__ tiles, int ntiles, const GcPairClass *cls,
+                                                const int *__restrict__ step_base, int step_off, int wait_limit,
+                                                int stall) {
     extern __shared__ __align__(128) char smem[];
     /* programmatic dependent launch: the previous kernel in the stream has
      * finished and its writes are visible past this point */
@@ -775,15 +807,28 @@ __device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFuse
     bool first = stall != 0 && blockIdx.x == 0 && warp == 0;
     for (int tile = blockIdx.x * W + warp; tile < ntiles; tile += gridDim.x * W) {
         bool ok;
-        if (MULTI) {
+        if constexpr (SRC == PairSrc::List) {
             const int2 w = tiles[tile];
             ok = pair_tile<S>(grids[w.x], w.y, step, wsm, seq, wait_limit, first);
+        } else if constexpr (SRC == PairSrc::Class) {
+            const int mi = tile % cls->nm, lt = tile / cls->nm;
+            const PairClassDesc G(cls->proto, cls->m[mi]);
+            ok = pair_tile<S>(G, lt, step, wsm, seq, wait_limit, first);
         } else {
             ok = pair_tile<S>(one, tile, step, wsm, seq, wait_limit, first);
         }
         first = false;
         if (!ok) return;
     }
+}
+
+template <int W, int S, bool MULTI>
+__device__ __forceinline__ void pair_kernel(const GcFusedGrid &one, const GcFusedGrid *__restrict__ grids,
+                                            const int2 *__restrict__ tiles, int ntiles,
+                                            const int *__restrict__ step_base, int step_off, int wait_limit,
+                                            int stall) {
+    pair_kernel_src<W, S, MULTI ? PairSrc::List : PairSrc::One>(one, grids, tiles, ntiles, nullptr, step_base,
+                                                                step_off, wait_limit, stall);
 }
 
 /* the single-grid form, held to 128 registers so that 16 warps fit an SM
@@ -815,14 +860,26 @@ __global__ void __launch_bounds__(32 * W, 16 / W) k_pair_capped(GcFusedGrid one,
     pair_kernel<W, S, true>(one, grids, tiles, ntiles, step_base, step_off, wait_limit, stall);
 }
 
+/* the class form: member table in the parameter bank, held to the single-grid
+ * form's register budget */
+template <int W, int S>
+__global__ void __launch_bounds__(32 * W, 16 / W) k_pair_class(const __grid_constant__ GcPairClass c,
+                                                                const int *__restrict__ step_base, int step_off,
+                                                                int wait_limit, int stall) {
+    GcFusedGrid none;
+    pair_kernel_src<W, S, PairSrc::Class>(none, nullptr, nullptr, c.nm * c.ntiles, &c, step_base, step_off,
+                                          wait_limit, stall);
+}
+
 struct PairVariant {
     int w, s;
     void (*one)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
     void (*multi)(GcFusedGrid, const GcFusedGrid *, const int2 *, int, const int *, int, int, int);
+    void (*cls)(const GcPairClass, const int *, int, int, int);
 };
 
-#define GC_PVARIANT(W, S) {W, S, k_pair_one<W, S>, k_pair_list<W, S>}
-#define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair_one<W, S>, k_pair_capped<W, S>}
+#define GC_PVARIANT(W, S) {W, S, k_pair_one<W, S>, k_pair_list<W, S>, k_pair_class<W, S>}
+#define GC_PVARIANT_CAPPED(W, S) {W, S, k_pair_one<W, S>, k_pair_capped<W, S>, k_pair_class<W, S>}
 const PairVariant kPairVariants[] = {
     GC_PVARIANT(4, 5), GC_PVARIANT(4, 4), GC_PVARIANT(2, 5), GC_PVARIANT(4, 6),
     GC_PVARIANT_CAPPED(4, 5), GC_PVARIANT_CAPPED(4, 4), GC_PVARIANT(1, 4), GC_PVARIANT(1, 5),
@@ -851,6 +908,7 @@ void prepare_pair(const PairVariant &v) {
     if (done[dev][idx]) return;
     cudaFuncSetAttribute(v.one, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem(v));
     cudaFuncSetAttribute(v.multi, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem(v));
+    cudaFuncSetAttribute(v.cls, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem(v));
     done[dev][idx] = true;
 }
 
@@ -949,6 +1007,28 @@ cudaError_t gc_pair_launch_multi(int variant, const GcFusedGrid *d_grids, const 
     prepare_pair(v);
     return launch_pair(v.multi, (ntiles + v.w - 1) / v.w, 32 * v.w, pair_smem(v), s, dummy, d_grids, d_tiles,
                        ntiles, d_step_base, step_off);
+}
+
+cudaError_t gc_pair_launch_class(int variant, const GcPairClass &c, const int *d_step_base, int step_off,
+                                 cudaStream_t s) {
+    if (variant < 0 || variant >= kNumPairVariants) variant = 0;
+    const PairVariant &v = kPairVariants[variant];
+    if (c.nm <= 0 || c.nm > GC_PAIR_CLASS_MAX || c.ntiles <= 0) return cudaErrorInvalidValue;
+    prepare_pair(v);
+    const int ntiles = c.nm * c.ntiles;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((ntiles + v.w - 1) / v.w));
+    cfg.blockDim = dim3((unsigned)(32 * v.w));
+    cfg.dynamicSmemBytes = (size_t)pair_smem(v);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = gc_pdl_on() ? 1 : 0;
+    const int stall = g_stall_next;
+    g_stall_next = 0;
+    return cudaLaunchKernelEx(&cfg, v.cls, c, d_step_base, step_off, g_wait_limit, stall);
 }
 
 int gc_pair_take_error() {

@@ -127,3 +127,31 @@ def test_one_step_and_two_step_kernels_agree_on_a_shared_grid(oracle_mod):
                 for k in ("z", "m", "n", "zmax"):
                     assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), (v, k)
                 assert np.array_equal(got["arrival"], ref["arrival"]), v
+
+
+def test_class_launch_members_of_one_grid(oracle_mod):
+    """members sharing one grid class go out as a class launch (member table in
+    the parameter bank): different initial surfaces, gauges, start steps and
+    lengths, in graphs and eagerly, against the oracle bit for bit"""
+    n1, pair = _candidates()
+    base = _case(300, 140, 71, 60, ngauges=4)
+    L = base.root
+    rng = np.random.default_rng(72)
+    z0s = [np.ascontiguousarray(L.Z0 * float(rng.uniform(0.5, 1.5)), dtype=np.float32) for _ in range(5)]
+    lens = [60, 31, 44, 60, 17]
+    cases = [synth.Case("k", [synth.LayerSpec(**{**L.__dict__, "Z0": z})], n, gauges=base.gauges)
+             for z, n in zip(z0s, lens)]
+    refs = [_oracle(c, oracle_mod) for c in cases]
+    for v in (pair[0], pair[-1], pair[-2]):
+        for graphs in (0, 1):
+            with Engine(budget=2 << 30) as eng:
+                eng.config(variant=v, use_graphs=graphs, chunk=8)
+                cls = eng.add_class(L)
+                ids = [eng.add(cases[0], cls=cls), eng.add(cases[1], cls=cls)]
+                eng.step(7)
+                ids += [eng.add(c, cls=cls) for c in cases[2:]]
+                eng.step(70)
+                eng.sync()
+                for c, mid, (ref, ts) in zip(cases, ids, refs):
+                    assert eng.done(mid)
+                    _same(eng.read(mid), ref, ts, (v, graphs, c.nsteps))
