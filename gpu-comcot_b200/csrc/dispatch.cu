@@ -49,6 +49,8 @@ void gc_flush() {
     rt.pend_mass = rt.pend_open = rt.pend_momt = rt.pend_maxamp = 0;
 }
 
+bool gc_arrival_on() { return g_arr.on; }
+
 /* called by cuda_update_layer_ for the outermost layer before its swap */
 void gc_root_change_hook(GcLayer &L) {
     if (!g_arr.on) return;

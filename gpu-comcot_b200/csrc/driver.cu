@@ -9,6 +9,7 @@
 
 #include <vector>
 
+#include "fused.h"
 #include "gcomcot.h"
 #include "runtime.h"
 
@@ -116,38 +117,124 @@ void gc_gauge_release() {
 
 extern "C" {
 
+/* two outer steps per launch inside gcomcot_drive (kernels_pair.cu): a lone
+ * linear spherical outer layer with factored R2/R4, the fused path on,
+ * max-eta recorded, no arrival tracking and every gauge on that layer (at
+ * most 64).  GCOMCOT_DRIVE_PAIRS=0 keeps one step per launch. */
+static bool drive_pairs_ok(const GcLayer &L, int maxamp, int ngauges, const int *g_layer) {
+    const GcRuntime &rt = gc_rt();
+    static const bool off = [] {
+        const char *v = getenv("GCOMCOT_DRIVE_PAIRS");
+        return v && v[0] == '0';
+    }();
+    if (off || !rt.fuse_enabled || !maxamp || gc_arrival_on() || ngauges > 64) return false;
+    if (!L.children.empty() || L.parent != -1 || L.laycord != 0 || L.laygov != 0 || L.explicit_r24) return false;
+    for (int g = 0; g < ngauges; g++)
+        if (gc_layer(g_layer[g]) != &L) return false;
+    return true;
+}
+
 int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const int *g_i,
                   const int *g_j, float *out4) {
     GcRuntime &rt = gc_rt();
     if (!rt.inited || rt.root < 0) return GC_ESTATE;
     if (nsteps < 0 || ngauges < 0 || (ngauges > 0 && (!g_layer || !g_i || !g_j || !out4))) return GC_EINVAL;
     int root = rt.root;
-    bool nested = !rt.layers[root].children.empty();
+    GcLayer &R = rt.layers[root];
+    bool nested = !R.children.empty();
     for (int g = 0; g < ngauges; g++) {
         GcLayer *L = gc_layer(g_layer[g]);
         if (!L || !L->used || g_i[g] < 1 || g_i[g] >= L->nx || g_j[g] < 1 || g_j[g] >= L->ny) return GC_EINVAL;
     }
     /* The caller of this entry point receives every step's stencils at the
      * end, so no step waits for the host: each step's stencils are gathered
-     * on the device (the kernel gcomcot_get_z_'s snapshot launches, at the
-     * same point of the step) into a history of up to kChunk steps, which
-     * goes to out4 with one copy per chunk.  Same values as the per-step
-     * calls. */
-    constexpr int kChunk = 1024;
+     * on the device (by the kernel gcomcot_get_z_'s snapshot launches, at the
+     * same point of the step, or inside a two-step launch) into a history of
+     * up to kChunk steps, which goes to out4 with one copy per chunk.  Same
+     * values as the per-step calls. */
+    constexpr int kChunk = 1024; /* even: a two-step launch never straddles chunks */
     int *d_ij = nullptr;
     float *d_hist = nullptr;
-    const int chunk = nsteps < kChunk ? (nsteps > 0 ? nsteps : 1) : kChunk;
+    const int chunk = nsteps < kChunk ? (nsteps > 0 ? nsteps + (nsteps & 1) : 2) : kChunk;
+    gc_flush();
     if (ngauges > 0) {
         std::vector<int> ij((size_t)2 * ngauges);
         for (int g = 0; g < ngauges; g++) { ij[2 * g] = g_i[g]; ij[2 * g + 1] = g_j[g]; }
-        gc_flush();
         GC_CUDA_OR_RET(cudaMallocAsync((void **)&d_ij, ij.size() * sizeof(int), rt.stream));
         GC_CUDA_OR_RET(cudaMallocAsync((void **)&d_hist, (size_t)chunk * ngauges * 4 * sizeof(float), rt.stream));
         GC_CUDA_OR_RET(cudaMemcpyAsync(d_ij, ij.data(), ij.size() * sizeof(int), cudaMemcpyHostToDevice, rt.stream));
         GC_CUDA_OR_RET(cudaStreamSynchronize(rt.stream)); /* ij is a local vector */
     }
     int rc = GC_OK;
-    for (int k = 0; k < nsteps && rc == GC_OK; k++) {
+    /* the history holds steps [first, k]: copy it out when the chunk is full
+     * or the run ends */
+    auto flush_hist = [&](int k) {
+        if (ngauges == 0 || rc != GC_OK) return;
+        if ((k + 1) % chunk != 0 && k + 1 != nsteps) return;
+        const int first = k - k % chunk, cnt = k - first + 1;
+        if (cudaMemcpyAsync(out4 + (size_t)first * ngauges * 4, d_hist, (size_t)cnt * ngauges * 4 * sizeof(float),
+                            cudaMemcpyDeviceToHost, rt.stream) != cudaSuccess ||
+            cudaStreamSynchronize(rt.stream) != cudaSuccess)
+            rc = GC_ECUDA;
+    };
+    /* the gauge stencils of the state after step k (the surface in z2 of
+     * the current view, as gcomcot_get_z_'s snapshot reads it) */
+    auto gauges_after = [&](int k, const float *z2) {
+        GcPdlScope pdl(true);
+        float *slot = d_hist + (size_t)(k % chunk) * ngauges * 4;
+        int g0 = 0;
+        while (g0 < ngauges) {
+            int g1 = g0;
+            while (g1 < ngauges && g_layer[g1] == g_layer[g0]) g1++;
+            GcLayer *L = gc_layer(g_layer[g0]);
+            GcLayerDev d = L->view();
+            if (z2) d.z2 = (float *)z2;
+            else if (!L->z2_valid) d.z2 = L->z[L->cur];
+            gc_launch_gauges(d, g1 - g0, d_ij + 2 * g0, slot + 4 * g0, rt.stream);
+            rt.launches++;
+            g0 = g1;
+        }
+    };
+    int k = 0;
+    if (nsteps >= 2 && drive_pairs_ok(R, maxamp, ngauges, g_layer)) {
+        /* each launch reads the current level (buffer A) and writes the level
+         * two steps on into the other buffer (B); the intermediate level is
+         * never stored.  Its gauge stencils are recorded inside the launch,
+         * the second step's by the gauge kernel after it. */
+        constexpr int kPairVariant = 7; /* 1 warp x 5 stages, the fastest single-grid form on B200 */
+        GcFusedGrid g;
+        gc_fill_fused_grid(R, g);
+        g.nbuf = 3;
+        g.pty = gc_pair_pick_ty(kPairVariant, 1, &R.nx, &R.ny, 2, false);
+        g.pte = gc_pair_short_ty(2, g.pty);
+        gc_pair_tiles(R.nx, R.ny, g.pty, g.pte, &g.ptiles_x);
+        g.step0 = 0;
+        g.nsteps = 2;
+        g.flags = GC_F_MAXAMP | (ngauges > 0 ? GC_F_STENCIL : 0);
+        g.ng = ngauges;
+        g.gij = d_ij;
+        g.gw = nullptr;
+        for (; k + 1 < nsteps && rc == GC_OK; k += 2) {
+            const int A = R.cur, B = A ^ 1;
+            g.z[0] = R.z[A]; g.m[0] = R.m[A]; g.n[0] = R.n[A];
+            g.z[1] = R.z[B]; g.m[1] = R.m[B]; g.n[1] = R.n[B];
+            g.z[2] = R.z[B]; g.m[2] = R.m[B]; g.n[2] = R.n[B];
+            g.ts = ngauges > 0 ? d_hist + (size_t)(k % chunk) * ngauges * 4 : nullptr;
+            {
+                GcPdlScope pdl(true);
+                if (gc_pair_launch_one_at(kPairVariant, g, nullptr, 0, rt.stream) != cudaSuccess) rc = GC_ECUDA;
+            }
+            rt.launches++;
+            if (ngauges > 0) {
+                flush_hist(k);
+                gauges_after(k + 1, R.z[B]);
+                flush_hist(k + 1);
+            }
+            gc_gauge_invalidate();
+            gc_swap(R);
+        }
+    }
+    for (; k < nsteps && rc == GC_OK; k++) {
         mass_launch_(nullptr, nullptr, nullptr, &root);
         openbd_launch_(nullptr);
         if (nested) all_grid_launch_();
@@ -155,26 +242,8 @@ int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const
         if (maxamp) maxamp_launch_(&root);
         if (ngauges > 0) {
             gc_flush();
-            GcPdlScope pdl(true);
-            float *slot = d_hist + (size_t)(k % chunk) * ngauges * 4;
-            int g0 = 0;
-            while (g0 < ngauges) {
-                int g1 = g0;
-                while (g1 < ngauges && g_layer[g1] == g_layer[g0]) g1++;
-                GcLayer *L = gc_layer(g_layer[g0]);
-                GcLayerDev d = L->view();
-                if (!L->z2_valid) d.z2 = L->z[L->cur];
-                gc_launch_gauges(d, g1 - g0, d_ij + 2 * g0, slot + 4 * g0, rt.stream);
-                rt.launches++;
-                g0 = g1;
-            }
-            if ((k + 1) % chunk == 0 || k + 1 == nsteps) {
-                const int first = k - k % chunk, cnt = k - first + 1;
-                if (cudaMemcpyAsync(out4 + (size_t)first * ngauges * 4, d_hist, (size_t)cnt * ngauges * 4 * sizeof(float),
-                                    cudaMemcpyDeviceToHost, rt.stream) != cudaSuccess ||
-                    cudaStreamSynchronize(rt.stream) != cudaSuccess)
-                    rc = GC_ECUDA;
-            }
+            gauges_after(k, nullptr);
+            flush_hist(k);
         }
         cuda_update_layer_(&root);
     }

@@ -13,6 +13,10 @@
  * max-eta every step and start arrival at 0 where the initial surface is
  * already above the threshold on a wet cell) */
 #define GC_F_ARR_BYMAX 4
+/* two-step kernel: gauge records are the raw 2x2 surface stencils (four
+ * values per gauge and step, as gcomcot_get_z_ returns them) instead of the
+ * GET_TS bilinear value */
+#define GC_F_STENCIL 8
 
 struct GcFusedGrid {
     int nx, ny, pitch, root, explicit_r24;

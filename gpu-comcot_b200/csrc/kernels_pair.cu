@@ -196,14 +196,22 @@ __device__ __forceinline__ void st4m(float *row, int ib, int lo, int hi, const f
     }
 }
 
-/* one gauge stencil from two rows held as float4 per lane (GET_TS weights) */
+/* the 2x2 surface stencil at column ki (0-based) of a strip starting at s,
+ * from two rows held as float4 per lane (every lane takes part) */
+__device__ __forceinline__ void gauge_stencil(const float4 &lo_row, const float4 &hi_row, int ki, int s, float &l1,
+                                              float &l2, float &l3, float &l4) {
+    const int c0 = ki - s, c1 = ki + 1 - s;
+    l1 = __shfl_sync(FULL, comp(lo_row, c0 & 3), c0 >> 2);
+    l2 = __shfl_sync(FULL, comp(lo_row, c1 & 3), c1 >> 2);
+    l3 = __shfl_sync(FULL, comp(hi_row, c0 & 3), c0 >> 2);
+    l4 = __shfl_sync(FULL, comp(hi_row, c1 & 3), c1 >> 2);
+}
+
+/* one gauge sample from two rows held as float4 per lane (GET_TS weights) */
 __device__ __forceinline__ float gauge_sample(const float4 &lo_row, const float4 &hi_row, int ki, int s, float cx,
                                               float cy) {
-    const int c0 = ki - s, c1 = ki + 1 - s;
-    const float l1 = __shfl_sync(FULL, comp(lo_row, c0 & 3), c0 >> 2);
-    const float l2 = __shfl_sync(FULL, comp(lo_row, c1 & 3), c1 >> 2);
-    const float l3 = __shfl_sync(FULL, comp(hi_row, c0 & 3), c0 >> 2);
-    const float l4 = __shfl_sync(FULL, comp(hi_row, c1 & 3), c1 >> 2);
+    float l1, l2, l3, l4;
+    gauge_stencil(lo_row, hi_row, ki, s, l1, l2, l3, l4);
     const float a = l1 * (1.0f - cx) * (1.0f - cy);
     const float b = l2 * (cx) * (1.0f - cy);
     const float d = l3 * (1.0f - cx) * (cy);
@@ -355,12 +363,17 @@ __device__ __forceinline__ void pair_gauge_setup(const Desc &G, int l0, int loca
             if (in && local > 0) {
                 const size_t c = (size_t)kj * P + ki;
                 const float l1 = z1g[c], l2v = z1g[c + 1], l3 = z1g[c + P], l4 = z1g[c + P + 1];
-                const float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
-                const float a = l1 * (1.0f - cx) * (1.0f - cy);
-                const float b = l2v * (cx) * (1.0f - cy);
-                const float d = l3 * (1.0f - cx) * (cy);
-                const float e = l4 * (cx) * (cy);
-                G.ts[(size_t)(local - 1) * ng + g] = a + b + d + e;
+                if (G.flags & GC_F_STENCIL) {
+                    float *o = G.ts + ((size_t)(local - 1) * ng + g) * 4;
+                    o[0] = l1; o[1] = l2v; o[2] = l3; o[3] = l4;
+                } else {
+                    const float cx = G.gw[2 * g], cy = G.gw[2 * g + 1];
+                    const float a = l1 * (1.0f - cx) * (1.0f - cy);
+                    const float b = l2v * (cx) * (1.0f - cy);
+                    const float d = l3 * (1.0f - cx) * (cy);
+                    const float e = l4 * (cx) * (cy);
+                    G.ts[(size_t)(local - 1) * ng + g] = a + b + d + e;
+                }
             }
         }
         if (h == 0) in0 = in;
@@ -381,8 +394,17 @@ __device__ __forceinline__ void pair_gauge_row(const Desc &G, unsigned gm0, unsi
             const int g = __ffs(bits) - 1 + 32 * h2;
             bits &= bits - 1;
             if (G.gij[2 * g + 1] - 1 != row) continue;
-            const float v = gauge_sample(lo_row, hi_row, G.gij[2 * g] - 1, s, G.gw[2 * g], G.gw[2 * g + 1]);
-            if ((threadIdx.x & 31) == 0) G.ts[(size_t)local * G.ng + g] = v;
+            if (G.flags & GC_F_STENCIL) {
+                float l1, l2, l3, l4;
+                gauge_stencil(lo_row, hi_row, G.gij[2 * g] - 1, s, l1, l2, l3, l4);
+                if ((threadIdx.x & 31) == 0) {
+                    float *o = G.ts + ((size_t)local * G.ng + g) * 4;
+                    o[0] = l1; o[1] = l2; o[2] = l3; o[3] = l4;
+                }
+            } else {
+                const float v = gauge_sample(lo_row, hi_row, G.gij[2 * g] - 1, s, G.gw[2 * g], G.gw[2 * g + 1]);
+                if ((threadIdx.x & 31) == 0) G.ts[(size_t)local * G.ng + g] = v;
+            }
         }
     }
 }

@@ -74,6 +74,11 @@ void gc_flush();
 void gc_subcycle(int parent_id);
 void gc_swap(GcLayer &L);
 void gc_root_change_hook(GcLayer &L);
+/* arrival tracking of the outer layer is on (gcomcot_set_arrival_) */
+bool gc_arrival_on();
+/* the fused kernels' descriptor of a layer (both time levels, per-row factors) */
+struct GcFusedGrid;
+void gc_fill_fused_grid(const GcLayer &L, GcFusedGrid &g);
 int gc_layer_alloc(GcLayer &L);
 int gc_layer_upload_field(GcLayer &L, float *dst, const float *src_nx_ny);
 int gc_layer_download_field(GcLayer &L, const float *src, float *dst_nx_ny);
