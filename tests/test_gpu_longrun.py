@@ -85,6 +85,33 @@ def test_c1_full_forecast_engine_and_reference_abi(oracle_mod):
         _check(ts, ots, tag + "gauges")
 
 
+def test_c1_drive_two_steps_per_launch(oracle_mod):
+    """gcomcot_drive's two-step path (a lone linear spherical layer, fused,
+    max-eta on, arrival off): a run of odd length that crosses the 1024-step
+    stencil history twice ends with one single step; fields, max-eta and the
+    raw gauge stencils against the oracle and against the per-phase path, bit
+    for bit"""
+    nsteps = 2051
+    case = synth.config_c1(nsteps=nsteps)
+    case.gauges = synth.wet_gauges(case.root, 8, np.random.default_rng(12))
+    o = oracle_mod.OracleRun(case)
+    ots = o.run(nsteps, threads=THREADS, arrival=False)
+    ref = o.layer(0)
+    got = {}
+    for fusion in (True, False):
+        s = ReferenceSession(case, fusion=fusion, arrival=False)
+        try:
+            st = s.drive(nsteps, maxamp=True)
+            got[fusion] = (st, s.getz(1), s.getmn(1), s.getzmax(1))
+        finally:
+            s.close()
+    st, z, (m, n), zmax = got[True]
+    for a, b, k in ((z, ref["z"], "z"), (m, ref["m"], "m"), (n, ref["n"], "n"), (zmax, ref["zmax"], "zmax")):
+        _check(a, b, "drive pairs " + k)
+    _check(_interp(st, case.gauges), ots, "drive pairs gauges")
+    assert np.array_equal(st.view(np.uint32), got[False][0].view(np.uint32))
+
+
 def test_c3_nested_600_steps_engine_and_reference_abi(oracle_mod):
     nsteps = 600
     case = synth.config_c3(nsteps=nsteps)
