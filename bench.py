@@ -329,7 +329,9 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
     case = Case("C4", [L], steps)
     tune_reps = 2
     ncand = _lib.load().gc_engine_num_candidates()  # tile variants x tile-height rules
-    extra = ncand * (2 * tune_reps + 2) + warmup  # the autotuner's steps (two-step candidates run pairs)
+    # the autotuner's steps (two-step candidates run pairs), its second round
+    # over the three fastest, and the warm-up
+    extra = ncand * (2 * tune_reps + 2) + 3 * (6 * tune_reps + 2) + warmup
     eng = Engine(budget=120 << 30)
     eng.config(variant=variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
@@ -585,14 +587,14 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
                 for k, (t, size, nsteps, nested, seed) in enumerate(trace)]
 
     reqs = make_requests()
-    # tile variant: tuned once on a warm batch of the largest class (not timed)
+    # tile variant: tuned once (not timed) on a warm batch of one request of
+    # each outer size, so that the launch forms are those of a mixed batch
+    # (the work list, not the one-class launch)
     if variant < 0:
-        big = [r for r in reqs if r.case.root.nx == 1921 and len(r.case.layers) == 1][:4]
-        if not big:
-            big = [serving.Request(0, 0.0, synth.c5_request_case(tpl, (1921, 1601), 64, False, 77))]
+        batch = [synth.c5_request_case(tpl, sz, 64, False, 77 + k) for k, sz in enumerate(synth.C5_SIZES)]
         with Engine(budget=16 << 30) as eng:
-            for r in big:
-                eng.add(r.case, nsteps=6 * _lib.load().gc_engine_num_candidates() + 8)
+            for c in batch:
+                eng.add(c, nsteps=6 * _lib.load().gc_engine_num_candidates() + 3 * 14 + 8)
             eng.autotune(2)
             variant = eng.variant()  # variant + variants x tile-height rule
     budget = int(budget_gb * (1 << 30))
@@ -731,7 +733,8 @@ def run_single(args, torch, dist, rank, world, local):
     tune_reps = 3
     lib = _lib.load()
     ncand = lib.gc_engine_num_candidates()  # the autotuner's candidates: tile variants x tile-height rules
-    total = ncand * (2 * tune_reps + 2) + args.warmup + args.steps + 8  # two-step candidates run pairs
+    # two-step candidates run pairs; the second round re-times the three fastest
+    total = ncand * (2 * tune_reps + 2) + 3 * (6 * tune_reps + 2) + args.warmup + args.steps + 8
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)
     cells = case.root.nx * case.root.ny
