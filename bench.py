@@ -330,8 +330,8 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
     tune_reps = 2
     ncand = _lib.load().gc_engine_num_candidates()  # tile variants x tile-height rules
     # the autotuner's steps (two-step candidates run pairs), its second round
-    # over the three fastest, and the warm-up
-    extra = ncand * (2 * tune_reps + 2) + 3 * (6 * tune_reps + 2) + warmup
+    # (the three fastest, three 64-step graph chunks each), and the warm-up
+    extra = ncand * (2 * tune_reps + 2) + 3 * 3 * 64 + warmup
     eng = Engine(budget=120 << 30)
     eng.config(variant=variant, use_graphs=1, chunk=64)
     cls = eng.add_class(L)
@@ -594,7 +594,7 @@ def bench_c5(torch, local, nreq, rate, budget_gb, chunk, variant, plain=True, ra
         batch = [synth.c5_request_case(tpl, sz, 64, False, 77 + k) for k, sz in enumerate(synth.C5_SIZES)]
         with Engine(budget=16 << 30) as eng:
             for c in batch:
-                eng.add(c, nsteps=6 * _lib.load().gc_engine_num_candidates() + 3 * 14 + 8)
+                eng.add(c, nsteps=6 * _lib.load().gc_engine_num_candidates() + 3 * 3 * 32 + 8)
             eng.autotune(2)
             variant = eng.variant()  # variant + variants x tile-height rule
     budget = int(budget_gb * (1 << 30))
@@ -733,8 +733,9 @@ def run_single(args, torch, dist, rank, world, local):
     tune_reps = 3
     lib = _lib.load()
     ncand = lib.gc_engine_num_candidates()  # the autotuner's candidates: tile variants x tile-height rules
-    # two-step candidates run pairs; the second round re-times the three fastest
-    total = ncand * (2 * tune_reps + 2) + 3 * (6 * tune_reps + 2) + args.warmup + args.steps + 8
+    # two-step candidates run pairs; the second round re-times the three
+    # fastest over three 64-step graph chunks each
+    total = ncand * (2 * tune_reps + 2) + 3 * 3 * 64 + args.warmup + args.steps + 8
     make_case = synth.config_c1 if args.workload == "c1" else synth.config_c2
     case = make_case(nsteps=total)
     cells = case.root.nx * case.root.ny

@@ -175,7 +175,9 @@ struct gc_engine {
     /* two steps per launch (kernels_pair.cu) for the single-grid members */
     int pair_on = 1;              /* the chosen candidate uses it */
     int pair_allowed = 1;         /* GCOMCOT_PAIR=0 turns it off altogether */
-    int pair_variant = 0, pair_rule = 0;
+    /* until tuned: one warp x 5 stages in the balanced layout, the fastest
+     * single-grid form on B200 */
+    int pair_variant = 7, pair_rule = 2;
     bool pair_ok = false;         /* the current members allow it */
     int2 *d_ptiles = nullptr;
     int ptiles_cap = 0, nptiles = 0;
@@ -1195,12 +1197,15 @@ int gc_engine_autotune(gc_engine *e, int reps) {
     int saved_graphs = e->use_graphs;
     e->use_graphs = 0;
     /* per-step time of candidate c over `rounds` x its steps (whole pairs for
-     * the two-step ones), after one warm launch; < 0 when the members ran
-     * out of steps */
-    auto time_candidate = [&](int c, int rounds) -> float {
+     * the two-step ones), after one warm launch; with `chunks` > 0, as the
+     * run issues them: graph replays of `chunks` step chunks after a warm
+     * chunk (which also builds the graph).  < 0 when the members ran out of
+     * steps. */
+    auto time_candidate = [&](int c, int rounds, int chunks = 0) -> float {
         eng_set_candidate(e, c);
-        const int n = (c >= n1 ? 2 * reps : reps) * rounds;
-        if (eng_issue(e, c >= n1 ? 2 : 1) < 0) return -1.0f; /* warm */
+        e->use_graphs = chunks > 0 ? saved_graphs : 0;
+        const int n = chunks > 0 ? chunks * e->chunk : (c >= n1 ? 2 * reps : reps) * rounds;
+        if (eng_issue(e, chunks > 0 ? e->chunk : (c >= n1 ? 2 : 1)) < 0) return -1.0f; /* warm */
         cudaEventRecord(a, e->stream);
         int got = eng_issue(e, n);
         cudaEventRecord(b, e->stream);
@@ -1222,14 +1227,16 @@ int gc_engine_autotune(gc_engine *e, int reps) {
         times.push_back({ms, c});
         if (ms < best_ms) { best_ms = ms; best = c; }
     }
-    /* the three fastest again over three times the steps: one short window
-     * cannot separate candidates a few percent apart */
+    /* the three fastest again, over more steps and issued as the run will
+     * issue them (step-chunk graphs when the engine uses them): one short
+     * window of eager launches cannot separate candidates a few percent
+     * apart */
     if (!short_of_steps && times.size() > 1) {
         std::sort(times.begin(), times.end());
         float best2 = 3.0e38f;
         int pick = -1;
         for (size_t k = 0; k < times.size() && k < 3; k++) {
-            const float ms = time_candidate(times[k].second, 3);
+            const float ms = saved_graphs ? time_candidate(times[k].second, 0, 2) : time_candidate(times[k].second, 3);
             if (ms < 0.0f) break;
             if (ms < best2) { best2 = ms; pick = times[k].second; }
         }
