@@ -853,7 +853,9 @@ def run_single(args, torch, dist, rank, world, local):
     line["parity"] = merge_parity(recs)
     # ---------------- the other workloads, compact (one GPU) ----------------
     if world == 1 and args.workload == "c2" and not args.no_sub:
-        sub_steps = max(1, min(args.steps, 3600))
+        # at least 256 steps, so that a short headline run still times the
+        # sub-records over whole step-chunk graphs
+        sub_steps = max(256, min(args.steps, 3600))
         for key, fn in (("nested", lambda: bench_c3(torch, None, 1, local, sub_steps, args.warmup, -1)),
                         ("ensemble", lambda: bench_c4(torch, None, 1, local, sub_steps, args.warmup, 64, 2, -1)),
                         ("serving", lambda: bench_c5(torch, local, args.sub_requests, args.rate, args.budget_gb,

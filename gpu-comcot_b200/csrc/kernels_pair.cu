@@ -184,6 +184,14 @@ __device__ __forceinline__ void arrive4(int *row, int ib, int lo, int hi, const 
         if (ib + q >= lo && ib + q <= hi && zv[q] > thr && hv[q] > CC_GX && xv[q] <= thr) row[ib + q] = step;
 }
 
+/* whether any of a lane's four cells can arrive at this step: a surface
+ * above the threshold, and a maximum before the step at or below it (a cell
+ * whose maximum already exceeds the threshold arrived before).  A lane this
+ * returns false for would store nothing in arrive4. */
+__device__ __forceinline__ bool may_arrive(const float4 &z, const float4 &xo, float thr) {
+    return fmaxf(fmaxf(z.x, z.y), fmaxf(z.z, z.w)) > thr && fminf(fminf(xo.x, xo.y), fminf(xo.z, xo.w)) <= thr;
+}
+
 /* store of a lane's four cells, masked to columns [lo, hi] */
 __device__ __forceinline__ void st4m(float *row, int ib, int lo, int hi, const float4 &v) {
     if (ib >= lo && ib + 3 <= hi) {
@@ -593,10 +601,8 @@ __device__ __forceinline__ bool pair_rows_edge(const Desc &G, int s, int lo, int
             st4m(G.zmax + ro, ib, lo, hi, xb);
             st4m(G.m[l2] + ro, ib, lo, hi, m3);
             if (do_arr) {
-                if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
-                    arrive4(G.arrival + ro, ib, lo, hi, z2p, xp, hp, thr, local + 1);
-                if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
-                    arrive4(G.arrival + ro, ib, lo, hi, z3, xa, hp, thr, local + 2);
+                if (may_arrive(z2p, xp, thr)) arrive4(G.arrival + ro, ib, lo, hi, z2p, xp, hp, thr, local + 1);
+                if (may_arrive(z3, xa, thr)) arrive4(G.arrival + ro, ib, lo, hi, z3, xa, hp, thr, local + 2);
             }
         }
         if (rb - 1 >= j0 && rb - 1 <= jl) {
@@ -720,9 +726,9 @@ __device__ __forceinline__ bool pair_rows_int(const Desc &G, int s, int j0, int 
                 *reinterpret_cast<float4 *>(G.zmax + ro) = xb;
                 *reinterpret_cast<float4 *>(G.m[l2] + ro) = m3;
                 if (do_arr) {
-                    if (fmaxf(fmaxf(z2p.x, z2p.y), fmaxf(z2p.z, z2p.w)) > thr)
+                    if (may_arrive(z2p, xp, thr))
                         arrive4(G.arrival + ro - ib, ib, ib, ib + 3, z2p, xp, hp, thr, local + 1);
-                    if (fmaxf(fmaxf(z3.x, z3.y), fmaxf(z3.z, z3.w)) > thr)
+                    if (may_arrive(z3, xa, thr))
                         arrive4(G.arrival + ro - ib, ib, ib, ib + 3, z3, xa, hp, thr, local + 2);
                 }
             }
