@@ -118,6 +118,7 @@ SIGNATURES = {
     "gc_okada_apply": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, VP, VP, C.c_float, C.c_float, VP,
                                  VP, VP]),
     "gc_engine_set_class_axes": (C.c_int, [VP, C.c_int, P_F, P_F]),
+    "gc_pair_layout_tile": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P_I]),
     "gc_engine_add_member_faults": (C.c_int, [VP, C.c_int, VP, C.c_int, C.c_int, C.c_int, P_I, P_F, C.c_float]),
 }
 

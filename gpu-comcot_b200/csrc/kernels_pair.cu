@@ -978,6 +978,22 @@ int gc_pair_tiles(int nx, int ny, int ty, int te, int *tiles_x) {
  * 1.5 interior rows) */
 int gc_pair_short_ty(int rule, int ty) { return (rule == 2 && ty > 6) ? (3 * ty + 2) / 5 : 0; }
 
+extern "C" int gc_pair_layout_tile(int nx, int ny, int ty, int rule, int lt, int *out5) {
+    if (nx < 1 || ny < 1 || ty < 1) return -1;
+    const PairLayout L = pair_layout(nx, ny, ty, gc_pair_short_ty(rule, ty));
+    if (out5 && lt >= 0 && lt < L.count) {
+        int tx, j0, h, s, lo, hi;
+        pair_tile_at(L, ny, lt, tx, j0, h);
+        pair_cols(tx, nx, s, lo, hi);
+        out5[0] = s;
+        out5[1] = lo;
+        out5[2] = hi;
+        out5[3] = j0;
+        out5[4] = h;
+    }
+    return L.count;
+}
+
 int gc_pair_max_ctas(int variant, bool multi) {
     if (variant < 0 || variant >= kNumPairVariants) variant = 0;
     const PairVariant &v = kPairVariants[variant];

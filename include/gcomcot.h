@@ -263,6 +263,13 @@ int gc_engine_num_candidates(void);
 long long gc_engine_launches(gc_engine *e);
 /* the cudaStream_t the engine issues its kernels on */
 void *gc_engine_stream(gc_engine *e);
+/* the two-step kernel's tile layout of an nx x ny grid at tile height ty
+ * under tile-height rule `rule` (0, 1: uniform; 2: balanced): returns the
+ * number of tiles; with 0 <= lt < that number, out5 = {first column of the
+ * tile's 128-column strip, first and last stored column, first output row,
+ * rows} of tile lt (rows past the grid's last are not stored).  Host-only
+ * (no device work); the kernel runs the same code. */
+int gc_pair_layout_tile(int nx, int ny, int ty, int rule, int lt, int *out5);
 
 /* ---- one fused step without any allocation (noalloc.cu) ---- */
 
