@@ -116,6 +116,9 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Starts polling and returns after the first sample (3 s at most):
+        nvidia-smi's start-up opens the driver and would otherwise overlap
+        the first launches of a short timed region."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
@@ -124,6 +127,10 @@ class ClockSampler:
             self.t.start()
         except Exception:
             self.proc = None
+            return
+        t_end = time.time() + 3.0
+        while not self.lines and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:

@@ -199,8 +199,10 @@ int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const
     if (nsteps >= 2 && drive_pairs_ok(R, maxamp, ngauges, g_layer)) {
         /* each launch reads the current level (buffer A) and writes the level
          * two steps on into the other buffer (B); the intermediate level is
-         * never stored.  Its gauge stencils are recorded inside the launch,
-         * the second step's by the gauge kernel after it. */
+         * never stored.  Its gauge stencils are recorded inside the launch.
+         * The second step's are taken by the next launch as it starts (from
+         * the level it reads), or by the gauge kernel when no launch of the
+         * same history chunk follows. */
         constexpr int kPairVariant = 7; /* 1 warp x 5 stages, the fastest single-grid form on B200 */
         GcFusedGrid g;
         gc_fill_fused_grid(R, g);
@@ -209,25 +211,33 @@ int gcomcot_drive(int nsteps, int maxamp, int ngauges, const int *g_layer, const
         g.pte = gc_pair_short_ty(2, g.pty);
         gc_pair_tiles(R.nx, R.ny, g.pty, g.pte, &g.ptiles_x);
         g.step0 = 0;
-        g.nsteps = 2;
+        g.nsteps = 3; /* a launch computes local steps 0-1 or 1-2 */
         g.flags = GC_F_MAXAMP | (ngauges > 0 ? GC_F_STENCIL : 0);
         g.ng = ngauges;
         g.gij = d_ij;
         g.gw = nullptr;
         for (; k + 1 < nsteps && rc == GC_OK; k += 2) {
             const int A = R.cur, B = A ^ 1;
-            g.z[0] = R.z[A]; g.m[0] = R.m[A]; g.n[0] = R.n[A];
-            g.z[1] = R.z[B]; g.m[1] = R.m[B]; g.n[1] = R.n[B];
-            g.z[2] = R.z[B]; g.m[2] = R.m[B]; g.n[2] = R.n[B];
-            g.ts = ngauges > 0 ? d_hist + (size_t)(k % chunk) * ngauges * 4 : nullptr;
+            /* local step 1 (level buffers: read 1, write 0) when the previous
+             * step's slot is in this history chunk: the launch then also
+             * samples the level it reads into that slot; local step 0 (read
+             * 0, write 2) at a chunk's first slot */
+            const int local = (ngauges > 0 && k % chunk > 0) ? 1 : 0;
+            const int rd = local, wr = local ? 0 : 2, mid = local ? 2 : 1;
+            g.z[rd] = R.z[A]; g.m[rd] = R.m[A]; g.n[rd] = R.n[A];
+            g.z[wr] = R.z[B]; g.m[wr] = R.m[B]; g.n[wr] = R.n[B];
+            g.z[mid] = R.z[B]; g.m[mid] = R.m[B]; g.n[mid] = R.n[B];
+            g.ts = ngauges > 0 ? d_hist + (size_t)(k % chunk - local) * ngauges * 4 : nullptr;
             {
                 GcPdlScope pdl(true);
-                if (gc_pair_launch_one_at(kPairVariant, g, nullptr, 0, rt.stream) != cudaSuccess) rc = GC_ECUDA;
+                if (gc_pair_launch_one_at(kPairVariant, g, nullptr, local, rt.stream) != cudaSuccess) rc = GC_ECUDA;
             }
             rt.launches++;
             if (ngauges > 0) {
-                flush_hist(k);
-                gauges_after(k + 1, R.z[B]);
+                /* the next launch samples step k + 1 when it exists and step
+                 * k + 1's slot is not the last of its chunk */
+                const bool next_samples = k + 3 < nsteps && (k + 2) % chunk != 0;
+                if (!next_samples) gauges_after(k + 1, R.z[B]);
                 flush_hist(k + 1);
             }
             gc_gauge_invalidate();

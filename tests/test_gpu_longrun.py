@@ -112,6 +112,27 @@ def test_c1_drive_two_steps_per_launch(oracle_mod):
     assert np.array_equal(st.view(np.uint32), got[False][0].view(np.uint32))
 
 
+@pytest.mark.parametrize("nsteps", [2, 3, 4, 40])
+def test_drive_two_steps_short_runs(nsteps):
+    """short gcomcot_drive runs on the two-step path: one history chunk that
+    ends on a launch's second step (even lengths) or on a single step (odd);
+    the raw gauge stencils and the fields equal the per-phase path's bit for
+    bit"""
+    case = synth.config_c1(nsteps=nsteps)
+    case.gauges = synth.wet_gauges(case.root, 8, np.random.default_rng(13))
+    got = {}
+    for fusion in (True, False):
+        s = ReferenceSession(case, fusion=fusion, arrival=False)
+        try:
+            st = s.drive(nsteps, maxamp=True)
+            got[fusion] = (st, s.getz(1), *s.getmn(1), s.getzmax(1))
+        finally:
+            s.close()
+    assert got[True][0].shape[0] == nsteps
+    for a, b in zip(got[True], got[False]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_c3_nested_600_steps_engine_and_reference_abi(oracle_mod):
     nsteps = 600
     case = synth.config_c3(nsteps=nsteps)
