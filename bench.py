@@ -244,6 +244,37 @@ def parity_record(got, ref, steps, H=None, ts=None, ts_ref=None, child=None, chi
     return rec
 
 
+def timed_engine_steps(torch, eng, steps, warmup, dist, local):
+    """The warm-up steps, then exactly `steps` timed steps with CUDA events on
+    the engine's stream, between a barrier and a synchronize on both sides.
+    The step-chunk graph and the clock sampler are set up first, so the
+    warm-up runs directly before the timed region: a B200 left idle for a
+    fraction of a second starts the next short region measurably slower.
+    Returns (ms, launches, clocks); ms is the max over ranks."""
+    eng.prepare()  # step-chunk graph built before the timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    eng.step(warmup)
+    eng.sync()
+    stream = torch.cuda.ExternalStream(eng.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = eng.launches()
+    ev0.record(stream)
+    eng.step(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+    launches = eng.launches() - l0
+    ms = replicas.reduce_max(ev0.elapsed_time(ev1), dist, 'cuda')
+    return ms, launches, ck
+
+
 def steps_per_launch(variant):
     """2 when the engine's chosen candidate is the two-step kernel
     (candidates past the one-step variants x their tile-height rules)"""
@@ -346,25 +377,7 @@ def bench_c4(torch, dist, world, local, steps, warmup, nscen, plain_sample, vari
     if variant < 0:
         eng.autotune(tune_reps)
     chosen = eng.variant()  # variant + variants x tile-height rule
-    eng.step(warmup)
-    eng.prepare()  # step-chunk graph built before the timed region
-    eng.sync()
-    stream = torch.cuda.ExternalStream(eng.stream())
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = eng.launches()
-    ev0.record(stream)
-    eng.step(steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    ck = clocks.stop()
-    launches = eng.launches() - l0
-    ms = ev0.elapsed_time(ev1)
-    ms = replicas.reduce_max(ms, dist, 'cuda')
+    ms, launches, ck = timed_engine_steps(torch, eng, steps, warmup, dist, local)
     eng.sync()
     sample = sorted({0, nscen - 1})[:parity_members]
     got = {q: (eng.steps_done(ids[q]), eng.read(ids[q], fields=("z", "m", "n", "zmax", "arrival"))) for q in sample}
@@ -473,25 +486,7 @@ def bench_c3(torch, dist, world, local, steps, warmup, variant, e2e_steps=0, cpu
     eng = Engine(budget=8 << 30)
     eng.config(variant=variant, use_graphs=1, chunk=64)
     mid = eng.add(case)
-    eng.step(warmup)
-    eng.prepare()  # step-chunk graph built before the timed region
-    eng.sync()
-    stream = torch.cuda.ExternalStream(eng.stream())
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = eng.launches()
-    ev0.record(stream)
-    eng.step(steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    ck = clocks.stop()
-    launches = eng.launches() - l0
-    ms = ev0.elapsed_time(ev1)
-    ms = replicas.reduce_max(ms, dist, 'cuda')
+    ms, launches, ck = timed_engine_steps(torch, eng, steps, warmup, dist, local)
     eng.sync()
     done = eng.steps_done(mid)
     got = eng.read(mid, fields=("z", "m", "n", "zmax", "arrival", "child"))
@@ -754,29 +749,8 @@ def run_single(args, torch, dist, rank, world, local):
     if args.variant < 0:
         eng.autotune(tune_reps)
     variant = eng.variant()  # variant + variants x tile-height rule
-    eng.step(args.warmup)
-    eng.prepare()  # step-chunk graph built before the timed region
-    eng.sync()
-    stream = torch.cuda.ExternalStream(eng.stream())
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = eng.launches()
-    ev0.record(stream)
-    eng.step(args.steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    torch.cuda.synchronize()
-    ck = clocks.stop()
-    if dist:
-        dist.barrier()
-    launches = eng.launches() - l0  # fused steps + the graphs' step-counter kernels
-    ms = ev0.elapsed_time(ev1)
-    ms = replicas.reduce_max(ms, dist, 'cuda')
+    # launches: the step kernels + the graphs' step-counter kernels
+    ms, launches, ck = timed_engine_steps(torch, eng, args.steps, args.warmup, dist, local)
     value = cells * args.steps * world / (ms * 1e-3)
     eng.sync()
     done = eng.steps_done(mid)

@@ -212,6 +212,16 @@ struct gc_engine {
  * differ, and the rectangle [IS-1,IE] x [JS-1,JE] is recomputed.  The child
  * reads the outer Z(:,:,2), M(:,:,1) and N(:,:,1) only.  Max-eta, arrival
  * and gauges follow in the outputs kernel, after the feedback. */
+/* GCOMCOT_FEEDBACK=0 keeps JNZ, the window's momentum and the outputs as
+ * three launches */
+static bool eng_feedback_on() {
+    static const bool on = [] {
+        const char *v = getenv("GCOMCOT_FEEDBACK");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_base, int step_off, int a) {
     cudaStream_t s = e->aux[a];
     const EngClass &C = e->classes[M.cls];
@@ -279,7 +289,10 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
         else gc_launch_jnz(P, Cv, C.rel_size, C.rel_time, C.corners, s);
         e->launches++;
     };
-    if (nhalf == 1) jnz(Cv1);
+    /* one sub-step and a JNZ ratio the feedback launch is built for: JNZ,
+     * the window's momentum and the outputs go out as one launch at the end */
+    const bool fb = nhalf == 1 && !C.has_sc && C.rel_size >= 2 && C.rel_size <= 5 && eng_feedback_on();
+    if (nhalf == 1 && !fb) jnz(Cv1);
     if (late_update1) {
         gc_launch_update_edges(Cv1, s);
         e->launches++;
@@ -313,6 +326,13 @@ static void eng_nested_step(gc_engine *e, EngMember &M, int local, const int *d_
      * max-eta / arrival / gauges, side by side; both read the final surface,
      * neither writes what the other reads.  Fortran (IS-1 .. IE, JS-1 .. JE)
      * -> 0-based (IS-2 .. IE-1, JS-2 .. JE-1) */
+    if (fb) {
+        const int rect[4] = {C.corners[0] - 2, C.corners[1] - 1, C.corners[2] - 2, C.corners[3] - 1};
+        gc_launch_feedback(P, Cv1, C.rel_size, C.rel_time, C.corners, rect, d_base, step_off, M.step0, flags, M.thr,
+                           M.ng, M.gij, M.gw, M.glayer, M.cz[cc], C.cpitch, M.ts, M.nsteps, s);
+        e->launches += 2; /* the fused step, the feedback */
+        return;
+    }
     cudaEventRecord(e->ev_cfork[a], s);
     cudaStreamWaitEvent(cs, e->ev_cfork[a], 0);
     gc_launch_step_outputs(P, d_base, step_off, M.step0, flags, M.thr, M.ng, M.gij, M.gw, M.glayer, M.cz[cc],

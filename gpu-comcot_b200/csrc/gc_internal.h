@@ -150,6 +150,14 @@ void gc_launch_gauges(const GcLayerDev &L, int ng, const int *d_ij, float *d_out
 void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_off, int step0, int flags,
                             float thr, int ng, const int *gij, const float *gw, const int *glayer,
                             const float *cz, int cpitch, float *ts, int ts_len, const int *win, cudaStream_t s);
+/* JNZ (window `corners`, 1-based IS, IE, JS, JE), the linear spherical
+ * momentum over the 0-based rectangle rect = {i0, i1, j0, j1} and the
+ * outputs of gc_launch_step_outputs over the JNZ window, in one launch;
+ * false (nothing launched) for a ratio it is not built for */
+bool gc_launch_feedback(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time, const int *corners,
+                        const int *rect, const int *step_base, int step_off, int step0, int flags, float thr, int ng,
+                        const int *gij, const float *gw, const int *glayer, const float *cz, int cpitch, float *ts,
+                        int ts_len, cudaStream_t s);
 
 /* ---- fused step (kernels_fused.cu) ---- */
 struct GcFusedGrid;

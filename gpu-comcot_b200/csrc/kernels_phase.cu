@@ -747,20 +747,20 @@ __global__ void k_conmome(GcLayerDev L, int upd) {
 }
 
 /* CONMOME with both directions per thread, the stencil staged through
- * shared memory: a block stages its (BX+4) x (BY+4) window of DZ, Z, M and
+ * shared memory: a block stages its (BX+4) x (TY+4) window of DZ, Z, M and
  * N (two cells of halo, at the same clamped indices the one-face kernel
  * reads) with one batch of independent loads, then each thread computes
  * its cell's x and y faces from shared memory.  Same values, same
  * arithmetic (conmome_x / conmome_y): the same bits. */
-template <bool SPH>
+template <bool SPH, int TY>
 __device__ __forceinline__ void conmome_tile_body(const GcLayerDev &L, int upd) {
     pdl_enter();
-    constexpr int TW = BX + 4, TH = BY + 4;
+    constexpr int TW = BX + 4, TH = TY + 4;
     __shared__ float tile[4][TH][TW];
     const int P = L.pitch, ix = L.nx, jy = L.ny;
-    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * TY;
     const float *fields[4] = {L.dz2, L.z2, L.m1, L.n1};
-    for (int t = threadIdx.y * BX + threadIdx.x; t < TW * TH; t += BX * BY) {
+    for (int t = threadIdx.y * BX + threadIdx.x; t < TW * TH; t += BX * TY) {
         const int tj = t / TW, ti = t - tj * TW;
         const int ii = min(max(i0 + ti - 2, 0), ix - 1), jj = min(max(j0 + tj - 2, 0), jy - 1);
         const size_t g = (size_t)jj * P + ii;
@@ -811,9 +811,9 @@ __device__ __forceinline__ void conmome_tile_body(const GcLayerDev &L, int upd) 
     L.m2[c] = outx;
     L.n2[c] = outy;
 }
-template <bool SPH>
-__global__ void __launch_bounds__(BX * BY) k_conmome_tile(GcLayerDev L, int upd) {
-    conmome_tile_body<SPH>(L, upd);
+template <bool SPH, int TY, int MINB>
+__global__ void __launch_bounds__(BX * TY, MINB) k_conmome_tile(GcLayerDev L, int upd) {
+    conmome_tile_body<SPH, TY>(L, upd);
 }
 
 /* ---------------------------------------------------------------- */
@@ -1396,6 +1396,109 @@ __global__ void k_step_outputs(GcLayerDev L, const int *step_base, int step_off,
     if ((flags & 2) && L.arrival[c] < 0 && L.h[c] > CC_GX && z > thr) L.arrival[c] = local + 1;
 }
 
+/* The end of a nested outer step whose child takes one sub-step, as one
+ * launch: JNZ's feedback (all_grids.f90:378-411), the outer momentum
+ * recomputed where that surface changed, and the step's outputs on the
+ * window.  Same values as k_jnz_r, k_momt_s over the rectangle and
+ * k_step_outputs in turn.
+ *
+ * A block owns a 31 x 7 patch of the momentum rectangle (0-based columns
+ * ri0 .. ri0+rni-1, rows rj0 .. rj0+rnj-1) and first takes the level-2
+ * surface of the 32 x 8 cells from the patch's corner: JNZ's mean inside
+ * the window (1-based IS..IE x JS..JE), the stored surface outside it,
+ * which nothing in this launch writes.  A patch cell's M reads its east
+ * neighbour and its N its north neighbour, both in that 32 x 8 block.
+ * Gauges on the outer layer take a window cell's surface the same way,
+ * since another block writes it. */
+template <int R, bool EVEN>
+__device__ __forceinline__ float feedback_z(const GcLayerDev &P, const GcLayerDev &C, int is, int ie, int js,
+                                            int je, int i, int j) {
+    const int I = i + 1, J = j + 1;
+    if (I >= is && I <= ie && J >= js && J <= je) return jnz_value<R, EVEN>(C, is, js, I, J);
+    return P.z2[(size_t)j * P.pitch + i];
+}
+
+constexpr int FB_W = BX - 1, FB_H = BY - 1; /* a block's patch of the momentum rectangle */
+
+template <int R, bool EVEN>
+__global__ void __launch_bounds__(BX * BY) k_feedback_r(GcLayerDev L, GcLayerDev C, int is, int ie, int js, int je,
+                                                        int ri0, int rj0, int rni, int rnj, const int *step_base,
+                                                        int step_off, int step0, int flags, float thr, int ng,
+                                                        const int *gij, const float *gw, const int *glayer,
+                                                        const float *cz, int cpitch, float *ts, int ts_len) {
+    pdl_enter();
+    __shared__ float zt[BY][BX + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = ri0 + blockIdx.x * FB_W + tx, j = rj0 + blockIdx.y * FB_H + ty;
+    const int P = L.pitch;
+    float z = 0.0f;
+    if (i < L.nx && j < L.ny) z = feedback_z<R, EVEN>(L, C, is, ie, js, je, i, j);
+    zt[ty][tx] = z;
+    __syncthreads();
+    const int local = step_off + (step_base ? *step_base : 0) - step0;
+    const bool outputs = local >= 0 && local < ts_len;
+    if (tx < FB_W && ty < FB_H && i < ri0 + rni && j < rj0 + rnj && i < L.nx && j < L.ny) {
+        const size_t c = (size_t)j * P + i;
+        const int I = i + 1, J = j + 1;
+        const bool win = I >= is && I <= ie && J >= js && J <= je;
+        if (win) L.z2[c] = z;
+        /* k_momt_s with the surface from the block's copy */
+        const int lo = L.root ? 0 : 1;
+        float xm = 0.0f;
+        if (i >= lo && i <= L.nx - 2 && j >= lo) {
+            float h = L.h[c], hp1 = L.h[c + 1];
+            if (h > CC_GX && hp1 > CC_GX) {
+                size_t cm = (j > 0) ? c - P : c; /* JM1 = max(J-1,1) */
+                float tot_n = L.n1[c] + L.n1[c + 1] + L.n1[cm] + L.n1[cm + 1];
+                xm = L.m1[c] - r2_at(L, i, j, c, h, hp1) * (zt[ty][tx + 1] - z) + GC_ROW(L, GC_R3, j) * tot_n;
+                if (fabsf(xm) < CC_EPS) xm = 0.0f;
+            }
+        }
+        L.m2[c] = xm;
+        float xn = 0.0f;
+        if (j >= lo && j <= L.ny - 2 && i >= lo) {
+            float h = L.h[c], hq1 = L.h[c + P];
+            if (h > CC_GX && hq1 > CC_GX) {
+                size_t cw = (i > 0) ? c - 1 : c; /* IM1 = max(I-1,1) */
+                float tot_m = L.m1[cw] + L.m1[cw + P] + L.m1[c] + L.m1[c + P];
+                xn = L.n1[c] - r4_at(L, i, j, c, h, hq1) * (zt[ty + 1][tx] - z) - GC_ROW(L, GC_R5, j) * tot_m;
+                if (fabsf(xn) < CC_EPS) xn = 0.0f;
+            }
+        }
+        L.n2[c] = xn;
+        /* k_step_outputs on the window */
+        if (win && outputs) {
+            if (flags & 1) {
+                float m = L.zmax[c];
+                if (!(m >= z)) L.zmax[c] = z;
+            }
+            if ((flags & 2) && L.arrival[c] < 0 && L.h[c] > CC_GX && z > thr) L.arrival[c] = local + 1;
+        }
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && ng > 0 && outputs) {
+        for (int g = ty * BX + tx; g < ng; g += BX * BY) {
+            const bool child = glayer && glayer[g] != 0;
+            const int gi = gij[2 * g] - 1, gj = gij[2 * g + 1] - 1;
+            float l1, l2, l3, l4;
+            if (child) {
+                const size_t cc = (size_t)gj * cpitch + gi;
+                l1 = cz[cc]; l2 = cz[cc + 1]; l3 = cz[cc + cpitch]; l4 = cz[cc + cpitch + 1];
+            } else {
+                l1 = feedback_z<R, EVEN>(L, C, is, ie, js, je, gi, gj);
+                l2 = feedback_z<R, EVEN>(L, C, is, ie, js, je, gi + 1, gj);
+                l3 = feedback_z<R, EVEN>(L, C, is, ie, js, je, gi, gj + 1);
+                l4 = feedback_z<R, EVEN>(L, C, is, ie, js, je, gi + 1, gj + 1);
+            }
+            float cx = gw[2 * g], cy = gw[2 * g + 1];
+            float a = l1 * (1.0f - cx) * (1.0f - cy);
+            float b = l2 * (cx) * (1.0f - cy);
+            float d = l3 * (1.0f - cx) * (cy);
+            float e = l4 * (cx) * (cy);
+            ts[(size_t)local * ng + g] = a + b + d + e;
+        }
+    }
+}
+
 thread_local bool t_pdl = false;
 
 /* ordinary launch, or one with programmatic stream serialization */
@@ -1434,22 +1537,31 @@ void gc_launch_mass(const GcLayerDev &L, cudaStream_t s) {
     else launch(k_mass_c<false>, grid2(L), dim3(BX, BY), 0, s, L);
 }
 
-/* CONMOME: the shared-memory tile form (both faces per thread), or with
- * GCOMCOT_CONMOME_TILE=0 the one-face form (x and y as two grid layers);
- * both compute the same bits */
-static bool conmome_tiled() {
-    static const int on = [] {
+/* CONMOME: the shared-memory tile form (both faces per thread) in blocks of
+ * 32 x 4 cells at 64 registers, eight blocks to an SM.  A 601 x 501 child
+ * takes 2.02 waves of them, the last 26 blocks short ones, against 2.7 waves
+ * of 32 x 8 blocks, which the compiler gives 72 registers (three to an SM).
+ * GCOMCOT_CONMOME_TILE=8 takes the 32 x 8 blocks, GCOMCOT_CONMOME_TILE=0 the
+ * one-face form (x and y as two grid layers).  All compute the same bits. */
+static int conmome_rows() {
+    static const int rows = [] {
         const char *v = getenv("GCOMCOT_CONMOME_TILE");
-        return (v && v[0] == '0') ? 0 : 1;
+        if (v && v[0] == '0') return 0;
+        return (v && atoi(v) == 8) ? 8 : 4;
     }();
-    return on != 0;
+    return rows;
 }
 
 static void launch_conmome(const GcLayerDev &L, int upd, cudaStream_t s) {
     const bool sph = L.laycord == 0;
-    if (conmome_tiled()) {
-        if (sph) launch(k_conmome_tile<true>, grid2(L), dim3(BX, BY), 0, s, L, upd);
-        else launch(k_conmome_tile<false>, grid2(L), dim3(BX, BY), 0, s, L, upd);
+    const int rows = conmome_rows();
+    if (rows == 4) {
+        const dim3 g4((unsigned)((L.nx + BX - 1) / BX), (unsigned)((L.ny + 3) / 4), 1);
+        if (sph) launch(k_conmome_tile<true, 4, 8>, g4, dim3(BX, 4), 0, s, L, upd);
+        else launch(k_conmome_tile<false, 4, 8>, g4, dim3(BX, 4), 0, s, L, upd);
+    } else if (rows == 8) {
+        if (sph) launch(k_conmome_tile<true, 8, 1>, grid2(L), dim3(BX, 8), 0, s, L, upd);
+        else launch(k_conmome_tile<false, 8, 1>, grid2(L), dim3(BX, 8), 0, s, L, upd);
     } else {
         const dim3 g2(grid2(L).x, grid2(L).y, 2);
         if (sph) launch(k_conmome<true>, g2, dim3(BX, BY), 0, s, L, upd);
@@ -1590,6 +1702,37 @@ void gc_launch_step_outputs(const GcLayerDev &L, const int *step_base, int step_
     dim3 grid((unsigned)((ni + BX - 1) / BX), (unsigned)((nj + BY - 1) / BY), 1);
     launch(k_step_outputs, grid, dim3(BX, BY), 0, s, L, step_base, step_off, step0, flags, thr, ng, gij, gw, glayer,
                                                  cz, cpitch, ts, ts_len, i0, j0, ni, nj);
+}
+
+bool gc_launch_feedback(const GcLayerDev &P, const GcLayerDev &C, int rel_size, int rel_time, const int *corners,
+                        const int *rect, const int *step_base, int step_off, int step0, int flags, float thr, int ng,
+                        const int *gij, const float *gw, const int *glayer, const float *cz, int cpitch, float *ts,
+                        int ts_len, cudaStream_t s) {
+    const int is = corners[0], ie = corners[1], js = corners[2], je = corners[3];
+    const int i0 = std::max(rect[0], 0), i1 = std::min(rect[1], P.nx - 1);
+    const int j0 = std::max(rect[2], 0), j1 = std::min(rect[3], P.ny - 1);
+    if (i1 < i0 || j1 < j0) return false;
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
+    const dim3 grid((unsigned)((ni + FB_W - 1) / FB_W), (unsigned)((nj + FB_H - 1) / FB_H), 1);
+    const bool even = (rel_time % 2) == 0;
+#define GC_FB_R(R)                                                                                              \
+    case R:                                                                                                     \
+        if (even)                                                                                               \
+            launch(k_feedback_r<R, true>, grid, dim3(BX, BY), 0, s, P, C, is, ie, js, je, i0, j0, ni, nj,       \
+                   step_base, step_off, step0, flags, thr, ng, gij, gw, glayer, cz, cpitch, ts, ts_len);        \
+        else                                                                                                    \
+            launch(k_feedback_r<R, false>, grid, dim3(BX, BY), 0, s, P, C, is, ie, js, je, i0, j0, ni, nj,      \
+                   step_base, step_off, step0, flags, thr, ng, gij, gw, glayer, cz, cpitch, ts, ts_len);        \
+        return true;
+    switch (rel_size) {
+        GC_FB_R(2)
+        GC_FB_R(3)
+        GC_FB_R(4)
+        GC_FB_R(5)
+        default: break;
+    }
+#undef GC_FB_R
+    return false;
 }
 
 void gc_set_pdl(bool on) { t_pdl = on; }

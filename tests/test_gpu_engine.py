@@ -110,6 +110,29 @@ def test_engine_nested_member_matches_oracle(oracle_mod, rel_time, graphs):
         _check_nested(eng.read(mid), case, oracle_mod)
 
 
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_engine_feedback_gauges_on_the_window(oracle_mod, graphs):
+    """one child sub-step per outer step (JNZ, the window's momentum and the
+    outputs in one launch): outer gauges whose stencils lie inside the JNZ
+    window, across its edges and at its corner, beside child gauges, bit for
+    bit against the oracle"""
+    case = _nested(71, 1, 40)
+    P, C = case.layers
+    jj, ii = np.mgrid[0:C.ny, 0:C.nx]
+    bump = 0.8 * np.exp(-((ii - 0.4 * C.nx) ** 2 + (jj - 0.6 * C.ny) ** 2) / (2.0 * 8.0 ** 2))
+    C.Z0 = np.where(C.H > 0.0, bump, 0.0).astype(np.float32)  # the feedback carries a wave from the start
+    is_, ie, js, je = 60, 79, 30, 49  # the child's window on the outer grid, 1-based
+    for ki, kj in ((is_ + 5, js + 5), (is_ - 1, js + 3), (ie, je), (is_ + 2, je), (ie - 3, js - 1)):
+        case.gauges.append((P.id, ki, kj, 0.3, 0.6))
+    with Engine(budget=2 << 30) as eng:
+        eng.config(variant=-1, use_graphs=graphs, chunk=8)
+        mid = eng.add(case)
+        eng.step(45)
+        eng.sync()
+        assert eng.done(mid)
+        _check_nested(eng.read(mid), case, oracle_mod)
+
+
 @pytest.mark.parametrize("laygov,rel_time", [(1, 1), (0, 2)])
 def test_engine_wide_child_matches_oracle(oracle_mod, laygov, rel_time):
     """a 151 x 151 child (interior CONMOME blocks, two-cell JNQ + mass threads)"""
